@@ -1,0 +1,181 @@
+/* tct_b200: C ABI of the B200 elastic-BEM operator-apply path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (TCT_OK = 0).  Device pointers are CUDA global-memory addresses on the
+ * current device; `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  Host pointers are marked "host".  The library never frees
+ * caller memory and keeps no per-call device allocations: scratch space is
+ * passed in by the caller (see the *_workspace_bytes queries).
+ *
+ * Arithmetic type: `prec` = TCT_F32 (float, the reference's default
+ * float_type) or TCT_F64 (double).  Real below means float or double
+ * according to `prec`.
+ *
+ * Kernel ids follow the reference's kernel names (tectosaur/kernels/__init__.py):
+ *   0 elasticU3  1 elasticT3  2 elasticA3  3 elasticH3
+ *   4 elasticRT3 5 elasticRA3 6 elasticRH3
+ * params = {mu (shear modulus G), nu} as host doubles.
+ */
+#ifndef TCT_B200_H
+#define TCT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCT_OK 0
+#define TCT_ERR_ARG 1        /* bad size, pointer, alignment or index       */
+#define TCT_ERR_KERNEL 2     /* kernel id not supported by this entry point */
+#define TCT_ERR_CUDA 3       /* CUDA runtime / launch error                  */
+#define TCT_ERR_OOM 4        /* workspace too small / allocation failed      */
+#define TCT_ERR_TIMEOUT 5    /* a bounded device wait gave up                */
+#define TCT_ERR_PREC 6       /* unsupported precision                        */
+
+#define TCT_F32 0
+#define TCT_F64 1
+
+/* Library version string and the last error message of the calling thread. */
+const char* tct_version(void);
+const char* tct_last_error(void);
+
+/* Kernel id of a reference kernel name ("elasticRH3" -> 6), or -1. */
+int tct_kernel_id(const char* name);
+
+/* ------------------------------------------------------------------------ */
+/* Triangle-pair quadrature (nearfield assembly).                            */
+/* Replaces the reference's single_pairsZ / single_pairsN / single_pairsN_adj
+ * kernels (tectosaur/assemble.cl:24-103) and PairsIntegrator.pairs_quad
+ * (tectosaur/nearfield/pairs_integrator.py:43-68).
+ *
+ * pairs:   n_pairs records of int32 (device): 2 ints (obs_tri, src_tri) when
+ *          adj == 0, 5 ints (obs_tri, src_tri, obs_clicks, src_clicks,
+ *          src_flip) when adj == 1 (assemble.cl:58-62).
+ * quad:    n_quad 4-D points (obs xhat, obs yhat, src xhat, src yhat) and
+ *          weights, Real, device.
+ * pts:     n_pts x 3 Real (device); tris: n_tris x 3 int32 (device).
+ * check0:  skip quadrature points with r^2 == 0 (the "Z" variant); adjacent
+ *          pairs always skip them (assemble.cl:67).
+ * out:     81 Real per pair, index b_obs*27 + d_obs*9 + b_src*3 + d_src.
+ *          When out_slot is non-NULL, pair i's 81 values go to block
+ *          out_slot[i] of a block array with `slot_stride` blocks between
+ *          consecutive entries of one block (structure-of-arrays BSR layout:
+ *          element e of block s at out[e * slot_stride + s]); otherwise to
+ *          out[i * 81 + e].  `sign` (+1 or -1) multiplies the result and
+ *          `accumulate` adds into the destination instead of overwriting
+ *          (used to subtract the farfield-rule correction in place,
+ *          nearfield/nearfield_op.py:135-141).
+ */
+int tct_pairs_integrate(int kernel, int prec, int adj, int check0,
+                        void* out, const int32_t* out_slot, int64_t slot_stride,
+                        int sign, int accumulate,
+                        int n_quad, const void* quad_pts, const void* quad_wts,
+                        const void* pts, const int32_t* tris,
+                        const int32_t* pairs, int64_t n_pairs,
+                        const double* params, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Direct tri-to-tri farfield matvec.                                        */
+/* Replaces farfield_tris_to_tris{K} (tectosaur/matrix_free.cl:19-107) behind
+ * TriToTriDirectFarfieldOp.dot (tectosaur/ops/sparse_farfield_op.py:16-62):
+ *   out[obs, b_obs, d] (+)= sum over all src tris and quadrature point pairs of
+ *   J_obs J_src w_i w_j phi_b_obs(x_i) K(x_i, y_j) . (sum_b phi_b(y_j) in[src, b, :]),
+ * skipping point pairs with r^2 == 0.
+ * quad_pts (n_q x 2) and quad_wts (n_q) are the host 2-D triangle rule
+ * (gauss2d_tri(nq_far)): n_q in {3, 4, 7, 13} (nq_far = 1..4).
+ * in:  n_src x 9 Real, out: n_obs x 9 Real (device).  accumulate != 0 adds to out.
+ * workspace: device scratch of at least tct_farfield_workspace_bytes() bytes,
+ * 256-byte aligned. */
+size_t tct_farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_src,
+                                    int n_q);
+int tct_farfield_tris_matvec(int kernel, int prec, void* out, const void* in,
+                             const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                             const int32_t* src_tris, int64_t n_src,
+                             int n_q, const double* quad_pts, const double* quad_wts,
+                             const double* params, int accumulate,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Point-to-point farfield.                                                  */
+/* Replaces farfield_pts{K} (tectosaur/farfield_direct.cl:15-113) behind
+ * farfield_pts_direct (tectosaur/farfield.py:15-38); kernels 0-3 only.
+ * obs/src points and normals n x 3 Real, in n_src x 3, out n_obs x 3 (device). */
+int tct_farfield_pts(int kernel, int prec, void* out, const void* obs_pts,
+                     const void* obs_ns, int64_t n_obs, const void* src_pts,
+                     const void* src_ns, int64_t n_src, const void* in,
+                     const double* params, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Dense farfield blocks.                                                    */
+/* Replaces farfield_tris (tectosaur/assemble.cl:105-138) behind
+ * FarfieldTriMatrix.assemble (tectosaur/ops/dense_integral_op.py:48-90).
+ * out: (n_obs, 3, 3, n_src, 3, 3) Real (device). */
+int tct_farfield_tris_dense(int kernel, int prec, void* out, int n_quad,
+                            const void* quad_pts, const void* quad_wts,
+                            const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                            const int32_t* src_tris, int64_t n_src,
+                            const double* params, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* 9x9 block-sparse (BSR) nearfield matvec.                                  */
+/* Replaces bsrmv9 / bcoomv9 (tectosaur/util/fast_sparse.cpp:71-163) behind
+ * BCOOMatrix.dot / BSRMatrix.dot (tectosaur/util/sparse.py:29-64) as summed
+ * by RegularizedNearfieldIntegralOp.dot (nearfield/nearfield_op.py:158-159).
+ * Layout: indptr (n_row_blocks + 1) and indices (nnzb) int32; data in
+ * structure-of-arrays order, element e (= i*9 + j) of block s at
+ * data[e * data_stride + s], data_stride >= nnzb.
+ * y[9*r + i] (+)= sum_{s in row r} sum_j A_s[i][j] x[9*indices[s] + j].
+ * With data2 != NULL the blocks are data + data2 (no-correction form). */
+int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
+                    const int32_t* indices, const void* data, const void* data2,
+                    int64_t data_stride, const void* x, void* y, int accumulate,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Host-side (CPU) structure builders.                                       */
+
+/* Near-pair search: all (i, j) with |c_i - c_j|^2 <= ((r_i + r_j) * threshold)^2
+ * evaluated in the same double arithmetic as the reference
+ * (mesh/fast_find_nearfield.cpp:22-74, get_nearfield :255-285).  The result
+ * set equals the reference's; its order is canonical (lexicographic by
+ * (i, j)) rather than the reference's thread-completion order.
+ * Two-phase: tct_find_near_pairs returns an opaque handle holding the pairs;
+ * read them with tct_pairs_count / tct_pairs_copy and release with
+ * tct_pairs_free.  All pointers host. */
+typedef struct tct_pair_list tct_pair_list;
+int tct_find_near_pairs(const double* obs_centers, const double* obs_radii, int64_t n_obs,
+                        const double* src_centers, const double* src_radii, int64_t n_src,
+                        double threshold, int n_threads, tct_pair_list** out);
+int64_t tct_pairs_count(const tct_pair_list* list);
+int tct_pairs_copy(const tct_pair_list* list, int64_t* dst);
+void tct_pairs_free(tct_pair_list* list);
+
+/* Split close pairs by the number of shared vertices
+ * (mesh/fast_find_nearfield.cpp:143-182): 0 -> near (2 cols), 1 -> vertex
+ * adjacent (4 cols: obs, src, obs corner, src corner), 2 -> edge adjacent
+ * (6 cols), 3 -> coincident (dropped).  Output capacities: n_pairs rows each.
+ * Order = input order.  Host. */
+int tct_split_adjacent_close(const int64_t* pairs, int64_t n_pairs,
+                             const int64_t* tris_a, const int64_t* tris_b,
+                             int64_t* near_out, int64_t* n_near,
+                             int64_t* va_out, int64_t* n_va,
+                             int64_t* ea_out, int64_t* n_ea);
+
+/* Edge-adjacent orientation records (obs, src, obs_clicks, src_clicks, flip)
+ * from the 6-column edge-adjacent rows (nearfield/nearfield_op.py:44-62). Host. */
+int tct_resolve_ea_rotation(const int64_t* tris, const int64_t* ea, int64_t n,
+                            int64_t* out);
+
+/* BSR index build (util/fast_sparse.cpp:14-68 semantics: stable counting
+ * sort by block row, duplicates kept).  slot[i] = position of input block i
+ * in the BSR order.  Host. */
+int tct_make_bsr_index(int64_t n_row_blocks, int64_t n_blocks, const int64_t* rows,
+                       const int64_t* cols, int64_t* indptr, int64_t* indices,
+                       int64_t* slot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TCT_B200_H */

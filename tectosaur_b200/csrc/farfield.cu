@@ -1,0 +1,785 @@
+// Direct farfield: matrix-free tri-to-tri matvec, point-to-point matvec and
+// dense farfield blocks.
+//
+// Tri-to-tri matvec (replaces farfield_tris_to_tris{K}, tectosaur/matrix_free.cl:19-107):
+//   out[o, b, d] = sum_s sum_{i,j} J_o J_s w_i w_j phi_b(x_i) v_d(x_i, y_j)
+// where v is the kernel's vector form (kernels/__init__.py, kernels/kernels.cl:100-206)
+// applied to the source input interpolated at y_j, point pairs with r^2 == 0 skipped.
+//
+// B200 design:
+//  * a prep pass writes one fixed-length record per source triangle: its
+//    quadrature points y_j, J_s w_j, and the input-dependent terms the
+//    kernel's vector form needs (interpolated input, normal, or the
+//    surface-curl contractions of RT/RH), so the point-pair loop reads no
+//    geometry and re-derives nothing;
+//  * the obs-side basis, weight and Jacobian are factored out of the pair
+//    loop: per obs triangle the loop accumulates one small set of sums
+//    (3 per obs quadrature point, or the 3x3 W of RH) and the 9 outputs are
+//    formed once at the end;
+//  * source records are staged through shared memory in tiles and read as
+//    warp-wide broadcasts; each tile's sum is added to the running total with
+//    Kahan compensation in FP32 ("compensated per-tile sums");
+//  * the source range is split into chunks (grid.y) so the grid covers all
+//    148 SMs several times over; chunk partials are summed in a fixed order
+//    by a second kernel, so results are deterministic.
+#include <algorithm>
+
+#include "pair_math.cuh"
+
+namespace tct {
+namespace {
+
+constexpr int MAXQ = 13;
+
+template <typename R>
+struct Rule2D {
+    R x[MAXQ], y[MAXQ], w[MAXQ];
+};
+
+// Record layout per source triangle (units of Real).
+template <int K, int NQ>
+struct Rec {
+    static constexpr int Y = 0;               // y[NQ][3]
+    static constexpr int SW = 3 * NQ;         // J_s * w_j (RH: times CsRH0)
+    static constexpr int N = 4 * NQ;          // source normal (T, H, RT)
+    static constexpr int C = 4 * NQ + 3;      // RT: curl c[3] of the input
+    static constexpr int INV = (K == kT || K == kH) ? 4 * NQ + 3
+                             : (K == kRT)          ? 4 * NQ + 6
+                                                   : 4 * NQ;  // interpolated input [NQ][3]
+    static constexpr int SSC = 4 * NQ;        // RH: -2 * ssc[3][3]
+    static constexpr int P = 4 * NQ + 9;      // RH: P[3][3]
+    static constexpr int RAW = (K == kRH) ? 4 * NQ + 18 : INV + 3 * NQ;
+    static constexpr int LEN = (RAW + 3) / 4 * 4;
+};
+
+template <int K, int NQ>
+struct NAcc {
+    static constexpr int n = (K == kRH) ? 9 : (K == kRA ? 3 * NQ + 3 : 3 * NQ);
+};
+
+template <typename R, int K, int NQ>
+__global__ void __launch_bounds__(128)
+far_prep(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
+         const int32_t* __restrict__ src_tris, int64_t n_src, const R* __restrict__ in,
+         R* __restrict__ rec) {
+    using L = Rec<K, NQ>;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_src) return;
+    TriGeom<R> s;
+    load_tri(s, pts, src_tris, i, 0, false, K == kRT || K == kRH);
+    R in9[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) in9[k] = in[i * 9 + k];
+    R* r = rec + i * L::LEN;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const R sx = rule.x[q], sy = rule.y[q];
+        const R sb[3] = {1 - sx - sy, sx, sy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            R y = 0;
+            y += sb[0] * s.v[0][d];
+            y += sb[1] * s.v[1][d];
+            y += sb[2] * s.v[2][d];
+            r[L::Y + 3 * q + d] = y;
+        }
+        R sw = s.J * rule.w[q];
+        if (K == kRH) sw = sw * c.CsRH0;
+        r[L::SW + q] = sw;
+        if (K != kRH) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                R a = 0;
+                a += in9[0 * 3 + d] * sb[0];
+                a += in9[1 * 3 + d] * sb[1];
+                a += in9[2 * 3 + d] * sb[2];
+                r[L::INV + 3 * q + d] = a;
+            }
+        }
+    }
+    if (K == kT || K == kH || K == kRT) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) r[L::N + d] = s.n[d];
+    }
+    if (K == kRT || K == kRH) {
+        // src_surf_curl[d][Ij] = sum_b bsrc_surf_curl[b][Ij] * in[b*3 + d]
+        R ssc[3][3];
+#pragma unroll
+        for (int Ij = 0; Ij < 3; Ij++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                R a = 0;
+#pragma unroll
+                for (int b = 0; b < 3; b++) a += s.sc[b][Ij] * in9[b * 3 + d];
+                ssc[d][Ij] = a;
+            }
+        if (K == kRT) {
+            // c[p] = sum_{m,j} e[m][p][j] ssc[j][m]
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                R a = 0;
+#pragma unroll
+                for (int m = 0; m < 3; m++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++)
+                        if (levi(m, p, j) != 0) a += (R)levi(m, p, j) * ssc[j][m];
+                r[L::C + p] = a;
+            }
+        } else {
+            R B = (ssc[0][0] + ssc[1][1] + ssc[2][2]) * c.CsRH1;
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    r[L::SSC + 3 * d + j] = R(-2) * ssc[d][j];
+                    r[L::P + 3 * d + j] = (d == j ? B : R(0)) + c.CsRH2 * ssc[j][d] - 2 * ssc[d][j];
+                }
+        }
+    }
+#pragma unroll
+    for (int k = L::RAW; k < L::LEN; k++) r[k] = 0;
+}
+
+// Vector forms of U/T/A/H at one point pair (kernels/__init__.py:28-36, 67-99,
+// 147-173): returns the 3-vector the reference adds to sum{x,y,z}.
+template <typename R, int K>
+__device__ __forceinline__ void vec_utah(const Consts<R>& c, const R D[3], R r2, const R no[3],
+                                         const R ns[3], const R a[3], R v[3]) {
+    if (K == kU) {
+        R invr = rsqrt_r(r2);
+        R Q1 = c.CsU0 * invr;
+        R Q2 = c.CsU1 * invr / r2;
+        R ddi = D[0] * a[0] + D[1] * a[1] + D[2] * a[2];
+#pragma unroll
+        for (int d = 0; d < 3; d++) v[d] = Q1 * a[d] + Q2 * D[d] * ddi;
+    } else if (K == kT || K == kA) {
+        const R mp = (K == kT) ? R(-1) : R(1);
+        const R pm = (K == kT) ? R(1) : R(-1);
+        const R* n = (K == kT) ? ns : no;
+        R invr = rsqrt_r(r2);
+        R invr2 = invr * invr;
+        R invr3 = invr2 * invr;
+        R rn = n[0] * D[0] + n[1] * D[1] + n[2] * D[2];
+        R A = pm * c.CsT0 * invr3;
+        R C = mp * c.CsT1 * invr3 * invr2;
+        R rnddi = C * rn * (D[0] * a[0] + D[1] * a[1] + D[2] * a[2]);
+        R nxdy = n[0] * D[1] - n[1] * D[0];
+        R nzdx = n[2] * D[0] - n[0] * D[2];
+        R nzdy = n[2] * D[1] - n[1] * D[2];
+        v[0] = A * (-rn * a[0] + mp * nxdy * a[1] + pm * nzdx * a[2]) + D[0] * rnddi;
+        v[1] = A * (pm * nxdy * a[0] - rn * a[1] + pm * nzdy * a[2]) + D[1] * rnddi;
+        v[2] = A * (mp * nzdx * a[0] + mp * nzdy * a[1] - rn * a[2]) + D[2] * rnddi;
+    } else {
+        R invr = rsqrt_r(r2);
+        R invr2 = invr * invr;
+        R invr3 = invr2 * invr;
+        R rn = invr * (ns[0] * D[0] + ns[1] * D[1] + ns[2] * D[2]);
+        R rm = invr * (no[0] * D[0] + no[1] * D[1] + no[2] * D[2]);
+        R mn = no[0] * ns[0] + no[1] * ns[1] + no[2] * ns[2];
+        R sn = a[0] * ns[0] + a[1] * ns[1] + a[2] * ns[2];
+        R sd = invr * (a[0] * D[0] + a[1] * D[1] + a[2] * D[2]);
+        R sm = a[0] * no[0] + a[1] * no[1] + a[2] * no[2];
+        R Q = c.CsH0 * invr3;
+        R A = Q * 3 * rn;
+        R B = Q * c.CsH1;
+        R C = Q * c.CsH3;
+        R MT = Q * c.CsH2 * sn + A * c.CsH1 * sd;
+        R NT = B * sm + C * sd * rm;
+        R DT = invr * (B * 3 * sn * rm + C * sd * mn + A * (c.nu * sm - 5 * sd * rm));
+        R ST = A * c.nu * rm + B * mn;
+#pragma unroll
+        for (int d = 0; d < 3; d++) v[d] = ns[d] * NT + no[d] * MT + D[d] * DT + ST * a[d];
+    }
+}
+
+template <typename R, bool KAHAN>
+__device__ __forceinline__ void fold(R& tot, R& cmp, R tile) {
+    if (KAHAN) {
+        R y = tile - cmp;
+        R t = tot + y;
+        cmp = (t - tot) - y;
+        tot = t;
+    } else {
+        tot += tile;
+    }
+}
+
+template <typename R, int K, int NQ, int TS>
+__global__ void __launch_bounds__(128)
+far_main(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
+         const int32_t* __restrict__ obs_tris, int64_t n_obs, const R* __restrict__ rec,
+         int64_t n_src, int64_t src_per_chunk, R* __restrict__ dst, int direct,
+         int accumulate) {
+    using L = Rec<K, NQ>;
+    constexpr int NA = NAcc<K, NQ>::n;
+    constexpr bool KAHAN = sizeof(R) == 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* sm = reinterpret_cast<R*>(smem_raw);
+
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_obs;
+    const int64_t s_begin = (int64_t)blockIdx.y * src_per_chunk;
+    const int64_t s_end = min(n_src, s_begin + src_per_chunk);
+
+    constexpr bool need_sc = (K == kRA || K == kRH);
+    TriGeom<R> o;
+    if (valid) {
+        load_tri(o, pts, obs_tris, i, 0, false, need_sc);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                o.v[a][d] = 0;
+                o.sc[a][d] = 0;
+            }
+        o.n[0] = o.n[1] = o.n[2] = 0;
+        o.J = 0;
+    }
+    R x[NQ][3];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const R ox = rule.x[q], oy = rule.y[q];
+        const R ob[3] = {1 - ox - oy, ox, oy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            R v = 0;
+            v += ob[0] * o.v[0][d];
+            v += ob[1] * o.v[1][d];
+            v += ob[2] * o.v[2][d];
+            x[q][d] = v;
+        }
+    }
+    R tot[NA], cmp[NA];
+#pragma unroll
+    for (int k = 0; k < NA; k++) {
+        tot[k] = 0;
+        cmp[k] = 0;
+    }
+
+    for (int64_t t0 = s_begin; t0 < s_end; t0 += TS) {
+        const int n_tile = (int)min((int64_t)TS, s_end - t0);
+        __syncthreads();
+        {
+            // cooperative, vectorised copy of n_tile records into shared memory
+            const int n_vec = n_tile * L::LEN / 4;
+            if (sizeof(R) == 4) {
+                const float4* srcv = reinterpret_cast<const float4*>(rec + t0 * L::LEN);
+                float4* dstv = reinterpret_cast<float4*>(sm);
+                for (int k = threadIdx.x; k < n_vec; k += blockDim.x) dstv[k] = __ldg(srcv + k);
+            } else {
+                const double2* srcv = reinterpret_cast<const double2*>(rec + t0 * L::LEN);
+                double2* dstv = reinterpret_cast<double2*>(sm);
+                for (int k = threadIdx.x; k < 2 * n_vec; k += blockDim.x) dstv[k] = __ldg(srcv + k);
+            }
+        }
+        __syncthreads();
+        if (!valid) continue;
+        R acc[NA];
+#pragma unroll
+        for (int k = 0; k < NA; k++) acc[k] = 0;
+        for (int j = 0; j < n_tile; j++) {
+            const R* r = sm + j * L::LEN;
+            if (K == kRH) {
+                R S0 = 0, T00 = 0, T01 = 0, T02 = 0, T11 = 0, T12 = 0, T22 = 0;
+#pragma unroll
+                for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+                    for (int q2 = 0; q2 < NQ; q2++) {
+                        R D0 = r[L::Y + 3 * q2 + 0] - x[q1][0];
+                        R D1 = r[L::Y + 3 * q2 + 1] - x[q1][1];
+                        R D2 = r[L::Y + 3 * q2 + 2] - x[q1][2];
+                        R r2 = D0 * D0 + D1 * D1 + D2 * D2;
+                        R invr = (r2 != R(0)) ? rsqrt_r(r2) : R(0);
+                        R f = (rule.w[q1] * r[L::SW + q2]) * invr;
+                        R g = f * (invr * invr);
+                        S0 += f;
+                        R g0 = g * D0, g1 = g * D1, g2 = g * D2;
+                        T00 += g0 * D0;
+                        T01 += g0 * D1;
+                        T02 += g0 * D2;
+                        T11 += g1 * D1;
+                        T12 += g1 * D2;
+                        T22 += g2 * D2;
+                    }
+                const R T[3][3] = {{T00, T01, T02}, {T01, T11, T12}, {T02, T12, T22}};
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+#pragma unroll
+                    for (int jj = 0; jj < 3; jj++) {
+                        R w = S0 * r[L::P + 3 * d + jj];
+                        w += T[d][0] * r[L::SSC + 0 * 3 + jj];
+                        w += T[d][1] * r[L::SSC + 1 * 3 + jj];
+                        w += T[d][2] * r[L::SSC + 2 * 3 + jj];
+                        acc[3 * d + jj] += w;
+                    }
+            } else {
+#pragma unroll
+                for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+                    for (int q2 = 0; q2 < NQ; q2++) {
+                        R D[3];
+                        D[0] = r[L::Y + 3 * q2 + 0] - x[q1][0];
+                        D[1] = r[L::Y + 3 * q2 + 1] - x[q1][1];
+                        D[2] = r[L::Y + 3 * q2 + 2] - x[q1][2];
+                        R r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+                        if (r2 == R(0)) continue;
+                        const R sw = r[L::SW + q2];
+                        const R a[3] = {r[L::INV + 3 * q2 + 0], r[L::INV + 3 * q2 + 1],
+                                        r[L::INV + 3 * q2 + 2]};
+                        if (K <= kH) {
+                            R ns[3] = {0, 0, 0};
+                            if (K == kT || K == kH) {
+                                ns[0] = r[L::N + 0];
+                                ns[1] = r[L::N + 1];
+                                ns[2] = r[L::N + 2];
+                            }
+                            R v[3];
+                            vec_utah<R, K>(c, D, r2, o.n, ns, a, v);
+#pragma unroll
+                            for (int d = 0; d < 3; d++) acc[3 * q1 + d] += sw * v[d];
+                        } else if (K == kRT) {
+                            // sum_d = Q1 c_d + Q2 D_d (D.c) + Q3 (n_s.D) a_d
+                            R invr = rsqrt_r(r2);
+                            R invr3 = invr * invr * invr;
+                            R Q1 = c.CsRT1 * invr, Q2 = c.CsRT0 * invr3, Q3 = c.CsRT2 * invr3;
+                            const R cc[3] = {r[L::C + 0], r[L::C + 1], r[L::C + 2]};
+                            R Dc = D[0] * cc[0] + D[1] * cc[1] + D[2] * cc[2];
+                            R nD = r[L::N + 0] * D[0] + r[L::N + 1] * D[1] + r[L::N + 2] * D[2];
+                            R Q3nD = Q3 * nD;
+#pragma unroll
+                            for (int d = 0; d < 3; d++)
+                                acc[3 * q1 + d] += sw * (Q1 * cc[d] + Q2 * D[d] * Dc + Q3nD * a[d]);
+                        } else {  // kRA
+                            // U_k += w1 sw (Q1 a_k + Q2 (D.a) D_k);
+                            // acc[q1] += sw * (-Q3 (n_o.D)) a
+                            R invr = rsqrt_r(r2);
+                            R invr3 = invr * invr * invr;
+                            R Q1 = c.CsRT1 * invr, Q2 = c.CsRT0 * invr3, Q3 = c.CsRT2 * invr3;
+                            R Da = D[0] * a[0] + D[1] * a[1] + D[2] * a[2];
+                            R nD = o.n[0] * D[0] + o.n[1] * D[1] + o.n[2] * D[2];
+                            R ww = rule.w[q1] * sw;
+#pragma unroll
+                            for (int d = 0; d < 3; d++) {
+                                acc[3 * NQ + d] += ww * (Q1 * a[d] + Q2 * Da * D[d]);
+                                acc[3 * q1 + d] -= sw * (Q3 * nD * a[d]);
+                            }
+                        }
+                    }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NA; k++) fold<R, KAHAN>(tot[k], cmp[k], acc[k]);
+    }
+    if (!valid) return;
+
+    // obs-side contraction: out[b][d]
+    R out9[9];
+    if (K == kRH) {
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                out9[b * 3 + d] = o.J * (o.sc[b][0] * tot[3 * d + 0] + o.sc[b][1] * tot[3 * d + 1] +
+                                         o.sc[b][2] * tot[3 * d + 2]);
+    } else {
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                R s = 0;
+#pragma unroll
+                for (int q = 0; q < NQ; q++) {
+                    const R ox = rule.x[q], oy = rule.y[q];
+                    const R ob = (b == 0) ? (1 - ox - oy) : (b == 1 ? ox : oy);
+                    s += (rule.w[q] * ob) * tot[3 * q + d];
+                }
+                if (K == kRA) {
+                    // + sum_Ij sc_o[b][Ij] V[Ij][d],  V[m][j] = -sum_k e[m][j][k] U_k
+#pragma unroll
+                    for (int m = 0; m < 3; m++)
+#pragma unroll
+                        for (int k = 0; k < 3; k++)
+                            if (levi(m, d, k) != 0)
+                                s -= (R)levi(m, d, k) * o.sc[b][m] * tot[3 * NQ + k];
+                }
+                out9[b * 3 + d] = o.J * s;
+            }
+    }
+    if (direct) {
+        R* op = dst + i * 9;
+#pragma unroll
+        for (int k = 0; k < 9; k++) op[k] = accumulate ? op[k] + out9[k] : out9[k];
+    } else {
+        R* op = dst + ((int64_t)blockIdx.y * n_obs + i) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; k++) op[k] = out9[k];
+    }
+}
+
+template <typename R>
+__global__ void chunk_reduce(const R* __restrict__ partial, int n_chunks, int64_t n,
+                             R* __restrict__ out, int accumulate) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    R s = accumulate ? out[i] : R(0);
+    for (int c = 0; c < n_chunks; c++) s += partial[(int64_t)c * n + i];
+    out[i] = s;
+}
+
+inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+int rec_len(int kernel, int nq) {
+#define TCT_LEN_CASE(KID)                                                  \
+    case KID:                                                              \
+        switch (nq) {                                                      \
+            case 3: return Rec<KID, 3>::LEN;                               \
+            case 4: return Rec<KID, 4>::LEN;                               \
+            case 7: return Rec<KID, 7>::LEN;                               \
+            case 13: return Rec<KID, 13>::LEN;                             \
+            default: return -1;                                            \
+        }
+    switch (kernel) {
+        TCT_LEN_CASE(kU)
+        TCT_LEN_CASE(kT)
+        TCT_LEN_CASE(kA)
+        TCT_LEN_CASE(kH)
+        TCT_LEN_CASE(kRT)
+        TCT_LEN_CASE(kRA)
+        TCT_LEN_CASE(kRH)
+        default: return -1;
+    }
+#undef TCT_LEN_CASE
+}
+
+// Number of source chunks: enough (obs-block, chunk) tiles to cover the 148
+// SMs about eight times, at least one tile of sources per chunk, at most 32.
+// Depends only on the problem size, so the workspace size is device-independent.
+int64_t n_chunks_for(int64_t n_obs, int64_t n_src, int ts) {
+    const int64_t obs_blocks = (n_obs + 127) / 128;
+    int64_t want = (148 * 8 + obs_blocks - 1) / std::max<int64_t>(obs_blocks, 1);
+    int64_t max_by_src = std::max<int64_t>(1, n_src / ts);
+    return std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, max_by_src), 32));
+}
+
+inline int tile_for(int nq) { return nq <= 4 ? 128 : 32; }
+
+template <typename R, int K, int NQ>
+int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, const R* pts,
+            const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris, int64_t n_src,
+            int accumulate, unsigned char* ws, cudaStream_t st) {
+    using L = Rec<K, NQ>;
+    constexpr int TS = NQ <= 4 ? 128 : 32;
+    R* rec = reinterpret_cast<R*>(ws);
+    const size_t rec_bytes = align256(sizeof(R) * L::LEN * (size_t)n_src);
+    far_prep<R, K, NQ><<<(unsigned)((n_src + 127) / 128), 128, 0, st>>>(c, rule, pts, src_tris,
+                                                                      n_src, in, rec);
+    int rc = launch_status("farfield prep");
+    if (rc) return rc;
+    const int64_t chunks = n_chunks_for(n_obs, n_src, TS);
+    const int64_t per_chunk = ((n_src + chunks - 1) / chunks + TS - 1) / TS * TS;
+    const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
+    const size_t smem = sizeof(R) * L::LEN * TS;
+    auto kfn = far_main<R, K, NQ, TS>;
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    dim3 grid((unsigned)((n_obs + 127) / 128), (unsigned)real_chunks);
+    if (real_chunks == 1) {
+        kfn<<<grid, 128, smem, st>>>(c, rule, pts, obs_tris, n_obs, rec, n_src, per_chunk, out, 1,
+                                      accumulate);
+        return launch_status("farfield main");
+    }
+    R* partial = reinterpret_cast<R*>(ws + rec_bytes);
+    kfn<<<grid, 128, smem, st>>>(c, rule, pts, obs_tris, n_obs, rec, n_src, per_chunk, partial, 0,
+                                  0);
+    rc = launch_status("farfield main");
+    if (rc) return rc;
+    const int64_t n = n_obs * 9;
+    chunk_reduce<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(partial, (int)real_chunks, n, out,
+                                                                accumulate);
+    return launch_status("farfield chunk reduce");
+}
+
+template <typename R, int K>
+int run_far_nq(int nq, const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in,
+               const R* pts, const int32_t* ot, int64_t n_obs, const int32_t* stris,
+               int64_t n_src, int acc, unsigned char* ws, cudaStream_t st) {
+    switch (nq) {
+        case 3: return run_far<R, K, 3>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
+        case 4: return run_far<R, K, 4>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
+        case 7: return run_far<R, K, 7>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
+        case 13: return run_far<R, K, 13>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
+        default:
+            set_error("tct_farfield_tris_matvec: %d-point triangle rules are not supported "
+                      "(supported: 3, 4, 7, 13 = gauss2d_tri(1..4))", nq);
+            return TCT_ERR_ARG;
+    }
+}
+
+template <typename R>
+int far_dispatch(int kernel, int nq, const double* qp, const double* qw, const double* params,
+                 void* out, const void* in, const void* pts, const int32_t* ot, int64_t n_obs,
+                 const int32_t* stris, int64_t n_src, int acc, void* ws, cudaStream_t st) {
+    Consts<R> c = make_consts<R>(params);
+    Rule2D<R> rule;
+    for (int q = 0; q < MAXQ; q++) {
+        rule.x[q] = q < nq ? (R)qp[2 * q] : R(0);
+        rule.y[q] = q < nq ? (R)qp[2 * q + 1] : R(0);
+        rule.w[q] = q < nq ? (R)qw[q] : R(0);
+    }
+    unsigned char* w = reinterpret_cast<unsigned char*>(ws);
+#define TCT_FAR_CASE(KID)                                                                   \
+    case KID:                                                                               \
+        return run_far_nq<R, KID>(nq, c, rule, (R*)out, (const R*)in, (const R*)pts, ot,   \
+                                  n_obs, stris, n_src, acc, w, st);
+    switch (kernel) {
+        TCT_FAR_CASE(kU)
+        TCT_FAR_CASE(kT)
+        TCT_FAR_CASE(kA)
+        TCT_FAR_CASE(kH)
+        TCT_FAR_CASE(kRT)
+        TCT_FAR_CASE(kRA)
+        TCT_FAR_CASE(kRH)
+        default:
+            set_error("tct_farfield_tris_matvec: unsupported kernel id %d", kernel);
+            return TCT_ERR_KERNEL;
+    }
+#undef TCT_FAR_CASE
+}
+
+// ---- point-to-point farfield (farfield_direct.cl:15-113) --------------------
+template <typename R, int K>
+__global__ void __launch_bounds__(128)
+pts_kernel(Consts<R> c, R* __restrict__ out, const R* __restrict__ obs_pts,
+           const R* __restrict__ obs_ns, int64_t n_obs, const R* __restrict__ src_pts,
+           const R* __restrict__ src_ns, int64_t n_src, const R* __restrict__ in) {
+    __shared__ R sh[128 * 9];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n_obs;
+    R xo[3] = {0, 0, 0}, no[3] = {0, 0, 0};
+    if (valid) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            xo[d] = obs_pts[i * 3 + d];
+            no[d] = obs_ns[i * 3 + d];
+        }
+    }
+    R sum[3] = {0, 0, 0};
+    for (int64_t t0 = 0; t0 < n_src; t0 += 128) {
+        const int n_tile = (int)min((int64_t)128, n_src - t0);
+        __syncthreads();
+        if (threadIdx.x < n_tile) {
+            const int64_t j = t0 + threadIdx.x;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                sh[threadIdx.x * 9 + d] = src_pts[j * 3 + d];
+                sh[threadIdx.x * 9 + 3 + d] = src_ns[j * 3 + d];
+                sh[threadIdx.x * 9 + 6 + d] = in[j * 3 + d];
+            }
+        }
+        __syncthreads();
+        if (!valid) continue;
+        for (int k = 0; k < n_tile; k++) {
+            const R* r = sh + k * 9;
+            R D[3] = {r[0] - xo[0], r[1] - xo[1], r[2] - xo[2]};
+            R r2 = D[0] * D[0];
+            r2 += D[1] * D[1];
+            r2 += D[2] * D[2];
+            if (r2 == R(0)) continue;
+            R v[3];
+            vec_utah<R, K>(c, D, r2, no, r + 3, r + 6, v);
+            sum[0] += v[0];
+            sum[1] += v[1];
+            sum[2] += v[2];
+        }
+    }
+    if (valid) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) out[i * 3 + d] = sum[d];
+    }
+}
+
+template <typename R>
+int pts_dispatch(int kernel, const double* params, void* out, const void* op, const void* on,
+                 int64_t n_obs, const void* sp, const void* sn, int64_t n_src, const void* in,
+                 cudaStream_t st) {
+    Consts<R> c = make_consts<R>(params);
+    unsigned blocks = (unsigned)((n_obs + 127) / 128);
+#define TCT_PTS_CASE(KID)                                                                 \
+    case KID:                                                                             \
+        pts_kernel<R, KID><<<blocks, 128, 0, st>>>(c, (R*)out, (const R*)op, (const R*)on, \
+                                                   n_obs, (const R*)sp, (const R*)sn,     \
+                                                   n_src, (const R*)in);                  \
+        break;
+    switch (kernel) {
+        TCT_PTS_CASE(kU)
+        TCT_PTS_CASE(kT)
+        TCT_PTS_CASE(kA)
+        TCT_PTS_CASE(kH)
+        default:
+            set_error("tct_farfield_pts: kernel id %d has no point form (surface-curl "
+                      "kernels need whole triangles)", kernel);
+            return TCT_ERR_KERNEL;
+    }
+#undef TCT_PTS_CASE
+    return launch_status("tct_farfield_pts");
+}
+
+// ---- dense farfield blocks (assemble.cl:105-138) ------------------------------
+template <typename R, int K>
+__global__ void __launch_bounds__(128)
+dense_kernel(Consts<R> c, R* __restrict__ out, int n_q, const R* __restrict__ qp,
+             const R* __restrict__ qw, const R* __restrict__ pts,
+             const int32_t* __restrict__ obs_tris, int64_t n_obs,
+             const int32_t* __restrict__ src_tris, int64_t n_src) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_obs * n_src) return;
+    const int64_t oi = p / n_src, si = p % n_src;
+    TriGeom<R> o, s;
+    load_tri(o, pts, obs_tris, oi, 0, false, K == kRA || K == kRH);
+    load_tri(s, pts, src_tris, si, 0, false, K == kRT || K == kRH);
+    R res[81];
+    integrate_pair<R, K, (sizeof(R) == 4) && (K <= kH)>(c, o, s, n_q, qp, qw, false, res);
+    const R scale = o.J * s.J;
+#pragma unroll
+    for (int bo = 0; bo < 3; bo++)
+#pragma unroll
+        for (int dob = 0; dob < 3; dob++)
+#pragma unroll
+            for (int bs = 0; bs < 3; bs++)
+#pragma unroll
+                for (int ds = 0; ds < 3; ds++)
+                    out[(oi * 9 + bo * 3 + dob) * n_src * 9 + (si * 9 + bs * 3 + ds)] =
+                        scale * res[bo * 27 + dob * 9 + bs * 3 + ds];
+}
+
+template <typename R>
+int dense_dispatch(int kernel, const double* params, void* out, int n_q, const void* qp,
+                   const void* qw, const void* pts, const int32_t* ot, int64_t n_obs,
+                   const int32_t* stris, int64_t n_src, cudaStream_t st) {
+    Consts<R> c = make_consts<R>(params);
+    const int64_t n = n_obs * n_src;
+    unsigned blocks = (unsigned)((n + 127) / 128);
+#define TCT_DENSE_CASE(KID)                                                               \
+    case KID:                                                                             \
+        dense_kernel<R, KID><<<blocks, 128, 0, st>>>(c, (R*)out, n_q, (const R*)qp,       \
+                                                     (const R*)qw, (const R*)pts, ot,     \
+                                                     n_obs, stris, n_src);                \
+        break;
+    switch (kernel) {
+        TCT_DENSE_CASE(kU)
+        TCT_DENSE_CASE(kT)
+        TCT_DENSE_CASE(kA)
+        TCT_DENSE_CASE(kH)
+        TCT_DENSE_CASE(kRT)
+        TCT_DENSE_CASE(kRA)
+        TCT_DENSE_CASE(kRH)
+        default:
+            set_error("tct_farfield_tris_dense: unsupported kernel id %d", kernel);
+            return TCT_ERR_KERNEL;
+    }
+#undef TCT_DENSE_CASE
+    return launch_status("tct_farfield_tris_dense");
+}
+
+}  // namespace
+
+size_t farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_src, int n_q) {
+    const int len = rec_len(kernel, n_q);
+    if (len < 0 || n_src < 0 || n_obs < 0) return 0;
+    const size_t rs = prec == TCT_F64 ? 8 : 4;
+    const size_t rec_bytes = align256(rs * len * (size_t)n_src);
+    const int64_t chunks = n_chunks_for(n_obs, n_src, tile_for(n_q));
+    const size_t part = chunks > 1 ? align256(rs * 9 * (size_t)n_obs * chunks) : 0;
+    return rec_bytes + part;
+}
+
+}  // namespace tct
+
+extern "C" size_t tct_farfield_workspace_bytes(int kernel, int prec, int64_t n_obs,
+                                               int64_t n_src, int n_q) {
+    return tct::farfield_workspace_bytes(kernel, prec, n_obs, n_src, n_q);
+}
+
+extern "C" int tct_farfield_tris_matvec(int kernel, int prec, void* out, const void* in,
+                                        const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                                        const int32_t* src_tris, int64_t n_src, int n_q,
+                                        const double* quad_pts, const double* quad_wts,
+                                        const double* params, int accumulate, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_tris_matvec: negative size");
+    TCT_CHECK_ARG(n_obs < (int64_t(1) << 31) && n_src < (int64_t(1) << 31),
+                  "tct_farfield_tris_matvec: more than 2^31 triangles");
+    TCT_CHECK_ARG(n_q >= 1 && n_q <= 13 && quad_pts && quad_wts && params,
+                  "tct_farfield_tris_matvec: bad quadrature rule or params");
+    if (n_obs == 0) return TCT_OK;
+    TCT_CHECK_ARG(out && pts && obs_tris, "tct_farfield_tris_matvec: null pointer");
+    if (n_src == 0) {
+        if (!accumulate) {
+            cudaMemsetAsync(out, 0, (prec == TCT_F64 ? 8 : 4) * 9 * (size_t)n_obs, as_stream(stream));
+            return launch_status("tct_farfield_tris_matvec memset");
+        }
+        return TCT_OK;
+    }
+    TCT_CHECK_ARG(in && src_tris && workspace, "tct_farfield_tris_matvec: null pointer");
+    TCT_CHECK_ARG(aligned(workspace, 256), "tct_farfield_tris_matvec: workspace not 256-byte aligned");
+    const size_t need = farfield_workspace_bytes(kernel, prec, n_obs, n_src, n_q);
+    if (need == 0) {
+        set_error("tct_farfield_tris_matvec: unsupported kernel %d or %d-point rule", kernel, n_q);
+        return TCT_ERR_ARG;
+    }
+    if (workspace_bytes < need) {
+        set_error("tct_farfield_tris_matvec: workspace %zu bytes < required %zu", workspace_bytes, need);
+        return TCT_ERR_OOM;
+    }
+    if (prec == TCT_F32)
+        return far_dispatch<float>(kernel, n_q, quad_pts, quad_wts, params, out, in, pts, obs_tris,
+                                   n_obs, src_tris, n_src, accumulate, workspace, as_stream(stream));
+    if (prec == TCT_F64)
+        return far_dispatch<double>(kernel, n_q, quad_pts, quad_wts, params, out, in, pts, obs_tris,
+                                    n_obs, src_tris, n_src, accumulate, workspace, as_stream(stream));
+    set_error("tct_farfield_tris_matvec: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
+
+extern "C" int tct_farfield_pts(int kernel, int prec, void* out, const void* obs_pts,
+                                const void* obs_ns, int64_t n_obs, const void* src_pts,
+                                const void* src_ns, int64_t n_src, const void* in,
+                                const double* params, void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_pts: negative size");
+    if (n_obs == 0) return TCT_OK;
+    TCT_CHECK_ARG(out && obs_pts && obs_ns && params, "tct_farfield_pts: null pointer");
+    TCT_CHECK_ARG(n_src == 0 || (src_pts && src_ns && in), "tct_farfield_pts: null pointer");
+    if (prec == TCT_F32)
+        return pts_dispatch<float>(kernel, params, out, obs_pts, obs_ns, n_obs, src_pts, src_ns,
+                                   n_src, in, as_stream(stream));
+    if (prec == TCT_F64)
+        return pts_dispatch<double>(kernel, params, out, obs_pts, obs_ns, n_obs, src_pts, src_ns,
+                                    n_src, in, as_stream(stream));
+    set_error("tct_farfield_pts: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
+
+extern "C" int tct_farfield_tris_dense(int kernel, int prec, void* out, int n_quad,
+                                       const void* quad_pts, const void* quad_wts,
+                                       const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                                       const int32_t* src_tris, int64_t n_src,
+                                       const double* params, void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_tris_dense: negative size");
+    if (n_obs == 0 || n_src == 0) return TCT_OK;
+    TCT_CHECK_ARG(n_obs * n_src < (int64_t(1) << 31) * 128, "tct_farfield_tris_dense: too large");
+    TCT_CHECK_ARG(out && quad_pts && quad_wts && pts && obs_tris && src_tris && params && n_quad > 0,
+                  "tct_farfield_tris_dense: null pointer or empty rule");
+    if (prec == TCT_F32)
+        return dense_dispatch<float>(kernel, params, out, n_quad, quad_pts, quad_wts, pts, obs_tris,
+                                     n_obs, src_tris, n_src, as_stream(stream));
+    if (prec == TCT_F64)
+        return dense_dispatch<double>(kernel, params, out, n_quad, quad_pts, quad_wts, pts,
+                                      obs_tris, n_obs, src_tris, n_src, as_stream(stream));
+    set_error("tct_farfield_tris_dense: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
