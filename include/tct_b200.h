@@ -134,6 +134,13 @@ int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
                     void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Measurement utility (no reference counterpart): FP32 FMA throughput probe.
+ * Launches n_blocks x 256 threads, each running `iters` steps of 8 independent
+ * fused multiply-adds (16 * iters flops per thread); out: >= 256 floats of
+ * device scratch.  Timed by the caller; the FP32 roofline denominator. */
+int tct_fp32_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Host-side (CPU) structure builders.                                       */
 
 /* Near-pair search: all (i, j) with |c_i - c_j|^2 <= ((r_i + r_j) * threshold)^2

@@ -5,6 +5,7 @@
 #include "oracle.h"
 
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 #include <omp.h>
@@ -600,17 +601,36 @@ int bsr_impl(long mb, int bs, const long* indptr, const long* indices,
     return 0;
 }
 
+// bcoomv: one block per iteration, atomic scatter into y
+// (util/fast_sparse.cpp:128-163); serial when n_threads == 1.
 template <typename R>
 int bcoo_impl(long nb, int bs, const long* rows, const long* cols,
-              const double* data, const double* x, double* y) {
+              const double* data, const double* x, double* y, int n_threads) {
+    std::vector<R> yr(std::max(0L, 0L));
+    long n_rows = 0;
+    for (long b = 0; b < nb; b++) n_rows = std::max(n_rows, rows[b] + 1);
+    yr.assign((size_t)n_rows * bs, R(0));
+    std::vector<R> xr;
+    long n_cols = 0;
+    for (long b = 0; b < nb; b++) n_cols = std::max(n_cols, cols[b] + 1);
+    xr.resize((size_t)n_cols * bs);
+    for (long k = 0; k < n_cols * bs; k++) xr[k] = R(x[k]);
+    std::vector<R> Ar((size_t)nb * bs * bs);
+    for (size_t k = 0; k < Ar.size(); k++) Ar[k] = R(data[k]);
+    for (long k = 0; k < n_rows * bs; k++) yr[k] = R(y[k]);
+#pragma omp parallel for num_threads(n_threads) schedule(static)
     for (long b = 0; b < nb; b++) {
-        const double* A = data + (size_t)bs * bs * b;
+        const R* A = Ar.data() + (size_t)bs * bs * b;
+        const R* xs = xr.data() + (size_t)bs * cols[b];
+        R* ys = yr.data() + (size_t)bs * rows[b];
         for (int i = 0; i < bs; i++) {
             R acc = 0;
-            for (int j = 0; j < bs; j++) acc = acc + R(A[i * bs + j]) * R(x[bs * cols[b] + j]);
-            y[bs * rows[b] + i] = R(y[bs * rows[b] + i]) + acc;
+            for (int j = 0; j < bs; j++) acc = acc + A[i * bs + j] * xs[j];
+#pragma omp atomic
+            ys[i] += acc;
         }
     }
+    for (long k = 0; k < n_rows * bs; k++) y[k] = yr[k];
     return 0;
 }
 
@@ -705,10 +725,11 @@ int orc_bsr_matvec(int prec, long n_row_blocks, int bs, const long* indptr,
 
 int orc_bcoo_matvec(int prec, long n_blocks, int bs, const long* rows,
                     const long* cols, const double* data, const double* x,
-                    double* y) {
+                    double* y, int n_threads) {
     if (bs < 1 || bs > 16) return 1;
-    if (prec == 0) return bcoo_impl<float>(n_blocks, bs, rows, cols, data, x, y);
-    return bcoo_impl<double>(n_blocks, bs, rows, cols, data, x, y);
+    if (n_threads < 1) n_threads = 1;
+    if (prec == 0) return bcoo_impl<float>(n_blocks, bs, rows, cols, data, x, y, n_threads);
+    return bcoo_impl<double>(n_blocks, bs, rows, cols, data, x, y, n_threads);
 }
 
 }  // extern "C"

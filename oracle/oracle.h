@@ -53,14 +53,15 @@ int orc_make_bsr(long n_row_blocks, long n_blocks, int bs, const long* rows,
                  const long* cols, const double* data, long* indptr,
                  long* indices, double* data_out);
 
-/* bsrmv{bs} and bcoomv{bs}: tectosaur/util/fast_sparse.cpp:71-163, serial
- * (deterministic order).  y is overwritten (bsr) / accumulated (bcoo). */
+/* bsrmv{bs} and bcoomv{bs}: tectosaur/util/fast_sparse.cpp:71-163.  bsr is
+ * serial (deterministic order) and overwrites y; bcoo accumulates into y with
+ * an atomic scatter over n_threads OpenMP threads, as the reference does. */
 int orc_bsr_matvec(int prec, long n_row_blocks, int bs, const long* indptr,
                    const long* indices, const double* data, const double* x,
                    double* y);
 int orc_bcoo_matvec(int prec, long n_blocks, int bs, const long* rows,
                     const long* cols, const double* data, const double* x,
-                    double* y);
+                    double* y, int n_threads);
 
 #ifdef __cplusplus
 }

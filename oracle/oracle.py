@@ -177,7 +177,7 @@ def bsr_matvec(float_type, indptr, indices, data, x):
     return y
 
 
-def bcoo_matvec(float_type, rows, cols, data, x, n_rows):
+def bcoo_matvec(float_type, rows, cols, data, x, n_rows, n_threads=1):
     data = np.ascontiguousarray(data, dtype=np.float64)
     bs = data.shape[1]
     y = np.zeros(n_rows)
@@ -187,6 +187,6 @@ def bcoo_matvec(float_type, rows, cols, data, x, n_rows):
     xx, xp = _d(x)
     _, yp = _d(y)
     rc = lib().orc_bcoo_matvec(_prec(float_type), ctypes.c_long(data.shape[0]), bs, ap,
-                               bp, dp, xp, yp)
+                               bp, dp, xp, yp, _threads(n_threads))
     _check(rc, "bcoo_matvec")
     return y

@@ -1,0 +1,123 @@
+"""ctypes binding of libtct_b200.so (the C ABI declared in include/tct_b200.h).
+
+The shared library is the only compute path: if it is missing this module
+raises at import, and every non-zero status becomes a RuntimeError carrying
+the library's last error message.  There is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtct_b200.so")
+
+TCT_OK = 0
+TCT_ERR_ARG = 1
+TCT_ERR_KERNEL = 2
+TCT_ERR_CUDA = 3
+TCT_ERR_OOM = 4
+TCT_ERR_TIMEOUT = 5
+TCT_ERR_PREC = 6
+TCT_F32 = 0
+TCT_F64 = 1
+
+_STATUS = {1: "bad argument", 2: "unsupported kernel", 3: "CUDA error", 4: "out of memory",
+           5: "timeout", 6: "unsupported precision"}
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        "tectosaur_b200: %s is not built; run `python tectosaur_b200/build.py` "
+        "(there is no CPU fallback)" % LIB_PATH)
+
+lib = ctypes.CDLL(LIB_PATH)
+
+c_p = ctypes.c_void_p
+c_i = ctypes.c_int
+c_i64 = ctypes.c_int64
+c_sz = ctypes.c_size_t
+c_dp = ctypes.POINTER(ctypes.c_double)
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+
+_SIGS = {
+    "tct_version": ([], ctypes.c_char_p),
+    "tct_last_error": ([], ctypes.c_char_p),
+    "tct_kernel_id": ([ctypes.c_char_p], c_i),
+    "tct_pairs_integrate": ([c_i, c_i, c_i, c_i, c_p, c_p, c_i64, c_i, c_i, c_i, c_p, c_p, c_p,
+                             c_p, c_p, c_i64, c_dp, c_p], c_i),
+    "tct_farfield_workspace_bytes": ([c_i, c_i, c_i64, c_i64, c_i], c_sz),
+    "tct_farfield_tris_matvec": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_dp,
+                                  c_dp, c_dp, c_i, c_p, c_sz, c_p], c_i),
+    "tct_farfield_pts": ([c_i, c_i, c_p, c_p, c_p, c_i64, c_p, c_p, c_i64, c_p, c_dp, c_p], c_i),
+    "tct_farfield_tris_dense": ([c_i, c_i, c_p, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_dp,
+                                 c_p], c_i),
+    "tct_fp32_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
+    "tct_bsr9_matvec": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_i, c_p], c_i),
+    "tct_find_near_pairs": ([c_dp, c_dp, c_i64, c_dp, c_dp, c_i64, ctypes.c_double, c_i,
+                             ctypes.POINTER(c_p)], c_i),
+    "tct_pairs_count": ([c_p], c_i64),
+    "tct_pairs_copy": ([c_p, c_i64p], c_i),
+    "tct_pairs_free": ([c_p], None),
+    "tct_split_adjacent_close": ([c_i64p, c_i64, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p,
+                                  c_i64p, c_i64p], c_i),
+    "tct_resolve_ea_rotation": ([c_i64p, c_i64p, c_i64, c_i64p], c_i),
+    "tct_make_bsr_index": ([c_i64, c_i64, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p], c_i),
+}
+
+for _name, (_args, _res) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+
+EXPORTED = sorted(_SIGS)
+
+
+def last_error():
+    msg = lib.tct_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status, what):
+    if status != TCT_OK:
+        raise RuntimeError("%s failed (%s): %s" % (what, _STATUS.get(status, status), last_error()))
+
+
+def prec_of(float_type):
+    dt = np.dtype(float_type)
+    if dt == np.float32:
+        return TCT_F32
+    if dt == np.float64:
+        return TCT_F64
+    raise ValueError("float_type must be float32 or float64, got %s" % dt)
+
+
+def kernel_id(name):
+    k = lib.tct_kernel_id(name.encode())
+    if k < 0:
+        raise ValueError("unknown kernel %r (supported: elasticU3, elasticT3, elasticA3, "
+                         "elasticH3, elasticRT3, elasticRA3, elasticRH3)" % name)
+    return k
+
+
+def dptr(a):
+    """ctypes double* of a C-contiguous float64 numpy array."""
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(c_dp)
+
+
+def i64ptr(a):
+    assert a.dtype == np.int64 and a.flags.c_contiguous
+    return a.ctypes.data_as(c_i64p)
+
+
+def tptr(t):
+    """Raw device pointer of a torch tensor (None for an empty/None tensor)."""
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)

@@ -1,6 +1,8 @@
 """Build libtct_b200.so in-tree for sm_100a.
 
-    python -m tectosaur_b200.build [-j N] [--force]
+    python tectosaur_b200/build.py [-j N] [--force]
+
+(run as a script: importing the package loads the library this builds)
 
 Each CUDA source compiles to its own object in parallel (nvcc
 -gencode arch=compute_100a,code=sm_100a -lineinfo -O3), the host C++ source
@@ -35,7 +37,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
              "-I" + INCLUDE, "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["pairs.cu", "farfield.cu", "bsr.cu"]
+CU_SOURCES = ["pairs.cu", "farfield.cu", "bsr.cu", "probe.cu"]
 CXX_SOURCES = ["host.cpp"]
 HEADERS = ["common.cuh", "pair_math.cuh"]
 

@@ -58,20 +58,177 @@ inline double dist2(const double* a, const double* b) {
     return out;
 }
 
-struct Grid {
-    double origin[3];
-    double h;
-    int64_t n[3];
-    std::vector<int64_t> cell_start;  // size n0*n1*n2 + 1
-    std::vector<int64_t> order;       // src indices sorted by cell
-
-    int64_t cell_coord(double v, int d) const {
-        double t = std::floor((v - origin[d]) / h);
-        if (t < 0) return 0;
-        if (t > (double)(n[d] - 1)) return n[d] - 1;
-        return (int64_t)t;
-    }
+// ---- ball octree (the reference's fmm/octree.cpp + fmm/tree_helpers.hpp) ----
+// Balls = triangle bounding spheres.  A node's bounds are the centre of mass
+// of its ball centres and the radius max(|c - com| + R); a node with more
+// than `leaf` balls splits into 8 octants by comparing each centre with the
+// node centre (x bit 2, y bit 1, z bit 0, "greater than" = 1), stably; an
+// empty child gets (parent centre, parent R / 50), a single-ball child the
+// ball itself.  Nodes are stored in depth-first preorder.
+struct Node {
+    int64_t start, end;
+    double c[3];
+    double R;
+    bool leaf;
+    int depth;
+    int64_t child[8];
 };
+
+struct Octree {
+    std::vector<double> centers;   // tree order, 3 per ball
+    std::vector<double> radii;     // tree order
+    std::vector<int64_t> orig;     // tree position -> original index
+    std::vector<Node> nodes;
+};
+
+inline double dist(const double* a, const double* b) { return std::sqrt(dist2(a, b)); }
+
+void com_bounds(const Octree& t, int64_t s, int64_t e, double* c, double* R) {
+    double com[3] = {0, 0, 0};
+    for (int64_t i = s; i < e; i++)
+        for (int d = 0; d < 3; d++) com[d] += t.centers[3 * i + d];
+    for (int d = 0; d < 3; d++) com[d] /= (double)(e - s);
+    double max_r = 0.0;
+    for (int64_t i = s; i < e; i++) max_r = std::max(max_r, dist(&t.centers[3 * i], com) + t.radii[i]);
+    for (int d = 0; d < 3; d++) c[d] = com[d];
+    *R = max_r;
+}
+
+int64_t add_node(Octree& t, int64_t s, int64_t e, int64_t leaf, int depth, const double* c,
+                 double R, std::vector<int64_t>& scratch) {
+    const int64_t idx = (int64_t)t.nodes.size();
+    Node n;
+    n.start = s;
+    n.end = e;
+    for (int d = 0; d < 3; d++) n.c[d] = c[d];
+    n.R = R;
+    // depth cap: more than `leaf` balls at one identical centre would never split
+    n.leaf = (e - s <= leaf) || depth >= 60;
+    n.depth = depth;
+    for (int k = 0; k < 8; k++) n.child[k] = -1;
+    t.nodes.push_back(n);
+    if (n.leaf) return idx;
+    // stable partition into octants
+    int64_t counts[9] = {0};
+    std::vector<int> oct(e - s);
+    for (int64_t i = s; i < e; i++) {
+        int o = 0;
+        for (int d = 0; d < 3; d++) {
+            if (t.centers[3 * i + d] > c[d]) o++;
+            if (d < 2) o <<= 1;
+        }
+        oct[i - s] = o;
+        counts[o + 1]++;
+    }
+    for (int k = 0; k < 8; k++) counts[k + 1] += counts[k];
+    {
+        std::vector<int64_t> fill(counts, counts + 8);
+        scratch.resize(e - s);
+        for (int64_t i = s; i < e; i++) scratch[fill[oct[i - s]]++] = i;
+        std::vector<double> cc(3 * (e - s)), rr(e - s);
+        std::vector<int64_t> oo(e - s);
+        for (int64_t k = 0; k < e - s; k++) {
+            const int64_t i = scratch[k];
+            for (int d = 0; d < 3; d++) cc[3 * k + d] = t.centers[3 * i + d];
+            rr[k] = t.radii[i];
+            oo[k] = t.orig[i];
+        }
+        std::copy(cc.begin(), cc.end(), t.centers.begin() + 3 * s);
+        std::copy(rr.begin(), rr.end(), t.radii.begin() + s);
+        std::copy(oo.begin(), oo.end(), t.orig.begin() + s);
+    }
+    for (int k = 0; k < 8; k++) {
+        const int64_t cs = s + counts[k], ce = s + counts[k + 1];
+        double cc[3], cr;
+        if (ce - cs == 0) {
+            for (int d = 0; d < 3; d++) cc[d] = c[d];
+            cr = R / 50.0;
+        } else if (ce - cs == 1) {
+            for (int d = 0; d < 3; d++) cc[d] = t.centers[3 * cs + d];
+            cr = t.radii[cs];
+        } else {
+            com_bounds(t, cs, ce, cc, &cr);
+        }
+        const int64_t ch = add_node(t, cs, ce, leaf, depth + 1, cc, cr, scratch);
+        t.nodes[idx].child[k] = ch;
+    }
+    return idx;
+}
+
+Octree build_octree(const double* centers, const double* radii, int64_t n, int64_t leaf) {
+    Octree t;
+    t.centers.assign(centers, centers + 3 * n);
+    t.radii.assign(radii, radii + n);
+    t.orig.resize(n);
+    for (int64_t i = 0; i < n; i++) t.orig[i] = i;
+    double c[3] = {0, 0, 0}, R = 1.0;
+    if (n == 1) {
+        for (int d = 0; d < 3; d++) c[d] = centers[d];
+        R = radii[0];
+    } else if (n > 1) {
+        com_bounds(t, 0, n, c, &R);
+    }
+    std::vector<int64_t> scratch;
+    add_node(t, 0, n, leaf, 0, c, R, scratch);
+    return t;
+}
+
+// Node radius enlarged to cover every member ball (fast_find_nearfield.cpp:77-94).
+std::vector<double> expanded_r(const Octree& t, const double* orig_radii) {
+    std::vector<double> out(t.nodes.size());
+    for (size_t k = 0; k < t.nodes.size(); k++) {
+        const Node& n = t.nodes[k];
+        double m = n.R;
+        for (int64_t j = n.start; j < n.end; j++) {
+            double md = dist(&t.centers[3 * j], n.c) + orig_radii[t.orig[j]];
+            if (md > m) m = md;
+        }
+        out[k] = m;
+    }
+    return out;
+}
+
+struct Query {
+    const Octree& ot;
+    const Octree& st;
+    const std::vector<double>& oer;
+    const std::vector<double>& ser;
+    const double* orad;  // original-order radii, indexed by TREE position (see below)
+    const double* srad;
+    double thr;
+};
+
+// Dual-tree ball query (fast_find_nearfield.cpp:22-74).  The leaf test reads
+// the radius arrays at the balls' tree positions i, j -- not at their
+// original indices -- exactly as the reference does; with near-uniform
+// triangle sizes this only moves pairs within rounding of the threshold, but
+// it is the reference's pair set, so it is kept.
+void query(const Query& q, int64_t on, int64_t sn, std::vector<int64_t>& out) {
+    const Node& o = q.ot.nodes[on];
+    const Node& s = q.st.nodes[sn];
+    const double r1 = q.oer[on], r2 = q.ser[sn];
+    const double limit = std::pow((r1 + r2) * q.thr, 2);
+    if (dist2(o.c, s.c) > limit) return;
+    if (o.leaf && s.leaf) {
+        for (int64_t i = o.start; i < o.end; i++) {
+            const int64_t oi = q.ot.orig[i];
+            for (int64_t j = s.start; j < s.end; j++) {
+                const double sep = q.orad[i] + q.srad[j];
+                const double pt_limit = std::pow(sep * q.thr, 2);
+                if (dist2(&q.ot.centers[3 * i], &q.st.centers[3 * j]) > pt_limit) continue;
+                out.push_back(oi);
+                out.push_back(q.st.orig[j]);
+            }
+        }
+        return;
+    }
+    const bool split_src = ((r1 < r2) && !s.leaf) || o.leaf;
+    if (split_src) {
+        for (int k = 0; k < 8; k++) query(q, on, s.child[k], out);
+    } else {
+        for (int k = 0; k < 8; k++) query(q, o.child[k], sn, out);
+    }
+}
 
 }  // namespace
 
@@ -90,14 +247,10 @@ int tct_kernel_id(const char* name) {
     return -1;
 }
 
-// Ball query of every obs ball against every src ball:
-// pair (i, j) iff |c_i - c_j|^2 <= ((r_i + r_j) * threshold)^2 (the leaf test
-// of mesh/fast_find_nearfield.cpp:72-84).  A uniform grid of cell width
-// >= 2 * threshold * max(r_src) (grown if the grid would be huge) bins the
-// src centres; each obs ball visits the cells within (r_i + max r_src) *
-// threshold of its centre, widened by a relative 1e-9, so every qualifying
-// pair is tested with the exact double-precision predicate.  Output order:
-// by obs index, then src index.
+// Near pairs (fast_find_nearfield.cpp:96-141, get_nearfield :255-285): octrees
+// with 50 balls per leaf on both sides, then one dual-tree query per obs node
+// at depth 2 (or shallower leaf), run in parallel.  The pair set is the
+// reference's; the output is ordered by (obs, src) with a counting sort.
 int tct_find_near_pairs(const double* obs_c, const double* obs_r, int64_t n_obs,
                         const double* src_c, const double* src_r, int64_t n_src,
                         double threshold, int n_threads, tct_pair_list** out) {
@@ -122,89 +275,45 @@ int tct_find_near_pairs(const double* obs_c, const double* obs_r, int64_t n_obs,
         return TCT_ERR_ARG;
     }
     if (n_threads <= 0) n_threads = omp_get_max_threads();
-
-    double lo[3], hi[3], rmax = 0;
-    for (int d = 0; d < 3; d++) {
-        lo[d] = src_c[d];
-        hi[d] = src_c[d];
+    const int64_t leaf = 50;
+    Octree ot = build_octree(obs_c, obs_r, n_obs, leaf);
+    Octree st = build_octree(src_c, src_r, n_src, leaf);
+    std::vector<double> oer = expanded_r(ot, obs_r);
+    std::vector<double> ser = expanded_r(st, src_r);
+    Query q{ot, st, oer, ser, obs_r, src_r, threshold};
+    std::vector<int64_t> starts;
+    for (size_t k = 0; k < ot.nodes.size(); k++) {
+        const Node& n = ot.nodes[k];
+        if (n.depth > 2) continue;
+        if (n.depth != 2 && !n.leaf) continue;
+        starts.push_back((int64_t)k);
     }
-    for (int64_t j = 0; j < n_src; j++) {
-        for (int d = 0; d < 3; d++) {
-            lo[d] = std::min(lo[d], src_c[3 * j + d]);
-            hi[d] = std::max(hi[d], src_c[3 * j + d]);
-        }
-        rmax = std::max(rmax, src_r[j]);
-    }
-    Grid g;
-    double extent = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
-    g.h = std::max(2.0 * threshold * rmax, extent * 1e-6);
-    if (!(g.h > 0)) g.h = 1.0;
-    for (;;) {
-        int64_t cells = 1;
-        for (int d = 0; d < 3; d++) {
-            g.n[d] = (int64_t)std::floor((hi[d] - lo[d]) / g.h) + 1;
-            cells *= g.n[d];
-        }
-        if (cells <= 4 * n_src + 4096) break;
-        g.h *= 1.5;
-    }
-    for (int d = 0; d < 3; d++) g.origin[d] = lo[d];
-    const int64_t n_cells = g.n[0] * g.n[1] * g.n[2];
-    std::vector<int64_t> cell_of(n_src);
-    g.cell_start.assign(n_cells + 1, 0);
-    for (int64_t j = 0; j < n_src; j++) {
-        int64_t cx = g.cell_coord(src_c[3 * j], 0), cy = g.cell_coord(src_c[3 * j + 1], 1),
-                cz = g.cell_coord(src_c[3 * j + 2], 2);
-        cell_of[j] = (cz * g.n[1] + cy) * g.n[0] + cx;
-        g.cell_start[cell_of[j] + 1]++;
-    }
-    for (int64_t c = 0; c < n_cells; c++) g.cell_start[c + 1] += g.cell_start[c];
-    g.order.resize(n_src);
-    {
-        std::vector<int64_t> fill(g.cell_start.begin(), g.cell_start.end() - 1);
-        for (int64_t j = 0; j < n_src; j++) g.order[fill[cell_of[j]]++] = j;
-    }
-
-    const int64_t chunk = 256;
-    const int64_t n_chunks = (n_obs + chunk - 1) / chunk;
-    std::vector<std::vector<int64_t>> parts(n_chunks);
+    std::vector<std::vector<int64_t>> parts(starts.size());
 #pragma omp parallel for num_threads(n_threads) schedule(dynamic, 1)
-    for (int64_t ch = 0; ch < n_chunks; ch++) {
-        std::vector<int64_t>& part = parts[ch];
-        std::vector<int64_t> hits;
-        const int64_t i_end = std::min(n_obs, (ch + 1) * chunk);
-        for (int64_t i = ch * chunk; i < i_end; i++) {
-            const double* ci = obs_c + 3 * i;
-            const double reach = (obs_r[i] + rmax) * threshold * (1.0 + 1e-9) + 1e-300;
-            int64_t c0[3], c1[3];
-            for (int d = 0; d < 3; d++) {
-                c0[d] = g.cell_coord(ci[d] - reach, d);
-                c1[d] = g.cell_coord(ci[d] + reach, d);
-            }
-            hits.clear();
-            for (int64_t cz = c0[2]; cz <= c1[2]; cz++)
-                for (int64_t cy = c0[1]; cy <= c1[1]; cy++)
-                    for (int64_t cx = c0[0]; cx <= c1[0]; cx++) {
-                        const int64_t cell = (cz * g.n[1] + cy) * g.n[0] + cx;
-                        for (int64_t k = g.cell_start[cell]; k < g.cell_start[cell + 1]; k++) {
-                            const int64_t j = g.order[k];
-                            const double sep = obs_r[i] + src_r[j];
-                            const double lim = std::pow(sep * threshold, 2);
-                            if (dist2(ci, src_c + 3 * j) > lim) continue;
-                            hits.push_back(j);
-                        }
-                    }
-            std::sort(hits.begin(), hits.end());
-            for (int64_t j : hits) {
-                part.push_back(i);
-                part.push_back(j);
-            }
+    for (int64_t k = 0; k < (int64_t)starts.size(); k++) query(q, starts[k], 0, parts[k]);
+    // counting sort by obs index, then sort each obs's sources
+    std::vector<int64_t> offs(n_obs + 1, 0);
+    int64_t total = 0;
+    for (auto& p : parts) {
+        for (size_t m = 0; m < p.size(); m += 2) offs[p[m] + 1]++;
+        total += (int64_t)p.size() / 2;
+    }
+    for (int64_t i = 0; i < n_obs; i++) offs[i + 1] += offs[i];
+    std::vector<int64_t> src_sorted(total);
+    {
+        std::vector<int64_t> fill(offs.begin(), offs.end() - 1);
+        for (auto& p : parts)
+            for (size_t m = 0; m < p.size(); m += 2) src_sorted[fill[p[m]]++] = p[m + 1];
+    }
+    list->pairs.resize(2 * total);
+#pragma omp parallel for num_threads(n_threads) schedule(dynamic, 256)
+    for (int64_t i = 0; i < n_obs; i++) {
+        std::sort(src_sorted.begin() + offs[i], src_sorted.begin() + offs[i + 1]);
+        for (int64_t k = offs[i]; k < offs[i + 1]; k++) {
+            list->pairs[2 * k] = i;
+            list->pairs[2 * k + 1] = src_sorted[k];
         }
     }
-    size_t total = 0;
-    for (auto& p : parts) total += p.size();
-    list->pairs.reserve(total);
-    for (auto& p : parts) list->pairs.insert(list->pairs.end(), p.begin(), p.end());
     *out = list;
     return TCT_OK;
 }

@@ -1,0 +1,63 @@
+"""Near-pair search and adjacency split (reference: tectosaur/mesh/find_near_adj.py
+and mesh/fast_find_nearfield.cpp), on the C++ side of libtct_b200.so."""
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+
+
+def get_tri_centroids_rs(pts, tris):
+    """Centroid and bounding radius (max centroid-vertex distance) of each
+    triangle, with the reference's NumPy reductions (find_near_adj.py:13-20),
+    so the radii -- and hence the near-pair set -- match bit for bit."""
+    tri_pts = pts[tris]
+    centroid = np.sum(tri_pts, axis=1) / 3.0
+    r = np.sqrt(np.max(np.sum((tri_pts - centroid[:, np.newaxis, :]) ** 2, axis=2), axis=1))
+    return centroid, r
+
+
+def get_nearfield(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads=0):
+    """All (i, j) with |c_i - c_j|^2 <= ((r_i + r_j) threshold)^2, int64 (P, 2),
+    lexicographically ordered."""
+    oc = np.ascontiguousarray(obs_centers, dtype=np.float64).reshape(-1, 3)
+    orr = np.ascontiguousarray(obs_radii, dtype=np.float64).reshape(-1)
+    sc = np.ascontiguousarray(src_centers, dtype=np.float64).reshape(-1, 3)
+    sr = np.ascontiguousarray(src_radii, dtype=np.float64).reshape(-1)
+    handle = ctypes.c_void_p()
+    _lib.check(_lib.lib.tct_find_near_pairs(
+        _lib.dptr(oc), _lib.dptr(orr), oc.shape[0], _lib.dptr(sc), _lib.dptr(sr), sc.shape[0],
+        float(threshold), int(n_threads), ctypes.byref(handle)), "tct_find_near_pairs")
+    try:
+        n = _lib.lib.tct_pairs_count(handle)
+        out = np.empty((n, 2), dtype=np.int64)
+        _lib.check(_lib.lib.tct_pairs_copy(handle, _lib.i64ptr(out)), "tct_pairs_copy")
+    finally:
+        _lib.lib.tct_pairs_free(handle)
+    return out
+
+
+def find_close_or_touching(a_pts, a_tris, b_pts, b_tris, threshold):
+    """Pairs (i in a, j in b) whose bounding balls, scaled by `threshold`,
+    touch (find_near_adj.py:29-35)."""
+    ca, ra = get_tri_centroids_rs(a_pts, a_tris)
+    cb, rb = get_tri_centroids_rs(b_pts, b_tris)
+    return get_nearfield(ca, ra, cb, rb, threshold)
+
+
+def split_adjacent_close(close_pairs, tris_a, tris_b):
+    """(near (n,2), vertex-adjacent (n,4), edge-adjacent (n,6)) by shared-vertex
+    count; coincident pairs are dropped (fast_find_nearfield.cpp:143-182)."""
+    cp = np.ascontiguousarray(close_pairs, dtype=np.int64).reshape(-1, 2)
+    ta = np.ascontiguousarray(tris_a, dtype=np.int64).reshape(-1, 3)
+    tb = np.ascontiguousarray(tris_b, dtype=np.int64).reshape(-1, 3)
+    n = cp.shape[0]
+    near = np.empty((max(n, 1), 2), dtype=np.int64)
+    va = np.empty((max(n, 1), 4), dtype=np.int64)
+    ea = np.empty((max(n, 1), 6), dtype=np.int64)
+    nn, nv, ne = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    _lib.check(_lib.lib.tct_split_adjacent_close(
+        _lib.i64ptr(cp), n, _lib.i64ptr(ta), _lib.i64ptr(tb), _lib.i64ptr(near), ctypes.byref(nn),
+        _lib.i64ptr(va), ctypes.byref(nv), _lib.i64ptr(ea), ctypes.byref(ne)),
+        "tct_split_adjacent_close")
+    return near[:nn.value].copy(), va[:nv.value].copy(), ea[:ne.value].copy()

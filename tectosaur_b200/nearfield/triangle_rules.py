@@ -21,7 +21,7 @@ import functools
 
 import numpy as np
 
-from . import quadrature as quad
+from ..util import quadrature as quad
 
 
 def _spow(x, k):

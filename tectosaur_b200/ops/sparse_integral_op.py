@@ -1,0 +1,81 @@
+"""The elastic BEM operator: corrected nearfield + farfield on all pairs
+(reference: tectosaur/ops/sparse_integral_op.py:10-62).
+
+``dot(v)`` = farfield(v) + nearfield(v).  On the device both terms write into
+one output buffer on one stream (farfield overwrites, the BSR nearfield
+accumulates), so a host-array apply costs one copy in and one copy out, and
+``capture_graph`` records the whole apply as a CUDA graph for repeated use.
+"""
+import numpy as np
+
+from ..nearfield.nearfield_op import RegularizedNearfieldIntegralOp
+from ..util import device
+
+
+class RegularizedSparseIntegralOp:
+    def __init__(self, nq_coincident, nq_edge_adj, nq_vert_adjacent,
+                 nq_far, nq_near, near_threshold,
+                 K_near_name, K_far_name, params, pts, tris, float_type, farfield_op_type,
+                 obs_subset=None, src_subset=None, keep_uncorrected=True):
+        tris = np.asarray(tris)
+        if obs_subset is None:
+            obs_subset = np.arange(tris.shape[0])
+        if src_subset is None:
+            src_subset = np.arange(tris.shape[0])
+        self.float_type = np.dtype(float_type)
+        self.nearfield = RegularizedNearfieldIntegralOp(
+            pts, tris, obs_subset, src_subset,
+            nq_coincident, nq_edge_adj, nq_vert_adjacent, nq_far, nq_near,
+            near_threshold, K_near_name, K_far_name, params, float_type,
+            keep_uncorrected=keep_uncorrected)
+        self.farfield = farfield_op_type(
+            nq_far, K_far_name, params, pts, tris, float_type, obs_subset, src_subset)
+        self.shape = self.nearfield.shape
+        self._graph = None
+
+    # -- device apply -------------------------------------------------------
+    def dot_device(self, x, y, stream=None):
+        """y = (Far + Near) x on device tensors of float_type."""
+        if hasattr(self.farfield, "dot_device"):
+            self.farfield.dot_device(x, y, accumulate=False, stream=stream)
+        else:
+            y.copy_(device.torch().as_tensor(self.farfield.dot(x.cpu().numpy()), device="cuda"))
+        self.nearfield.dot_device(x, y, accumulate=True, stream=stream)
+        return y
+
+    def capture_graph(self):
+        """Record one full apply (farfield + nearfield) as a CUDA graph on
+        private input/output buffers; returns (graph, x, y): fill x, call
+        graph.replay(), read y."""
+        t = device.torch()
+        x = device.zeros(self.shape[1], self.float_type)
+        y = device.zeros(self.shape[0], self.float_type)
+        s = t.cuda.Stream()
+        s.wait_stream(t.cuda.current_stream())
+        with t.cuda.stream(s):
+            self.dot_device(x, y)  # warm-up outside the capture
+        t.cuda.current_stream().wait_stream(s)
+        g = t.cuda.CUDAGraph()
+        with t.cuda.graph(g):
+            self.dot_device(x, y)
+        self._graph = (g, x, y)
+        return self._graph
+
+    def dot(self, v):
+        if device.is_device_tensor(v):
+            x = v.to(device.torch_dtype(self.float_type)).contiguous()
+            y = device.empty(self.shape[0], self.float_type)
+            return self.dot_device(x, y)
+        x = device.to_dev(np.asarray(v).reshape(-1), self.float_type)
+        y = device.empty(self.shape[0], self.float_type)
+        self.dot_device(x, y)
+        return y.cpu().numpy()
+
+    async def nearfield_dot(self, v):
+        return self.nearfield.dot(v)
+
+    def nearfield_no_correction_dot(self, v):
+        return self.nearfield.nearfield_no_correction_dot(v)
+
+    async def farfield_dot(self, v):
+        return await self.farfield.async_dot(v)

@@ -1,0 +1,154 @@
+"""Block-sparse matrices of 9x9 blocks.
+
+``DeviceBSR9`` is the device-resident nearfield matrix the operator apply
+uses: block-row pointers and block-column indices (int32) plus the blocks in
+structure-of-arrays order (element e = i*9 + j of block s at
+data[e * nnzb + s]), applied by tct_bsr9_matvec (one warp per block row, no
+atomics).
+
+``BCOOMatrix`` / ``BSRMatrix`` mirror the reference's host classes
+(tectosaur/util/sparse.py:14-70) for callers that read ``op.mat`` directly:
+same attributes and ``dot``, ``to_bsr``, ``to_scipy``, ``to_dense``.  Their
+``dot`` runs on the device through the same BSR kernel.
+"""
+import ctypes
+
+import numpy as np
+import scipy.sparse
+
+from .. import _lib
+from . import device
+
+
+def make_bsr_index(n_row_blocks, rows, cols):
+    """(indptr, indices, slot) of the reference's make_bsr_matrix
+    (util/fast_sparse.cpp:14-68): stable counting sort by block row,
+    duplicates kept; slot[i] = BSR position of input block i."""
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int64)
+    n = rows.shape[0]
+    indptr = np.empty(n_row_blocks + 1, dtype=np.int64)
+    indices = np.empty(max(n, 1), dtype=np.int64)
+    slot = np.empty(max(n, 1), dtype=np.int64)
+    _lib.check(_lib.lib.tct_make_bsr_index(n_row_blocks, n, _lib.i64ptr(rows), _lib.i64ptr(cols),
+                                           _lib.i64ptr(indptr), _lib.i64ptr(indices),
+                                           _lib.i64ptr(slot)), "tct_make_bsr_index")
+    return indptr, indices[:n].copy(), slot[:n].copy()
+
+
+class DeviceBSR9:
+    """Device 9x9-block BSR matrix, SoA block storage (see module docstring)."""
+
+    def __init__(self, shape, indptr, indices, float_type, data=None):
+        self.shape = tuple(shape)
+        self.float_type = np.dtype(float_type)
+        self.n_row_blocks = self.shape[0] // 9
+        self.nnzb = int(indices.shape[0])
+        self.indptr_host = np.asarray(indptr, dtype=np.int64)
+        self.indices_host = np.asarray(indices, dtype=np.int64)
+        if self.nnzb >= 2 ** 31:
+            raise ValueError("more than 2^31 nearfield blocks")
+        self.indptr = device.to_dev(self.indptr_host.astype(np.int32))
+        self.indices = device.to_dev(np.maximum(self.indices_host, 0).astype(np.int32)) \
+            if self.nnzb > 0 else device.to_dev(np.zeros(1, dtype=np.int32))
+        self.data = data if data is not None else device.zeros(max(81 * self.nnzb, 1),
+                                                                self.float_type)
+
+    @property
+    def nbytes(self):
+        return int(self.data.numel() * self.data.element_size() + 4 * (self.nnzb + self.n_row_blocks + 1))
+
+    def matvec(self, x, y, accumulate=False, extra=None, stream=None):
+        """y (+)= A x on device tensors (A + extra when `extra` is another
+        block array with the same structure)."""
+        _lib.check(_lib.lib.tct_bsr9_matvec(
+            _lib.prec_of(self.float_type), self.n_row_blocks, _lib.tptr(self.indptr),
+            _lib.tptr(self.indices), _lib.tptr(self.data),
+            _lib.tptr(extra) if extra is not None else None, max(self.nnzb, 1),
+            _lib.tptr(x), _lib.tptr(y), int(bool(accumulate)), _lib.stream_ptr(stream)),
+            "tct_bsr9_matvec")
+        return y
+
+    def blocks_host(self, data=None):
+        """(nnzb, 9, 9) host array of the blocks in BSR order."""
+        d = (self.data if data is None else data)[:81 * self.nnzb]
+        return d.reshape(81, self.nnzb).t().reshape(self.nnzb, 9, 9).cpu().numpy()
+
+    def rows_host(self):
+        return np.repeat(np.arange(self.n_row_blocks, dtype=np.int64), np.diff(self.indptr_host))
+
+
+class BCOOMatrix:
+    """Block-COO matrix (util/sparse.py:14-42); ``dot`` runs on the device."""
+
+    def __init__(self, rows, cols, data, shape):
+        self.rows = rows
+        self.cols = cols
+        self.data = data
+        self.shape = shape
+
+    @property
+    def dtype(self):
+        return self.data.dtype
+
+    @property
+    def blocksize(self):
+        return self.data.shape[1]
+
+    def dot(self, v):
+        return self.to_bsr().dot(v)
+
+    def to_bsr(self):
+        n_row_blocks = self.shape[0] // self.blocksize
+        indptr, indices, slot = make_bsr_index(n_row_blocks, self.rows, self.cols)
+        data = np.empty_like(self.data)
+        data[slot] = self.data
+        return BSRMatrix(indptr, indices, data, self.shape)
+
+    def to_dense(self):
+        return self.to_bsr().to_scipy().todense()
+
+
+class BSRMatrix:
+    """Block-CSR matrix (util/sparse.py:44-70); ``dot`` runs on the device for
+    9x9 blocks.  The reference allocates the output with shape[1] (only right
+    for square matrices, util/sparse.py:61); this one uses shape[0]."""
+
+    def __init__(self, indptr, indices, data, shape):
+        assert data.shape[1] == data.shape[2]
+        self.indptr = indptr
+        self.indices = indices
+        self.data = data
+        self.shape = shape
+
+    @property
+    def dtype(self):
+        return self.data.dtype
+
+    @property
+    def blocksize(self):
+        return self.data.shape[1]
+
+    def dot(self, v):
+        if self.blocksize != 9:
+            return self.to_scipy().dot(v).astype(self.dtype)
+        ft = self.dtype
+        nnzb = self.data.shape[0]
+        m = DeviceBSR9(self.shape, self.indptr, self.indices, ft)
+        if nnzb:
+            soa = np.ascontiguousarray(self.data.reshape(nnzb, 81).T, dtype=ft)
+            m.data = device.to_dev(soa.reshape(-1))
+        x = device.to_dev(np.asarray(v), ft)
+        y = device.empty(self.shape[0], ft)
+        m.matvec(x, y)
+        return y.cpu().numpy()
+
+    def to_scipy(self):
+        return scipy.sparse.bsr_matrix((self.data, self.indices, self.indptr), self.shape)
+
+    def to_dense(self):
+        return self.to_scipy().todense()
+
+
+def from_scipy_bsr(A):
+    return BSRMatrix(A.indptr, A.indices, A.data, A.shape)

@@ -1,0 +1,73 @@
+"""The C-ABI library loads and exports every entry point include/tct_b200.h
+declares (no device calls)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(REPO, "include", "tct_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tct_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_header():
+    lib = ctypes.CDLL(os.path.join(REPO, "tectosaur_b200", "libtct_b200.so"))
+    names = declared_symbols()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_binding_covers_header():
+    from tectosaur_b200 import _lib
+    assert set(declared_symbols()) <= set(_lib.EXPORTED)
+
+
+def test_kernel_ids_and_errors():
+    from tectosaur_b200 import _lib
+    assert _lib.kernel_id("elasticRH3") == 6
+    assert _lib.lib.tct_kernel_id(b"nope") == -1
+    # host-only entry point reports a bad argument with a message
+    rc = _lib.lib.tct_make_bsr_index(2, 1, _lib.i64ptr(np.array([5], np.int64)),
+                                     _lib.i64ptr(np.array([0], np.int64)),
+                                     _lib.i64ptr(np.zeros(3, np.int64)),
+                                     _lib.i64ptr(np.zeros(1, np.int64)),
+                                     _lib.i64ptr(np.zeros(1, np.int64)))
+    assert rc == _lib.TCT_ERR_ARG and "out of range" in _lib.last_error()
+    assert _lib.lib.tct_farfield_workspace_bytes(6, 0, 100, 100, 5) == 0
+    assert _lib.lib.tct_farfield_workspace_bytes(6, 0, 100, 100, 3) > 0
+
+
+def test_make_bsr_index_matches_oracle(orc):
+    from tectosaur_b200.util.sparse import make_bsr_index
+    rng = np.random.default_rng(1)
+    rows = rng.integers(0, 40, 500)
+    cols = rng.integers(0, 40, 500)
+    data = rng.standard_normal((500, 9, 9))
+    indptr, indices, slot = make_bsr_index(40, rows, cols)
+    i2, j2, d2 = orc.make_bsr(40, rows, cols, data)
+    assert np.array_equal(indptr, i2) and np.array_equal(indices, j2)
+    out = np.empty_like(data)
+    out[slot] = data
+    assert np.array_equal(out, d2)
+
+
+def test_mass_op_matches_reference(golden):
+    from tectosaur_b200.ops.mass_op import MassOp
+    g = golden("mass_op.npz")
+    for nq in [2, 3]:
+        for td in [1, 3]:
+            m = MassOp(nq, g["pts"], g["tris"], tensor_dim=td).mat.toarray()
+            np.testing.assert_allclose(m, g["mat_%d_%d" % (nq, td)], rtol=1e-14, atol=1e-16)
+
+
+def test_make_rect_matches_reference_order():
+    from tectosaur_b200.mesh.mesh_gen import make_rect
+    pts, tris = make_rect(3, 3, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
+    assert tris.shape == (8, 3)
+    assert np.array_equal(tris[:4], [[0, 3, 1], [3, 4, 1], [3, 6, 4], [6, 7, 4]])
