@@ -139,6 +139,9 @@ int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
  * fused multiply-adds (16 * iters flops per thread); out: >= 256 floats of
  * device scratch.  Timed by the caller; the FP32 roofline denominator. */
 int tct_fp32_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
+/* Same with packed fma.rn.f32x2 (2 FMAs per instruction, 32 * iters flops per
+ * thread). */
+int tct_fp32x2_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Host-side (CPU) structure builders.                                       */

@@ -15,8 +15,12 @@
 namespace tct {
 namespace {
 
+// At most 64 registers per thread (4 blocks of 256 threads per SM): left
+// unconstrained the compiler hoists all 81 block loads into registers (222
+// registers, 1 block per SM) and the per-row shuffle reduction then leaves
+// the SM with no loads in flight.
 template <typename R, bool TWO>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             const int32_t* __restrict__ indices, const R* __restrict__ data,
             const R* __restrict__ data2, int64_t stride, const R* __restrict__ x,

@@ -154,4 +154,18 @@ __device__ __forceinline__ void load_tri(TriGeom<R>& t, const R* __restrict__ pt
     }
 }
 
+// Point of a triangle at basis values b (pts_from_basis of
+// integral_primitives.cl:121-128: v = 0; v += b0 t0; v += b1 t1; v += b2 t2).
+// Every kernel forms observation and source quadrature points through this one
+// function, so a triangle's own points agree bit for bit wherever they are
+// computed (coincident points then give r^2 == 0 exactly, as in the reference).
+template <typename R>
+__device__ __forceinline__ R bary_point(const TriGeom<R>& t, const R b[3], int d) {
+    R v = 0;
+    v += b[0] * t.v[0][d];
+    v += b[1] * t.v[1][d];
+    v += b[2] * t.v[2][d];
+    return v;
+}
+
 }  // namespace tct

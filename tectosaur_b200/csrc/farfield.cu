@@ -76,13 +76,7 @@ far_prep(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
         const R sx = rule.x[q], sy = rule.y[q];
         const R sb[3] = {1 - sx - sy, sx, sy};
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            R y = 0;
-            y += sb[0] * s.v[0][d];
-            y += sb[1] * s.v[1][d];
-            y += sb[2] * s.v[2][d];
-            r[L::Y + 3 * q + d] = y;
-        }
+        for (int d = 0; d < 3; d++) r[L::Y + 3 * q + d] = bary_point(s, sb, d);
         R sw = s.J * rule.w[q];
         if (K == kRH) sw = sw * c.CsRH0;
         r[L::SW + q] = sw;
@@ -242,13 +236,7 @@ far_main(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
         const R ox = rule.x[q], oy = rule.y[q];
         const R ob[3] = {1 - ox - oy, ox, oy};
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            R v = 0;
-            v += ob[0] * o.v[0][d];
-            v += ob[1] * o.v[1][d];
-            v += ob[2] * o.v[2][d];
-            x[q][d] = v;
-        }
+        for (int d = 0; d < 3; d++) x[q][d] = bary_point(o, ob, d);
     }
     R tot[NA], cmp[NA];
 #pragma unroll
@@ -417,6 +405,252 @@ far_main(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
     }
 }
 
+// ---- packed-FP32 elasticRH3 farfield -----------------------------------------
+// Two observation triangles per thread, one in each half of an f32x2 register
+// pair, so every point-pair operation is one fma/mul/add.rn.f32x2 instruction
+// for both.  Per point pair (both halves): D = y - x, r2e = |D|^2 + EPS,
+// invr = rsqrt(r2e) (two MUFU ops), g = invr^3, T += g D D^T; per triangle
+// pair S0 = trace(T) (= sum of 1/r, since trace(D D^T) / r^3 = 1/r) and
+// W += S0 P + T (-2 ssc).  EPS = 1e-24 keeps invr^3 finite at r2 == 0, where
+// D == 0 makes the point pair contribute exactly nothing -- the reference's
+// "skip r^2 == 0" (matrix_free.cl:79-81) without a per-pair select.  EPS is
+// below the FP32 rounding of any r2 above ~1e-17 (point separations above
+// ~3e-9 in mesh units).  J_s * CsRH0 (and, for equal-weight rules, w^2) are
+// folded into P and -2 ssc by the prep kernel.
+constexpr float RH2_EPS = 1e-24f;
+
+typedef unsigned long long f2_t;
+
+__device__ __forceinline__ f2_t pk(float x, float y) {
+    f2_t d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(x), "f"(y));
+    return d;
+}
+__device__ __forceinline__ void upk(f2_t d, float& x, float& y) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(d));
+}
+__device__ __forceinline__ f2_t add2(f2_t a, f2_t b) {
+    f2_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) {
+    f2_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) {
+    f2_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// Record of one source triangle for the packed kernel, every value stored
+// twice (an f32x2 operand): y[q][d] (3 NQ pairs), P (9), M = -2 ssc (9).
+template <int NQ>
+struct RecRH2 {
+    static constexpr int Y = 0;
+    static constexpr int P = 3 * NQ;
+    static constexpr int M = 3 * NQ + 9;
+    static constexpr int PAIRS = 3 * NQ + 18;
+    static constexpr int LEN = (2 * PAIRS + 3) / 4 * 4;  // floats
+};
+
+template <int NQ, bool UNIFORM>
+__global__ void __launch_bounds__(128)
+far_prep_rh2(Consts<float> c, Rule2D<float> rule, const float* __restrict__ pts,
+             const int32_t* __restrict__ src_tris, int64_t n_src, const float* __restrict__ in,
+             float* __restrict__ rec) {
+    using L = RecRH2<NQ>;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_src) return;
+    TriGeom<float> s;
+    load_tri(s, pts, src_tris, i, 0, false, true);
+    float in9[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) in9[k] = in[i * 9 + k];
+    float* r = rec + i * L::LEN;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const float sx = rule.x[q], sy = rule.y[q];
+        const float sb[3] = {1 - sx - sy, sx, sy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const float y = bary_point(s, sb, d);
+            r[2 * (L::Y + 3 * q + d)] = y;
+            r[2 * (L::Y + 3 * q + d) + 1] = y;
+        }
+    }
+    float ssc[3][3];
+#pragma unroll
+    for (int Ij = 0; Ij < 3; Ij++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            float a = 0;
+#pragma unroll
+            for (int b = 0; b < 3; b++) a += s.sc[b][Ij] * in9[b * 3 + d];
+            ssc[d][Ij] = a;
+        }
+    float scale = s.J * c.CsRH0;
+    if (UNIFORM) scale *= rule.w[0] * rule.w[0];
+    const float B = (ssc[0][0] + ssc[1][1] + ssc[2][2]) * c.CsRH1;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float p = scale * ((d == j ? B : 0.f) + c.CsRH2 * ssc[j][d] - 2 * ssc[d][j]);
+            const float m = scale * (-2.f * ssc[d][j]);
+            r[2 * (L::P + 3 * d + j)] = p;
+            r[2 * (L::P + 3 * d + j) + 1] = p;
+            r[2 * (L::M + 3 * d + j)] = m;
+            r[2 * (L::M + 3 * d + j) + 1] = m;
+        }
+#pragma unroll
+    for (int k = 2 * L::PAIRS; k < L::LEN; k++) r[k] = 0;
+}
+
+template <int NQ, bool UNIFORM>
+__global__ void __launch_bounds__(128)
+far_main_rh2(Consts<float> c, Rule2D<float> rule, const float* __restrict__ pts,
+             const int32_t* __restrict__ obs_tris, int64_t n_obs, const float* __restrict__ rec,
+             int64_t n_src, int64_t src_per_chunk, float* __restrict__ dst, int direct,
+             int accumulate) {
+    using L = RecRH2<NQ>;
+    constexpr int TS = 128;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sm = reinterpret_cast<float*>(smem_raw);
+
+    // obs triangles a and b of this thread (coalesced: a block covers 256)
+    const int64_t ia = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    const int64_t ib = ia + 128;
+    const bool va = ia < n_obs, vb = ib < n_obs;
+    const int64_t s_begin = (int64_t)blockIdx.y * src_per_chunk;
+    const int64_t s_end = min(n_src, s_begin + src_per_chunk);
+
+    TriGeom<float> oa, ob;
+    if (va) load_tri(oa, pts, obs_tris, ia, 0, false, true);
+    if (vb) load_tri(ob, pts, obs_tris, ib, 0, false, true);
+    f2_t negx[NQ][3];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const float ox = rule.x[q], oy = rule.y[q];
+        const float bq[3] = {1 - ox - oy, ox, oy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const float xa = va ? bary_point(oa, bq, d) : 0.f;
+            const float xb = vb ? bary_point(ob, bq, d) : 0.f;
+            negx[q][d] = pk(-xa, -xb);
+        }
+    }
+    f2_t wq[UNIFORM ? 1 : NQ * NQ];
+    if (!UNIFORM) {
+#pragma unroll
+        for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+            for (int q2 = 0; q2 < NQ; q2++) {
+                const float w = rule.w[q1] * rule.w[q2];
+                wq[q1 * NQ + q2] = pk(w, w);
+            }
+    }
+    const f2_t eps = pk(RH2_EPS, RH2_EPS);
+    float tot[2][9], cmp[2][9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        tot[0][k] = tot[1][k] = 0.f;
+        cmp[0][k] = cmp[1][k] = 0.f;
+    }
+
+    for (int64_t t0 = s_begin; t0 < s_end; t0 += TS) {
+        const int n_tile = (int)min((int64_t)TS, s_end - t0);
+        __syncthreads();
+        {
+            const int n_vec = n_tile * L::LEN / 4;
+            const float4* srcv = reinterpret_cast<const float4*>(rec + t0 * L::LEN);
+            float4* dstv = reinterpret_cast<float4*>(sm);
+            for (int k = threadIdx.x; k < n_vec; k += blockDim.x) dstv[k] = __ldg(srcv + k);
+        }
+        __syncthreads();
+        f2_t W[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) W[k] = 0ull;
+#pragma unroll 2
+        for (int j = 0; j < n_tile; j++) {
+            const f2_t* r = reinterpret_cast<const f2_t*>(sm + j * L::LEN);
+            f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
+#pragma unroll
+            for (int q2 = 0; q2 < NQ; q2++) {
+                const f2_t y0 = r[L::Y + 3 * q2 + 0], y1 = r[L::Y + 3 * q2 + 1],
+                           y2 = r[L::Y + 3 * q2 + 2];
+#pragma unroll
+                for (int q1 = 0; q1 < NQ; q1++) {
+                    const f2_t D0 = add2(y0, negx[q1][0]);
+                    const f2_t D1 = add2(y1, negx[q1][1]);
+                    const f2_t D2 = add2(y2, negx[q1][2]);
+                    f2_t r2 = fma2(D0, D0, eps);
+                    r2 = fma2(D1, D1, r2);
+                    r2 = fma2(D2, D2, r2);
+                    float ra, rb;
+                    upk(r2, ra, rb);
+                    const f2_t invr = pk(rsqrtf(ra), rsqrtf(rb));
+                    f2_t g = mul2(mul2(invr, invr), invr);
+                    if (!UNIFORM) g = mul2(g, wq[q1 * NQ + q2]);
+                    const f2_t g0 = mul2(g, D0), g1 = mul2(g, D1), g2 = mul2(g, D2);
+                    T00 = fma2(g0, D0, T00);
+                    T01 = fma2(g0, D1, T01);
+                    T02 = fma2(g0, D2, T02);
+                    T11 = fma2(g1, D1, T11);
+                    T12 = fma2(g1, D2, T12);
+                    T22 = fma2(g2, D2, T22);
+                }
+            }
+            const f2_t S0 = add2(add2(T00, T11), T22);
+            const f2_t T[3][3] = {{T00, T01, T02}, {T01, T11, T12}, {T02, T12, T22}};
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int jj = 0; jj < 3; jj++) {
+                    f2_t w = fma2(S0, r[L::P + 3 * d + jj], W[3 * d + jj]);
+                    w = fma2(T[d][0], r[L::M + 0 * 3 + jj], w);
+                    w = fma2(T[d][1], r[L::M + 1 * 3 + jj], w);
+                    w = fma2(T[d][2], r[L::M + 2 * 3 + jj], w);
+                    W[3 * d + jj] = w;
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            float wa, wb;
+            upk(W[k], wa, wb);
+            fold<float, true>(tot[0][k], cmp[0][k], wa);
+            fold<float, true>(tot[1][k], cmp[1][k], wb);
+        }
+    }
+
+    // out[b][d] = J_o sum_j sc_o[b][j] W[d][j]
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const bool v = h == 0 ? va : vb;
+        if (!v) continue;
+        const TriGeom<float>& o = h == 0 ? oa : ob;
+        const int64_t i = h == 0 ? ia : ib;
+        float out9[9];
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                out9[b * 3 + d] = o.J * (o.sc[b][0] * tot[h][3 * d + 0] + o.sc[b][1] * tot[h][3 * d + 1] +
+                                         o.sc[b][2] * tot[h][3 * d + 2]);
+        if (direct) {
+            float* op = dst + i * 9;
+#pragma unroll
+            for (int k = 0; k < 9; k++) op[k] = accumulate ? op[k] + out9[k] : out9[k];
+        } else {
+            float* op = dst + ((int64_t)blockIdx.y * n_obs + i) * 9;
+#pragma unroll
+            for (int k = 0; k < 9; k++) op[k] = out9[k];
+        }
+    }
+}
+
 template <typename R>
 __global__ void chunk_reduce(const R* __restrict__ partial, int n_chunks, int64_t n,
                              R* __restrict__ out, int accumulate) {
@@ -501,6 +735,86 @@ int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, cons
     return launch_status("farfield chunk reduce");
 }
 
+// Source chunks for the packed RH kernel (256 observation triangles per block).
+int64_t n_chunks_rh2(int64_t n_obs, int64_t n_src) {
+    const int64_t obs_blocks = (n_obs + 255) / 256;
+    int64_t want = (148 * 8 + obs_blocks - 1) / std::max<int64_t>(obs_blocks, 1);
+    int64_t max_by_src = std::max<int64_t>(1, n_src / 128);
+    return std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, max_by_src), 32));
+}
+
+int rec_len_rh2(int nq) {
+    switch (nq) {
+        case 3: return RecRH2<3>::LEN;
+        case 4: return RecRH2<4>::LEN;
+        case 7: return RecRH2<7>::LEN;
+        default: return -1;
+    }
+}
+
+template <int NQ, bool UNIFORM>
+int run_far_rh2(const Consts<float>& c, const Rule2D<float>& rule, float* out, const float* in,
+                const float* pts, const int32_t* obs_tris, int64_t n_obs,
+                const int32_t* src_tris, int64_t n_src, int accumulate, unsigned char* ws,
+                cudaStream_t st) {
+    using L = RecRH2<NQ>;
+    float* rec = reinterpret_cast<float*>(ws);
+    const size_t rec_bytes = align256(sizeof(float) * L::LEN * (size_t)n_src);
+    far_prep_rh2<NQ, UNIFORM><<<(unsigned)((n_src + 127) / 128), 128, 0, st>>>(
+        c, rule, pts, src_tris, n_src, in, rec);
+    int rc = launch_status("farfield prep (RH, packed)");
+    if (rc) return rc;
+    const int64_t chunks = n_chunks_rh2(n_obs, n_src);
+    const int64_t per_chunk = ((n_src + chunks - 1) / chunks + 127) / 128 * 128;
+    const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
+    const size_t smem = sizeof(float) * L::LEN * 128;
+    auto kfn = far_main_rh2<NQ, UNIFORM>;
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    dim3 grid((unsigned)((n_obs + 255) / 256), (unsigned)real_chunks);
+    if (real_chunks == 1) {
+        kfn<<<grid, 128, smem, st>>>(c, rule, pts, obs_tris, n_obs, rec, n_src, per_chunk, out, 1,
+                                      accumulate);
+        return launch_status("farfield main (RH, packed)");
+    }
+    float* partial = reinterpret_cast<float*>(ws + rec_bytes);
+    kfn<<<grid, 128, smem, st>>>(c, rule, pts, obs_tris, n_obs, rec, n_src, per_chunk, partial, 0,
+                                  0);
+    rc = launch_status("farfield main (RH, packed)");
+    if (rc) return rc;
+    const int64_t n = n_obs * 9;
+    chunk_reduce<float><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(partial, (int)real_chunks, n,
+                                                                    out, accumulate);
+    return launch_status("farfield chunk reduce");
+}
+
+int run_far_rh2_nq(int nq, bool uniform, const Consts<float>& c, const Rule2D<float>& rule,
+                   float* out, const float* in, const float* pts, const int32_t* ot,
+                   int64_t n_obs, const int32_t* stris, int64_t n_src, int acc,
+                   unsigned char* ws, cudaStream_t st) {
+#define TCT_RH2(NQV)                                                                          \
+    return uniform ? run_far_rh2<NQV, true>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, \
+                                            ws, st)                                           \
+                   : run_far_rh2<NQV, false>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, \
+                                             ws, st);
+    switch (nq) {
+        case 3: TCT_RH2(3)
+        case 4: TCT_RH2(4)
+        case 7: TCT_RH2(7)
+        default:
+            set_error("tct_farfield_tris_matvec: %d-point rule not supported by the packed RH path",
+                      nq);
+            return TCT_ERR_ARG;
+    }
+#undef TCT_RH2
+}
+
+// The packed FP32 elasticRH3 path serves 3-, 4- and 7-point rules.
+inline bool use_rh2(int kernel, int prec, int nq) {
+    return kernel == kRH && prec == TCT_F32 && (nq == 3 || nq == 4 || nq == 7);
+}
+
 template <typename R, int K>
 int run_far_nq(int nq, const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in,
                const R* pts, const int32_t* ot, int64_t n_obs, const int32_t* stris,
@@ -529,7 +843,15 @@ int far_dispatch(int kernel, int nq, const double* qp, const double* qw, const d
         rule.w[q] = q < nq ? (R)qw[q] : R(0);
     }
     unsigned char* w = reinterpret_cast<unsigned char*>(ws);
-#define TCT_FAR_CASE(KID)                                                                   \
+    if constexpr (sizeof(R) == 4) {
+        if (use_rh2(kernel, TCT_F32, nq)) {
+            bool uniform = true;
+            for (int q = 1; q < nq; q++) uniform = uniform && (qw[q] == qw[0]);
+            return run_far_rh2_nq(nq, uniform, c, rule, (float*)out, (const float*)in,
+                                  (const float*)pts, ot, n_obs, stris, n_src, acc, w, st);
+        }
+    }
+#define TCT_FAR_CASE(KID)                                                                 \
     case KID:                                                                               \
         return run_far_nq<R, KID>(nq, c, rule, (R*)out, (const R*)in, (const R*)pts, ot,   \
                                   n_obs, stris, n_src, acc, w, st);
@@ -686,6 +1008,13 @@ int dense_dispatch(int kernel, const double* params, void* out, int n_q, const v
 }  // namespace
 
 size_t farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_src, int n_q) {
+    if (n_src < 0 || n_obs < 0) return 0;
+    if (use_rh2(kernel, prec, n_q)) {
+        const size_t rec_bytes = align256(4 * (size_t)rec_len_rh2(n_q) * (size_t)n_src);
+        const int64_t chunks = n_chunks_rh2(n_obs, n_src);
+        const size_t part = chunks > 1 ? align256(4 * 9 * (size_t)n_obs * chunks) : 0;
+        return rec_bytes + part;
+    }
     const int len = rec_len(kernel, n_q);
     if (len < 0 || n_src < 0 || n_obs < 0) return 0;
     const size_t rs = prec == TCT_F64 ? 8 : 4;

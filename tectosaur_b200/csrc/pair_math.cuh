@@ -106,16 +106,7 @@ __device__ void integrate_pair(const Consts<R>& c, const TriGeom<R>& o, const Tr
         R sb[3] = {1 - sx - sy, sx, sy};
         R D[3];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            R x = 0, y = 0;
-            x += ob[0] * o.v[0][d];
-            x += ob[1] * o.v[1][d];
-            x += ob[2] * o.v[2][d];
-            y += sb[0] * s.v[0][d];
-            y += sb[1] * s.v[1][d];
-            y += sb[2] * s.v[2][d];
-            D[d] = y - x;
-        }
+        for (int d = 0; d < 3; d++) D[d] = bary_point(s, sb, d) - bary_point(o, ob, d);
         R r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
         if (check0 && r2 == R(0)) continue;
         if (K <= kH) {
