@@ -144,6 +144,28 @@ int tct_fp32_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
 int tct_fp32x2_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Allocation-free farfield matvec (no counterpart in the reference).        */
+/* For callers that cannot allocate device memory when they apply the
+ * operator -- inside a stream capture that must not add memory nodes, under
+ * an embedding application's own memory pool, or where cudaMalloc's implicit
+ * synchronisation is not acceptable.  Same arguments and results as
+ * tct_farfield_tris_matvec minus the workspace: the scratch is a fixed
+ * TCT_NOALLOC_SCRATCH_BYTES array compiled into the library (held on every
+ * GPU that loads the library until the process exits).  Problems whose
+ * workspace (tct_farfield_workspace_bytes) exceeds it are rejected with
+ * TCT_ERR_ARG and a message; nothing is ever allocated.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) -- make
+ * it before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams or host threads) race. */
+#define TCT_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+size_t tct_farfield_noalloc_capacity(void);
+int tct_farfield_tris_matvec_noalloc(int kernel, int prec, void* out, const void* in,
+                                     const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                                     const int32_t* src_tris, int64_t n_src,
+                                     int n_q, const double* quad_pts, const double* quad_wts,
+                                     const double* params, int accumulate, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Host-side (CPU) structure builders.                                       */
 
 /* Near-pair search: all (i, j) with |c_i - c_j|^2 <= ((r_i + r_j) * threshold)^2

@@ -53,6 +53,9 @@ _SIGS = {
                                  c_p], c_i),
     "tct_fp32_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
     "tct_fp32x2_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
+    "tct_farfield_noalloc_capacity": ([], c_sz),
+    "tct_farfield_tris_matvec_noalloc": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i,
+                                          c_dp, c_dp, c_dp, c_i, c_p], c_i),
     "tct_bsr9_matvec": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_i, c_p], c_i),
     "tct_find_near_pairs": ([c_dp, c_dp, c_i64, c_dp, c_dp, c_i64, ctypes.c_double, c_i,
                              ctypes.POINTER(c_p)], c_i),
