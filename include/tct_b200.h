@@ -76,6 +76,35 @@ int tct_pairs_integrate(int kernel, int prec, int adj, int check0,
                         const int32_t* pairs, int64_t n_pairs,
                         const double* params, void* stream);
 
+/* Batched form: pairs of every class and quadrature order in one persistent
+ * launch (replaces the per-class, one-rule-per-launch calls of
+ * nearfield/pairs_integrator.py:70-93).
+ * pairs:      n_pairs x 7 int32 (device): obs, src, obs_clicks, src_clicks,
+ *             src_flip, rule index, parameter-set index.
+ * rule_off:   n_rules + 1 int64 (device): point ranges of the concatenated
+ *             rules in rule_pts (n x 4 Real) / rule_wts (n Real).
+ * rule_flags: n_rules int32 (device): bit 0 = adjacent record (rotate, flip,
+ *             de-rotate), bit 1 = skip r^2 == 0 points.
+ * items:      (n_warp_items + n_thread_items) x 4 int32 (device): pair, first
+ *             point, end point (relative to the rule), split flag.  Warp items
+ *             (first n_warp_items) are integrated by a warp each and, when the
+ *             pair is split over several items (flag 1), atomically added;
+ *             thread items are whole pairs, one per thread.
+ * params:     n_param_sets (1..8) x {mu, nu} host doubles.
+ * out:        n_pairs x 81 Real (device), zeroed first unless accumulate.
+ * workspace:  >= 2048 bytes, 256-byte aligned (queue counters and the
+ *             kernel constants of each parameter set; the constants are
+ *             uploaded with cudaMemcpyAsync from host memory). */
+int tct_pairs_integrate_batched(int kernel, int prec, void* out, int64_t n_pairs,
+                                const void* pts, const int32_t* tris,
+                                const int32_t* pairs, const int64_t* rule_off,
+                                const int32_t* rule_flags, const void* rule_pts,
+                                const void* rule_wts, const int32_t* items,
+                                int64_t n_warp_items, int64_t n_thread_items,
+                                const double* params, int n_param_sets,
+                                int accumulate, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Direct tri-to-tri farfield matvec.                                        */
 /* Replaces farfield_tris_to_tris{K} (tectosaur/matrix_free.cl:19-107) behind

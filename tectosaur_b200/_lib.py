@@ -45,6 +45,8 @@ _SIGS = {
     "tct_kernel_id": ([ctypes.c_char_p], c_i),
     "tct_pairs_integrate": ([c_i, c_i, c_i, c_i, c_p, c_p, c_i64, c_i, c_i, c_i, c_p, c_p, c_p,
                              c_p, c_p, c_i64, c_dp, c_p], c_i),
+    "tct_pairs_integrate_batched": ([c_i, c_i, c_p, c_i64, c_p, c_p, c_p, c_p, c_p, c_p, c_p,
+                                     c_p, c_i64, c_i64, c_dp, c_i, c_i, c_p, c_sz, c_p], c_i),
     "tct_farfield_workspace_bytes": ([c_i, c_i, c_i64, c_i64, c_i], c_sz),
     "tct_farfield_tris_matvec": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_dp,
                                   c_dp, c_dp, c_i, c_p, c_sz, c_p], c_i),

@@ -42,8 +42,11 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             for (int i = 0; i < 9; i++)
 #pragma unroll
                 for (int j = 0; j < 9; j++) {
-                    R a = __ldcs(data + (int64_t)(i * 9 + j) * stride + s);
-                    if (TWO) a += __ldcs(data2 + (int64_t)(i * 9 + j) * stride + s);
+                    // default (L2-retaining) loads: a row's segment of each
+                    // element plane shares its first and last 128-byte lines
+                    // with the neighbouring rows, read by nearby warps
+                    R a = __ldg(data + (int64_t)(i * 9 + j) * stride + s);
+                    if (TWO) a += __ldg(data2 + (int64_t)(i * 9 + j) * stride + s);
                     acc[i] += a * xv[j];
                 }
         }

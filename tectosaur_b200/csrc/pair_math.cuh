@@ -87,28 +87,42 @@ __device__ __forceinline__ R gimk(int p, int m, int j, R Q1, R Q2, const R D[3])
     return A + Q2 * D[p] * B;
 }
 
+// Per-pair accumulator of the tensor-form integrand.
+//
+// U/T/A/H and RT/RA keep the 81 outputs per point (U/T/A/H Kahan-compensated
+// in FP32, as the reference).  RH is separable: its tensor form
+// (kernels/kernels.cl:70-98) multiplies the constant surface curls of the two
+// triangles, so
+//   sum_q K_q[dob][ds][It][Im] osc[bo][It] ssc[bs][Im]
+//     = A (CsRH1 osc[bo][dob] ssc[bs][ds] + CsRH2 osc[bo][ds] ssc[bs][dob]
+//          - 2 delta(dob, ds) G[bo][bs]) - 2 S[dob][ds] G[bo][bs]
+// with A = sum_q w CsRH0 / r, S = sum_q w CsRH0 D D^T / r^3 and
+// G[bo][bs] = osc[bo] . ssc[bs]: seven running sums instead of 81.
 template <typename R, int K, bool KAHAN>
-__device__ void integrate_pair(const Consts<R>& c, const TriGeom<R>& o, const TriGeom<R>& s,
-                               int n_q, const R* __restrict__ qp, const R* __restrict__ qw,
-                               bool check0, R res[81]) {
-    R kc[KAHAN ? 81 : 1];
+struct PairAcc {
+    static constexpr int N = (K == kRH) ? 7 : 81;
+    R v[N];
+    R kc[(KAHAN && K != kRH) ? 81 : 1];
+
+    __device__ __forceinline__ void init() {
 #pragma unroll
-    for (int i = 0; i < 81; i++) res[i] = 0;
-    if (KAHAN) {
+        for (int i = 0; i < N; i++) v[i] = 0;
+        if (KAHAN && K != kRH) {
 #pragma unroll
-        for (int i = 0; i < 81; i++) kc[i] = 0;
+            for (int i = 0; i < 81; i++) kc[i] = 0;
+        }
     }
-    for (int iq = 0; iq < n_q; iq++) {
-        const R ox = __ldg(qp + 4 * iq + 0), oy = __ldg(qp + 4 * iq + 1);
-        const R sx = __ldg(qp + 4 * iq + 2), sy = __ldg(qp + 4 * iq + 3);
-        const R w = __ldg(qw + iq);
+
+    __device__ __forceinline__ void add(const Consts<R>& c, const TriGeom<R>& o,
+                                        const TriGeom<R>& s, R ox, R oy, R sx, R sy, R w,
+                                        bool check0) {
         R ob[3] = {1 - ox - oy, ox, oy};
         R sb[3] = {1 - sx - sy, sx, sy};
         R D[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) D[d] = bary_point(s, sb, d) - bary_point(o, ob, d);
         R r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
-        if (check0 && r2 == R(0)) continue;
+        if (check0 && r2 == R(0)) return;
         if (K <= kH) {
             R Karr[9];
             karr_utah<R, K>(c, D, r2, o.n, s.n, Karr);
@@ -126,11 +140,11 @@ __device__ void integrate_pair(const Consts<R>& c, const TriGeom<R>& o, const Tr
                             R val = ob[bo] * sb[bs] * Karr[dob * 3 + ds];
                             if (KAHAN) {
                                 R yk = val - kc[idx];
-                                R t = res[idx] + yk;
-                                kc[idx] = (t - res[idx]) - yk;
-                                res[idx] = t;
+                                R t = v[idx] + yk;
+                                kc[idx] = (t - v[idx]) - yk;
+                                v[idx] = t;
                             } else {
-                                res[idx] += val;
+                                v[idx] += val;
                             }
                         }
         } else if (K == kRT || K == kRA) {
@@ -163,36 +177,78 @@ __device__ void integrate_pair(const Consts<R>& c, const TriGeom<R>& o, const Tr
                             R val = w * (RT ? ob[bL] : sb[bL]) * Kval;
                             const int b_obs = RT ? bL : bR;
                             const int b_src = RT ? bR : bL;
-                            res[b_obs * 27 + dob * 9 + b_src * 3 + ds] += val;
+                            v[b_obs * 27 + dob * 9 + b_src * 3 + ds] += val;
                         }
                     }
                 }
         } else {
-            // elasticRH3_tensor (kernels/kernels.cl:70-98)
-            const R invr2 = R(1) / r2;
-            const R invr = sqrt(invr2);
-#pragma unroll
-            for (int dob = 0; dob < 3; dob++)
-#pragma unroll
-                for (int ds = 0; ds < 3; ds++)
-#pragma unroll
-                    for (int It = 0; It < 3; It++)
-#pragma unroll
-                        for (int Im = 0; Im < 3; Im++) {
-                            R Kval = w * c.CsRH0 * invr *
-                                     (-2 * D[dob] * D[ds] * invr2 * (R)(It == Im) +
-                                      c.CsRH1 * (R)(dob == It && ds == Im) +
-                                      c.CsRH2 * (R)(dob == Im && ds == It) -
-                                      2 * (R)(dob == ds && It == Im));
-#pragma unroll
-                            for (int bs = 0; bs < 3; bs++)
-#pragma unroll
-                                for (int bo = 0; bo < 3; bo++)
-                                    res[bo * 27 + dob * 9 + bs * 3 + ds] +=
-                                        Kval * o.sc[bo][It] * s.sc[bs][Im];
-                        }
+            const R invr = rsqrt_r(r2);
+            const R a = w * c.CsRH0 * invr;
+            const R b = a * (invr * invr);
+            v[0] += a;
+            const R b0 = b * D[0], b1 = b * D[1], b2 = b * D[2];
+            v[1] += b0 * D[0];
+            v[2] += b0 * D[1];
+            v[3] += b0 * D[2];
+            v[4] += b1 * D[1];
+            v[5] += b1 * D[2];
+            v[6] += b2 * D[2];
         }
     }
+
+    // Sum the accumulators of a warp's 32 lanes (every lane gets the total).
+    __device__ __forceinline__ void warp_reduce() {
+        if (KAHAN && K != kRH) {
+#pragma unroll
+            for (int i = 0; i < 81; i++) v[i] -= kc[i];
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
+        }
+    }
+
+    // The 81 outputs b_obs*27 + d_obs*9 + b_src*3 + d_src (before J_o J_s).
+    __device__ __forceinline__ void finish(const Consts<R>& c, const TriGeom<R>& o,
+                                           const TriGeom<R>& s, R res[81]) const {
+        if (K != kRH) {
+#pragma unroll
+            for (int i = 0; i < 81; i++) res[i] = v[i];
+            return;
+        }
+        const R A = v[0];
+        const R S[3][3] = {{v[1], v[2], v[3]}, {v[2], v[4], v[5]}, {v[3], v[5], v[6]}};
+#pragma unroll
+        for (int bo = 0; bo < 3; bo++)
+#pragma unroll
+            for (int bs = 0; bs < 3; bs++) {
+                const R G = o.sc[bo][0] * s.sc[bs][0] + o.sc[bo][1] * s.sc[bs][1] +
+                            o.sc[bo][2] * s.sc[bs][2];
+#pragma unroll
+                for (int dob = 0; dob < 3; dob++)
+#pragma unroll
+                    for (int ds = 0; ds < 3; ds++)
+                        res[bo * 27 + dob * 9 + bs * 3 + ds] =
+                            A * (c.CsRH1 * o.sc[bo][dob] * s.sc[bs][ds] +
+                                 c.CsRH2 * o.sc[bo][ds] * s.sc[bs][dob] -
+                                 (dob == ds ? 2 * G : R(0))) -
+                            2 * S[dob][ds] * G;
+            }
+    }
+};
+
+template <typename R, int K, bool KAHAN>
+__device__ void integrate_pair(const Consts<R>& c, const TriGeom<R>& o, const TriGeom<R>& s,
+                               int n_q, const R* __restrict__ qp, const R* __restrict__ qw,
+                               bool check0, R res[81]) {
+    PairAcc<R, K, KAHAN> acc;
+    acc.init();
+    for (int iq = 0; iq < n_q; iq++) {
+        acc.add(c, o, s, __ldg(qp + 4 * iq + 0), __ldg(qp + 4 * iq + 1), __ldg(qp + 4 * iq + 2),
+                __ldg(qp + 4 * iq + 3), __ldg(qw + iq), check0);
+    }
+    acc.finish(c, o, s, res);
 }
 
 }  // namespace tct

@@ -85,6 +85,73 @@ class PairsIntegrator:
         self.integrate_into(out, rule, device.to_dev(rec), n, adj, check0)
         return out.cpu().numpy().reshape((n, 3, 3, 3, 3))
 
+    def batched_device(self, records, rule_ids, rules, param_set_ids=None, param_sets=None,
+                       chunk=4096, small=768, out=None, stream=None):
+        """All pairs of mixed classes and orders in one persistent launch.
+
+        records: (n, 5) int (obs, src, obs_clicks, src_clicks, src_flip);
+        rule_ids: (n,) index into `rules`, a list of (pts (m, 4), wts (m,),
+        adjacent, check0); param_set_ids: (n,) index into `param_sets`
+        ((k, 2) [mu, nu], k <= 8; default: this integrator's params).
+        Returns the (n * 81) device array of blocks (before any correction).
+        Work schedule: pairs whose rule has <= `small` points are whole-pair
+        thread items; larger ones are cut into warp items of <= `chunk`
+        points; each queue is ordered by decreasing size."""
+        records = np.asarray(records).reshape(-1, 5).astype(np.int64)
+        n = records.shape[0]
+        rule_ids = np.asarray(rule_ids, dtype=np.int64).reshape(n)
+        if param_sets is None:
+            param_sets = self.params.reshape(1, 2)
+        param_sets = np.ascontiguousarray(np.asarray(param_sets, dtype=np.float64).reshape(-1, 2))
+        if param_set_ids is None:
+            param_set_ids = np.zeros(n, dtype=np.int64)
+        sizes = np.array([r[0].shape[0] for r in rules], dtype=np.int64)
+        rule_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        rule_flags = np.array([(1 if r[2] else 0) | (2 if r[3] else 0) for r in rules], np.int32)
+        pts_all = np.concatenate([np.asarray(r[0], np.float64).reshape(-1, 4) for r in rules])
+        wts_all = np.concatenate([np.asarray(r[1], np.float64).reshape(-1) for r in rules])
+        rec7 = np.concatenate([records, rule_ids[:, None], np.asarray(param_set_ids)[:, None]],
+                              axis=1).astype(np.int32)
+        psize = sizes[rule_ids]
+        big = psize > small
+        # warp items: split large pairs into chunks
+        bp = np.nonzero(big)[0]
+        nchunk = (psize[bp] + chunk - 1) // chunk
+        wi_pair = np.repeat(bp, nchunk)
+        first = np.concatenate([np.arange(k) for k in nchunk]) * chunk if bp.size else \
+            np.zeros(0, np.int64)
+        wi_p0 = first
+        wi_p1 = np.minimum(first + chunk, psize[wi_pair])
+        wi_split = np.repeat((nchunk > 1).astype(np.int64), nchunk)
+        order = np.argsort(-(wi_p1 - wi_p0), kind="stable")
+        witems = np.stack([wi_pair, wi_p0, wi_p1, wi_split], axis=1)[order]
+        tp = np.nonzero(~big)[0]
+        tp = tp[np.argsort(-psize[tp], kind="stable")]
+        titems = np.stack([tp, np.zeros_like(tp), psize[tp], np.zeros_like(tp)], axis=1)
+        items = np.ascontiguousarray(np.concatenate([witems, titems]).astype(np.int32))
+        ft = self.float_type
+        out = out if out is not None else device.empty(max(n * 81, 1), ft)
+        ws = device.workspace(2048)
+        dev = [device.to_dev(rec7), device.to_dev(rule_off), device.to_dev(rule_flags),
+               device.to_dev(pts_all, ft), device.to_dev(wts_all, ft),
+               device.to_dev(items if items.size else np.zeros((1, 4), np.int32))]
+        _lib.check(_lib.lib.tct_pairs_integrate_batched(
+            self.kid, self.prec, _lib.tptr(out), n, _lib.tptr(self.gpu_pts),
+            _lib.tptr(self.gpu_tris), _lib.tptr(dev[0]), _lib.tptr(dev[1]), _lib.tptr(dev[2]),
+            _lib.tptr(dev[3]), _lib.tptr(dev[4]), _lib.tptr(dev[5]), witems.shape[0],
+            titems.shape[0], _lib.dptr(param_sets), param_sets.shape[0], 0, _lib.tptr(ws), 2048,
+            _lib.stream_ptr(stream)), "tct_pairs_integrate_batched")
+        self._batched_keepalive = dev + [ws]
+        return out
+
+    def batched(self, records, rule_ids, rules, param_set_ids=None, param_sets=None, **kw):
+        """Host (n, 3, 3, 3, 3) blocks of batched_device."""
+        n = np.asarray(records).reshape(-1, 5).shape[0]
+        if n == 0:
+            return np.empty((0, 3, 3, 3, 3), dtype=self.float_type)
+        out = self.batched_device(records, rule_ids, rules, param_set_ids, param_sets, **kw)
+        return out[:n * 81].cpu().numpy().reshape(n, 3, 3, 3, 3)
+
     def correction(self, pairs_list, check0):
         return self.pairs_quad(self.far_rule(), pairs_list, False, check0)
 
