@@ -236,6 +236,69 @@ int tct_make_bsr_index(int64_t n_row_blocks, int64_t n_blocks, const int64_t* ro
                        const int64_t* cols, int64_t* indptr, int64_t* indices,
                        int64_t* slot);
 
+/* ---- treecode farfield (fmm/tsfmm.py, fmm/traversal.cpp, fmm/octree.cpp) -- */
+
+typedef struct tct_tree tct_tree;
+typedef struct tct_lists tct_lists;
+
+/* Ball octree over n balls (centers n x 3, radii n), at most leaf_size balls
+ * per leaf; replaces Octree<3>::build (fmm/octree.cpp:28-79, bound through
+ * fmm/traversal_wrapper.cpp:31-40).  Node order, orig_idxs, bounds and
+ * children match the reference exactly.  Host. */
+int tct_tree_build(const double* centers, const double* radii, int64_t n, int64_t leaf_size,
+                   tct_tree** out);
+int64_t tct_tree_n_nodes(const tct_tree* tree);
+int tct_tree_max_height(const tct_tree* tree);
+/* Per-node arrays (any may be NULL): orig_idx (n balls: tree position ->
+ * input index), start/end (ball range), center (x3), R, leaf, depth, height
+ * (0 at leaves), children (8 per node, -1 for leaves).  Host. */
+int tct_tree_export(const tct_tree* tree, int64_t* orig_idx, int64_t* start, int64_t* end,
+                    double* center, double* R, int32_t* leaf, int32_t* depth,
+                    int32_t* height, int64_t* children);
+void tct_tree_free(tct_tree* tree);
+
+/* Dual traversal producing the compressed P2P and M2P lists; replaces
+ * fmmmm_interactions (fmm/traversal.cpp:120-243) with treecode = 1 (the only
+ * mode fmm/tsfmm.py:66-70 uses).  Host. */
+int tct_treecode_lists(const tct_tree* obs, const tct_tree* src, double inner_r,
+                       double outer_r, int64_t order, int treecode, tct_lists** out);
+/* sizes[0..3] = lengths of p2p_obs, p2p_src, m2p_obs, m2p_src (the start
+ * arrays hold one more entry than their obs arrays). */
+int tct_lists_sizes(const tct_lists* lists, int64_t* sizes);
+int tct_lists_export(const tct_lists* lists, int64_t* p2p_obs, int64_t* p2p_start,
+                     int64_t* p2p_src, int64_t* m2p_obs, int64_t* m2p_start,
+                     int64_t* m2p_src);
+void tct_lists_free(tct_lists* lists);
+
+/* Workspace bytes for tct_treecode_matvec (0 for an unsupported kernel or
+ * order).  order is the Cartesian multipole order p (0..12). */
+size_t tct_treecode_workspace_bytes(int kernel, int prec, int order, int64_t n_obs,
+                                    int64_t n_src, int64_t n_src_nodes, int n_q);
+
+/* Treecode farfield matvec for elasticU3, elasticRT3, elasticRA3, elasticRH3; replaces
+ * TSFMM.dot (fmm/tsfmm.py:241-256: p2m, m2m by height, p2p, m2p kernels of
+ * fmm/ts_kernels.cl:428-1003).  Cartesian multipoles of order `order` on
+ * monopole/dipole Laplace channels instead of the reference's spherical
+ * harmonics (the interaction lists, hence which pairs are direct, are the
+ * reference's).  All pointers are device memory except
+ * m2m_height_counts_host (host, n_heights + 1 prefix counts of
+ * m2m_parents, grouped by height 1..max).  Triangles are in tree order;
+ * obs_orig / src_orig map tree positions -> original indices; `in`
+ * (n_src x 9) and `out` (n_obs x 9) are in original order; `out` is scaled
+ * by out_scale.  quad_pts (n_q x 2), quad_wts, src node centres are Real. */
+int tct_treecode_matvec(
+    int kernel, int prec, int order, int n_q, const void* quad_pts, const void* quad_wts,
+    const double* params, double out_scale, const void* obs_pts, const int32_t* obs_tris,
+    int64_t n_obs, const int64_t* obs_orig, const int64_t* o_start, const int64_t* o_end,
+    const void* src_pts, const int32_t* src_tris, int64_t n_src, const int64_t* src_orig,
+    const int64_t* s_start, const int64_t* s_end, const void* s_centers, const int64_t* s_children,
+    int64_t n_src_nodes, const int64_t* src_leaves, int64_t n_src_leaves,
+    const int64_t* m2m_parents, const int64_t* m2m_height_counts_host, int n_heights,
+    const int64_t* p2p_obs, const int64_t* p2p_start, const int64_t* p2p_src, int64_t n_p2p_obs,
+    const int64_t* m2p_obs, const int64_t* m2p_start, const int64_t* m2p_src, int64_t n_m2p_obs,
+    const void* in, void* out, int accumulate, void* workspace, size_t workspace_bytes,
+    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,3 +127,34 @@ def stream_ptr(stream=None):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
+
+_TREE_SIGS = {
+    "tct_tree_build": ([c_dp, c_dp, c_i64, c_i64, ctypes.POINTER(c_p)], c_i),
+    "tct_tree_n_nodes": ([c_p], c_i64),
+    "tct_tree_max_height": ([c_p], c_i),
+    "tct_tree_export": ([c_p, c_i64p, c_i64p, c_i64p, c_dp, c_dp, c_p, c_p, c_p, c_i64p], c_i),
+    "tct_tree_free": ([c_p], None),
+    "tct_treecode_lists": ([c_p, c_p, ctypes.c_double, ctypes.c_double, c_i64, c_i,
+                            ctypes.POINTER(c_p)], c_i),
+    "tct_lists_sizes": ([c_p, c_i64p], c_i),
+    "tct_lists_export": ([c_p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p], c_i),
+    "tct_lists_free": ([c_p], None),
+}
+for _name, (_args, _res) in _TREE_SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+EXPORTED = sorted(set(EXPORTED) | set(_TREE_SIGS))
+
+_FMM_SIGS = {
+    "tct_treecode_workspace_bytes": ([c_i, c_i, c_i, c_i64, c_i64, c_i64, c_i], c_sz),
+    "tct_treecode_matvec": ([c_i, c_i, c_i, c_i, c_p, c_p, c_dp, ctypes.c_double, c_p, c_p, c_i64,
+                             c_p, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_p, c_p, c_i64, c_p,
+                             c_i64, c_p, c_i64p, c_i, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_i64,
+                             c_p, c_p, c_i, c_p, c_sz, c_p], c_i),
+}
+for _name, (_args, _res) in _FMM_SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+EXPORTED = sorted(set(EXPORTED) | set(_FMM_SIGS))

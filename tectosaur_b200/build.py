@@ -37,7 +37,8 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
              "-I" + INCLUDE, "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["pairs.cu", "pairs_batched.cu", "farfield.cu", "bsr.cu", "probe.cu", "noalloc.cu"]
+CU_SOURCES = ["pairs.cu", "pairs_batched.cu", "farfield.cu", "bsr.cu", "probe.cu", "noalloc.cu",
+              "fmm.cu"]
 CXX_SOURCES = ["host.cpp"]
 HEADERS = ["common.cuh", "pair_math.cuh"]
 

@@ -318,6 +318,189 @@ int tct_find_near_pairs(const double* obs_c, const double* obs_r, int64_t n_obs,
     return TCT_OK;
 }
 
+// ---- treecode trees and interaction lists (fmm/tsfmm.py:22-28, 66-70) --------
+}  // extern "C"
+
+struct tct_tree {
+    Octree t;
+    int max_height = 0;
+    std::vector<int> height;
+};
+
+struct tct_lists {
+    // compressed lists (fmm/traversal.cpp:20-53): obs nodes with a non-empty
+    // list, CSR starts, source node indices
+    std::vector<int64_t> p2p_obs, p2p_start, p2p_src;
+    std::vector<int64_t> m2p_obs, m2p_start, m2p_src;
+};
+
+namespace {
+
+int node_height(tct_tree& tr, int64_t k) {
+    const Node& n = tr.t.nodes[k];
+    if (n.leaf) return tr.height[k] = 0;
+    int h = 0;
+    for (int c = 0; c < 8; c++) h = std::max(h, node_height(tr, n.child[c]));
+    return tr.height[k] = h + 1;
+}
+
+template <typename F>
+void for_all_leaves(const Octree& t, int64_t k, const F& f) {
+    const Node& n = t.nodes[k];
+    if (n.leaf) {
+        f(k);
+        return;
+    }
+    for (int c = 0; c < 8; c++) for_all_leaves(t, n.child[c], f);
+}
+
+// Dual-tree traversal with the multipole acceptance criterion
+// outer_r * R_src + inner_r * R_obs < 0.98 * |c_obs - c_src| (fmm/traversal.cpp:119-192).
+void traverse(const Octree& ot, const Octree& st, int64_t on, int64_t sn, double inner_r,
+              double outer_r, int64_t order, bool treecode,
+              std::vector<std::vector<int64_t>>& p2p, std::vector<std::vector<int64_t>>& m2p) {
+    const Node& o = ot.nodes[on];
+    const Node& s = st.nodes[sn];
+    const double r_src = s.R, r_obs = o.R;
+    double d0 = o.c[0] - s.c[0], d1 = o.c[1] - s.c[1], d2 = o.c[2] - s.c[2];
+    const double sep = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    if (outer_r * r_src + inner_r * r_obs < 0.98 * sep) {
+        const int64_t n_src = s.end - s.start, n_obs = o.end - o.start;
+        if (n_src == 0 || n_obs == 0) return;
+        const bool small_src = n_src < order, small_obs = n_obs < order;
+        if (small_src && small_obs) {
+            for_all_leaves(ot, on, [&](int64_t leaf) { p2p[leaf].push_back(sn); });
+        } else if (small_obs || treecode) {
+            for_all_leaves(ot, on, [&](int64_t leaf) { m2p[leaf].push_back(sn); });
+        }
+        // (p2l / m2l only arise without treecode; the treecode does not use them)
+        return;
+    }
+    if (s.leaf && o.leaf) {
+        p2p[on].push_back(sn);
+        return;
+    }
+    const bool split_src = ((r_obs < r_src) && !s.leaf) || o.leaf;
+    if (split_src) {
+        for (int c = 0; c < 8; c++)
+            traverse(ot, st, on, s.child[c], inner_r, outer_r, order, treecode, p2p, m2p);
+    } else {
+        for (int c = 0; c < 8; c++)
+            traverse(ot, st, o.child[c], sn, inner_r, outer_r, order, treecode, p2p, m2p);
+    }
+}
+
+void compress(const std::vector<std::vector<int64_t>>& list, std::vector<int64_t>& obs,
+              std::vector<int64_t>& start, std::vector<int64_t>& src) {
+    obs.clear();
+    start.assign(1, 0);
+    src.clear();
+    for (size_t i = 0; i < list.size(); i++) {
+        if (list[i].empty()) continue;
+        obs.push_back((int64_t)i);
+        src.insert(src.end(), list[i].begin(), list[i].end());
+        start.push_back((int64_t)src.size());
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Ball octree on triangle centres and radii (fmm/octree.cpp via the treecode's
+// make_tree, fmm/tsfmm.py:22-28): the same tree as the near-pair search.
+int tct_tree_build(const double* centers, const double* radii, int64_t n, int64_t leaf_size,
+                   tct_tree** out) {
+    if (!out || n < 0 || leaf_size < 1 || (n > 0 && (!centers || !radii))) {
+        tct::set_error("tct_tree_build: bad arguments");
+        return TCT_ERR_ARG;
+    }
+    auto* tr = new tct_tree();
+    tr->t = build_octree(centers, radii, n, leaf_size);
+    tr->height.assign(tr->t.nodes.size(), 0);
+    tr->max_height = node_height(*tr, 0);
+    *out = tr;
+    return TCT_OK;
+}
+
+int64_t tct_tree_n_nodes(const tct_tree* tr) { return tr ? (int64_t)tr->t.nodes.size() : 0; }
+
+int tct_tree_max_height(const tct_tree* tr) { return tr ? tr->max_height : -1; }
+
+// Node arrays: start, end (int64), centre (3 doubles), R, leaf flag, depth,
+// height (int32) and the 8 children (int64, -1 for leaves); orig_idx[i] is the
+// original index of the ball at tree position i.  Any pointer may be NULL.
+int tct_tree_export(const tct_tree* tr, int64_t* orig_idx, int64_t* start, int64_t* end,
+                    double* center, double* R, int32_t* leaf, int32_t* depth, int32_t* height,
+                    int64_t* children) {
+    if (!tr) {
+        tct::set_error("tct_tree_export: null tree");
+        return TCT_ERR_ARG;
+    }
+    const Octree& t = tr->t;
+    if (orig_idx) std::copy(t.orig.begin(), t.orig.end(), orig_idx);
+    for (size_t k = 0; k < t.nodes.size(); k++) {
+        const Node& n = t.nodes[k];
+        if (start) start[k] = n.start;
+        if (end) end[k] = n.end;
+        if (center)
+            for (int d = 0; d < 3; d++) center[3 * k + d] = n.c[d];
+        if (R) R[k] = n.R;
+        if (leaf) leaf[k] = n.leaf ? 1 : 0;
+        if (depth) depth[k] = n.depth;
+        if (height) height[k] = tr->height[k];
+        if (children)
+            for (int c = 0; c < 8; c++) children[8 * k + c] = n.leaf ? -1 : n.child[c];
+    }
+    return TCT_OK;
+}
+
+void tct_tree_free(tct_tree* tr) { delete tr; }
+
+// P2P and M2P lists of the dual traversal (fmm/traversal.cpp:227-242 with
+// order and treecode as the reference's treecode passes them: 0 and true).
+int tct_treecode_lists(const tct_tree* obs, const tct_tree* src, double inner_r, double outer_r,
+                       int64_t order, int treecode, tct_lists** out) {
+    if (!obs || !src || !out) {
+        tct::set_error("tct_treecode_lists: null argument");
+        return TCT_ERR_ARG;
+    }
+    std::vector<std::vector<int64_t>> p2p(obs->t.nodes.size()), m2p(obs->t.nodes.size());
+    traverse(obs->t, src->t, 0, 0, inner_r, outer_r, order, treecode != 0, p2p, m2p);
+    auto* l = new tct_lists();
+    compress(p2p, l->p2p_obs, l->p2p_start, l->p2p_src);
+    compress(m2p, l->m2p_obs, l->m2p_start, l->m2p_src);
+    *out = l;
+    return TCT_OK;
+}
+
+// sizes[0..3] = n p2p obs nodes, n p2p src entries, n m2p obs nodes, n m2p src entries
+int tct_lists_sizes(const tct_lists* l, int64_t* sizes) {
+    if (!l || !sizes) return TCT_ERR_ARG;
+    sizes[0] = (int64_t)l->p2p_obs.size();
+    sizes[1] = (int64_t)l->p2p_src.size();
+    sizes[2] = (int64_t)l->m2p_obs.size();
+    sizes[3] = (int64_t)l->m2p_src.size();
+    return TCT_OK;
+}
+
+int tct_lists_export(const tct_lists* l, int64_t* p2p_obs, int64_t* p2p_start, int64_t* p2p_src,
+                     int64_t* m2p_obs, int64_t* m2p_start, int64_t* m2p_src) {
+    if (!l) return TCT_ERR_ARG;
+    auto cp = [](const std::vector<int64_t>& v, int64_t* d) {
+        if (d && !v.empty()) std::memcpy(d, v.data(), v.size() * sizeof(int64_t));
+    };
+    cp(l->p2p_obs, p2p_obs);
+    cp(l->p2p_start, p2p_start);
+    cp(l->p2p_src, p2p_src);
+    cp(l->m2p_obs, m2p_obs);
+    cp(l->m2p_start, m2p_start);
+    cp(l->m2p_src, m2p_src);
+    return TCT_OK;
+}
+
+void tct_lists_free(tct_lists* l) { delete l; }
+
 int64_t tct_pairs_count(const tct_pair_list* list) {
     return list ? (int64_t)(list->pairs.size() / 2) : 0;
 }

@@ -1,0 +1,78 @@
+"""Treecode trees and interaction lists (reference: tectosaur/fmm/tsfmm.py:22-28,
+66-70; fmm/octree.cpp; fmm/traversal.cpp), built in libtct_b200.so."""
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+
+
+def tri_centers_radii(pts, tris):
+    """Centre (vertex mean) and max centre-vertex distance of each triangle
+    (make_tree of fmm/tsfmm.py:22-28)."""
+    tri_pts = pts[tris]
+    centers = np.mean(tri_pts, axis=1)
+    Rs = np.max(np.linalg.norm(tri_pts - centers[:, np.newaxis, :], axis=2), axis=1)
+    return centers, Rs
+
+
+class Tree:
+    """Ball octree: node arrays in depth-first preorder and the permutation
+    from tree positions to original indices."""
+
+    def __init__(self, centers, radii, max_pts_per_cell):
+        c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+        r = np.ascontiguousarray(radii, dtype=np.float64).reshape(-1)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib.tct_tree_build(_lib.dptr(c), _lib.dptr(r), c.shape[0],
+                                           int(max_pts_per_cell), ctypes.byref(h)),
+                   "tct_tree_build")
+        self._h = h
+        n = _lib.lib.tct_tree_n_nodes(h)
+        self.n_nodes = n
+        self.max_height = _lib.lib.tct_tree_max_height(h)
+        self.orig_idxs = np.empty(c.shape[0], np.int64)
+        self.start = np.empty(n, np.int64)
+        self.end = np.empty(n, np.int64)
+        self.centers = np.empty((n, 3))
+        self.R = np.empty(n)
+        self.is_leaf = np.empty(n, np.int32)
+        self.depth = np.empty(n, np.int32)
+        self.height = np.empty(n, np.int32)
+        self.children = np.empty((n, 8), np.int64)
+        i32 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        _lib.check(_lib.lib.tct_tree_export(
+            h, _lib.i64ptr(self.orig_idxs), _lib.i64ptr(self.start), _lib.i64ptr(self.end),
+            _lib.dptr(self.centers), _lib.dptr(self.R), i32(self.is_leaf), i32(self.depth),
+            i32(self.height), _lib.i64ptr(self.children)), "tct_tree_export")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.lib.tct_tree_free(self._h)
+            self._h = None
+
+
+class CompressedList:
+    def __init__(self, obs_n_idxs, obs_src_starts, src_n_idxs):
+        self.obs_n_idxs = obs_n_idxs
+        self.obs_src_starts = obs_src_starts
+        self.src_n_idxs = src_n_idxs
+
+
+def treecode_interactions(obs_tree, src_tree, inner_r, outer_r, order=0, treecode=True):
+    """(p2p, m2p) compressed lists of the dual traversal."""
+    h = ctypes.c_void_p()
+    _lib.check(_lib.lib.tct_treecode_lists(obs_tree._h, src_tree._h, float(inner_r),
+                                           float(outer_r), int(order), int(bool(treecode)),
+                                           ctypes.byref(h)), "tct_treecode_lists")
+    try:
+        sizes = np.zeros(4, np.int64)
+        _lib.check(_lib.lib.tct_lists_sizes(h, _lib.i64ptr(sizes)), "tct_lists_sizes")
+        arrs = [np.empty(sizes[0], np.int64), np.empty(sizes[0] + 1, np.int64),
+                np.empty(sizes[1], np.int64), np.empty(sizes[2], np.int64),
+                np.empty(sizes[2] + 1, np.int64), np.empty(sizes[3], np.int64)]
+        _lib.check(_lib.lib.tct_lists_export(h, *[_lib.i64ptr(a) for a in arrs]),
+                   "tct_lists_export")
+    finally:
+        _lib.lib.tct_lists_free(h)
+    return CompressedList(*arrs[:3]), CompressedList(*arrs[3:])

@@ -75,3 +75,6 @@ class TriToTriDirectFarfieldOp:
 
     def farfield_dot(self, v):
         return self.dot(v)
+
+
+from ..fmm.tsfmm import FMMFarfieldOp, FMMFarfieldOpImpl  # noqa: E402,F401
