@@ -257,47 +257,76 @@ int tct_tree_export(const tct_tree* tree, int64_t* orig_idx, int64_t* start, int
                     int32_t* height, int64_t* children);
 void tct_tree_free(tct_tree* tree);
 
-/* Dual traversal producing the compressed P2P and M2P lists; replaces
- * fmmmm_interactions (fmm/traversal.cpp:120-243) with treecode = 1 (the only
- * mode fmm/tsfmm.py:66-70 uses).  Host. */
+/* Dual traversal producing the compressed P2P, M2P, P2L and M2L lists;
+ * replaces fmmmm_interactions (fmm/traversal.cpp:120-243).  treecode = 1 is
+ * the mode fmm/tsfmm.py:66-70 uses.  Host. */
 int tct_treecode_lists(const tct_tree* obs, const tct_tree* src, double inner_r,
                        double outer_r, int64_t order, int treecode, tct_lists** out);
-/* sizes[0..3] = lengths of p2p_obs, p2p_src, m2p_obs, m2p_src (the start
- * arrays hold one more entry than their obs arrays). */
+/* sizes[0..7] = lengths of the obs and src arrays of the p2p, m2p, p2l and
+ * m2l lists, in that order (each start array holds one more entry than its
+ * obs array).  p2l and m2l are only filled without treecode. */
 int tct_lists_sizes(const tct_lists* lists, int64_t* sizes);
-int tct_lists_export(const tct_lists* lists, int64_t* p2p_obs, int64_t* p2p_start,
-                     int64_t* p2p_src, int64_t* m2p_obs, int64_t* m2p_start,
-                     int64_t* m2p_src);
+/* Copies list `which` (0 p2p, 1 m2p, 2 p2l, 3 m2l) into obs / start / src. */
+int tct_lists_export(const tct_lists* lists, int which, int64_t* obs, int64_t* start,
+                     int64_t* src);
 void tct_lists_free(tct_lists* lists);
 
-/* Workspace bytes for tct_treecode_matvec (0 for an unsupported kernel or
- * order).  order is the Cartesian multipole order p (0..12). */
-size_t tct_treecode_workspace_bytes(int kernel, int prec, int order, int64_t n_obs,
-                                    int64_t n_src, int64_t n_src_nodes, int n_q);
+/* Device-side description of one tree for tct_fmm_matvec (all pointers
+ * device memory unless marked host). */
+typedef struct tct_fmm_tree {
+    int64_t n_nodes;
+    const int64_t* start;         /* first triangle (tree order) of each node */
+    const int64_t* end;           /* one past its last triangle */
+    const void* centers;          /* Real, 3 per node: ball centre */
+    const void* radii;            /* Real: ball radius (> 0) */
+    const int64_t* children;      /* 8 per node, -1 at leaves (source tree: M2M) */
+    const int64_t* parent;        /* parent node, -1 at the root (obs tree: L2L) */
+    const int64_t* orig;          /* tree position -> original triangle index */
+    const int64_t* leaves;        /* leaf nodes (source: P2M; obs: L2P) */
+    int64_t n_leaves;
+    const int64_t* levels;        /* nodes grouped by level: source tree = non-leaf
+                                     nodes by height 1, 2, ... (M2M order); obs
+                                     tree = nodes by depth 1, 2, ... (L2L order) */
+    const int64_t* level_offsets; /* HOST: n_levels + 1 offsets into levels */
+    int n_levels;
+} tct_fmm_tree;
 
-/* Treecode farfield matvec for elasticU3, elasticRT3, elasticRA3, elasticRH3; replaces
- * TSFMM.dot (fmm/tsfmm.py:241-256: p2m, m2m by height, p2p, m2p kernels of
- * fmm/ts_kernels.cl:428-1003).  Cartesian multipoles of order `order` on
- * monopole/dipole Laplace channels instead of the reference's spherical
- * harmonics (the interaction lists, hence which pairs are direct, are the
- * reference's).  All pointers are device memory except
- * m2m_height_counts_host (host, n_heights + 1 prefix counts of
- * m2m_parents, grouped by height 1..max).  Triangles are in tree order;
- * obs_orig / src_orig map tree positions -> original indices; `in`
- * (n_src x 9) and `out` (n_obs x 9) are in original order; `out` is scaled
- * by out_scale.  quad_pts (n_q x 2), quad_wts, src node centres are Real. */
-int tct_treecode_matvec(
-    int kernel, int prec, int order, int n_q, const void* quad_pts, const void* quad_wts,
-    const double* params, double out_scale, const void* obs_pts, const int32_t* obs_tris,
-    int64_t n_obs, const int64_t* obs_orig, const int64_t* o_start, const int64_t* o_end,
-    const void* src_pts, const int32_t* src_tris, int64_t n_src, const int64_t* src_orig,
-    const int64_t* s_start, const int64_t* s_end, const void* s_centers, const int64_t* s_children,
-    int64_t n_src_nodes, const int64_t* src_leaves, int64_t n_src_leaves,
-    const int64_t* m2m_parents, const int64_t* m2m_height_counts_host, int n_heights,
-    const int64_t* p2p_obs, const int64_t* p2p_start, const int64_t* p2p_src, int64_t n_p2p_obs,
-    const int64_t* m2p_obs, const int64_t* m2p_start, const int64_t* m2p_src, int64_t n_m2p_obs,
-    const void* in, void* out, int accumulate, void* workspace, size_t workspace_bytes,
-    void* stream);
+/* One compressed interaction list (fmm/traversal.cpp:20-53 layout), device. */
+typedef struct tct_fmm_list {
+    const int64_t* obs;    /* obs nodes with a non-empty list */
+    const int64_t* start;  /* n_obs + 1 offsets into src */
+    const int64_t* src;    /* source nodes */
+    int64_t n_obs;
+} tct_fmm_list;
+
+/* Workspace bytes for tct_fmm_matvec (0 for an unsupported kernel, rule,
+ * order or mode).  order is the Cartesian expansion order p (0..12). */
+size_t tct_fmm_workspace_bytes(int kernel, int prec, int mode, int order, int n_q,
+                               int64_t n_obs, int64_t n_src, int64_t n_obs_nodes,
+                               int64_t n_src_nodes);
+
+/* Treecode / FMM farfield matvec for elasticU3, elasticRT3, elasticRA3 and
+ * elasticRH3; replaces TSFMM.dot (fmm/tsfmm.py:241-256, the p2m, m2m, p2p and
+ * m2p kernels of fmm/ts_kernels.cl:428-1003).
+ *   mode 0 (treecode, the reference's): far = the M2P list; P2M, M2M by
+ *          height, P2P, M2P.
+ *   mode 1 (FMM): far = the M2L list (traversal without treecode); P2M, M2M,
+ *          M2L, L2L by depth, L2P, P2P.
+ * Expansions are Cartesian multipoles / locals of order `order` on
+ * monopole and dipole Laplace channels (the reference uses spherical
+ * harmonics); which pairs are direct (P2P) is decided by the lists.
+ * quad_pts (n_q x 2) and quad_wts are the host 2-D rule (n_q in 3, 4, 7,
+ * 13); obs_pts / src_pts Real (device); obs_tris / src_tris in tree order;
+ * `in` (n_src x 9) and `out` (n_obs x 9) in original order; out (+)=
+ * out_scale * result. */
+int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
+                   const double* quad_pts, const double* quad_wts, const double* params,
+                   double out_scale, const void* obs_pts, const int32_t* obs_tris,
+                   int64_t n_obs, const tct_fmm_tree* obs_tree, const void* src_pts,
+                   const int32_t* src_tris, int64_t n_src, const tct_fmm_tree* src_tree,
+                   const tct_fmm_list* p2p, const tct_fmm_list* far, const void* in,
+                   void* out, int accumulate, void* workspace, size_t workspace_bytes,
+                   void* stream);
 
 #ifdef __cplusplus
 }

@@ -137,7 +137,7 @@ _TREE_SIGS = {
     "tct_treecode_lists": ([c_p, c_p, ctypes.c_double, ctypes.c_double, c_i64, c_i,
                             ctypes.POINTER(c_p)], c_i),
     "tct_lists_sizes": ([c_p, c_i64p], c_i),
-    "tct_lists_export": ([c_p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p], c_i),
+    "tct_lists_export": ([c_p, c_i, c_i64p, c_i64p, c_i64p], c_i),
     "tct_lists_free": ([c_p], None),
 }
 for _name, (_args, _res) in _TREE_SIGS.items():
@@ -146,12 +146,25 @@ for _name, (_args, _res) in _TREE_SIGS.items():
     _f.restype = _res
 EXPORTED = sorted(set(EXPORTED) | set(_TREE_SIGS))
 
+class FmmTree(ctypes.Structure):
+    """Mirror of tct_fmm_tree (include/tct_b200.h)."""
+    _fields_ = [("n_nodes", c_i64), ("start", c_p), ("end", c_p), ("centers", c_p),
+                ("radii", c_p), ("children", c_p), ("parent", c_p), ("orig", c_p),
+                ("leaves", c_p), ("n_leaves", c_i64), ("levels", c_p),
+                ("level_offsets", c_i64p), ("n_levels", c_i)]
+
+
+class FmmList(ctypes.Structure):
+    """Mirror of tct_fmm_list."""
+    _fields_ = [("obs", c_p), ("start", c_p), ("src", c_p), ("n_obs", c_i64)]
+
+
 _FMM_SIGS = {
-    "tct_treecode_workspace_bytes": ([c_i, c_i, c_i, c_i64, c_i64, c_i64, c_i], c_sz),
-    "tct_treecode_matvec": ([c_i, c_i, c_i, c_i, c_p, c_p, c_dp, ctypes.c_double, c_p, c_p, c_i64,
-                             c_p, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_p, c_p, c_i64, c_p,
-                             c_i64, c_p, c_i64p, c_i, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_i64,
-                             c_p, c_p, c_i, c_p, c_sz, c_p], c_i),
+    "tct_fmm_workspace_bytes": ([c_i, c_i, c_i, c_i, c_i, c_i64, c_i64, c_i64, c_i64], c_sz),
+    "tct_fmm_matvec": ([c_i, c_i, c_i, c_i, c_i, c_dp, c_dp, c_dp, ctypes.c_double, c_p, c_p,
+                        c_i64, ctypes.POINTER(FmmTree), c_p, c_p, c_i64,
+                        ctypes.POINTER(FmmTree), ctypes.POINTER(FmmList),
+                        ctypes.POINTER(FmmList), c_p, c_p, c_i, c_p, c_sz, c_p], c_i),
 }
 for _name, (_args, _res) in _FMM_SIGS.items():
     _f = getattr(lib, _name)

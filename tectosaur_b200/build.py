@@ -40,7 +40,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
 CU_SOURCES = ["pairs.cu", "pairs_batched.cu", "farfield.cu", "bsr.cu", "probe.cu", "noalloc.cu",
               "fmm.cu"]
 CXX_SOURCES = ["host.cpp"]
-HEADERS = ["common.cuh", "pair_math.cuh"]
+HEADERS = ["common.cuh", "pair_math.cuh", "far_common.cuh"]
 
 
 def _newer(target, deps):

@@ -329,9 +329,8 @@ struct tct_tree {
 
 struct tct_lists {
     // compressed lists (fmm/traversal.cpp:20-53): obs nodes with a non-empty
-    // list, CSR starts, source node indices
-    std::vector<int64_t> p2p_obs, p2p_start, p2p_src;
-    std::vector<int64_t> m2p_obs, m2p_start, m2p_src;
+    // list, CSR starts, source node indices; 0 p2p, 1 m2p, 2 p2l, 3 m2l
+    std::vector<int64_t> obs[4], start[4], src[4];
 };
 
 namespace {
@@ -356,9 +355,11 @@ void for_all_leaves(const Octree& t, int64_t k, const F& f) {
 
 // Dual-tree traversal with the multipole acceptance criterion
 // outer_r * R_src + inner_r * R_obs < 0.98 * |c_obs - c_src| (fmm/traversal.cpp:119-192).
+typedef std::vector<std::vector<int64_t>> NodeLists;
+
 void traverse(const Octree& ot, const Octree& st, int64_t on, int64_t sn, double inner_r,
-              double outer_r, int64_t order, bool treecode,
-              std::vector<std::vector<int64_t>>& p2p, std::vector<std::vector<int64_t>>& m2p) {
+              double outer_r, int64_t order, bool treecode, NodeLists& p2p, NodeLists& m2p,
+              NodeLists& p2l, NodeLists& m2l) {
     const Node& o = ot.nodes[on];
     const Node& s = st.nodes[sn];
     const double r_src = s.R, r_obs = o.R;
@@ -372,8 +373,11 @@ void traverse(const Octree& ot, const Octree& st, int64_t on, int64_t sn, double
             for_all_leaves(ot, on, [&](int64_t leaf) { p2p[leaf].push_back(sn); });
         } else if (small_obs || treecode) {
             for_all_leaves(ot, on, [&](int64_t leaf) { m2p[leaf].push_back(sn); });
+        } else if (small_src) {
+            p2l[on].push_back(sn);
+        } else {
+            m2l[on].push_back(sn);
         }
-        // (p2l / m2l only arise without treecode; the treecode does not use them)
         return;
     }
     if (s.leaf && o.leaf) {
@@ -383,10 +387,12 @@ void traverse(const Octree& ot, const Octree& st, int64_t on, int64_t sn, double
     const bool split_src = ((r_obs < r_src) && !s.leaf) || o.leaf;
     if (split_src) {
         for (int c = 0; c < 8; c++)
-            traverse(ot, st, on, s.child[c], inner_r, outer_r, order, treecode, p2p, m2p);
+            traverse(ot, st, on, s.child[c], inner_r, outer_r, order, treecode, p2p, m2p, p2l,
+                     m2l);
     } else {
         for (int c = 0; c < 8; c++)
-            traverse(ot, st, o.child[c], sn, inner_r, outer_r, order, treecode, p2p, m2p);
+            traverse(ot, st, o.child[c], sn, inner_r, outer_r, order, treecode, p2p, m2p, p2l,
+                     m2l);
     }
 }
 
@@ -465,37 +471,36 @@ int tct_treecode_lists(const tct_tree* obs, const tct_tree* src, double inner_r,
         tct::set_error("tct_treecode_lists: null argument");
         return TCT_ERR_ARG;
     }
-    std::vector<std::vector<int64_t>> p2p(obs->t.nodes.size()), m2p(obs->t.nodes.size());
-    traverse(obs->t, src->t, 0, 0, inner_r, outer_r, order, treecode != 0, p2p, m2p);
+    const size_t nn = obs->t.nodes.size();
+    NodeLists lists[4] = {NodeLists(nn), NodeLists(nn), NodeLists(nn), NodeLists(nn)};
+    traverse(obs->t, src->t, 0, 0, inner_r, outer_r, order, treecode != 0, lists[0], lists[1],
+             lists[2], lists[3]);
     auto* l = new tct_lists();
-    compress(p2p, l->p2p_obs, l->p2p_start, l->p2p_src);
-    compress(m2p, l->m2p_obs, l->m2p_start, l->m2p_src);
+    for (int k = 0; k < 4; k++) compress(lists[k], l->obs[k], l->start[k], l->src[k]);
     *out = l;
     return TCT_OK;
 }
 
-// sizes[0..3] = n p2p obs nodes, n p2p src entries, n m2p obs nodes, n m2p src entries
 int tct_lists_sizes(const tct_lists* l, int64_t* sizes) {
     if (!l || !sizes) return TCT_ERR_ARG;
-    sizes[0] = (int64_t)l->p2p_obs.size();
-    sizes[1] = (int64_t)l->p2p_src.size();
-    sizes[2] = (int64_t)l->m2p_obs.size();
-    sizes[3] = (int64_t)l->m2p_src.size();
+    for (int k = 0; k < 4; k++) {
+        sizes[2 * k] = (int64_t)l->obs[k].size();
+        sizes[2 * k + 1] = (int64_t)l->src[k].size();
+    }
     return TCT_OK;
 }
 
-int tct_lists_export(const tct_lists* l, int64_t* p2p_obs, int64_t* p2p_start, int64_t* p2p_src,
-                     int64_t* m2p_obs, int64_t* m2p_start, int64_t* m2p_src) {
-    if (!l) return TCT_ERR_ARG;
+int tct_lists_export(const tct_lists* l, int which, int64_t* obs, int64_t* start, int64_t* src) {
+    if (!l || which < 0 || which > 3) {
+        tct::set_error("tct_lists_export: bad list handle or index %d", which);
+        return TCT_ERR_ARG;
+    }
     auto cp = [](const std::vector<int64_t>& v, int64_t* d) {
         if (d && !v.empty()) std::memcpy(d, v.data(), v.size() * sizeof(int64_t));
     };
-    cp(l->p2p_obs, p2p_obs);
-    cp(l->p2p_start, p2p_start);
-    cp(l->p2p_src, p2p_src);
-    cp(l->m2p_obs, m2p_obs);
-    cp(l->m2p_start, m2p_start);
-    cp(l->m2p_src, m2p_src);
+    cp(l->obs[which], obs);
+    cp(l->start[which], start);
+    cp(l->src[which], src);
     return TCT_OK;
 }
 

@@ -45,11 +45,34 @@ class Tree:
             h, _lib.i64ptr(self.orig_idxs), _lib.i64ptr(self.start), _lib.i64ptr(self.end),
             _lib.dptr(self.centers), _lib.dptr(self.R), i32(self.is_leaf), i32(self.depth),
             i32(self.height), _lib.i64ptr(self.children)), "tct_tree_export")
+        self.parent = np.full(n, -1, np.int64)
+        inner = np.nonzero(self.is_leaf == 0)[0]
+        self.parent[self.children[inner].reshape(-1)] = np.repeat(inner, 8)
+
+    def leaves(self):
+        return np.nonzero(self.is_leaf)[0].astype(np.int64)
+
+    def m2m_levels(self):
+        """Non-leaf nodes grouped by height 1, 2, ... (children before parents)."""
+        groups = [np.nonzero((self.is_leaf == 0) & (self.height == h))[0]
+                  for h in range(1, self.max_height + 1)]
+        return _grouped(groups)
+
+    def l2l_levels(self):
+        """Non-root nodes grouped by depth 1, 2, ... (parents before children)."""
+        groups = [np.nonzero(self.depth == d)[0] for d in range(1, int(self.depth.max()) + 1)]
+        return _grouped(groups)
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and _lib is not None and _lib.lib is not None:
             _lib.lib.tct_tree_free(self._h)
             self._h = None
+
+
+def _grouped(groups):
+    offsets = np.concatenate([[0], np.cumsum([g.shape[0] for g in groups])]).astype(np.int64)
+    nodes = np.concatenate(groups).astype(np.int64) if groups else np.zeros(0, np.int64)
+    return nodes, offsets
 
 
 class CompressedList:
@@ -59,20 +82,31 @@ class CompressedList:
         self.src_n_idxs = src_n_idxs
 
 
-def treecode_interactions(obs_tree, src_tree, inner_r, outer_r, order=0, treecode=True):
-    """(p2p, m2p) compressed lists of the dual traversal."""
+LIST_NAMES = ("p2p", "m2p", "p2l", "m2l")
+
+
+def interactions(obs_tree, src_tree, inner_r, outer_r, order=0, treecode=True):
+    """All four compressed lists of the dual traversal, keyed by name."""
     h = ctypes.c_void_p()
     _lib.check(_lib.lib.tct_treecode_lists(obs_tree._h, src_tree._h, float(inner_r),
                                            float(outer_r), int(order), int(bool(treecode)),
                                            ctypes.byref(h)), "tct_treecode_lists")
+    out = {}
     try:
-        sizes = np.zeros(4, np.int64)
+        sizes = np.zeros(8, np.int64)
         _lib.check(_lib.lib.tct_lists_sizes(h, _lib.i64ptr(sizes)), "tct_lists_sizes")
-        arrs = [np.empty(sizes[0], np.int64), np.empty(sizes[0] + 1, np.int64),
-                np.empty(sizes[1], np.int64), np.empty(sizes[2], np.int64),
-                np.empty(sizes[2] + 1, np.int64), np.empty(sizes[3], np.int64)]
-        _lib.check(_lib.lib.tct_lists_export(h, *[_lib.i64ptr(a) for a in arrs]),
-                   "tct_lists_export")
+        for k, name in enumerate(LIST_NAMES):
+            arrs = [np.empty(sizes[2 * k], np.int64), np.empty(sizes[2 * k] + 1, np.int64),
+                    np.empty(sizes[2 * k + 1], np.int64)]
+            _lib.check(_lib.lib.tct_lists_export(h, k, *[_lib.i64ptr(a) for a in arrs]),
+                       "tct_lists_export")
+            out[name] = CompressedList(*arrs)
     finally:
         _lib.lib.tct_lists_free(h)
-    return CompressedList(*arrs[:3]), CompressedList(*arrs[3:])
+    return out
+
+
+def treecode_interactions(obs_tree, src_tree, inner_r, outer_r, order=0, treecode=True):
+    """(p2p, m2p) compressed lists of the dual traversal."""
+    lists = interactions(obs_tree, src_tree, inner_r, outer_r, order, treecode)
+    return lists["p2p"], lists["m2p"]

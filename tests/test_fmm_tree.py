@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from tectosaur_b200.fmm.tree import Tree, tri_centers_radii, treecode_interactions
+from tectosaur_b200.fmm.tree import Tree, interactions, tri_centers_radii, treecode_interactions
 
 from helpers import bumpy_mesh, two_surfaces
 
@@ -63,6 +63,41 @@ def test_treecode_lists_match_reference(mac, leaf, offset):
         assert np.array_equal(mine.src_n_idxs, np.array(theirs.src_n_idxs))
 
 
+@pytest.mark.parametrize("order,inner", [(0, 2.5), (10, 1.0), (60, 2.0)])
+def test_fmm_lists_match_reference(order, inner):
+    """Without the treecode flag the traversal also yields P2L and M2L lists
+    (and M2P / P2P for small nodes, by `order`)."""
+    ref = _ref()
+    (pts, tris), s1, s2 = two_surfaces(n=18, sep=0.7)
+    co, ro = tri_centers_radii(pts, tris[s1])
+    cs, rs = tri_centers_radii(pts, tris[s2])
+    mo, ms = Tree(co, ro, 8), Tree(cs, rs, 8)
+    to, ts = ref.Tree.build(co, ro, 8), ref.Tree.build(cs, rs, 8)
+    mine = interactions(mo, ms, inner, 2.5, order, False)
+    ri = ref.fmmmm_interactions(to, ts, inner, 2.5, order, False)
+    if order == 0:
+        assert mine["m2l"].src_n_idxs.shape[0] > 0 and mine["m2p"].src_n_idxs.shape[0] == 0
+    for name in ["p2p", "m2p", "p2l", "m2l"]:
+        theirs = getattr(ri, name)
+        assert np.array_equal(mine[name].obs_n_idxs, np.array(theirs.obs_n_idxs)), name
+        assert np.array_equal(mine[name].obs_src_starts, np.array(theirs.obs_src_starts)), name
+        assert np.array_equal(mine[name].src_n_idxs, np.array(theirs.src_n_idxs)), name
+
+
+def test_tree_parent_and_levels():
+    pts, tris = bumpy_mesh(20, seed=4)
+    t = Tree(*tri_centers_radii(pts, tris), 5)
+    inner = np.nonzero(t.is_leaf == 0)[0]
+    for k in inner:
+        assert np.all(t.parent[t.children[k]] == k)
+    assert t.parent[0] == -1 and np.sum(t.parent < 0) == 1
+    nodes, off = t.m2m_levels()
+    assert np.all(np.diff(t.height[nodes]) >= 0) and np.all(t.is_leaf[nodes] == 0)
+    assert nodes.shape[0] == inner.shape[0]
+    nodes, off = t.l2l_levels()
+    assert np.all(np.diff(t.depth[nodes]) >= 0) and nodes.shape[0] == t.n_nodes - 1
+
+
 def test_treecode_rejects_unsupported_kernel():
     from tectosaur_b200.fmm.tsfmm import TSFMM
     from tectosaur_b200.mesh.mesh_gen import make_rect
@@ -71,8 +106,12 @@ def test_treecode_rejects_unsupported_kernel():
         TSFMM(m, m, [1.0, 0.25], 4, 2, np.float64, "elasticH3", 2.5, 2)
 
 
-def test_treecode_abi_rejects_bad_order():
+def test_fmm_abi_rejects_bad_arguments():
     from tectosaur_b200 import _lib
-    assert _lib.lib.tct_treecode_workspace_bytes(6, 1, 13, 10, 10, 5, 3) == 0
-    assert _lib.lib.tct_treecode_workspace_bytes(3, 1, 8, 10, 10, 5, 3) == 0  # elasticH3
-    assert _lib.lib.tct_treecode_workspace_bytes(6, 1, 8, 10, 10, 5, 3) > 0
+    ws = _lib.lib.tct_fmm_workspace_bytes
+    assert ws(6, 1, 0, 13, 3, 10, 10, 5, 5) == 0  # order > 12
+    assert ws(3, 1, 0, 8, 3, 10, 10, 5, 5) == 0  # elasticH3
+    assert ws(6, 1, 2, 8, 3, 10, 10, 5, 5) == 0  # mode
+    assert ws(6, 1, 0, 8, 6, 10, 10, 5, 5) == 0  # 6-point rule
+    assert ws(6, 1, 0, 8, 3, 10, 10, 5, 5) > 0
+    assert ws(6, 1, 1, 8, 3, 10, 10, 5, 5) > ws(6, 1, 0, 8, 3, 10, 10, 5, 5)  # locals

@@ -15,7 +15,8 @@ CORNERS = [[-1.0, -1.0, 0], [-1.0, 1.0, 0], [1.0, 1.0, 0], [1.0, -1.0, 0]]
 TREECODE_KERNELS = ["elasticU3", "elasticRT3", "elasticRA3", "elasticRH3"]
 
 
-def fmm_case(K_name, float_type=np.float64, offset=0.0, order=8, ppc=2, n=20, seed=123987):
+def fmm_case(K_name, float_type=np.float64, offset=0.0, order=8, ppc=2, n=20, seed=123987,
+             mode="treecode", mac=2.5):
     rng = np.random.default_rng(seed)
     params = np.array([1.0, 0.25])
     m_src = make_rect(n, n, CORNERS)
@@ -28,7 +29,7 @@ def fmm_case(K_name, float_type=np.float64, offset=0.0, order=8, ppc=2, n=20, se
     direct = TriToTriDirectFarfieldOp(2, K_name, params, full[0], full[1], float_type,
                                       obs_subset, src_subset)
     y1 = direct.dot(v.astype(float_type))
-    fmm = TSFMM(m_obs, m_src, params, order, 2, float_type, K_name, 2.5, ppc)
+    fmm = TSFMM(m_obs, m_src, params, order, 2, float_type, K_name, mac, ppc, mode)
     y2 = fmm.dot(v.astype(float_type))
     return fmm, y1, y2
 
@@ -49,12 +50,34 @@ def test_treecode_far_only(cuda, K):
     np.testing.assert_almost_equal(y1, y2, 7)
 
 
-def test_treecode_error_falls_with_order(cuda):
+@pytest.mark.parametrize("mode", ["treecode", "fmm"])
+def test_error_falls_with_order(cuda, mode):
     errs = []
-    for order in [2, 4, 6, 8]:
-        _, y1, y2 = fmm_case("elasticRH3", order=order)
+    for order in [2, 4, 6, 8, 10]:
+        _, y1, y2 = fmm_case("elasticRH3", order=order, mode=mode, ppc=4)
         errs.append(np.linalg.norm(y1 - y2) / np.linalg.norm(y1))
     assert all(b < a for a, b in zip(errs, errs[1:])), errs
+    assert errs[-1] < 1e-6, errs
+
+
+@pytest.mark.parametrize("K", TREECODE_KERNELS)
+def test_fmm_mode_matches_direct_fp64(cuda, K):
+    fmm, y1, y2 = fmm_case(K, mode="fmm", ppc=4)
+    assert fmm.m2l.src_n_idxs.shape[0] > 0 and fmm.p2p.src_n_idxs.shape[0] > 0
+    assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) < 1e-5
+
+
+@pytest.mark.parametrize("K", ["elasticU3", "elasticRA3", "elasticRH3"])
+def test_fmm_mode_fp32(cuda, K):
+    _, y1, y2 = fmm_case(K, float_type=np.float32, order=6, mode="fmm", ppc=4)
+    assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) < 1e-4
+
+
+def test_fmm_mode_high_order_fp32_in_range(cuda):
+    # order 12 with small leaves: the radius-scaled expansions stay finite in FP32
+    _, y1, y2 = fmm_case("elasticRH3", float_type=np.float32, order=12, mode="fmm", ppc=1, n=24)
+    assert np.all(np.isfinite(y2))
+    assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) < 2e-5
 
 
 @pytest.mark.parametrize("K", ["elasticU3", "elasticRT3", "elasticRA3", "elasticRH3"])
@@ -70,7 +93,8 @@ def test_treecode_one_leaf_is_direct(cuda):
     assert np.linalg.norm(y1 - y2) / np.linalg.norm(y1) < 1e-12
 
 
-def test_fmm_farfield_op_in_sparse_op(cuda):
+@pytest.mark.parametrize("mode", ["treecode", "fmm"])
+def test_fmm_farfield_op_in_sparse_op(cuda, mode):
     """RegularizedSparseIntegralOp with farfield_op_type = FMMFarfieldOp agrees
     with the direct-farfield operator (the reference's fmm path of
     ops/sparse_integral_op.py)."""
@@ -81,7 +105,7 @@ def test_fmm_farfield_op_in_sparse_op(cuda):
     pts[:, :2] += 2.0  # positive coordinates, so the max(pts) scaling is used
     args = (6, 6, 5, 2, 4, 2.5, "elasticRH3", "elasticRH3", [1.0, 0.25], pts, tris, np.float64)
     direct = RegularizedSparseIntegralOp(*args, farfield_op_type=TriToTriDirectFarfieldOp)
-    fmm = RegularizedSparseIntegralOp(*args, farfield_op_type=FMMFarfieldOp(2.5, 8, 8))
+    fmm = RegularizedSparseIntegralOp(*args, farfield_op_type=FMMFarfieldOp(2.5, 8, 8, mode))
     v = np.random.default_rng(5).random(tris.shape[0] * 9)
     a = direct.dot(v)
     b = fmm.dot(v)
