@@ -27,8 +27,8 @@
 //   M2L: L_b = (1/rho) (s_o/rho)^|b| sum_a (-1)^|a| (s_s/rho)^|a| C(a+b, b)
 //              D_(a+b)(R0 / rho) N_a,   R0 = C_o - C_s, rho = |R0|, |a|+|b| <= p;
 //   L2L: L^C_b = (s_C/s_P)^|b| sum_{c >= b} C(c, b) (del / s_P)^(c - b) L^P_c;
-// the Y_d m channel becomes Yl = Phi[Y_d m] - R0_d Phi[m] (folded into the
-// source moments as they are staged), so that at the target
+// the Y_d m channel becomes Yl = Phi[Y_d m] - R0_d Phi[m] (applied to each
+// pair's sums), so that at the target
 //   F[d][j] = L[c_dj](xi) + L[Yl_dj](xi) - xi_d L[m_.j](xi).
 //
 // Multi-indices a = (a0, a1, a2), |a| = n <= p, are stored graded:
@@ -47,6 +47,10 @@ constexpr int FMM_MAXP = 12;
 constexpr int FMM_LVL = (FMM_MAXP + 1) * (FMM_MAXP + 2) / 2;  // 91 terms in the top level
 
 __host__ __device__ constexpr int n_terms(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }
+// number of (a, b) pairs with |a| + |b| <= p: C(p + 6, 6)
+__host__ __device__ constexpr int n_terms6(int p) {
+    return (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) / 720;
+}
 __device__ __forceinline__ int midx(int a0, int a1, int a2) {
     const int n = a0 + a1 + a2;
     return n * (n + 1) * (n + 2) / 6 + (n - a0) * (n - a0 + 1) / 2 + a2;
@@ -492,107 +496,268 @@ fmm_m2p(int p, Rule2D<R> rule, int nq, const int64_t* __restrict__ obs_nodes,
 }
 
 // ---- M2L (FMM) -------------------------------------------------------------
-// One block per obs node with a non-empty M2L list; thread b owns local term b
-// (loops when the expansion has more terms than threads).  Per listed source
-// node: its moments are staged with the Yl transform, D_c(R0 / rho) is built
-// level by level in shared memory, and every thread contracts.
+// Written as L_b = (s_o/rho)^|b| / (rho b!) sum_a f_|a| Dc_(a+b) Nt_a with
+// Dc_c = c! D_c(R0 / rho), f_n = (-1)^n (s_s/rho)^n and Nt_a = N_a / a! (the
+// moments are divided by a! once, after M2M, by fmm_moment_factorials), so a
+// pair's source moments are used as stored.  One warp per obs node walks its
+// M2L list; per pair the lanes copy the source node's moments into the warp's
+// shared memory and build Dc level by level there (warp syncs only), then
+// lane l contracts the local terms b dealt to it in snake order (b = 32k + l,
+// 32k + 31 - l, ... balances the trip counts, which fall with |b|), reading
+// the moment rows as shared-memory broadcasts.  The
+// pair's sums get the Yl correction (- R0_d times the m channel) and the b
+// scaling, and are added to the warp's local expansion in shared memory.
+template <typename R>
+__global__ void __launch_bounds__(128)
+fmm_moment_factorials(int p, int nchp, int64_t n_nodes, R* __restrict__ mom) {
+    const int NT = n_terms(p);
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_nodes * NT * nchp) return;
+    int a0, a1, a2;
+    decode((int)((e / nchp) % NT), a0, a1, a2);
+    R f = 1;
+    for (int k = 2; k <= a0; k++) f *= (R)k;
+    for (int k = 2; k <= a1; k++) f *= (R)k;
+    for (int k = 2; k <= a2; k++) f *= (R)k;
+    mom[e] /= f;
+}
+
+// Lane plan of the M2L contraction for order p (one warp, written to the
+// workspace each call).  The work of local term b is n_terms(p - |b|)
+// source terms; terms are cut into chunks of at most CH = ceil(total / 32)
+// iterations and the chunks are dealt, in order, to the lane with the least
+// work so far (ties to the lowest lane), so every lane runs about CH
+// iterations.  A term cut into several chunks gets consecutive partial slots,
+// summed in a fixed order after the contraction (deterministic results).
+constexpr int M2L_MAXI = 32;   // chunks per lane (15 at most for p <= 12)
+constexpr int M2L_SLOTS = 32;  // partial slots (31 at most for p <= 12)
+struct M2LPlan {
+    int item[32][M2L_MAXI][4];  // b, first, end (graded source-term range), slot or -1
+    int cnt[32];
+    int split[M2L_SLOTS][3];    // b, first slot, end slot
+    int nsplit;
+};
+
+__global__ void __launch_bounds__(32) fmm_m2l_plan(int p, M2LPlan* __restrict__ plan) {
+    const int lane = threadIdx.x;
+    const int NT = n_terms(p);
+    const int CH = (n_terms6(p) + 31) / 32;
+    int load = 0, cnt = 0, slot = 0, nsplit = 0;
+    for (int b = 0; b < NT; b++) {
+        int b0, b1, b2;
+        decode(b, b0, b1, b2);
+        const int t = n_terms(p - (b0 + b1 + b2));
+        const int nch = (t + CH - 1) / CH;
+        const bool split = nch > 1 && slot + nch <= M2L_SLOTS;
+        const int step = split ? CH : t;
+        for (int c = 0, g0 = 0; g0 < t; c++, g0 += step) {
+            const int g1 = min(t, g0 + step);
+            const unsigned key = ((unsigned)load << 5) | (unsigned)lane;
+            const unsigned win = __reduce_min_sync(0xffffffffu, key) & 31u;
+            if ((unsigned)lane == win && cnt < M2L_MAXI) {
+                plan->item[lane][cnt][0] = b;
+                plan->item[lane][cnt][1] = g0;
+                plan->item[lane][cnt][2] = g1;
+                plan->item[lane][cnt][3] = split ? slot + c : -1;
+                cnt++;
+                load += g1 - g0;
+            }
+        }
+        if (split) {
+            if (lane == 0) {
+                plan->split[nsplit][0] = b;
+                plan->split[nsplit][1] = slot;
+                plan->split[nsplit][2] = slot + nch;
+            }
+            slot += nch;
+            nsplit++;
+        }
+    }
+    plan->cnt[lane] = cnt;
+    if (lane == 0) plan->nsplit = nsplit;
+}
+
 template <typename R, int K>
-__global__ void __launch_bounds__(256)
-fmm_m2l(int p, const int64_t* __restrict__ obs_nodes, const int64_t* __restrict__ starts,
-        const int64_t* __restrict__ srcs, const R* __restrict__ ocent, const R* __restrict__ orad,
-        const R* __restrict__ scent, const R* __restrict__ srad, const R* __restrict__ mom,
+__device__ __forceinline__ void m2l_flush(R (&acc)[Chan<K>::NCH], const R R0[3], R sc, R* lrow) {
+    using C = Chan<K>;
+    // Yl = Y - R0_d m; scaled add into the warp's local expansion
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int j = 0; j < C::J; j++) acc[C::CH_Y + d * C::J + j] -= R0[d] * acc[C::CH_M + j];
+#pragma unroll
+    for (int k = 0; k < C::NCH; k++) lrow[k] += sc * acc[k];
+}
+
+template <typename R>
+__device__ __forceinline__ R mfact(int b0, int b1, int b2) {
+    R f = 1;
+    for (int k = 2; k <= b0; k++) f *= (R)k;
+    for (int k = 2; k <= b1; k++) f *= (R)k;
+    for (int k = 2; k <= b2; k++) f *= (R)k;
+    return f;
+}
+
+template <typename R, int K>
+__global__ void __launch_bounds__(128)
+fmm_m2l(int p, int wpb, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
+        const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
+        const R* __restrict__ ocent, const R* __restrict__ orad, const R* __restrict__ scent,
+        const R* __restrict__ srad, const R* __restrict__ mom, const M2LPlan* __restrict__ plan,
         R* __restrict__ loc) {
     using C = Chan<K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NT = n_terms(p);
-    R* Ns = reinterpret_cast<R*>(smem_raw);         // NT x NCHP
-    R* Dt = Ns + NT * C::NCHP;                       // NT
-    R* bin = Dt + NT;                                // (P+1)^2
-    R* ps = bin + (FMM_MAXP + 1) * (FMM_MAXP + 1);   // (-1)^n (s_s/rho)^n
-    R* po = ps + (FMM_MAXP + 1);                     // (s_o/rho)^n / rho
-    fill_binom(bin);
-    const int64_t node = obs_nodes[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t oi = (int64_t)blockIdx.x * wpb + warp;
+    if (warp >= wpb || oi >= n_obs_nodes) return;  // whole warps only: no block barriers below
+    // per-warp segment: Lw, Ns (NT x NCHP each), partial slots, Dc, fw, pw;
+    // padded to 4 Reals so that every warp's Ns stays 16-byte aligned
+    const int seg = (2 * NT + M2L_SLOTS) * C::NCHP + (NT + 32 + 3) / 4 * 4;
+    R* Lw = reinterpret_cast<R*>(smem_raw) + (size_t)warp * seg;
+    R* Ns = Lw + NT * C::NCHP;        // the current source node's moments
+    R* Ps = Ns + NT * C::NCHP;        // partial sums of split terms
+    R* Dc = Ps + M2L_SLOTS * C::NCHP;  // NT
+    R* fw = Dc + NT;                  // f_n, n <= p
+    R* pw = fw + 16;                  // (s_o/rho)^n / rho
+    for (int e = lane; e < NT * C::NCHP; e += 32) Lw[e] = 0;
+    const int mycnt = plan->cnt[lane];
+    const int nsplit = plan->nsplit;
+    const int64_t node = obs_nodes[oi];
     const R co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
     const R so = orad[node];
-    const int64_t l0 = starts[blockIdx.x], l1 = starts[blockIdx.x + 1];
-    for (int bb = 0; bb < NT; bb += blockDim.x) {
-        const int b = bb + threadIdx.x;
-        const bool valid = b < NT;
-        int b0 = 0, b1 = 0, b2 = 0;
-        if (valid) decode(b, b0, b1, b2);
-        const int nb = b0 + b1 + b2;
-        R acc[C::NCH];
-#pragma unroll
-        for (int k = 0; k < C::NCH; k++) acc[k] = 0;
-        for (int64_t l = l0; l < l1; l++) {
-            const int64_t sn = srcs[l];
-            const R R0[3] = {co[0] - scent[3 * sn], co[1] - scent[3 * sn + 1], co[2] - scent[3 * sn + 2]};
-            const R rho = sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
-            const R inv_rho = R(1) / rho;
-            const R Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
-            __syncthreads();
-            // stage moments; Yl = Y - R0_d M
-            const R* Msrc = mom + sn * (int64_t)C::NCHP * NT;
-            for (int e = threadIdx.x; e < NT * C::NCHP; e += blockDim.x) {
-                const int k = e % C::NCHP;
-                R v = __ldg(Msrc + e);
-                if (k >= C::CH_Y && k < C::CH_M) {
-                    const int o = k - C::CH_Y, d = o / C::J, j = o % C::J;
-                    v -= R0[d] * __ldg(Msrc + (e - k) + C::CH_M + j);
-                }
-                Ns[e] = v;
-            }
-            if (threadIdx.x <= p) {
-                const int n = threadIdx.x;
-                ps[n] = ((n & 1) ? R(-1) : R(1)) * ipow(srad[sn] * inv_rho, n);
-                po[n] = ipow(so * inv_rho, n) * inv_rho;
-            }
-            if (threadIdx.x == 0) Dt[0] = 1;
-            __syncthreads();
-            for (int n = 1; n <= p; n++) {
-                const int lsz = (n + 1) * (n + 2) / 2;
-                const R cA = -(R)(2 * n - 1) / (R)n, cB = -(R)(n - 1) / (R)n;
-                for (int w = threadIdx.x; w < lsz; w += blockDim.x) {
-                    // decode w within level n: a0 descending, a2 ascending
-                    int a0 = n, off = 0;
-                    while (off + (n - a0 + 1) <= w) {
-                        off += n - a0 + 1;
-                        a0--;
-                    }
-                    const int a2 = w - off, a1 = n - a0 - a2;
-                    R s1 = 0, s2 = 0;
-                    if (a0 > 0) s1 += Rh[0] * Dt[midx(a0 - 1, a1, a2)];
-                    if (a1 > 0) s1 += Rh[1] * Dt[midx(a0, a1 - 1, a2)];
-                    if (a2 > 0) s1 += Rh[2] * Dt[midx(a0, a1, a2 - 1)];
-                    if (a0 > 1) s2 += Dt[midx(a0 - 2, a1, a2)];
-                    if (a1 > 1) s2 += Dt[midx(a0, a1 - 2, a2)];
-                    if (a2 > 1) s2 += Dt[midx(a0, a1, a2 - 2)];
-                    Dt[n_terms(n - 1) + w] = cA * s1 + cB * s2;
-                }
-                __syncthreads();
-            }
-            if (!valid) continue;
-            const R pb = po[nb];
-            int g = 0;
-            for (int na = 0; na <= p - nb; na++) {
-                const R sa = ps[na] * pb;
-                for (int a0 = na; a0 >= 0; a0--)
-                    for (int a2 = 0; a2 <= na - a0; a2++, g++) {
-                        const int a1 = na - a0 - a2;
-                        const R coef = sa * BIN(a0 + b0, b0) * BIN(a1 + b1, b1) * BIN(a2 + b2, b2) *
-                                       Dt[midx(a0 + b0, a1 + b1, a2 + b2)];
-                        const R* nrow = Ns + g * C::NCHP;
-#pragma unroll
-                        for (int k = 0; k < C::NCH; k++) acc[k] += coef * nrow[k];
-                    }
+    for (int64_t l = starts[oi]; l < starts[oi + 1]; l++) {
+        const int64_t sn = srcs[l];
+        const R R0[3] = {co[0] - scent[3 * sn], co[1] - scent[3 * sn + 1], co[2] - scent[3 * sn + 2]};
+        const R rho = sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
+        const R inv_rho = R(1) / rho;
+        const R Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
+        __syncwarp();  // the previous pair's readers are done
+        if (lane <= p) {
+            fw[lane] = ((lane & 1) ? R(-1) : R(1)) * ipow(srad[sn] * inv_rho, lane);
+            pw[lane] = ipow(so * inv_rho, lane) * inv_rho;
+        } else if (lane < 16) {
+            fw[lane] = 0;
+            pw[lane] = 0;
+        }
+        if (lane == 0) Dc[0] = 1;
+        {
+            const R* Ms = mom + sn * (int64_t)C::NCHP * NT;
+            if (sizeof(R) == 4) {
+                const float4* sv = reinterpret_cast<const float4*>(Ms);
+                float4* dv = reinterpret_cast<float4*>(Ns);
+                for (int k = lane; k < NT * C::NCHP / 4; k += 32) dv[k] = __ldg(sv + k);
+            } else {
+                const double2* sv = reinterpret_cast<const double2*>(Ms);
+                double2* dv = reinterpret_cast<double2*>(Ns);
+                for (int k = lane; k < NT * C::NCHP / 2; k += 32) dv[k] = __ldg(sv + k);
             }
         }
-        if (valid) {
-            R* Lp = loc + node * (int64_t)C::NCHP * NT + b * C::NCHP;
+        __syncwarp();
+        for (int n = 1; n <= p; n++) {
+            const int lsz = (n + 1) * (n + 2) / 2;
+            const R cA = -(R)(2 * n - 1) / (R)n, cB = -(R)(n - 1) / (R)n;
+            for (int w = lane; w < lsz; w += 32) {
+                int a0 = n, off = 0;
+                while (off + (n - a0 + 1) <= w) {
+                    off += n - a0 + 1;
+                    a0--;
+                }
+                const int a2 = w - off, a1 = n - a0 - a2;
+                R s1 = 0, s2 = 0;
+                if (a0 > 0) s1 += Rh[0] * (R)a0 * Dc[midx(a0 - 1, a1, a2)];
+                if (a1 > 0) s1 += Rh[1] * (R)a1 * Dc[midx(a0, a1 - 1, a2)];
+                if (a2 > 0) s1 += Rh[2] * (R)a2 * Dc[midx(a0, a1, a2 - 1)];
+                if (a0 > 1) s2 += (R)(a0 * (a0 - 1)) * Dc[midx(a0 - 2, a1, a2)];
+                if (a1 > 1) s2 += (R)(a1 * (a1 - 1)) * Dc[midx(a0, a1 - 2, a2)];
+                if (a2 > 1) s2 += (R)(a2 * (a2 - 1)) * Dc[midx(a0, a1, a2 - 2)];
+                Dc[n_terms(n - 1) + w] = cA * s1 + cB * s2;
+            }
+            __syncwarp();
+        }
+        // flat loop over this lane's chunks: every lane runs ~CH iterations
+        int k = 0;
+        int b = 0, b0 = 0, b1 = 0, b2 = 0, g = 0, g1 = 0, slot = -1, na = 0, a0 = 0, a2 = 0,
+            n = 0, rowbase = 0;
+        R f = 0;
+        R acc[C::NCH];
+        while (k < mycnt) {
+            if (g == g1) {  // start chunk k
+                b = plan->item[lane][k][0];
+                g = plan->item[lane][k][1];
+                g1 = plan->item[lane][k][2];
+                slot = plan->item[lane][k][3];
+                decode(b, b0, b1, b2);
+                int a1;
+                decode(g, a0, a1, a2);
+                na = a0 + a1 + a2;
+                n = na + b0 + b1 + b2;
+                rowbase = n_terms(n - 1) + (n - a0 - b0) * (n - a0 - b0 + 1) / 2 + b2;
+                f = fw[na];
 #pragma unroll
-            for (int k = 0; k < C::NCHP; k++) Lp[k] = k < C::NCH ? acc[k] : R(0);
+                for (int c = 0; c < C::NCH; c++) acc[c] = 0;
+            }
+            const R coef = f * Dc[rowbase + a2];
+            const R* nrow = Ns + g * C::NCHP;
+            if (sizeof(R) == 4) {
+#pragma unroll
+                for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
+                    const float4 v = reinterpret_cast<const float4*>(nrow)[k4];
+                    const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        if (4 * k4 + u < C::NCH) acc[4 * k4 + u] += coef * (R)vv[u];
+                }
+            } else {
+#pragma unroll
+                for (int k2 = 0; k2 < C::NCHP / 2; k2++) {
+                    const double2 v = reinterpret_cast<const double2*>(nrow)[k2];
+                    if (2 * k2 < C::NCH) acc[2 * k2] += coef * (R)v.x;
+                    if (2 * k2 + 1 < C::NCH) acc[2 * k2 + 1] += coef * (R)v.y;
+                }
+            }
+            // next source term in graded order
+            g++;
+            a2++;
+            if (a2 > na - a0) {
+                a2 = 0;
+                a0--;
+                if (a0 < 0) {
+                    na++;
+                    a0 = na;
+                    n++;
+                    f = fw[na];
+                }
+                rowbase = n_terms(n - 1) + (n - a0 - b0) * (n - a0 - b0 + 1) / 2 + b2;
+            }
+            if (g == g1) {  // end of chunk k
+                if (slot < 0) {
+                    m2l_flush<R, K>(acc, R0, pw[b0 + b1 + b2] / mfact<R>(b0, b1, b2),
+                                    Lw + b * C::NCHP);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < C::NCH; c++) Ps[slot * C::NCHP + c] = acc[c];
+                }
+                k++;
+            }
+        }
+        __syncwarp();
+        for (int j = lane; j < nsplit; j += 32) {
+            const int bs = plan->split[j][0];
+            int c0, c1, c2;
+            decode(bs, c0, c1, c2);
+            R sacc[C::NCH];
+#pragma unroll
+            for (int c = 0; c < C::NCH; c++) sacc[c] = 0;
+            for (int sl = plan->split[j][1]; sl < plan->split[j][2]; sl++)
+#pragma unroll
+                for (int c = 0; c < C::NCH; c++) sacc[c] += Ps[sl * C::NCHP + c];
+            m2l_flush<R, K>(sacc, R0, pw[c0 + c1 + c2] / mfact<R>(c0, c1, c2), Lw + bs * C::NCHP);
         }
     }
+    __syncwarp();
+    R* Lg = loc + node * (int64_t)C::NCHP * NT;
+    for (int e = lane; e < NT * C::NCHP; e += 32) Lg[e] = Lw[e];
 }
 
 // ---- L2L (FMM) -------------------------------------------------------------
@@ -760,7 +925,7 @@ fmm_finish(Rule2D<R> rule, const R* __restrict__ pts, const int32_t* __restrict_
 inline size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 
 struct Sizes {
-    size_t rec, mom, loc, W, F;
+    size_t rec, mom, loc, plan, W, F;
 };
 
 template <int K, int NQ>
@@ -771,6 +936,7 @@ Sizes sizes_for(size_t rs, int mode, int order, int64_t n_obs, int64_t n_src, in
     s.rec = al256(rs * Rec<K, NQ>::LEN * (size_t)n_src);
     s.mom = al256(rs * C::NCHP * (size_t)n_terms(order) * n_src_nodes);
     s.loc = mode == 1 ? al256(rs * C::NCHP * (size_t)n_terms(order) * n_obs_nodes) : 0;
+    s.plan = mode == 1 ? al256(sizeof(M2LPlan)) : 0;
     s.W = al256(rs * NAcc<K, NQ>::n * (size_t)n_obs);
     s.F = al256(rs * C::NO * (size_t)NQ * n_obs);
     return s;
@@ -797,7 +963,7 @@ Sizes sizes_dispatch(int kernel, int prec, int mode, int order, int nq, int64_t 
     TCT_SZ_K(kRH)
 #undef TCT_SZ_K
 #undef TCT_SZ_NQ
-    return Sizes{0, 0, 0, 0, 0};
+    return Sizes{0, 0, 0, 0, 0, 0};
 }
 
 template <typename KF>
@@ -823,8 +989,9 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
     R* rec = reinterpret_cast<R*>(ws);
     R* mom = reinterpret_cast<R*>(ws + sz.rec);
     R* loc = reinterpret_cast<R*>(ws + sz.rec + sz.mom);
-    R* W = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc);
-    R* F = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.W);
+    M2LPlan* plan = reinterpret_cast<M2LPlan*>(ws + sz.rec + sz.mom + sz.loc);
+    R* W = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan);
+    R* F = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan + sz.W);
     const R* scent = (const R*)stt.centers;
     const R* srad = (const R*)stt.radii;
     const R* ocent = (const R*)ot.centers;
@@ -870,11 +1037,20 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
     } else {
         if (cudaMemsetAsync(loc, 0, sz.loc, st) != cudaSuccess) return launch_status("fmm memset");
         if (far.n_obs > 0) {
-            const size_t smem =
-                sizeof(R) * ((size_t)C::NCHP * NT + NT + (FMM_MAXP + 1) * (FMM_MAXP + 3));
+            const int64_t n_el = stt.n_nodes * (int64_t)NT * C::NCHP;
+            fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, st>>>(
+                p, C::NCHP, stt.n_nodes, mom);
+            if ((rc = launch_status("fmm moment factorials"))) return rc;
+            fmm_m2l_plan<<<1, 32, 0, st>>>(p, plan);
+            if ((rc = launch_status("fmm m2l plan"))) return rc;
+            const size_t per_warp =
+                sizeof(R) * ((2 * (size_t)NT + M2L_SLOTS) * C::NCHP + (NT + 32 + 3) / 4 * 4);
+            const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp));
+            const size_t smem = per_warp * wpb;
             if ((rc = set_smem(fmm_m2l<R, K>, smem))) return rc;
-            fmm_m2l<R, K><<<(unsigned)far.n_obs, 256, smem, st>>>(
-                p, far.obs, far.start, far.src, ocent, orad, scent, srad, mom, loc);
+            fmm_m2l<R, K><<<(unsigned)((far.n_obs + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
+                p, wpb, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
+                plan, loc);
             if ((rc = launch_status("fmm m2l"))) return rc;
         }
         const size_t smem_l2l =
@@ -913,7 +1089,7 @@ extern "C" size_t tct_fmm_workspace_bytes(int kernel, int prec, int mode, int or
         return 0;
     const Sizes s = sizes_dispatch(kernel, prec, mode, order, n_q, n_obs, n_src, n_obs_nodes,
                                    n_src_nodes);
-    return s.rec + s.mom + s.loc + s.W + s.F;
+    return s.rec + s.mom + s.loc + s.plan + s.W + s.F;
 }
 
 extern "C" int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,

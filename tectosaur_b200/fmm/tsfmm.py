@@ -107,9 +107,16 @@ class TSFMM:
 
     @staticmethod
     def _list_desc(lst, dev):
-        return _lib.FmmList(obs=dev(lst.obs_n_idxs).data_ptr(),
-                            start=dev(lst.obs_src_starts).data_ptr(),
-                            src=dev(lst.src_n_idxs).data_ptr(), n_obs=lst.obs_n_idxs.shape[0])
+        """Device copy of a compressed list with its obs entries ordered longest
+        list first (one block or warp per entry: the long ones start first)."""
+        obs, start, src = lst.obs_n_idxs, lst.obs_src_starts, lst.src_n_idxs
+        lens = np.diff(start)
+        order = np.argsort(-lens, kind="stable")
+        new_start = np.concatenate([[0], np.cumsum(lens[order])]).astype(np.int64)
+        new_src = (np.concatenate([src[start[i]:start[i + 1]] for i in order])
+                   if order.size else src)
+        return _lib.FmmList(obs=dev(obs[order]).data_ptr(), start=dev(new_start).data_ptr(),
+                            src=dev(new_src).data_ptr(), n_obs=obs.shape[0])
 
     def dot_device(self, x, y, scale=1.0, accumulate=False, stream=None):
         """y (+)= scale * farfield(x) for device tensors in original order."""
