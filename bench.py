@@ -52,6 +52,29 @@ def c2_mesh(n=174, seed=2):
     return pts, tris
 
 
+def c4_mesh(n=707, seed=5):
+    """The 1M-triangle FMM configuration: an n x n vertex grid over [-50, 50]^2
+    with three seeded Gaussian hills (amplitude U[0.5, 2], width U[3, 10],
+    centres U[-30, 30]^2) plus a 20 x 10 planar thrust fault dipping 30 degrees
+    (top edge at z = -0.5, strike along x) meshed at the surface's spacing;
+    surface and fault concatenated without merging vertices."""
+    from tectosaur_b200.mesh.mesh_gen import concat_no_dedupe, make_rect
+    rng = np.random.default_rng(seed)
+    pts, tris = make_rect(n, n, [[-50, -50, 0], [50, -50, 0], [50, 50, 0], [-50, 50, 0]])
+    pts = pts.copy()
+    for _ in range(3):
+        amp, width = rng.uniform(0.5, 2.0), rng.uniform(3.0, 10.0)
+        cx, cy = rng.uniform(-30.0, 30.0, 2)
+        pts[:, 2] += amp * np.exp(-((pts[:, 0] - cx) ** 2 + (pts[:, 1] - cy) ** 2) /
+                                  (2.0 * width * width))
+    h = 100.0 / (n - 1)
+    dip = np.radians(30.0)
+    y1, z1 = 10.0 * np.cos(dip), -0.5 - 10.0 * np.sin(dip)
+    fault = make_rect(int(round(20.0 / h)) + 1, int(round(10.0 / h)) + 1,
+                      [[-10, 0, -0.5], [10, 0, -0.5], [10, y1, z1], [-10, y1, z1]])
+    return concat_no_dedupe((pts, tris), fault)
+
+
 def build_op(pts, tris):
     import tectosaur_b200 as tct
     from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
@@ -252,6 +275,325 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+FMM_CFG = dict(mac=3.0, pts_per_cell=128, order=8, mode="fmm")
+
+
+def fmm_algorithmic_flops(fmm, n_q):
+    """FP32 flops of one FMM apply counted from the interaction lists: P2P
+    point pairs x 36 (the hoisted elasticRH3 pair loop) + M2L pairs x
+    C(p+6, 6) (a, b) products x 21 channels x 2."""
+    st, ot = fmm.src_tree, fmm.obs_tree
+    l = fmm.p2p
+    n_o = (ot.end - ot.start)[l.obs_n_idxs]
+    lens = np.diff(l.obs_src_starts)
+    n_s = (st.end - st.start)[l.src_n_idxs]
+    src_per_obs = np.add.reduceat(n_s, l.obs_src_starts[:-1]) if lens.size else np.zeros(0)
+    p2p_pairs = float(np.sum(n_o * src_per_obs)) * n_q * n_q
+    p = fmm.order
+    ab = (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) / 720.0
+    m2l = float(fmm.m2l.src_n_idxs.shape[0]) * ab * 21 * 2
+    return p2p_pairs * FLOPS_PER_POINT_PAIR_RH + m2l, p2p_pairs, m2l
+
+
+def cpu_direct_far_baseline(pts, tris, target_s=10.0):
+    """The direct farfield on the host cores (oracle restatement, FP32, all
+    threads) for a sample of observation triangles against all sources,
+    extrapolated to one full apply (the reference's FMM has no CPU path)."""
+    from oracle import oracle as orc
+    from tectosaur_b200.util.quadrature import gauss2d_tri
+    n = tris.shape[0]
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(n * 9)
+    q = gauss2d_tri(1)
+    def t_sample(m):
+        obs = np.sort(rng.choice(n, size=m, replace=False))
+        t0 = time.perf_counter()
+        orc.farfield_tris(K_NAME, np.float32, q, pts, tris[obs], tris, x, PARAMS)
+        return time.perf_counter() - t0
+    probe = 4
+    per = max(t_sample(probe) / probe, 1e-6)
+    m = int(min(max(probe, target_s / per), n // 4))
+    t = t_sample(m)
+    t_full = t * n / m
+    return {"value": 1.0 / t_full, "unit": "matvecs/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": ("direct farfield (the reference's CPU-runnable algorithm; its treecode "
+                       "has no CPU path) of %d of %d observation triangles against all "
+                       "sources, oracle restatement FP32 on %d threads, %.1f s, extrapolated "
+                       "to one apply (%.0f s)" % (m, n, os.cpu_count() or 1, t, t_full))}
+
+
+def run_fmm_workload(args, rank, world, torch, dist):
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.fmm.tsfmm import FMMFarfieldOpImpl
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    pts, tris = c4_mesh(args.grid or 707)
+    n = tris.shape[0]
+    idx = np.arange(n)
+    cfg = dict(FMM_CFG)
+    if args.fmm_order is not None:
+        cfg["order"] = args.fmm_order
+    if args.fmm_ppc is not None:
+        cfg["pts_per_cell"] = args.fmm_ppc
+    if args.fmm_mode is not None:
+        cfg["mode"] = args.fmm_mode
+    t0 = time.perf_counter()
+    op = FMMFarfieldOpImpl(1, K_NAME, PARAMS, pts, tris, np.float32, idx, idx, cfg["mac"],
+                           cfg["pts_per_cell"], cfg["order"], cfg["mode"])
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    x = torch.from_numpy(np.random.default_rng(3 + rank).standard_normal(9 * n)
+                         .astype(np.float32)).cuda()
+    y = torch.empty_like(x)
+    for _ in range(args.warmup):
+        op.dot_device(x, y)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        op.dot_device(x, y)
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    # accuracy on sampled rows against the direct farfield
+    sample = np.sort(np.random.default_rng(7).choice(n, 2048, replace=False))
+    d = TriToTriDirectFarfieldOp(1, K_NAME, PARAMS, pts, tris, np.float32, sample, idx)
+    yd = torch.empty(9 * sample.shape[0], dtype=torch.float32, device="cuda")
+    d.dot_device(x, yd)
+    rows = (sample[:, None] * 9 + np.arange(9)).reshape(-1)
+    ref = yd.double().cpu().numpy()
+    err = float(np.linalg.norm(y.double().cpu().numpy()[rows] - ref) / np.linalg.norm(ref))
+    del d
+    # e2e through the public API with host arrays
+    xh = x.cpu().numpy()
+    op.dot(xh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        yh = op.dot(xh)
+    t_e2e = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    if rank != 0:
+        return
+    flops, p2p_pairs, m2l_flops = fmm_algorithmic_flops(op.fmm, op.fmm.nq)
+    peak_ffma, peak_ffma2 = fp32_peak_tflops(torch, _lib.lib)
+    peak = max(peak_ffma, peak_ffma2)
+    achieved = flops / (ms * 1e-3) / 1e12
+    n_launch = 8 + op.fmm.src_desc.n_levels + op.fmm.obs_desc.n_levels
+    line = {
+        "metric": "BEM farfield matvecs/s (FMM)", "value": world * args.steps / (total_ms * 1e-3),
+        "unit": "matvecs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded mesh and inputs)",
+        "config": {"workload": ("FMM farfield of the 1M-triangle topographic surface + "
+                                "dipping thrust fault (%d triangles), elasticRH3, 3-point "
+                                "rule, FMMFarfieldOp(mac=%g, pts_per_cell=%d, order=%d, "
+                                "mode=%s)" % (n, cfg["mac"], cfg["pts_per_cell"],
+                                              cfg["order"], cfg["mode"])),
+                   "n_tris": int(n), "dof": int(9 * n), "p2p_leaf_pairs":
+                   int(op.fmm.p2p.src_n_idxs.shape[0]), "m2l_pairs":
+                   int(op.fmm.m2l.src_n_idxs.shape[0]), "m2p_pairs":
+                   int(op.fmm.m2p.src_n_idxs.shape[0]), "tree_nodes": int(op.fmm.src_tree.n_nodes),
+                   "setup_s": t_build, "rel_err_vs_direct_2048_rows": err,
+                   "l2": "inputs larger than L2 (workspace %.0f MB per apply)"
+                         % (op.fmm.ws_bytes / 1e6), "parallelism": "replicas"},
+        "roofline": {"kernel": "whole FMM apply (P2P + M2L dominate)", "bound": "fp32",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured live: best FP32 FMA probe (scalar %.1f, packed "
+                                    "%.1f TFLOP/s)" % (peak_ffma, peak_ffma2),
+                     "algorithmic": "%.3e flops per apply: %.3e P2P point pairs x 36 + M2L "
+                                    "%.3e" % (flops, p2p_pairs, m2l_flops)},
+        "e2e": {"value": world * args.steps / t_e2e, "unit": "matvecs/s",
+                "h2d_bytes_per_step": int(xh.nbytes), "d2h_bytes_per_step": int(yh.nbytes),
+                "api": "FMMFarfieldOpImpl.dot(numpy float32) -> numpy"},
+        "gpu_launches": args.steps * n_launch,
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_direct_far_baseline(pts, tris)
+    print(json.dumps(line), flush=True)
+
+
+def c1_mesh():
+    """The small plain-method configuration: make_rect(20, 20) over [-1, 1]^2
+    (722 triangles, 6,498 DOF)."""
+    from tectosaur_b200.mesh.mesh_gen import make_rect
+    return make_rect(20, 20, [[-1, -1, 0], [-1, 1, 0], [1, 1, 0], [1, -1, 0]])
+
+
+C1_NQ = (6, 6, 6, 2, 5, 2.5)
+
+
+def cpu_solve_baseline(pts, tris, cm, rhs, tol):
+    """scipy GMRES (restart 200) on the host driving the oracle restatement
+    of the FP64 operator (nearfield blocks assembled once, untimed; farfield
+    recomputed per matvec on all host threads): the reference's
+    examples/solve.py:25-61 algorithm on the host cores."""
+    import scipy.sparse
+    import scipy.sparse.linalg
+    from oracle import oracle as orc
+    from tectosaur_b200.nearfield import triangle_rules as trr
+    from tectosaur_b200.nearfield.nearfield_op import nearfield_pairs
+    from tectosaur_b200.util.quadrature import gauss2d_tri, gauss4d_tri
+    nq_co, nq_ea, nq_va, nq_far, nq_near, thr = C1_NQ
+    n = tris.shape[0]
+    idx = np.arange(n)
+    cl = nearfield_pairs(pts, tris, idx, idx, thr)
+    rules = {"co": (trr.coincident_quad(nq_co), False, True),
+             "ea": (trr.edge_adj_quad(nq_ea), True, True),
+             "va": (trr.vertex_adj_quad(nq_va, nq_va, nq_va), True, True),
+             "near": (gauss4d_tri(nq_near, nq_near), False, False)}
+    far4 = gauss4d_tri(nq_far, nq_far)
+    rows, cols, vals = [], [], []
+    for c, (rule, adj, check0) in rules.items():
+        recs, dofs = cl[c]
+        b = orc.pairs(K_NAME, np.float64, rule, pts, tris, recs[:, :5 if adj else 2], PARAMS,
+                      adj=adj, check0=check0)
+        b = b - orc.pairs(K_NAME, np.float64, far4, pts, tris, recs[:, :2], PARAMS,
+                          check0=(c == "co"))
+        b = b.reshape(-1, 9, 9)
+        r = np.broadcast_to(dofs[:, 0][:, None, None] * 9 + np.arange(9)[None, :, None], b.shape)
+        cc = np.broadcast_to(dofs[:, 1][:, None, None] * 9 + np.arange(9)[None, None, :], b.shape)
+        rows.append(r.reshape(-1))
+        cols.append(cc.reshape(-1))
+        vals.append(b.reshape(-1))
+    near = scipy.sparse.csr_matrix((np.concatenate(vals), (np.concatenate(rows),
+                                    np.concatenate(cols))), shape=(9 * n, 9 * n))
+    q = gauss2d_tri(nq_far)
+    cmT = cm.T.tocsr()
+
+    def mv(v):
+        u = cm @ v
+        return cmT @ (orc.farfield_tris(K_NAME, np.float64, q, pts, tris, tris, u, PARAMS) +
+                      near @ u)
+    m = cm.shape[1]
+    A = scipy.sparse.linalg.LinearOperator((m, m), matvec=mv)
+    count = [0]
+
+    def cb(_):
+        count[0] += 1
+    t0 = time.perf_counter()
+    scipy.sparse.linalg.gmres(A, cmT @ rhs, rtol=tol, restart=200, callback=cb,
+                              callback_type="pr_norm")
+    t = time.perf_counter() - t0
+    return {"value": 1.0 / t, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": ("one full solve: scipy GMRES (restart 200, rtol %g, %d iterations) on "
+                       "the host with the oracle restatement of the FP64 operator (farfield "
+                       "per matvec on %d threads, nearfield blocks assembled beforehand), "
+                       "%.2f s" % (tol, count[0], os.cpu_count() or 1, t))}
+
+
+def run_solve_workload(args, rank, world, torch, dist):
+    import tectosaur_b200 as tct
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    from tectosaur_b200.simple_solver import (ConstrainedOperator, free_edge_vertices, gmres,
+                                              iterative_solve, shared_vertex_matrix)
+    tol = 1e-8
+    pts, tris = c1_mesh()
+    n = tris.shape[0]
+    op = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris, np.float64,
+                                         TriToTriDirectFarfieldOp)
+    cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+    rhs = np.random.default_rng(1 + rank).standard_normal(9 * n)
+    cop = ConstrainedOperator(op, cm)
+    b = torch.empty(cm.shape[1], dtype=torch.float64, device="cuda")
+    cop.cmT.dot_device(torch.from_numpy(rhs).cuda(), b)
+    # one matvec of the seeded slip vector (seed 0), then the solves
+    xs = torch.from_numpy(np.random.default_rng(0).standard_normal(9 * n)).cuda()
+    ys = torch.empty_like(xs)
+    op.dot_device(xs, ys)
+    for _ in range(args.warmup):
+        gmres(cop, b, tol=tol, restart=200)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    lat, iters = [], []
+    cop.n_matvecs = 0
+    a = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        x, info, it, _ = gmres(cop, b, tol=tol, restart=200)
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t0)
+        iters.append(it)
+    e.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = a.elapsed_time(e)
+    if dist is not None:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    # e2e: the public drop-in with host arrays
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        u = iterative_solve(op, cm, rhs, cfg=dict(solver_tol=tol))
+    t_e2e = time.perf_counter() - t0
+    if rank != 0:
+        return
+    ms = total_ms / args.steps
+    it_mean = float(np.mean(iters))
+    nnzb = op.nearfield.bsr.nnzb
+    m = cm.shape[1]
+    # bytes one GMRES step must move: nearfield blocks + x/y, and the two
+    # classical Gram-Schmidt passes over the basis (read twice each)
+    avg_basis = min(it_mean, 200) / 2.0 + 1
+    bytes_step = nnzb * (81 * 8 + 4) + 2 * 9 * n * 8 + 4 * avg_basis * m * 8
+    achieved = bytes_step * it_mean / (ms * 1e-3) / 1e9
+    mp = measured_peaks()
+    hbm = mp.get("hbm_gbs") if mp else 6650.0
+    line = {
+        "metric": "BEM solves/s (GMRES to 1e-8)", "value": world * args.steps / (total_ms * 1e-3),
+        "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded mesh and right-hand sides)",
+        "config": {"workload": ("plain FP64 solve: make_rect(20, 20) over [-1, 1]^2 (722 "
+                                "triangles, 6,498 DOF), RegularizedSparseIntegralOp(6, 6, 6, 2, "
+                                "5, 2.5, elasticRH3) with the direct farfield, vertex continuity + "
+                                "zero slip on the free edges, GMRES(200) to 1e-8 for a N(0, 1) "
+                                "traction"),
+                   "n_tris": int(n), "dof": int(9 * n), "free_dof": int(m),
+                   "gmres_iterations": it_mean, "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+                   "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)),
+                   "l2": "small problem: working set fits in L2 (latency-bound solve)",
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "whole GMRES step (operator apply + CGS2 orthogonalisation)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json" if mp else "fallback",
+                     "algorithmic": "%.3e bytes per GMRES step" % bytes_step},
+        "e2e": {"value": args.steps / t_e2e, "unit": "solves/s",
+                "h2d_bytes_per_step": int(rhs.nbytes), "d2h_bytes_per_step": int(u.nbytes),
+                "api": "simple_solver.iterative_solve(op, cm, numpy rhs) -> numpy"},
+        "gpu_launches": int(args.steps * it_mean * 6),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_solve_baseline(pts, tris, cm, rhs, tol)
+    print(json.dumps(line), flush=True)
+
+
 def config_block(n_tris, nnzb):
     return {
         "workload": ("direct-farfield 60k-triangle topographic surface (174x174 grid over "
@@ -271,9 +613,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--grid", type=int, default=174,
+    ap.add_argument("--grid", type=int, default=None,
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
-                         "workload; smaller for profiling)")
+                         "workload; smaller for profiling; the fmm workload uses 707)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "fmm", "solve"],
+                    help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
+                         "farfield; solve: the 722-triangle FP64 GMRES solve")
+    ap.add_argument("--fmm-order", type=int, default=None)
+    ap.add_argument("--fmm-ppc", type=int, default=None)
+    ap.add_argument("--fmm-mode", default=None, choices=["fmm", "treecode"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -294,8 +642,16 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
+    if args.workload in ("fmm", "solve"):
+        (run_fmm_workload if args.workload == "fmm" else run_solve_workload)(
+            args, rank, world, torch, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     from tectosaur_b200 import _lib
-    pts, tris = c2_mesh(args.grid)
+    pts, tris = c2_mesh(args.grid or 174)
     t_build = time.perf_counter()
     op = build_op(pts, tris)
     torch.cuda.synchronize()

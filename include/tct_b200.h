@@ -328,6 +328,15 @@ int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
                    void* out, int accumulate, void* workspace, size_t workspace_bytes,
                    void* stream);
 
+/* ---- constrained solve -------------------------------------------------- */
+
+/* y (+)= A x for a CSR matrix with double values (device): the constraint
+ * matrix cm or its transpose in the constrained GMRES; replaces the host
+ * csr_matrix.dot calls of examples/solve.py:44-49 and
+ * simple_solver.py:18-22.  x, y Real according to prec. */
+int tct_csr_matvec(int prec, int64_t n_rows, const int64_t* indptr, const int64_t* indices,
+                   const double* data, const void* x, void* y, int accumulate, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

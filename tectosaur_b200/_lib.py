@@ -171,3 +171,12 @@ for _name, (_args, _res) in _FMM_SIGS.items():
     _f.argtypes = _args
     _f.restype = _res
 EXPORTED = sorted(set(EXPORTED) | set(_FMM_SIGS))
+
+_SOLVE_SIGS = {
+    "tct_csr_matvec": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_p, c_i, c_p], c_i),
+}
+for _name, (_args, _res) in _SOLVE_SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+EXPORTED = sorted(set(EXPORTED) | set(_SOLVE_SIGS))
