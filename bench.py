@@ -310,7 +310,7 @@ def cpu_direct_far_baseline(pts, tris, target_s=10.0):
         t0 = time.perf_counter()
         orc.farfield_tris(K_NAME, np.float32, q, pts, tris[obs], tris, x, PARAMS)
         return time.perf_counter() - t0
-    probe = 4
+    probe = 16
     per = max(t_sample(probe) / probe, 1e-6)
     m = int(min(max(probe, target_s / per), n // 4))
     t = t_sample(m)
