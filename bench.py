@@ -594,6 +594,347 @@ def run_solve_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+# ---- C3: batched singular / near-singular pair quadrature --------------------
+# (singular-class kernel, near-class kernel) per family
+C3_FAMILIES = [("elasticU3", "elasticU3"), ("elasticRT3", "elasticT3"),
+               ("elasticRA3", "elasticA3"), ("elasticRH3", "elasticH3")]
+# FP64 flops per quadrature point of this build's pair integrand
+# (csrc/pair_math.cuh, FMA = 2): 42 shared (two barycentric points, D, r^2)
+# + the kernel's tensor/separable form + the 81-output accumulation
+# (U 241, T/A 283, H 361, RT/RA 971 -- the Levi-Civita surface-curl
+# contraction -- and RH 63, whose separable form keeps 7 sums instead of 81).
+PAIR_POINT_FLOPS = {"elasticU3": 241, "elasticT3": 283, "elasticA3": 283, "elasticH3": 361,
+                    "elasticRT3": 971, "elasticRA3": 971, "elasticRH3": 63}
+
+
+def _rand_planar_tris(rng, m, max_aspect=5.0):
+    """m random triangles in 2-D with v0 at the origin, v1 on +x: edge lengths
+    U[0.5, 2], aspect (longest edge / shortest altitude) <= max_aspect."""
+    out = np.zeros((m, 3, 2))
+    todo = np.arange(m)
+    while todo.size:
+        k = todo.size
+        L1, L2 = rng.uniform(0.5, 2.0, k), rng.uniform(0.5, 2.0, k)
+        th = rng.uniform(np.radians(20), np.radians(160), k)
+        v2 = np.stack([L2 * np.cos(th), L2 * np.sin(th)], axis=1)
+        L3 = np.hypot(v2[:, 0] - L1, v2[:, 1])
+        area = 0.5 * L1 * v2[:, 1]
+        longest = np.maximum(np.maximum(L1, L2), L3)
+        ok = (L3 >= 0.5) & (L3 <= 2.0) & (longest ** 2 / (2 * area) <= max_aspect)
+        good = todo[ok]
+        out[good, 1, 0] = L1[ok]
+        out[good, 2] = v2[ok]
+        todo = todo[~ok]
+    return out
+
+
+def c3_pairs(n_pairs=400_000, seed=4):
+    """Seeded random triangle pairs: 10 % coincident / 30 % edge-adjacent /
+    30 % vertex-adjacent / 30 % separate (parallel, gap U[0.01, 1] x mean edge),
+    edge lengths U[0.5, 2], aspect <= 5; per pair a quadrature order U{3..20},
+    a kernel family (U / T / A / H, the singular classes taking the
+    regularized RT / RA / RH) and nu in {0.25, 0.35}.  Returns the mesh and
+    per-class records in the operator's pair-record format."""
+    from tectosaur_b200.mesh.find_near_adj import split_adjacent_close
+    from tectosaur_b200.nearfield.nearfield_op import resolve_ea_rotation
+    rng = np.random.default_rng(seed)
+    n = n_pairs
+    cls = rng.choice(4, size=n, p=[0.1, 0.3, 0.3, 0.3])  # co, ea, va, near
+    fam = rng.integers(0, 4, n)
+    nq = rng.integers(3, 21, n)
+    nu_id = rng.integers(0, 2, n)
+    # a random orthonormal frame per pair
+    nrm = rng.standard_normal((n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+    a = rng.standard_normal((n, 3))
+    e1 = np.cross(nrm, a)
+    e1 /= np.linalg.norm(e1, axis=1)[:, None]
+    e2 = np.cross(nrm, e1)
+    centre = np.stack([(np.arange(n) % 1000) * 20.0, (np.arange(n) // 1000) * 20.0,
+                       np.zeros(n)], axis=1)
+
+    def place(p2, z=0.0):  # (m, 2) in-plane coordinates (+ normal offset) -> 3-D
+        return centre + p2[:, :1] * e1 + p2[:, 1:2] * e2 + np.asarray(z).reshape(-1, 1) * nrm
+
+    t1 = _rand_planar_tris(rng, n)
+    v = [place(t1[:, k]) for k in range(3)]
+    extra = []
+    # edge-adjacent: across edge v0 v1, tilted about it by a dihedral angle
+    t2 = _rand_planar_tris(rng, n)
+    xm = rng.uniform(0.25, 0.75, n) * t1[:, 1, 0]
+    h = np.abs(t2[:, 2, 1])
+    phi = rng.uniform(-np.radians(80), np.radians(80), n)
+    v3 = centre + xm[:, None] * e1 - (h * np.cos(phi))[:, None] * e2 + (h * np.sin(phi))[:, None] * nrm
+    # vertex-adjacent: a second triangle at v0 in the other half-plane, tilted
+    t3 = _rand_planar_tris(rng, n)
+    th3 = np.arctan2(t3[:, 2, 1], t3[:, 2, 0])
+    psi = np.pi + 0.2 + rng.uniform(0, 1, n) * (np.pi - 0.4 - th3)
+    rot = lambda p, ang: np.stack([p[:, 0] * np.cos(ang) - p[:, 1] * np.sin(ang),
+                                   p[:, 0] * np.sin(ang) + p[:, 1] * np.cos(ang)], axis=1)
+    tilt = rng.uniform(-np.radians(60), np.radians(60), n)
+    def tilted(p):
+        q = rot(p, psi)
+        return centre + q[:, :1] * e1 + (q[:, 1] * np.cos(tilt))[:, None] * e2 + \
+            (q[:, 1] * np.sin(tilt))[:, None] * nrm
+    v4, v5 = tilted(t3[:, 1]), tilted(t3[:, 2])
+    # separate: a parallel triangle at a small gap
+    t4 = _rand_planar_tris(rng, n)
+    mean_edge = (t1[:, 1, 0] + np.hypot(*t1[:, 2].T) + np.hypot(t1[:, 2, 0] - t1[:, 1, 0],
+                                                               t1[:, 2, 1])) / 3
+    gap = rng.uniform(0.01, 1.0, n) * mean_edge
+    ang = rng.uniform(0, 2 * np.pi, n)
+    shift = rng.uniform(-0.3, 0.3, (n, 2))
+    w = [place(rot(t4[:, k], ang) + shift, gap) for k in range(3)]
+    pts, tris, t1_idx, t2_idx = [], [], np.zeros(n, np.int64), np.zeros(n, np.int64)
+    base = 0
+    # vectorised assembly, pair by class
+    nv = np.array([3, 4, 5, 6])[cls]
+    start = np.concatenate([[0], np.cumsum(nv)])[:-1]
+    P = np.zeros((int(nv.sum()), 3))
+    for k in range(3):
+        P[start + k] = v[k]
+    co, ea, va, nr = (cls == 0), (cls == 1), (cls == 2), (cls == 3)
+    P[start[ea] + 3] = v3[ea]
+    P[start[va] + 3] = v4[va]
+    P[start[va] + 4] = v5[va]
+    for k in range(3):
+        P[start[nr] + 3 + k] = w[k][nr]
+    ntri = np.where(co, 1, 2)
+    tstart = np.concatenate([[0], np.cumsum(ntri)])[:-1]
+    T = np.zeros((int(ntri.sum()), 3), np.int64)
+    T[tstart] = start[:, None] + np.arange(3)
+    T[tstart[ea] + 1] = np.stack([start[ea] + 1, start[ea], start[ea] + 3], axis=1)
+    T[tstart[va] + 1] = np.stack([start[va], start[va] + 3, start[va] + 4], axis=1)
+    T[tstart[nr] + 1] = start[nr][:, None] + 3 + np.arange(3)
+    t1_idx = tstart
+    t2_idx = np.where(co, tstart, tstart + 1)
+    close = np.stack([t1_idx[~co], t2_idx[~co]], axis=1)
+    near_d, va_d, ea_d = split_adjacent_close(close, T, T)
+    ea_rec = resolve_ea_rotation(T, ea_d)
+    va_rec = np.hstack([va_d[:, :4], np.zeros((va_d.shape[0], 1), np.int64)])
+    near_rec = np.hstack([near_d[:, :2], np.zeros((near_d.shape[0], 3), np.int64)])
+    co_rec = np.stack([t1_idx[co], t1_idx[co]] + [np.zeros(int(co.sum()), np.int64)] * 3, axis=1)
+    pair_of_tri = np.zeros(T.shape[0], np.int64)
+    pair_of_tri[t1_idx] = np.arange(n)
+    recs = {"co": co_rec, "ea": ea_rec, "va": va_rec, "near": near_rec}
+    owner = {c: pair_of_tri[r[:, 0]] for c, r in recs.items()}
+    return P, T, recs, owner, dict(cls=cls, fam=fam, nq=nq, nu_id=nu_id)
+
+
+def c3_rule(kind, nq):
+    from tectosaur_b200.nearfield import triangle_rules as trr
+    from tectosaur_b200.util.quadrature import gauss4d_tri
+    if kind == "co":
+        return (*trr.coincident_quad(nq), False, True)
+    if kind == "ea":
+        return (*trr.edge_adj_quad(nq), True, True)
+    if kind == "va":
+        return (*trr.vertex_adj_quad(nq, nq, nq), True, True)
+    return (*gauss4d_tri(nq, nq), False, False)
+
+
+def c3_groups(recs, owner, attr):
+    """Per kernel: records, rule ids into a per-kernel rule list, nu ids."""
+    groups = {}
+    for kind, r in recs.items():
+        o = owner[kind]
+        for f, (ks, kn) in enumerate(C3_FAMILIES):
+            K = kn if kind == "near" else ks
+            sel = attr["fam"][o] == f
+            if not sel.any():
+                continue
+            g = groups.setdefault(K, dict(recs=[], keys=[], nu=[]))
+            g["recs"].append(r[sel])
+            g["keys"].append(np.stack([np.full(int(sel.sum()), ["co", "ea", "va", "near"].index(kind)),
+                                       attr["nq"][o[sel]]], axis=1))
+            g["nu"].append(attr["nu_id"][o[sel]])
+    out = {}
+    for K, g in groups.items():
+        keys = np.concatenate(g["keys"])
+        uk, rid = np.unique(keys, axis=0, return_inverse=True)
+        rules = [c3_rule(["co", "ea", "va", "near"][k], int(q)) for k, q in uk]
+        out[K] = dict(recs=np.concatenate(g["recs"]), rule_ids=rid.reshape(-1), rules=rules,
+                      nu=np.concatenate(g["nu"]))
+    return out
+
+
+def fp64_peak_tflops(torch, lib):
+    from tectosaur_b200 import _lib
+    out = torch.empty(256, dtype=torch.float64, device="cuda")
+    n_blocks, iters = 148 * 16, 2048
+    for _ in range(2):
+        _lib.check(lib.tct_fp64_fma_probe(_lib.tptr(out), n_blocks, iters, _lib.stream_ptr()),
+                   "fp64 probe")
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        _lib.check(lib.tct_fp64_fma_probe(_lib.tptr(out), n_blocks, iters, _lib.stream_ptr()),
+                   "fp64 probe")
+        b.record()
+        b.synchronize()
+        best = max(best, n_blocks * 256.0 * iters * 16 / (a.elapsed_time(b) * 1e-3) / 1e12)
+    return best
+
+
+def cpu_pairs_baseline(P, T, groups, flops_total, target_s=12.0):
+    """The oracle restatement of the reference's pair kernels (FP64, all host
+    threads) on a random sample of each kernel's pairs, extrapolated to the
+    whole workload by algorithmic flops."""
+    from oracle import oracle as orc
+    rng = np.random.default_rng(12)
+    psets = np.array([[1.0, 0.25], [1.0, 0.35]])
+
+    def run(frac):
+        t_all, fl = 0.0, 0.0
+        for K, g in groups.items():
+            m = max(1, int(frac * g["recs"].shape[0]))
+            pick = rng.choice(g["recs"].shape[0], m, replace=False)
+            # one oracle call per (rule, nu) group, so its OpenMP loop has pairs to share
+            key = g["rule_ids"][pick] * 2 + g["nu"][pick]
+            for k in np.unique(key):
+                sel = pick[key == k]
+                pts4, wts, adj, c0 = g["rules"][g["rule_ids"][sel[0]]]
+                t0 = time.perf_counter()
+                orc.pairs(K, np.float64, (pts4, wts), P, T, g["recs"][sel, :5 if adj else 2],
+                          psets[g["nu"][sel[0]]], adj=adj, check0=c0)
+                t_all += time.perf_counter() - t0
+                fl += sel.size * wts.shape[0] * PAIR_POINT_FLOPS[K]
+        return t_all, fl
+    t, fl = run(2e-5)
+    frac = min(2e-5 * target_s / max(t, 1e-3), 1e-2)
+    t, fl = run(frac)
+    t_full = t * flops_total / fl
+    n = sum(g["recs"].shape[0] for g in groups.values())
+    return {"value": n / t_full, "unit": "pairs/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": ("oracle restatement of the reference's pair kernels (FP64, OpenMP all "
+                       "threads) on %.2g of each kernel's pairs (%.1f s), extrapolated by "
+                       "algorithmic flops to the %d-pair workload (%.0f s)"
+                       % (frac, t, n, t_full))}
+
+
+def run_pairs_workload(args, rank, world, torch, dist):
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.nearfield.pairs_integrator import PairsIntegrator
+    from tectosaur_b200.util.sparse import DeviceBSR9, make_bsr_index
+    n_pairs = args.pairs
+    t0 = time.perf_counter()
+    P, T, recs, owner, attr = c3_pairs(n_pairs, seed=4 + rank)
+    groups = c3_groups(recs, owner, attr)
+    psets = np.array([[1.0, 0.25], [1.0, 0.35]])
+    runs, flops, points = [], 0.0, 0
+    for K, g in groups.items():
+        pi = PairsIntegrator(K, psets[0], np.float64, 2, 2, P, T)
+        plan = pi.batched_plan(g["recs"], g["rule_ids"], g["rules"], g["nu"], psets)
+        out = torch.empty(plan["n"] * 81, dtype=torch.float64, device="cuda")
+        runs.append((pi, plan, out, K))
+        sizes = np.array([r[0].shape[0] for r in g["rules"]])[g["rule_ids"]]
+        points += int(sizes.sum())
+        flops += float(sizes.sum()) * PAIR_POINT_FLOPS[K]
+    t_setup = time.perf_counter() - t0
+
+    def step():
+        for pi, plan, out, _ in runs:
+            pi.batched_run(plan, out)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    # BSR matvec on the assembled blocks (rows = obs triangle, cols = source)
+    allrec = np.concatenate([g["recs"] for g in groups.values()])
+    blocks = torch.cat([out for _, _, out, _ in runs]).view(-1, 81)
+    n_tri = T.shape[0]
+    indptr, indices, slot = make_bsr_index(n_tri, allrec[:, 0], allrec[:, 1])
+    bsr = DeviceBSR9((9 * n_tri, 9 * n_tri), indptr, indices, np.float64)
+    order = torch.from_numpy(np.argsort(slot)).cuda()
+    bsr.data.view(81, -1)[:, :blocks.shape[0]] = blocks.index_select(0, order).t()
+    xb = torch.from_numpy(np.random.default_rng(5).standard_normal(9 * n_tri)).cuda()
+    yb = torch.empty_like(xb)
+    for _ in range(3):
+        bsr.matvec(xb, yb)
+    torch.cuda.synchronize()
+    c = torch.cuda.Event(enable_timing=True)
+    d = torch.cuda.Event(enable_timing=True)
+    c.record()
+    for _ in range(20):
+        bsr.matvec(xb, yb)
+    d.record()
+    torch.cuda.synchronize()
+    bsr_ms = c.elapsed_time(d) / 20
+    nnzb = bsr.nnzb
+    bsr_bytes = nnzb * (81 * 8 + 4) + (n_tri + 1) * 4 + 2 * 9 * n_tri * 8
+    # e2e: the public per-call API (plan + upload + launch + copy out)
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 2))):
+        for K, g in groups.items():
+            pi = [r[0] for r in runs if r[3] == K][0]
+            hb = pi.batched(g["recs"], g["rule_ids"], g["rules"], g["nu"], psets)
+    k_e2e = max(1, min(args.steps, 2))
+    t_e2e = (time.perf_counter() - t0) / k_e2e
+    if rank != 0:
+        return
+    peak64 = fp64_peak_tflops(torch, _lib.lib)
+    achieved = flops / (ms * 1e-3) / 1e12
+    mp = measured_peaks()
+    hbm = mp.get("hbm_gbs") if mp else 6650.0
+    line = {
+        "metric": "pair integrals/s (batched singular quadrature)",
+        "value": world * n_pairs / (ms * 1e-3), "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded random triangle pairs)",
+        "config": {"workload": ("%d seeded random triangle pairs (10 %% coincident, 30 %% "
+                                "edge-adjacent, 30 %% vertex-adjacent, 30 %% separate with gap "
+                                "U[0.01, 1] x edge; edges U[0.5, 2], aspect <= 5), order "
+                                "U{3..20} per pair, kernels U/T/A/H (RT/RA/RH for the singular "
+                                "classes), nu in {0.25, 0.35}, FP64, %d batched launches "
+                                "(one per kernel)" % (n_pairs, len(runs))),
+                   "quadrature_points": points, "setup_s": t_setup,
+                   "bsr": {"blocks": int(nnzb), "ms": bsr_ms, "bytes": int(bsr_bytes),
+                           "achieved_gbs": bsr_bytes / (bsr_ms * 1e-3) / 1e9,
+                           "blocks_per_s": nnzb / (bsr_ms * 1e-3), "hbm_peak_gbs": hbm},
+                   "l2": "inputs larger than L2 (blocks %.0f MB per step)" % (n_pairs * 648 / 1e6),
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "pairs_batched<double, K> (all kernels of the step)",
+                     "bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                     "frac": achieved / peak64, "traffic": None,
+                     "peak_source": "measured live: FP64 FMA probe (tct_fp64_fma_probe)",
+                     "algorithmic": "%.3e flops per step = %.3e quadrature points x per-kernel "
+                                    "point flops" % (flops, points)},
+        "e2e": {"value": n_pairs / t_e2e, "unit": "pairs/s",
+                "h2d_bytes_per_step": int(sum(g["recs"].nbytes for g in groups.values())),
+                "d2h_bytes_per_step": int(n_pairs * 81 * 8),
+                "api": "PairsIntegrator.batched(records, rule_ids, rules, nu ids, params) -> "
+                       "numpy blocks, per kernel"},
+        "gpu_launches": args.steps * len(runs),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_pairs_baseline(P, T, groups, flops)
+    print(json.dumps(line), flush=True)
+
+
 def config_block(n_tris, nnzb):
     return {
         "workload": ("direct-farfield 60k-triangle topographic surface (174x174 grid over "
@@ -616,9 +957,11 @@ def main():
     ap.add_argument("--grid", type=int, default=None,
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "fmm", "solve"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "fmm", "solve", "pairs"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
-                         "farfield; solve: the 722-triangle FP64 GMRES solve")
+                         "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
+                         "400k-pair batched singular quadrature + BSR matvec")
+    ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--fmm-order", type=int, default=None)
     ap.add_argument("--fmm-ppc", type=int, default=None)
     ap.add_argument("--fmm-mode", default=None, choices=["fmm", "treecode"])
@@ -642,9 +985,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve"):
-        (run_fmm_workload if args.workload == "fmm" else run_solve_workload)(
-            args, rank, world, torch, dist)
+    if args.workload in ("fmm", "solve", "pairs"):
+        {"fmm": run_fmm_workload, "solve": run_solve_workload,
+         "pairs": run_pairs_workload}[args.workload](args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()

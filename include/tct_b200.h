@@ -171,6 +171,8 @@ int tct_fp32_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
 /* Same with packed fma.rn.f32x2 (2 FMAs per instruction, 32 * iters flops per
  * thread). */
 int tct_fp32x2_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
+/* FP64 FMA throughput probe: n_blocks x 256 threads x iters x 8 fma.rn.f64. */
+int tct_fp64_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Allocation-free farfield matvec (no counterpart in the reference).        */

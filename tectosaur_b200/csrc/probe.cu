@@ -1,5 +1,6 @@
-// FP32 FMA-throughput probe: the denominator of the farfield kernel's
-// roofline (an FP32 CUDA-core kernel; no library peak covers that pipe).
+// FMA-throughput probes: the denominators of the CUDA-core kernels'
+// rooflines (FP32 farfield, FP64 pair quadrature; no library peak covers
+// those pipes).
 // Each thread runs 8 independent FMA chains so the pipe, not latency, bounds it.
 #include "common.cuh"
 
@@ -50,8 +51,32 @@ __global__ void __launch_bounds__(256) fma2_probe(float* out, int iters, float s
     if (s == 12345.678f) out[threadIdx.x] = s;
 }
 
+// FP64 variant: the denominator of the FP64 pair-quadrature roofline.
+__global__ void __launch_bounds__(256) dfma_probe(double* out, int iters, double seed) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + 0.001 * (threadIdx.x + k);
+    const double m = 0.999999999, c = 1e-12;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = fma(a[k], m, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == 12345.678) out[threadIdx.x] = s;
+}
+
 }  // namespace
 }  // namespace tct
+
+extern "C" int tct_fp64_fma_probe(void* out, int64_t n_blocks, int iters, void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(out && n_blocks > 0 && n_blocks < (1 << 30) && iters > 0,
+                  "tct_fp64_fma_probe: bad arguments");
+    dfma_probe<<<(unsigned)n_blocks, 256, 0, as_stream(stream)>>>((double*)out, iters, 1.0);
+    return launch_status("tct_fp64_fma_probe");
+}
 
 extern "C" int tct_fp32_fma_probe(void* out, int64_t n_blocks, int iters, void* stream) {
     using namespace tct;

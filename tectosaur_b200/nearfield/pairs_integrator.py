@@ -85,15 +85,14 @@ class PairsIntegrator:
         self.integrate_into(out, rule, device.to_dev(rec), n, adj, check0)
         return out.cpu().numpy().reshape((n, 3, 3, 3, 3))
 
-    def batched_device(self, records, rule_ids, rules, param_set_ids=None, param_sets=None,
-                       chunk=4096, small=768, out=None, stream=None):
-        """All pairs of mixed classes and orders in one persistent launch.
+    def batched_plan(self, records, rule_ids, rules, param_set_ids=None, param_sets=None,
+                     chunk=4096, small=768):
+        """Work plan of one batched launch, uploaded to the device once.
 
         records: (n, 5) int (obs, src, obs_clicks, src_clicks, src_flip);
         rule_ids: (n,) index into `rules`, a list of (pts (m, 4), wts (m,),
         adjacent, check0); param_set_ids: (n,) index into `param_sets`
         ((k, 2) [mu, nu], k <= 8; default: this integrator's params).
-        Returns the (n * 81) device array of blocks (before any correction).
         Work schedule: pairs whose rule has <= `small` points are whole-pair
         thread items; larger ones are cut into warp items of <= `chunk`
         points; each queue is ordered by decreasing size."""
@@ -130,18 +129,36 @@ class PairsIntegrator:
         titems = np.stack([tp, np.zeros_like(tp), psize[tp], np.zeros_like(tp)], axis=1)
         items = np.ascontiguousarray(np.concatenate([witems, titems]).astype(np.int32))
         ft = self.float_type
-        out = out if out is not None else device.empty(max(n * 81, 1), ft)
-        ws = device.workspace(2048)
-        dev = [device.to_dev(rec7), device.to_dev(rule_off), device.to_dev(rule_flags),
-               device.to_dev(pts_all, ft), device.to_dev(wts_all, ft),
-               device.to_dev(items if items.size else np.zeros((1, 4), np.int32))]
+        plan = dict(n=n, n_warp=witems.shape[0], n_thread=titems.shape[0],
+                    param_sets=param_sets, n_points=int(psize.sum()),
+                    ws=device.workspace(2048),
+                    dev=[device.to_dev(rec7), device.to_dev(rule_off),
+                         device.to_dev(rule_flags), device.to_dev(pts_all, ft),
+                         device.to_dev(wts_all, ft),
+                         device.to_dev(items if items.size else np.zeros((1, 4), np.int32))])
+        return plan
+
+    def batched_run(self, plan, out=None, stream=None):
+        """Launch a batched plan: out (n * 81 device array, allocated when
+        None) receives the blocks (before any correction)."""
+        out = out if out is not None else device.empty(max(plan["n"] * 81, 1), self.float_type)
+        d = plan["dev"]
         _lib.check(_lib.lib.tct_pairs_integrate_batched(
-            self.kid, self.prec, _lib.tptr(out), n, _lib.tptr(self.gpu_pts),
-            _lib.tptr(self.gpu_tris), _lib.tptr(dev[0]), _lib.tptr(dev[1]), _lib.tptr(dev[2]),
-            _lib.tptr(dev[3]), _lib.tptr(dev[4]), _lib.tptr(dev[5]), witems.shape[0],
-            titems.shape[0], _lib.dptr(param_sets), param_sets.shape[0], 0, _lib.tptr(ws), 2048,
-            _lib.stream_ptr(stream)), "tct_pairs_integrate_batched")
-        self._batched_keepalive = dev + [ws]
+            self.kid, self.prec, _lib.tptr(out), plan["n"], _lib.tptr(self.gpu_pts),
+            _lib.tptr(self.gpu_tris), _lib.tptr(d[0]), _lib.tptr(d[1]), _lib.tptr(d[2]),
+            _lib.tptr(d[3]), _lib.tptr(d[4]), _lib.tptr(d[5]), plan["n_warp"],
+            plan["n_thread"], _lib.dptr(plan["param_sets"]), plan["param_sets"].shape[0], 0,
+            _lib.tptr(plan["ws"]), 2048, _lib.stream_ptr(stream)), "tct_pairs_integrate_batched")
+        return out
+
+    def batched_device(self, records, rule_ids, rules, param_set_ids=None, param_sets=None,
+                       chunk=4096, small=768, out=None, stream=None):
+        """All pairs of mixed classes and orders in one persistent launch
+        (plan + run); returns the (n * 81) device array of blocks."""
+        plan = self.batched_plan(records, rule_ids, rules, param_set_ids, param_sets, chunk,
+                                 small)
+        out = self.batched_run(plan, out, stream)
+        self._batched_keepalive = plan
         return out
 
     def batched(self, records, rule_ids, rules, param_set_ids=None, param_sets=None, **kw):

@@ -102,3 +102,25 @@ def test_batched_matches_per_class_launches(cuda):
     got = pi.batched(np.concatenate(recs), np.concatenate(rids), rules)
     want = np.concatenate(per)
     assert rel(got, want) < 1e-12
+
+
+def test_batched_c3_sample_vs_oracle_fp64(cuda, orc):
+    """A sample of the benchmark's random pair workload (all four classes,
+    orders 3..20, seven kernels, two nu values): every pair's 81 values
+    against the oracle."""
+    import bench
+    P, T, recs, owner, attr = bench.c3_pairs(160, seed=21)
+    groups = bench.c3_groups(recs, owner, attr)
+    psets = np.array([[1.0, 0.25], [1.0, 0.35]])
+    checked = 0
+    for K, g in groups.items():
+        pi = PairsIntegrator(K, psets[0], np.float64, 2, 2, P, T)
+        got = pi.batched(g["recs"], g["rule_ids"], g["rules"], g["nu"], psets)
+        for i in range(0, g["recs"].shape[0], 3):
+            pts4, wts, adj, c0 = g["rules"][g["rule_ids"][i]]
+            want = orc.pairs(K, np.float64, (pts4, wts), P, T,
+                             g["recs"][i:i + 1, :5 if adj else 2], psets[g["nu"][i]], adj=adj,
+                             check0=c0)[0]
+            assert rel(got[i], want) < 1e-10, (K, i, rel(got[i], want))
+            checked += 1
+    assert checked > 40
