@@ -400,12 +400,15 @@ int rec_len(int kernel, int nq) {
 }
 
 // Number of source chunks: enough (obs-block, chunk) tiles to cover the 148
-// SMs about eight times, at least one tile of sources per chunk, at most 32.
-// Depends only on the problem size, so the workspace size is device-independent.
-int64_t n_chunks_for(int64_t n_obs, int64_t n_src, int ts) {
+// SMs about eight times, at least CHUNK_GRAIN sources per chunk (chunks need
+// not be whole shared-memory tiles: the main kernels handle a partial last
+// tile), at most 32.  Depends only on the problem size, so the workspace size
+// is device-independent.
+constexpr int64_t CHUNK_GRAIN = 16;
+int64_t n_chunks_for(int64_t n_obs, int64_t n_src, int /*ts*/) {
     const int64_t obs_blocks = (n_obs + 127) / 128;
     int64_t want = (148 * 8 + obs_blocks - 1) / std::max<int64_t>(obs_blocks, 1);
-    int64_t max_by_src = std::max<int64_t>(1, n_src / ts);
+    int64_t max_by_src = std::max<int64_t>(1, n_src / CHUNK_GRAIN);
     return std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, max_by_src), 32));
 }
 
@@ -424,7 +427,8 @@ int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, cons
     int rc = launch_status("farfield prep");
     if (rc) return rc;
     const int64_t chunks = n_chunks_for(n_obs, n_src, TS);
-    const int64_t per_chunk = ((n_src + chunks - 1) / chunks + TS - 1) / TS * TS;
+    const int64_t per_chunk =
+        ((n_src + chunks - 1) / chunks + CHUNK_GRAIN - 1) / CHUNK_GRAIN * CHUNK_GRAIN;
     const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
     const size_t smem = sizeof(R) * L::LEN * TS;
     auto kfn = far_main<R, K, NQ, TS>;
@@ -452,7 +456,7 @@ int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, cons
 int64_t n_chunks_rh2(int64_t n_obs, int64_t n_src) {
     const int64_t obs_blocks = (n_obs + 255) / 256;
     int64_t want = (148 * 8 + obs_blocks - 1) / std::max<int64_t>(obs_blocks, 1);
-    int64_t max_by_src = std::max<int64_t>(1, n_src / 128);
+    int64_t max_by_src = std::max<int64_t>(1, n_src / CHUNK_GRAIN);
     return std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, max_by_src), 32));
 }
 
@@ -478,7 +482,8 @@ int run_far_rh2(const Consts<float>& c, const Rule2D<float>& rule, float* out, c
     int rc = launch_status("farfield prep (RH, packed)");
     if (rc) return rc;
     const int64_t chunks = n_chunks_rh2(n_obs, n_src);
-    const int64_t per_chunk = ((n_src + chunks - 1) / chunks + 127) / 128 * 128;
+    const int64_t per_chunk =
+        ((n_src + chunks - 1) / chunks + CHUNK_GRAIN - 1) / CHUNK_GRAIN * CHUNK_GRAIN;
     const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
     const size_t smem = sizeof(float) * L::LEN * 128;
     auto kfn = far_main_rh2<NQ, UNIFORM>;
