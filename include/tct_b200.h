@@ -330,6 +330,27 @@ int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
                    void* out, int accumulate, void* workspace, size_t workspace_bytes,
                    void* stream);
 
+/* ---- multi-RHS farfield on the tensor cores ------------------------------- */
+
+/* Direct farfield of elasticRH3 (FP32, 3-point rule) applied to a panel of R
+ * input vectors at once: out[r] (+)= Far in[r] for r < R (R = 16 or 32).
+ * The reference applies farfield_tris_to_tris{K} (matrix_free.cl:19-107) to
+ * one vector per call; here the per-triangle-pair kernel scalars are
+ * generated on the CUDA cores and contracted with the input panel by
+ * tcgen05.mma (split TF32, FP32 accumulation in tensor memory).
+ * in: R x (9 n_src) floats, out: R x (9 n_obs) floats (device, vector after
+ * vector); pts / tris as in tct_farfield_tris_matvec. */
+size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R);
+int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
+                                 const int32_t* obs_tris, int64_t n_obs,
+                                 const int32_t* src_tris, int64_t n_src, int R,
+                                 const double* params, int accumulate, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+/* Reads (synchronising the stream) the error word of the last panel apply
+ * with this workspace: 0 = ok, 1 = a bounded wait on the tensor cores gave up. */
+int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
+                                void* stream, int* host_flag);
+
 /* ---- constrained solve -------------------------------------------------- */
 
 /* y (+)= A x for a CSR matrix with double values (device): the constraint

@@ -1,0 +1,564 @@
+// Multi-RHS direct farfield for elasticRH3 (FP32, 3-point rule) on the
+// 5th-generation tensor cores: y_r = Far x_r for a panel of R right-hand
+// sides (the reference applies farfield_tris_to_tris once per vector,
+// tectosaur/matrix_free.cl:19-107).
+//
+// For elasticRH3 the 9 point pairs of a triangle pair reduce to the scalar
+// S0 and the symmetric 3x3 T (the direct kernel's factorisation), and the
+// input enters only through per-source 3x3 matrices P and M = -2 ssc:
+//   W_o[d][j] += S0 P_s[d][j] + sum_k T[d][k] M_s[k][j].
+// With R inputs this is a GEMM:
+//   W[o, (dj, r)] = sum_{s, c} A[o, (s, c)] B[(s, c), (dj, r)]
+// with A = (S0, T00, T01, T02, T11, T12, T22) per triangle pair -- generated
+// on the fly by the CUDA cores, never stored in HBM -- and B built once per
+// apply from the input panel.  Per tile of 128 observation and 8 source
+// triangles: the 128 threads compute A (K = 56) into shared memory, the tile
+// of B is copied in, and one thread issues tcgen05.mma (kind::tf32, M = 128,
+// N = 9R) accumulating in tensor memory.  Split TF32: A = Ah + Al and
+// B = Bh + Bl with every part rounded to TF32; Ah Bh + Ah Bl + Al Bh are
+// accumulated in FP32 (the dropped Al Bl term is below 2^-22 relative).
+// The source range is split into chunks (grid.y) whose partial results are
+// summed in a fixed order (deterministic, and each TMEM accumulator sums a
+// bounded number of terms).
+//
+// Operand layout in shared memory (K-major, no swizzle, the canonical UMMA
+// layout): 8-row x 16-byte core matrices; element (row, k) of an operand with
+// `rows` rows at byte (k / 4) * LBO + (row / 8) * 128 + (row % 8) * 16 +
+// (k % 4) * 4 with LBO = rows / 8 * 128.  B is stored in HBM already in this
+// layout, tile by tile (hi block, then lo block), so a tile is one contiguous
+// copy.
+//
+// Waits on the MMA completion barrier are bounded in time (MRHS_WAIT_NS, by
+// %globaltimer) and their outcome is made CTA-uniform with
+// __syncthreads_and, so no thread is left at a barrier; on timeout the kernel
+// records an error word in the workspace, waits once more (bounded), frees
+// its tensor memory and returns; CTAs that start after an error exit before
+// allocating tensor memory.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace tct {
+namespace {
+
+constexpr int MR_M = 128;            // observation triangles per CTA (MMA M)
+constexpr int MR_S = 8;              // source triangles per tile
+constexpr int MR_K = 7 * MR_S;       // 56: GEMM K per tile
+constexpr int MR_KSTEPS = MR_K / 8;  // tf32 MMA K = 8
+constexpr float MR_EPS = 1e-24f;     // r^2 offset (see far_main_rh2)
+constexpr unsigned long long MRHS_WAIT_NS = 200000000ull;  // 0.2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ float tf32_round(float x) {
+    uint32_t y;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
+    return __uint_as_float(y);
+}
+
+// shared-memory matrix descriptor, K-major, no swizzle (version 1)
+__host__ __device__ __forceinline__ uint64_t mr_smem_desc(uint32_t saddr, uint32_t lbo_bytes,
+                                                          uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3fff);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3fff) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3fff) << 32;
+    d |= (uint64_t)1 << 46;  // version
+    // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+    return d;
+}
+
+// instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N
+__host__ __device__ __forceinline__ uint32_t mr_instr_desc(int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(MR_M >> 4) << 24);
+}
+
+// byte offset of element (row, k) in a K-major no-swizzle operand tile
+__host__ __device__ __forceinline__ uint32_t mr_off(int row, int k, int rows) {
+    return (uint32_t)((k >> 2) * (rows / 8) * 128 + (row >> 3) * 128 + (row & 7) * 16 +
+                      (k & 3) * 4);
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for phase `phase` of an mbarrier (the MMA completion).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    const unsigned long long start = gtimer();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if (gtimer() - start > MRHS_WAIT_NS) return false;
+    }
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+    uint32_t mask[4] = {0, 0, 0, 0};
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask[0]), "r"(mask[1]),
+          "r"(mask[2]), "r"(mask[3]));
+}
+
+// ---- B panel: per source triangle and RHS, the 7 x 9 GEMM rows --------------
+// B[(s, c), (dj, r)]: c = 0 (S0): P_r[d][j]; c = T_ab: (d == a) M_r[b][j] +
+// (d == b, a != b) M_r[a][j].  One thread per (padded source triangle, r).
+__global__ void __launch_bounds__(128)
+mrhs_prep(Consts<float> c, float w2, const float* __restrict__ pts,
+          const int32_t* __restrict__ src_tris, int64_t n_src, int64_t n_src_pad,
+          const float* __restrict__ in, int R, float* __restrict__ Bg) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_src_pad * R) return;
+    const int64_t s = g / R;
+    const int r = (int)(g % R);
+    const int N = 9 * R;
+    float P[3][3] = {}, M[3][3] = {};
+    if (s < n_src) {
+        TriGeom<float> t;
+        load_tri(t, pts, src_tris, s, 0, false, true);
+        const float* x = in + (int64_t)r * n_src * 9 + s * 9;
+        float ssc[3][3];
+#pragma unroll
+        for (int Ij = 0; Ij < 3; Ij++)
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                float a = 0.f;
+#pragma unroll
+                for (int b = 0; b < 3; b++) a += t.sc[b][Ij] * x[b * 3 + d];
+                ssc[d][Ij] = a;
+            }
+        const float scale = t.J * c.CsRH0 * w2;
+        const float Bt = (ssc[0][0] + ssc[1][1] + ssc[2][2]) * c.CsRH1;
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                P[d][j] = scale * ((d == j ? Bt : 0.f) + c.CsRH2 * ssc[j][d] - 2.f * ssc[d][j]);
+                M[d][j] = scale * (-2.f * ssc[d][j]);
+            }
+    }
+    const int64_t tile = s / MR_S;
+    const int sl = (int)(s % MR_S);
+    unsigned char* base = reinterpret_cast<unsigned char*>(Bg) + tile * (int64_t)2 * N * MR_K * 4;
+    const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+    for (int cc = 0; cc < 7; cc++) {
+        const int k = 7 * sl + cc;
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                float v;
+                if (cc == 0) {
+                    v = P[d][j];
+                } else {
+                    const int a = ab[cc - 1][0], b = ab[cc - 1][1];
+                    v = (d == a ? M[b][j] : 0.f) + ((d == b && a != b) ? M[a][j] : 0.f);
+                }
+                const int n = (d * 3 + j) * R + r;
+                const float hi = tf32_round(v);
+                const float lo = tf32_round(v - hi);
+                const uint32_t off = mr_off(n, k, N);
+                *reinterpret_cast<float*>(base + off) = hi;
+                *reinterpret_cast<float*>(base + (int64_t)N * MR_K * 4 + off) = lo;
+            }
+    }
+}
+
+// ---- main: generate A, copy B, tcgen05.mma into TMEM ------------------------
+// grid (obs blocks of 128, source chunks); block 128 threads; dynamic smem:
+// A hi/lo (2 x 128 x 56 x 4), B hi/lo (2 x N x 56 x 4), source points.
+template <int R>
+__global__ void __launch_bounds__(128, 1)
+mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, int64_t n_obs,
+          const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
+          const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
+    constexpr int N = 9 * R;
+    constexpr int NCOL = N <= 256 ? 256 : 512;  // TMEM columns (power of two)
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char* Ah = smem;
+    unsigned char* Al = Ah + MR_M * MR_K * 4;
+    unsigned char* Bs = Al + MR_M * MR_K * 4;  // hi then lo, 2 * N * MR_K * 4
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x;
+    if (tid == 0) abort_flag = *reinterpret_cast<volatile int*>(err);
+    __syncthreads();
+    if (abort_flag) return;  // an earlier CTA timed out: no tensor memory taken yet
+    const int warp = tid >> 5;
+    const int64_t o = (int64_t)blockIdx.x * MR_M + tid;
+    const bool valid = o < n_obs;
+    const int64_t t0 = (int64_t)blockIdx.y * tiles_per_chunk;
+    const int64_t t1 = min(n_tiles, t0 + tiles_per_chunk);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(NCOL));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t barp = smem_u32(&bar);
+
+    // obs quadrature points (3-point rule: barycentric 2/3, 1/6, 1/6)
+    float x[3][3];
+    {
+        TriGeom<float> ot;
+        if (valid) {
+            load_tri(ot, pts, obs_tris, o, 0, false, false);
+        } else {
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int d = 0; d < 3; d++) ot.v[a][d] = 0.f;
+        }
+        const float wb[3][3] = {{2.f / 3.f, 1.f / 6.f, 1.f / 6.f},
+                                {1.f / 6.f, 2.f / 3.f, 1.f / 6.f},
+                                {1.f / 6.f, 1.f / 6.f, 2.f / 3.f}};
+#pragma unroll
+        for (int q = 0; q < 3; q++)
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                x[q][d] = wb[q][0] * ot.v[0][d] + wb[q][1] * ot.v[1][d] + wb[q][2] * ot.v[2][d];
+    }
+
+    uint32_t phase = 0;
+    bool ok = true;  // CTA-uniform
+    const uint32_t idesc_lo = mr_instr_desc(N <= 256 ? N : 256);
+    const uint32_t idesc_hi = mr_instr_desc(N <= 256 ? 8 : N - 256);
+    for (int64_t t = t0; t < t1; t++) {
+        if (t > t0) {
+            const bool w = mbar_wait(barp, phase);
+            if (!__syncthreads_and(w)) {
+                ok = false;  // the MMAs of the previous tile did not complete in time
+                break;
+            }
+            phase ^= 1;
+        }
+        // B tile: one contiguous copy (hi + lo)
+        {
+            const float4* src = reinterpret_cast<const float4*>(Bg + t * (int64_t)2 * N * MR_K);
+            float4* dst = reinterpret_cast<float4*>(Bs);
+            for (int k = tid; k < 2 * N * MR_K / 4; k += 128) dst[k] = __ldg(src + k);
+        }
+        // A tile: the 7 kernel scalars per (obs, source) pair, split hi / lo
+        float av[MR_K];
+#pragma unroll
+        for (int sl = 0; sl < MR_S; sl++) {
+            const float* y = srcy + (t * MR_S + sl) * 9;
+            float T00 = 0.f, T01 = 0.f, T02 = 0.f, T11 = 0.f, T12 = 0.f, T22 = 0.f;
+#pragma unroll
+            for (int q2 = 0; q2 < 3; q2++) {
+                const float y0 = __ldg(y + 3 * q2), y1 = __ldg(y + 3 * q2 + 1),
+                            y2 = __ldg(y + 3 * q2 + 2);
+#pragma unroll
+                for (int q1 = 0; q1 < 3; q1++) {
+                    const float D0 = y0 - x[q1][0], D1 = y1 - x[q1][1], D2 = y2 - x[q1][2];
+                    const float r2 = fmaf(D0, D0, fmaf(D1, D1, fmaf(D2, D2, MR_EPS)));
+                    const float ir = rsqrtf(r2);
+                    const float g = ir * ir * ir;
+                    const float g0 = g * D0, g1 = g * D1, g2 = g * D2;
+                    T00 = fmaf(g0, D0, T00);
+                    T01 = fmaf(g0, D1, T01);
+                    T02 = fmaf(g0, D2, T02);
+                    T11 = fmaf(g1, D1, T11);
+                    T12 = fmaf(g1, D2, T12);
+                    T22 = fmaf(g2, D2, T22);
+                }
+            }
+            av[7 * sl + 0] = valid ? T00 + T11 + T22 : 0.f;
+            av[7 * sl + 1] = valid ? T00 : 0.f;
+            av[7 * sl + 2] = valid ? T01 : 0.f;
+            av[7 * sl + 3] = valid ? T02 : 0.f;
+            av[7 * sl + 4] = valid ? T11 : 0.f;
+            av[7 * sl + 5] = valid ? T12 : 0.f;
+            av[7 * sl + 6] = valid ? T22 : 0.f;
+        }
+#pragma unroll
+        for (int ch = 0; ch < MR_K / 4; ch++) {
+            float4 h, l;
+            h.x = tf32_round(av[4 * ch + 0]);
+            h.y = tf32_round(av[4 * ch + 1]);
+            h.z = tf32_round(av[4 * ch + 2]);
+            h.w = tf32_round(av[4 * ch + 3]);
+            l.x = tf32_round(av[4 * ch + 0] - h.x);
+            l.y = tf32_round(av[4 * ch + 1] - h.y);
+            l.z = tf32_round(av[4 * ch + 2] - h.z);
+            l.w = tf32_round(av[4 * ch + 3] - h.w);
+            const uint32_t off = mr_off(tid, 4 * ch, MR_M);
+            *reinterpret_cast<float4*>(Ah + off) = h;
+            *reinterpret_cast<float4*>(Al + off) = l;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t lboA = MR_M / 8 * 128, lboB = N / 8 * 128;
+            const uint32_t aH = smem_u32(Ah), aL = smem_u32(Al), bH = smem_u32(Bs),
+                           bL = smem_u32(Bs + N * MR_K * 4);
+#pragma unroll
+            for (int ks = 0; ks < MR_KSTEPS; ks++) {
+                const uint64_t dAh = mr_smem_desc(aH + 2 * ks * lboA, lboA, 128);
+                const uint64_t dAl = mr_smem_desc(aL + 2 * ks * lboA, lboA, 128);
+                const uint32_t first = (t == t0 && ks == 0) ? 0u : 1u;
+#pragma unroll
+                for (int half = 0; half < (N <= 256 ? 1 : 2); half++) {
+                    const uint32_t boff = half * 256 / 8 * 128;  // rows 256.. of B
+                    const uint64_t dBh = mr_smem_desc(bH + 2 * ks * lboB + boff, lboB, 128);
+                    const uint64_t dBl = mr_smem_desc(bL + 2 * ks * lboB + boff, lboB, 128);
+                    const uint32_t dcol = tmem + half * 256;
+                    const uint32_t id = half ? idesc_hi : idesc_lo;
+                    mma_tf32(dcol, dAh, dBh, id, first);
+                    mma_tf32(dcol, dAh, dBl, id, 1u);
+                    mma_tf32(dcol, dAl, dBh, id, 1u);
+                }
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    barp)
+                : "memory");
+        }
+    }
+    if (t1 > t0) {
+        // the last commit (or, after a timeout, one more bounded wait for it)
+        const bool w = mbar_wait(barp, phase);
+        if (!__syncthreads_and(w)) ok = false;
+        if (!ok && tid == 0) atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+
+    // epilogue: W[(dj, r)] of this thread's row from TMEM -> partial[chunk][r][o][9]
+    // (obs-side contraction out[b][d] = J_o sum_j sc_o[b][j] W[d][j] done by the
+    // reduce kernel, which has the obs geometry)
+    if (ok && t1 > t0) {
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 8) {
+            uint32_t v[8];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7])
+                : "r"(lane_base + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (valid) {
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int n = c0 + u;
+                    const int dj = n / R, r = n % R;
+                    partial[(((int64_t)blockIdx.y * R + r) * n_obs + o) * 9 + dj] =
+                        __uint_as_float(v[u]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(NCOL));
+    }
+}
+
+// Source quadrature points (3 x 3 per source triangle, padded with far-away
+// points that contribute nothing: their A entries are multiplied by zero rows
+// of B).
+__global__ void __launch_bounds__(128)
+mrhs_points(const float* __restrict__ pts, const int32_t* __restrict__ src_tris, int64_t n_src,
+            int64_t n_src_pad, float* __restrict__ srcy) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_src_pad) return;
+    const float wb[3][3] = {{2.f / 3.f, 1.f / 6.f, 1.f / 6.f},
+                            {1.f / 6.f, 2.f / 3.f, 1.f / 6.f},
+                            {1.f / 6.f, 1.f / 6.f, 2.f / 3.f}};
+    float* y = srcy + s * 9;
+    if (s >= n_src) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) y[k] = 1e18f;
+        return;
+    }
+    TriGeom<float> t;
+    load_tri(t, pts, src_tris, s, 0, false, false);
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            y[3 * q + d] = wb[q][0] * t.v[0][d] + wb[q][1] * t.v[1][d] + wb[q][2] * t.v[2][d];
+}
+
+// Sum the chunk partials in a fixed order and apply the obs-side contraction:
+// out[r][o][b][d] (+)= J_o sum_j sc_o[b][j] W[r][o][d][j].
+__global__ void __launch_bounds__(128)
+mrhs_reduce(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, int64_t n_obs,
+            int R, int n_chunks, const float* __restrict__ partial, float* __restrict__ out,
+            int accumulate) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_obs * R) return;
+    const int64_t o = g % n_obs;
+    const int r = (int)(g / n_obs);
+    float W[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        float s = 0.f, cmp = 0.f;
+        for (int c = 0; c < n_chunks; c++) {
+            const float y = partial[(((int64_t)c * R + r) * n_obs + o) * 9 + k] - cmp;
+            const float t = s + y;
+            cmp = (t - s) - y;
+            s = t;
+        }
+        W[k] = s;
+    }
+    TriGeom<float> ot;
+    load_tri(ot, pts, obs_tris, o, 0, false, true);
+    float* op = out + ((int64_t)r * n_obs + o) * 9;
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const float v = ot.J * (ot.sc[b][0] * W[3 * d + 0] + ot.sc[b][1] * W[3 * d + 1] +
+                                    ot.sc[b][2] * W[3 * d + 2]);
+            op[b * 3 + d] = accumulate ? op[b * 3 + d] + v : v;
+        }
+}
+
+inline size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+
+int64_t mrhs_chunks(int64_t n_obs, int64_t n_tiles) {
+    const int64_t obs_blocks = (n_obs + MR_M - 1) / MR_M;
+    // a few waves over the 148 SMs, at least 8 tiles per chunk, at most 64
+    int64_t want = (148 * 4 + obs_blocks - 1) / std::max<int64_t>(obs_blocks, 1);
+    want = std::max<int64_t>(want, (n_tiles + 511) / 512);  // <= 512 tiles per accumulator
+    return std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, n_tiles / 8 + 1), 64));
+}
+
+struct MrhsSizes {
+    size_t B, y, partial, err;
+};
+
+MrhsSizes mrhs_sizes(int64_t n_obs, int64_t n_src, int R) {
+    const int64_t n_pad = (n_src + MR_S - 1) / MR_S * MR_S;
+    const int64_t n_tiles = n_pad / MR_S;
+    MrhsSizes s;
+    s.B = al256((size_t)n_tiles * 2 * 9 * R * MR_K * 4);
+    s.y = al256((size_t)n_pad * 9 * 4);
+    s.partial = al256((size_t)mrhs_chunks(n_obs, n_tiles) * R * n_obs * 9 * 4);
+    s.err = 256;
+    return s;
+}
+
+template <int R>
+int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, const float* pts,
+             const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris, int64_t n_src,
+             int accumulate, unsigned char* ws, cudaStream_t st) {
+    constexpr int N = 9 * R;
+    const int64_t n_pad = (n_src + MR_S - 1) / MR_S * MR_S;
+    const int64_t n_tiles = n_pad / MR_S;
+    const MrhsSizes sz = mrhs_sizes(n_obs, n_src, R);
+    float* Bg = reinterpret_cast<float*>(ws);
+    float* srcy = reinterpret_cast<float*>(ws + sz.B);
+    float* partial = reinterpret_cast<float*>(ws + sz.B + sz.y);
+    int* err = reinterpret_cast<int*>(ws + sz.B + sz.y + sz.partial);
+    if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return launch_status("mrhs memset");
+    mrhs_points<<<(unsigned)((n_pad + 127) / 128), 128, 0, st>>>(pts, src_tris, n_src, n_pad,
+                                                                 srcy);
+    int rc = launch_status("mrhs points");
+    if (rc) return rc;
+    mrhs_prep<<<(unsigned)((n_pad * R + 127) / 128), 128, 0, st>>>(c, w2, pts, src_tris, n_src,
+                                                                   n_pad, in, R, Bg);
+    if ((rc = launch_status("mrhs prep"))) return rc;
+    const int64_t chunks = mrhs_chunks(n_obs, n_tiles);
+    const int64_t per = (n_tiles + chunks - 1) / chunks;
+    const int64_t real = (n_tiles + per - 1) / per;
+    const size_t smem = (size_t)2 * MR_M * MR_K * 4 + (size_t)2 * N * MR_K * 4;
+    if (cudaFuncSetAttribute(mrhs_main<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return launch_status("mrhs smem attribute");
+    dim3 grid((unsigned)((n_obs + MR_M - 1) / MR_M), (unsigned)real);
+    mrhs_main<R><<<grid, 128, smem, st>>>(pts, obs_tris, n_obs, srcy, n_tiles, per, Bg, partial,
+                                          err);
+    if ((rc = launch_status("mrhs main"))) return rc;
+    mrhs_reduce<<<(unsigned)((n_obs * R + 127) / 128), 128, 0, st>>>(
+        pts, obs_tris, n_obs, R, (int)real, partial, out, accumulate);
+    return launch_status("mrhs reduce");
+}
+
+}  // namespace
+}  // namespace tct
+
+using namespace tct;
+
+extern "C" size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R) {
+    if (R != 16 && R != 32) return 0;
+    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
+    return s.B + s.y + s.partial + s.err;
+}
+
+extern "C" int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src,
+                                           int R, void* stream, int* host_flag) {
+    TCT_CHECK_ARG(workspace && host_flag && (R == 16 || R == 32),
+                  "tct_farfield_rh_panel_error: bad arguments");
+    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
+    cudaStream_t st = as_stream(stream);
+    if (cudaMemcpyAsync(host_flag, reinterpret_cast<const unsigned char*>(workspace) + s.B + s.y +
+                                       s.partial,
+                        sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return launch_status("tct_farfield_rh_panel_error");
+    return TCT_OK;
+}
+
+extern "C" int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
+                                            const int32_t* obs_tris, int64_t n_obs,
+                                            const int32_t* src_tris, int64_t n_src, int R,
+                                            const double* params, int accumulate, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+    TCT_CHECK_ARG(R == 16 || R == 32, "tct_farfield_rh_panel_matvec: R must be 16 or 32 (got %d)",
+                  R);
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_rh_panel_matvec: negative size");
+    TCT_CHECK_ARG(params, "tct_farfield_rh_panel_matvec: null params");
+    if (n_obs == 0) return TCT_OK;
+    const size_t need = tct_farfield_rh_panel_workspace_bytes(n_obs, n_src, R);
+    TCT_CHECK_ARG(workspace && workspace_bytes >= need && aligned(workspace, 256),
+                  "tct_farfield_rh_panel_matvec: workspace of %zu bytes (256-aligned) required",
+                  need);
+    const Consts<float> c = make_consts<float>(params);
+    const float w = 1.f / 6.f;  // the 3-point rule's weights
+    unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
+    cudaStream_t st = as_stream(stream);
+    if (n_src == 0) {
+        if (!accumulate && cudaMemsetAsync(out, 0, sizeof(float) * 9 * n_obs * R, st) != cudaSuccess)
+            return launch_status("tct_farfield_rh_panel_matvec memset");
+        return TCT_OK;
+    }
+    if (R == 16)
+        return run_mrhs<16>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
+                            n_obs, src_tris, n_src, accumulate, ws, st);
+    return run_mrhs<32>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
+                        n_obs, src_tris, n_src, accumulate, ws, st);
+}

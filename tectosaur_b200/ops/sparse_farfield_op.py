@@ -43,6 +43,7 @@ class TriToTriDirectFarfieldOp:
         if self.ws_bytes == 0 and self.n_src > 0:
             raise ValueError("farfield: unsupported kernel/rule (%s, %d points)" % (K_name, self.n_q))
         self.workspace = device.workspace(self.ws_bytes)
+        self._panel_ws = {}
 
     def dot_device(self, x, y, accumulate=False, stream=None):
         """y (+)= Far x on device tensors of float_type."""
@@ -63,6 +64,71 @@ class TriToTriDirectFarfieldOp:
         y = device.empty(self.shape[0], self.float_type)
         self.dot_device(x, y)
         return y.cpu().numpy()
+
+    # -- many right-hand sides ------------------------------------------------
+    def panel_supported(self):
+        """The tensor-core panel path: elasticRH3, FP32, the 3-point rule."""
+        return self.K_name == "elasticRH3" and self.prec == _lib.TCT_F32 and self.n_q == 3
+
+    def dot_panel_device(self, X, Y, accumulate=False, stream=None):
+        """Y[r] (+)= Far X[r] for device tensors X (R, 9 n_src), Y (R, 9 n_obs).
+        elasticRH3 / FP32 / 3-point rule runs on the tensor cores in panels
+        of 16 or 32 vectors (split TF32, FP32 accumulation); other kernels
+        apply dot_device vector by vector."""
+        t = device.torch()
+        R = X.shape[0]
+        if not self.panel_supported():
+            for r in range(R):
+                self.dot_device(X[r].contiguous(), Y[r], accumulate=accumulate, stream=stream)
+            return Y
+        r0 = 0
+        while r0 < R:
+            width = 32 if R - r0 > 16 else 16
+            take = min(width, R - r0)
+            if take == width:
+                xin = X[r0:r0 + take].contiguous()
+            else:
+                xin = t.zeros((width, X.shape[1]), dtype=X.dtype, device=X.device)
+                xin[:take] = X[r0:r0 + take]
+            out = Y[r0:r0 + take] if take == width else t.empty(
+                (width, Y.shape[1]), dtype=Y.dtype, device=Y.device)
+            if take != width and accumulate:
+                out[:take] = Y[r0:r0 + take]
+            nbytes = _lib.lib.tct_farfield_rh_panel_workspace_bytes(self.n_obs, self.n_src, width)
+            ws = self._panel_ws.get(width)
+            if ws is None or ws.numel() < nbytes:
+                ws = device.workspace(nbytes)
+                self._panel_ws[width] = ws
+            _lib.check(_lib.lib.tct_farfield_rh_panel_matvec(
+                _lib.tptr(out), _lib.tptr(xin), _lib.tptr(self.gpu_pts),
+                _lib.tptr(self.gpu_obs_tris), self.n_obs, _lib.tptr(self.gpu_src_tris), self.n_src,
+                width, _lib.dptr(self.params), int(bool(accumulate)), _lib.tptr(ws), nbytes,
+                _lib.stream_ptr(stream)), "tct_farfield_rh_panel_matvec")
+            if take != width:
+                Y[r0:r0 + take] = out[:take]
+            r0 += take
+        return Y
+
+    def panel_error(self, width=16, stream=None):
+        """Error word of the last panel apply of this width (0 = ok)."""
+        import ctypes
+        flag = ctypes.c_int(0)
+        ws = self._panel_ws.get(width)
+        if ws is None:
+            return 0
+        _lib.check(_lib.lib.tct_farfield_rh_panel_error(
+            _lib.tptr(ws), self.n_obs, self.n_src, width, _lib.stream_ptr(stream),
+            ctypes.byref(flag)), "tct_farfield_rh_panel_error")
+        return flag.value
+
+    def dot_panel(self, X):
+        """Host (R, 9 n_src) in, host (R, 9 n_obs) out."""
+        t = device.torch()
+        Xd = device.to_dev(np.asarray(X, dtype=self.float_type).reshape(-1, self.shape[1]),
+                           self.float_type)
+        Yd = t.empty((Xd.shape[0], self.shape[0]), dtype=Xd.dtype, device="cuda")
+        self.dot_panel_device(Xd, Yd)
+        return Yd.cpu().numpy()
 
     async def async_dot(self, v):
         return self.dot(v)
