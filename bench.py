@@ -935,6 +935,117 @@ def run_pairs_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_panel_workload(args, rank, world, torch, dist):
+    """C2 farfield applied to a panel of R right-hand sides on the tensor cores."""
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    R = args.rhs
+    pts, tris = c2_mesh(args.grid or 174)
+    n = tris.shape[0]
+    idx = np.arange(n)
+    op = TriToTriDirectFarfieldOp(NQ["nq_far"], K_NAME, PARAMS, pts, tris, np.float32, idx, idx)
+    X = torch.from_numpy(np.random.default_rng(3 + rank).standard_normal((R, 9 * n))
+                         .astype(np.float32)).cuda()
+    Y = torch.empty((R, 9 * n), dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        op.dot_panel_device(X, Y)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        op.dot_panel_device(X, Y)
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    errs = [int(op.panel_error(16))]
+    # the single-vector path on the same mesh, and the panel's error against it
+    y1 = torch.empty(9 * n, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        op.dot_device(X[0].contiguous(), y1)
+    torch.cuda.synchronize()
+    c = torch.cuda.Event(enable_timing=True)
+    d = torch.cuda.Event(enable_timing=True)
+    c.record()
+    for _ in range(5):
+        op.dot_device(X[0].contiguous(), y1)
+    d.record()
+    torch.cuda.synchronize()
+    single_ms = c.elapsed_time(d) / 5
+    rel = []
+    for r in sorted({0, R // 2, R - 1}):
+        op.dot_device(X[r].contiguous(), y1)
+        rel.append(float(torch.linalg.norm(Y[r] - y1) / torch.linalg.norm(y1)))
+    # e2e: host panel in, host panel out
+    Xh = X.cpu().numpy()
+    op.dot_panel(Xh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 3))):
+        Yh = op.dot_panel(Xh)
+    t_e2e = (time.perf_counter() - t0) / max(1, min(args.steps, 3))
+    if rank != 0:
+        return
+    # executed tensor work: per panel of width w, 3 split-TF32 products of
+    # (n_obs padded to 128) x (7 n_src padded to 56) x 9w
+    widths, r0 = [], 0
+    while r0 < R:
+        widths.append(16)
+        r0 += 16
+    n_obs_p = (n + 127) // 128 * 128
+    n_src_p = (n + 7) // 8 * 8
+    mma_flops = sum(3 * 2.0 * n_obs_p * 7 * n_src_p * 9 * w for w in widths)
+    mp = measured_peaks()
+    bf16 = mp.get("bf16_tflops") if mp else 1590.0
+    tf32_peak = bf16 / 2.0
+    achieved = mma_flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "farfield vector applies/s (multi-RHS panel, tensor cores)",
+        "value": world * R / (ms * 1e-3), "unit": "vector applies/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded mesh and inputs)",
+        "config": {"workload": ("direct farfield of the 60k-triangle topographic surface "
+                                "(elasticRH3, 3-point rule) applied to a panel of %d N(0, 1) "
+                                "vectors: kernel scalars on the CUDA cores, contraction with "
+                                "the panel by split-TF32 tcgen05.mma (panels of %s)"
+                                % (R, "+".join(str(w) for w in widths))),
+                   "n_tris": int(n), "rhs": R, "single_vector_ms": single_ms,
+                   "speedup_vs_single_vector": single_ms * R / ms,
+                   "rel_err_vs_single_vector_fp32": rel, "error_words": errs,
+                   "l2": "inputs larger than L2 (panel B operand %.0f MB)" % (
+                       n_src_p * 7 * 9 * max(widths) * 8 / 1e6),
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "mrhs_main<R> (tcgen05.mma kind::tf32, split TF32)",
+                     "bound": "tensor", "achieved": achieved, "peak": tf32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / tf32_peak, "traffic": None,
+                     "peak_source": "TF32 dense = half of the measured BF16 GEMM rate "
+                                    "(MEASURED_PEAKS.json bf16_tflops %.0f)" % bf16,
+                     "algorithmic": "%.3e tensor flops per panel apply (3 split products)"
+                                    % mma_flops},
+        "e2e": {"value": R / t_e2e, "unit": "vector applies/s",
+                "h2d_bytes_per_step": int(Xh.nbytes), "d2h_bytes_per_step": int(Yh.nbytes),
+                "api": "TriToTriDirectFarfieldOp.dot_panel(numpy (R, 9n)) -> numpy"},
+        "gpu_launches": args.steps * len(widths) * 4,
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        cb = cpu_direct_far_baseline(pts, tris)
+        cb["unit"] = "vector applies/s"
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+
+
 def config_block(n_tris, nnzb):
     return {
         "workload": ("direct-farfield 60k-triangle topographic surface (174x174 grid over "
@@ -957,10 +1068,13 @@ def main():
     ap.add_argument("--grid", type=int, default=None,
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "fmm", "solve", "pairs"],
+    ap.add_argument("--workload", default="c2",
+                    choices=["c2", "fmm", "solve", "pairs", "panel"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
-                         "400k-pair batched singular quadrature + BSR matvec")
+                         "400k-pair batched singular quadrature + BSR matvec; panel: the "
+                         "C2 farfield on a panel of --rhs vectors (tensor cores)")
+    ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--fmm-order", type=int, default=None)
     ap.add_argument("--fmm-ppc", type=int, default=None)
@@ -985,9 +1099,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs"):
-        {"fmm": run_fmm_workload, "solve": run_solve_workload,
-         "pairs": run_pairs_workload}[args.workload](args, rank, world, torch, dist)
+    if args.workload in ("fmm", "solve", "pairs", "panel"):
+        {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
+         "panel": run_panel_workload}[args.workload](args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()

@@ -333,11 +333,12 @@ int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
 /* ---- multi-RHS farfield on the tensor cores ------------------------------- */
 
 /* Direct farfield of elasticRH3 (FP32, 3-point rule) applied to a panel of R
- * input vectors at once: out[r] (+)= Far in[r] for r < R (R = 16 or 32).
+ * input vectors at once: out[r] (+)= Far in[r] for r < R (R = 16).
  * The reference applies farfield_tris_to_tris{K} (matrix_free.cl:19-107) to
  * one vector per call; here the per-triangle-pair kernel scalars are
  * generated on the CUDA cores and contracted with the input panel by
- * tcgen05.mma (split TF32, FP32 accumulation in tensor memory).
+ * tcgen05.mma (split TF32, FP32 accumulation in tensor memory folded into
+ * a Kahan pair every 4 source tiles).
  * in: R x (9 n_src) floats, out: R x (9 n_obs) floats (device, vector after
  * vector); pts / tris as in tct_farfield_tris_matvec. */
 size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R);

@@ -17,9 +17,14 @@
 // N = 9R) accumulating in tensor memory.  Split TF32: A = Ah + Al and
 // B = Bh + Bl with every part rounded to TF32; Ah Bh + Ah Bl + Al Bh are
 // accumulated in FP32 (the dropped Al Bl term is below 2^-22 relative).
-// The source range is split into chunks (grid.y) whose partial results are
-// summed in a fixed order (deterministic, and each TMEM accumulator sums a
-// bounded number of terms).
+// Compensated accumulation: the tensor-memory accumulator D takes only
+// MR_FLUSH tiles; it is then folded into a Kahan pair (S, C) kept in spare
+// tensor-memory columns (tcgen05.ld / st, 8 columns at a time), and the next
+// tile overwrites D.  (Plain FP32 accumulation over a whole source chunk
+// loses ~2e-4 relative on the 60k-triangle surface, where near pairs add
+// large, partly cancelling terms; the single-vector kernel keeps Kahan per
+// tile for the same reason.)  The source range is split into chunks (grid.y)
+// whose partial results are summed in a fixed order (deterministic).
 //
 // Operand layout in shared memory (K-major, no swizzle, the canonical UMMA
 // layout): 8-row x 16-byte core matrices; element (row, k) of an operand with
@@ -46,6 +51,7 @@ constexpr int MR_S = 8;              // source triangles per tile
 constexpr int MR_K = 7 * MR_S;       // 56: GEMM K per tile
 constexpr int MR_KSTEPS = MR_K / 8;  // tf32 MMA K = 8
 constexpr float MR_EPS = 1e-24f;     // r^2 offset (see far_main_rh2)
+constexpr int MR_FLUSH = 4;          // tiles per tensor-memory accumulation
 constexpr unsigned long long MRHS_WAIT_NS = 200000000ull;  // 0.2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -115,6 +121,60 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
         :
         : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask[0]), "r"(mask[1]),
           "r"(mask[2]), "r"(mask[3]));
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t u[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]),
+          "=r"(u[7])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k] = __uint_as_float(u[k]);
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(
+            taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])));
+}
+
+// Fold the accumulator D (columns [0, N)) into the Kahan pair S = [N, 2N),
+// C = [2N, 3N) of this warp's lanes; `first` initialises S = D, C = 0.
+template <int N>
+__device__ __forceinline__ void tmem_fold(uint32_t lane_base, bool first) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < N; c0 += 8) {
+        float d[8], sv[8], cv[8];
+        tmem_ld8(lane_base + c0, d);
+        if (!first) {
+            tmem_ld8(lane_base + N + c0, sv);
+            tmem_ld8(lane_base + 2 * N + c0, cv);
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (first) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                sv[k] = d[k];
+                cv[k] = 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const float y = d[k] - cv[k];
+                const float t = sv[k] + y;
+                cv[k] = (t - sv[k]) - y;
+                sv[k] = t;
+            }
+        }
+        tmem_st8(lane_base + N + c0, sv);
+        tmem_st8(lane_base + 2 * N + c0, cv);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // ---- B panel: per source triangle and RHS, the 7 x 9 GEMM rows --------------
@@ -191,7 +251,8 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
           const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
           const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
     constexpr int N = 9 * R;
-    constexpr int NCOL = N <= 256 ? 256 : 512;  // TMEM columns (power of two)
+    static_assert(3 * N <= 512, "D, S and C must fit the 512 tensor-memory columns");
+    constexpr int NCOL = 512;
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* Ah = smem;
     unsigned char* Al = Ah + MR_M * MR_K * 4;
@@ -250,8 +311,8 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
 
     uint32_t phase = 0;
     bool ok = true;  // CTA-uniform
-    const uint32_t idesc_lo = mr_instr_desc(N <= 256 ? N : 256);
-    const uint32_t idesc_hi = mr_instr_desc(N <= 256 ? 8 : N - 256);
+    const uint32_t idesc = mr_instr_desc(N);
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     for (int64_t t = t0; t < t1; t++) {
         if (t > t0) {
             const bool w = mbar_wait(barp, phase);
@@ -260,6 +321,11 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
                 break;
             }
             phase ^= 1;
+            if ((t - t0) % MR_FLUSH == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                tmem_fold<N>(lane_base, t - t0 == MR_FLUSH);
+                asm volatile("tcgen05.fence::before_thread_sync;");
+            }
         }
         // B tile: one contiguous copy (hi + lo)
         {
@@ -326,18 +392,13 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
             for (int ks = 0; ks < MR_KSTEPS; ks++) {
                 const uint64_t dAh = mr_smem_desc(aH + 2 * ks * lboA, lboA, 128);
                 const uint64_t dAl = mr_smem_desc(aL + 2 * ks * lboA, lboA, 128);
-                const uint32_t first = (t == t0 && ks == 0) ? 0u : 1u;
-#pragma unroll
-                for (int half = 0; half < (N <= 256 ? 1 : 2); half++) {
-                    const uint32_t boff = half * 256 / 8 * 128;  // rows 256.. of B
-                    const uint64_t dBh = mr_smem_desc(bH + 2 * ks * lboB + boff, lboB, 128);
-                    const uint64_t dBl = mr_smem_desc(bL + 2 * ks * lboB + boff, lboB, 128);
-                    const uint32_t dcol = tmem + half * 256;
-                    const uint32_t id = half ? idesc_hi : idesc_lo;
-                    mma_tf32(dcol, dAh, dBh, id, first);
-                    mma_tf32(dcol, dAh, dBl, id, 1u);
-                    mma_tf32(dcol, dAl, dBh, id, 1u);
-                }
+                // D restarts at the first tile of every MR_FLUSH group
+                const uint32_t first = ((t - t0) % MR_FLUSH == 0 && ks == 0) ? 0u : 1u;
+                const uint64_t dBh = mr_smem_desc(bH + 2 * ks * lboB, lboB, 128);
+                const uint64_t dBl = mr_smem_desc(bL + 2 * ks * lboB, lboB, 128);
+                mma_tf32(tmem, dAh, dBh, idesc, first);
+                mma_tf32(tmem, dAh, dBl, idesc, 1u);
+                mma_tf32(tmem, dAl, dBh, idesc, 1u);
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -353,27 +414,23 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
 
-    // epilogue: W[(dj, r)] of this thread's row from TMEM -> partial[chunk][r][o][9]
-    // (obs-side contraction out[b][d] = J_o sum_j sc_o[b][j] W[d][j] done by the
-    // reduce kernel, which has the obs geometry)
+    // epilogue: fold the last group, then S (+ C) of this thread's row ->
+    // partial[chunk][r][o][9] (the obs-side contraction out[b][d] = J_o
+    // sum_j sc_o[b][j] W[d][j] is done by the reduce kernel)
     if (ok && t1 > t0) {
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
+        tmem_fold<N>(lane_base, t1 - t0 <= MR_FLUSH);
+#pragma unroll 1
         for (int c0 = 0; c0 < N; c0 += 8) {
-            uint32_t v[8];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7])
-                : "r"(lane_base + (uint32_t)c0));
+            float sv[8], cv[8];
+            tmem_ld8(lane_base + N + c0, sv);
+            tmem_ld8(lane_base + 2 * N + c0, cv);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (valid) {
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
                     const int n = c0 + u;
                     const int dj = n / R, r = n % R;
-                    partial[(((int64_t)blockIdx.y * R + r) * n_obs + o) * 9 + dj] =
-                        __uint_as_float(v[u]);
+                    partial[(((int64_t)blockIdx.y * R + r) * n_obs + o) * 9 + dj] = sv[u] - cv[u];
                 }
             }
         }
@@ -514,14 +571,14 @@ int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, cons
 using namespace tct;
 
 extern "C" size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R) {
-    if (R != 16 && R != 32) return 0;
+    if (R != 16) return 0;
     const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
     return s.B + s.y + s.partial + s.err;
 }
 
 extern "C" int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src,
                                            int R, void* stream, int* host_flag) {
-    TCT_CHECK_ARG(workspace && host_flag && (R == 16 || R == 32),
+    TCT_CHECK_ARG(workspace && host_flag && R == 16,
                   "tct_farfield_rh_panel_error: bad arguments");
     const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
     cudaStream_t st = as_stream(stream);
@@ -538,8 +595,7 @@ extern "C" int tct_farfield_rh_panel_matvec(void* out, const void* in, const voi
                                             const int32_t* src_tris, int64_t n_src, int R,
                                             const double* params, int accumulate, void* workspace,
                                             size_t workspace_bytes, void* stream) {
-    TCT_CHECK_ARG(R == 16 || R == 32, "tct_farfield_rh_panel_matvec: R must be 16 or 32 (got %d)",
-                  R);
+    TCT_CHECK_ARG(R == 16, "tct_farfield_rh_panel_matvec: R must be 16 (got %d)", R);
     TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_rh_panel_matvec: negative size");
     TCT_CHECK_ARG(params, "tct_farfield_rh_panel_matvec: null params");
     if (n_obs == 0) return TCT_OK;
@@ -556,9 +612,6 @@ extern "C" int tct_farfield_rh_panel_matvec(void* out, const void* in, const voi
             return launch_status("tct_farfield_rh_panel_matvec memset");
         return TCT_OK;
     }
-    if (R == 16)
-        return run_mrhs<16>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
-                            n_obs, src_tris, n_src, accumulate, ws, st);
-    return run_mrhs<32>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
+    return run_mrhs<16>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
                         n_obs, src_tris, n_src, accumulate, ws, st);
 }

