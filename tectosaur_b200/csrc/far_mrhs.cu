@@ -143,12 +143,13 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
         "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])));
 }
 
-// Fold the accumulator D (columns [0, N)) into the Kahan pair S = [N, 2N),
-// C = [2N, 3N) of this warp's lanes; `first` initialises S = D, C = 0.
+// Fold columns [c_begin, c_end) of the accumulator D (columns [0, N)) into
+// the Kahan pair S = [N, 2N), C = [2N, 3N) of this warp's lanes; `first`
+// initialises S = D, C = 0.
 template <int N>
-__device__ __forceinline__ void tmem_fold(uint32_t lane_base, bool first) {
+__device__ __forceinline__ void tmem_fold(uint32_t lane_base, int c_begin, int c_end, bool first) {
 #pragma unroll 1
-    for (int c0 = 0; c0 < N; c0 += 8) {
+    for (int c0 = c_begin; c0 < c_end; c0 += 8) {
         float d[8], sv[8], cv[8];
         tmem_ld8(lane_base + c0, d);
         if (!first) {
@@ -243,21 +244,43 @@ mrhs_prep(Consts<float> c, float w2, const float* __restrict__ pts,
 }
 
 // ---- main: generate A, copy B, tcgen05.mma into TMEM ------------------------
-// grid (obs blocks of 128, source chunks); block 128 threads; dynamic smem:
-// A hi/lo (2 x 128 x 56 x 4), B hi/lo (2 x N x 56 x 4), source points.
+// grid (obs blocks of 128, source chunks); 256 threads: thread (row, half)
+// generates row `row` of A for the half `half` of the tile's 8 source
+// triangles; one thread issues the B tile as a bulk async copy (completing
+// on bar_b) before the generation starts, so the copy overlaps it, and then
+// the MMAs (completing on bar_mma).  The two warp groups split the tensor-
+// memory columns of the fold and the epilogue.  Dynamic smem: A hi/lo
+// (2 x 128 x 56 x 4), B hi/lo (2 x N x 56 x 4).
+constexpr int MR_THREADS = 256;
+constexpr int MR_COPIES = 4;  // bulk copies per B tile
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
 template <int R>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(MR_THREADS, 1)
 mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, int64_t n_obs,
           const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
           const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
     constexpr int N = 9 * R;
+    constexpr int NH = N / 2;  // tensor-memory columns per warp group
     static_assert(3 * N <= 512, "D, S and C must fit the 512 tensor-memory columns");
+    static_assert(NH % 8 == 0, "column halves must be whole 8-column groups");
     constexpr int NCOL = 512;
+    constexpr uint32_t B_BYTES = 2u * N * MR_K * 4;
+    static_assert(B_BYTES % (16 * MR_COPIES) == 0, "bulk copies must be 16-byte multiples");
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* Ah = smem;
     unsigned char* Al = Ah + MR_M * MR_K * 4;
     unsigned char* Bs = Al + MR_M * MR_K * 4;  // hi then lo, 2 * N * MR_K * 4
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar_mma;
+    __shared__ __align__(8) uint64_t bar_b;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
@@ -266,7 +289,9 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
     __syncthreads();
     if (abort_flag) return;  // an earlier CTA timed out: no tensor memory taken yet
     const int warp = tid >> 5;
-    const int64_t o = (int64_t)blockIdx.x * MR_M + tid;
+    const int row = tid & (MR_M - 1);
+    const int half = tid >> 7;
+    const int64_t o = (int64_t)blockIdx.x * MR_M + row;
     const bool valid = o < n_obs;
     const int64_t t0 = (int64_t)blockIdx.y * tiles_per_chunk;
     const int64_t t1 = min(n_tiles, t0 + tiles_per_chunk);
@@ -278,14 +303,16 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_mma)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_slot;
-    const uint32_t barp = smem_u32(&bar);
+    const uint32_t barm = smem_u32(&bar_mma);
+    const uint32_t barb = smem_u32(&bar_b);
 
     // obs quadrature points (3-point rule: barycentric 2/3, 1/6, 1/6)
     float x[3][3];
@@ -309,35 +336,45 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
                 x[q][d] = wb[q][0] * ot.v[0][d] + wb[q][1] * ot.v[1][d] + wb[q][2] * ot.v[2][d];
     }
 
-    uint32_t phase = 0;
-    bool ok = true;  // CTA-uniform
+    uint32_t phase_m = 0, phase_b = 0;
+    bool ok = true;            // CTA-uniform
+    bool mma_pending = false;  // CTA-uniform: a commit not yet waited for
+    bool copy_timeout = false;
     const uint32_t idesc = mr_instr_desc(N);
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const int col0 = half * NH;
     for (int64_t t = t0; t < t1; t++) {
-        if (t > t0) {
-            const bool w = mbar_wait(barp, phase);
+        if (mma_pending) {
+            const bool w = mbar_wait(barm, phase_m);
             if (!__syncthreads_and(w)) {
                 ok = false;  // the MMAs of the previous tile did not complete in time
                 break;
             }
-            phase ^= 1;
+            phase_m ^= 1;
+            mma_pending = false;
             if ((t - t0) % MR_FLUSH == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                tmem_fold<N>(lane_base, t - t0 == MR_FLUSH);
+                tmem_fold<N>(lane_base, col0, col0 + NH, t - t0 == MR_FLUSH);
                 asm volatile("tcgen05.fence::before_thread_sync;");
             }
         }
-        // B tile: one contiguous copy (hi + lo)
-        {
-            const float4* src = reinterpret_cast<const float4*>(Bg + t * (int64_t)2 * N * MR_K);
-            float4* dst = reinterpret_cast<float4*>(Bs);
-            for (int k = tid; k < 2 * N * MR_K / 4; k += 128) dst[k] = __ldg(src + k);
-        }
-        // A tile: the 7 kernel scalars per (obs, source) pair, split hi / lo
-        float av[MR_K];
+        // B tile: bulk async copy issued first, overlapping the generation
+        if (tid == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barb),
+                         "r"(B_BYTES)
+                         : "memory");
+            const unsigned char* src =
+                reinterpret_cast<const unsigned char*>(Bg) + t * (int64_t)B_BYTES;
 #pragma unroll
-        for (int sl = 0; sl < MR_S; sl++) {
-            const float* y = srcy + (t * MR_S + sl) * 9;
+            for (int cpy = 0; cpy < MR_COPIES; cpy++)
+                bulk_g2s(smem_u32(Bs) + cpy * (B_BYTES / MR_COPIES),
+                         src + cpy * (B_BYTES / MR_COPIES), B_BYTES / MR_COPIES, barb);
+        }
+        // A: this thread's half of the tile, 4 source triangles = 28 values
+        float av[MR_K / 2];
+#pragma unroll
+        for (int sl = 0; sl < MR_S / 2; sl++) {
+            const float* y = srcy + (t * MR_S + half * (MR_S / 2) + sl) * 9;
             float T00 = 0.f, T01 = 0.f, T02 = 0.f, T11 = 0.f, T12 = 0.f, T22 = 0.f;
 #pragma unroll
             for (int q2 = 0; q2 < 3; q2++) {
@@ -367,7 +404,7 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
             av[7 * sl + 6] = valid ? T22 : 0.f;
         }
 #pragma unroll
-        for (int ch = 0; ch < MR_K / 4; ch++) {
+        for (int ch = 0; ch < MR_K / 8; ch++) {
             float4 h, l;
             h.x = tf32_round(av[4 * ch + 0]);
             h.y = tf32_round(av[4 * ch + 1]);
@@ -377,12 +414,20 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
             l.y = tf32_round(av[4 * ch + 1] - h.y);
             l.z = tf32_round(av[4 * ch + 2] - h.z);
             l.w = tf32_round(av[4 * ch + 3] - h.w);
-            const uint32_t off = mr_off(tid, 4 * ch, MR_M);
+            const uint32_t off = mr_off(row, 4 * (half * (MR_K / 8) + ch), MR_M);
             *reinterpret_cast<float4*>(Ah + off) = h;
             *reinterpret_cast<float4*>(Al + off) = l;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        {
+            const bool wb = mbar_wait(barb, phase_b);
+            if (!__syncthreads_and(wb)) {
+                ok = false;
+                copy_timeout = true;
+                break;
+            }
+            phase_b ^= 1;
+        }
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t lboA = MR_M / 8 * 128, lboB = N / 8 * 128;
@@ -402,25 +447,30 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    barp)
+                    barm)
                 : "memory");
         }
+        mma_pending = true;
     }
-    if (t1 > t0) {
-        // the last commit (or, after a timeout, one more bounded wait for it)
-        const bool w = mbar_wait(barp, phase);
+    if (ok && mma_pending) {
+        const bool w = mbar_wait(barm, phase_m);
         if (!__syncthreads_and(w)) ok = false;
-        if (!ok && tid == 0) atomicExch(err, 1);
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+        // one more bounded wait for whatever is still in flight
+        if (copy_timeout) mbar_wait(barb, phase_b);
+        else mbar_wait(barm, phase_m);
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
 
-    // epilogue: fold the last group, then S (+ C) of this thread's row ->
-    // partial[chunk][r][o][9] (the obs-side contraction out[b][d] = J_o
-    // sum_j sc_o[b][j] W[d][j] is done by the reduce kernel)
+    // epilogue: fold the last group, then S - C of this thread's row and
+    // column half -> partial[chunk][r][o][9] (the obs-side contraction
+    // out[b][d] = J_o sum_j sc_o[b][j] W[d][j] is done by the reduce kernel)
     if (ok && t1 > t0) {
-        tmem_fold<N>(lane_base, t1 - t0 <= MR_FLUSH);
+        tmem_fold<N>(lane_base, col0, col0 + NH, t1 - t0 <= MR_FLUSH);
 #pragma unroll 1
-        for (int c0 = 0; c0 < N; c0 += 8) {
+        for (int c0 = col0; c0 < col0 + NH; c0 += 8) {
             float sv[8], cv[8];
             tmem_ld8(lane_base + N + c0, sv);
             tmem_ld8(lane_base + 2 * N + c0, cv);
@@ -557,8 +607,8 @@ int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, cons
                              (int)smem) != cudaSuccess)
         return launch_status("mrhs smem attribute");
     dim3 grid((unsigned)((n_obs + MR_M - 1) / MR_M), (unsigned)real);
-    mrhs_main<R><<<grid, 128, smem, st>>>(pts, obs_tris, n_obs, srcy, n_tiles, per, Bg, partial,
-                                          err);
+    mrhs_main<R><<<grid, MR_THREADS, smem, st>>>(pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
+                                                 partial, err);
     if ((rc = launch_status("mrhs main"))) return rc;
     mrhs_reduce<<<(unsigned)((n_obs * R + 127) / 128), 128, 0, st>>>(
         pts, obs_tris, n_obs, R, (int)real, partial, out, accumulate);
