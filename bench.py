@@ -1046,6 +1046,92 @@ def run_panel_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_workload(args, rank, world, torch, dist):
+    """Batched mixed-precision solves against the plain FP64 one-at-a-time
+    solve on the 722-triangle configuration."""
+    import tectosaur_b200 as tct
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    from tectosaur_b200.simple_solver import (free_edge_vertices, iterative_solve,
+                                              iterative_solve_batch, shared_vertex_matrix)
+    tol = 1e-8
+    R = args.rhs if args.rhs != 64 else 16
+    pts, tris = c1_mesh()
+    n = tris.shape[0]
+    op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
+                                           np.float64, TriToTriDirectFarfieldOp)
+    op32 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
+                                           np.float32, TriToTriDirectFarfieldOp)
+    cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+    rhs = np.random.default_rng(1 + rank).standard_normal((R, 9 * n))
+    rhs_d = torch.from_numpy(rhs).cuda()
+    for _ in range(args.warmup):
+        iterative_solve_batch(op64, op32, cm, rhs_d, tol=tol)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    lat = []
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        U = iterative_solve_batch(op64, op32, cm, rhs_d, tol=tol)
+        lat.append(time.perf_counter() - t0)
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    hist = iterative_solve_batch.last
+    # the plain path: FP64 operator, one solve at a time, same right-hand sides
+    iterative_solve(op64, cm, rhs[0], cfg=dict(solver_tol=tol))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    U64 = [iterative_solve(op64, cm, rhs[r], cfg=dict(solver_tol=tol)) for r in range(R)]
+    t_plain = time.perf_counter() - t0
+    err = max(float(np.linalg.norm(U[r] - U64[r]) / np.linalg.norm(U64[r])) for r in range(R))
+    if rank != 0:
+        return
+    ms = total_ms / args.steps
+    value = world * R * args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": "BEM solves/s: batched mixed precision (served) vs plain FP64",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 tensor-core farfield panel + f64 refinement",
+        "data": "synthetic (seeded mesh and right-hand sides)",
+        "config": {"workload": ("%d seeded N(0, 1) tractions on the 722-triangle plain-method "
+                                "mesh (elasticRH3, continuity + free edges) solved together: "
+                                "batched GMRES on the FP32 operator (farfield as one "
+                                "tensor-core panel apply per step) inside FP64 iterative "
+                                "refinement to 1e-8 FP64 residual" % R),
+                   "rhs_per_batch": R, "plain_fp64_solves_per_s": R / t_plain,
+                   "speedup_vs_plain": value / (R / t_plain),
+                   "max_rel_diff_vs_plain_fp64": err,
+                   "refinement_gmres_steps": hist["gmres_steps"],
+                   "refinement_residuals": hist["residuals"],
+                   "batch_latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+                   "batch_latency_ms_p99": 1e3 * float(np.percentile(lat, 99)),
+                   "l2": "small problem: working set in L2 (latency-bound solve)",
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "whole batched solve (launch- and sync-bound at this size)",
+                     "bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s",
+                     "frac": None, "traffic": None},
+        "e2e": {"value": value, "unit": "solves/s",
+                "h2d_bytes_per_step": int(rhs.nbytes), "d2h_bytes_per_step": int(U.nbytes),
+                "api": "simple_solver.iterative_solve_batch(op64, op32, cm, rhs panel) -> numpy"},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def config_block(n_tris, nnzb):
     return {
         "workload": ("direct-farfield 60k-triangle topographic surface (174x174 grid over "
@@ -1069,11 +1155,12 @@ def main():
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "fmm", "solve", "pairs", "panel"],
+                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
-                         "C2 farfield on a panel of --rhs vectors (tensor cores)")
+                         "C2 farfield on a panel of --rhs vectors (tensor cores); batch: "
+                         "batched mixed-precision solves vs the plain FP64 solve")
     ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--fmm-order", type=int, default=None)
@@ -1099,9 +1186,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs", "panel"):
+    if args.workload in ("fmm", "solve", "pairs", "panel", "batch"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
-         "panel": run_panel_workload}[args.workload](args, rank, world, torch, dist)
+         "panel": run_panel_workload, "batch": run_batch_workload}[args.workload](
+            args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()

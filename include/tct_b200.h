@@ -360,6 +360,11 @@ int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_
  * simple_solver.py:18-22.  x, y Real according to prec. */
 int tct_csr_matvec(int prec, int64_t n_rows, const int64_t* indptr, const int64_t* indices,
                    const double* data, const void* x, void* y, int accumulate, void* stream);
+/* The same for a panel of n_vec vectors: x + v * x_stride -> y + v * y_stride
+ * (strides in elements), one launch. */
+int tct_csr_matvec_panel(int prec, int64_t n_rows, const int64_t* indptr, const int64_t* indices,
+                         const double* data, const void* x, int64_t x_stride, void* y,
+                         int64_t y_stride, int n_vec, int accumulate, void* stream);
 
 #ifdef __cplusplus
 }

@@ -174,6 +174,8 @@ EXPORTED = sorted(set(EXPORTED) | set(_FMM_SIGS))
 
 _SOLVE_SIGS = {
     "tct_csr_matvec": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_p, c_i, c_p], c_i),
+    "tct_csr_matvec_panel": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_p],
+                             c_i),
     "tct_fp64_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
     "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i], c_sz),
     "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_dp, c_i, c_p,

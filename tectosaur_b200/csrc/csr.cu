@@ -12,9 +12,12 @@ template <typename R>
 __global__ void __launch_bounds__(256)
 csr_kernel(int64_t n_rows, const int64_t* __restrict__ indptr,
            const int64_t* __restrict__ indices, const double* __restrict__ data,
-           const R* __restrict__ x, R* __restrict__ y, int accumulate) {
+           const R* __restrict__ x, R* __restrict__ y, int accumulate, int64_t x_stride,
+           int64_t y_stride) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_rows) return;
+    x += blockIdx.y * x_stride;  // vector blockIdx.y of a panel
+    y += blockIdx.y * y_stride;
     double s = 0;
     for (int64_t k = indptr[i]; k < indptr[i + 1]; k++) s += data[k] * (double)x[indices[k]];
     y[i] = accumulate ? (R)((double)y[i] + s) : (R)s;
@@ -25,23 +28,32 @@ csr_kernel(int64_t n_rows, const int64_t* __restrict__ indptr,
 
 using namespace tct;
 
-extern "C" int tct_csr_matvec(int prec, int64_t n_rows, const int64_t* indptr,
-                              const int64_t* indices, const double* data, const void* x, void* y,
-                              int accumulate, void* stream) {
-    TCT_CHECK_ARG(n_rows >= 0, "tct_csr_matvec: negative row count");
-    if (n_rows == 0) return TCT_OK;
+extern "C" int tct_csr_matvec_panel(int prec, int64_t n_rows, const int64_t* indptr,
+                                    const int64_t* indices, const double* data, const void* x,
+                                    int64_t x_stride, void* y, int64_t y_stride, int n_vec,
+                                    int accumulate, void* stream) {
+    TCT_CHECK_ARG(n_rows >= 0 && n_vec >= 0 && n_vec < 65536,
+                  "tct_csr_matvec: bad row or vector count");
+    if (n_rows == 0 || n_vec == 0) return TCT_OK;
     TCT_CHECK_ARG(indptr && x && y, "tct_csr_matvec: null pointer");
     cudaStream_t st = as_stream(stream);
-    const unsigned grid = (unsigned)((n_rows + 255) / 256);
+    const dim3 grid((unsigned)((n_rows + 255) / 256), (unsigned)n_vec);
     if (prec == TCT_F64) {
         csr_kernel<double><<<grid, 256, 0, st>>>(n_rows, indptr, indices, data, (const double*)x,
-                                                 (double*)y, accumulate);
+                                                 (double*)y, accumulate, x_stride, y_stride);
     } else if (prec == TCT_F32) {
         csr_kernel<float><<<grid, 256, 0, st>>>(n_rows, indptr, indices, data, (const float*)x,
-                                                (float*)y, accumulate);
+                                                (float*)y, accumulate, x_stride, y_stride);
     } else {
         set_error("tct_csr_matvec: unsupported precision %d", prec);
         return TCT_ERR_PREC;
     }
     return launch_status("csr matvec");
+}
+
+extern "C" int tct_csr_matvec(int prec, int64_t n_rows, const int64_t* indptr,
+                              const int64_t* indices, const double* data, const void* x, void* y,
+                              int accumulate, void* stream) {
+    return tct_csr_matvec_panel(prec, n_rows, indptr, indices, data, x, 0, y, 0, 1, accumulate,
+                                stream);
 }

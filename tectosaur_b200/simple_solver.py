@@ -219,3 +219,166 @@ def iterative_solve(iop, cm, rhs, prec=None, cfg=None):
         op.cm.dot_device(x, full)
         return full.cpu().numpy()
     return x.cpu().numpy()
+
+
+# ---- many right-hand sides at once -----------------------------------------
+
+def gmres_batch(A, B, tol=1e-8, restart=200, maxiter=None):
+    """R independent restarted GMRES solves advancing in lockstep.
+
+    A: callable (R, n) -> (R, n) on torch tensors; B: (R, n) float64.  Every
+    step applies A to all R current basis vectors at once (the panel apply)
+    and brings back one (R, j + 2) Hessenberg block; each system keeps its own
+    Krylov basis, Givens rotations and stopping step, so a system that
+    converges or breaks down early stops updating.  Returns (X, info, n_iter)
+    with info[r] = 0 when system r reached ||b - A x|| <= tol ||b||."""
+    t = device.torch()
+    R, n = B.shape
+    bnorm = t.linalg.norm(B, dim=1).cpu().numpy()
+    X = t.zeros_like(B)
+    maxiter = 10 * n if maxiter is None else maxiter
+    m = max(1, min(restart, n))
+    V = t.empty((R, m + 1, n), dtype=B.dtype, device=B.device)
+    total = 0
+    first = True
+    bsafe = np.where(bnorm > 0, bnorm, 1.0)
+    while True:
+        Rr = B.clone() if first else B - A(X)
+        first = False
+        beta = t.linalg.norm(Rr, dim=1).cpu().numpy()
+        done0 = beta <= tol * bnorm
+        if done0.all():
+            return X, np.zeros(R, np.int64), total
+        bt = t.as_tensor(np.where(beta > 0, beta, 1.0), dtype=B.dtype, device=B.device)
+        V[:, 0] = Rr / bt[:, None]
+        H = np.zeros((R, m + 1, m))
+        cs = np.zeros((R, m))
+        sn = np.zeros((R, m))
+        g = np.zeros((R, m + 1))
+        g[:, 0] = beta
+        stop = np.where(done0, 0, -1)  # per system: steps used in this cycle (-1 = running)
+        j_end = m
+        for j in range(m):
+            W = A(V[:, j])
+            Vj = V[:, : j + 1]
+            h = t.bmm(Vj, W[:, :, None])[:, :, 0]
+            W = W - t.bmm(h[:, None, :], Vj)[:, 0]
+            h2 = t.bmm(Vj, W[:, :, None])[:, :, 0]
+            W = W - t.bmm(h2[:, None, :], Vj)[:, 0]
+            h = h + h2
+            hn = t.linalg.norm(W, dim=1)
+            col = t.cat([h, hn[:, None]], dim=1).cpu().numpy()  # the one sync of a step
+            H[:, : j + 2, j] = col
+            hs = t.where(hn > 0, hn, t.ones_like(hn))
+            V[:, j + 1] = W / hs[:, None]
+            for i in range(j):
+                a, c = H[:, i, j].copy(), H[:, i + 1, j].copy()
+                H[:, i, j] = cs[:, i] * a + sn[:, i] * c
+                H[:, i + 1, j] = -sn[:, i] * a + cs[:, i] * c
+            den = np.hypot(H[:, j, j], H[:, j + 1, j])
+            ok = den > 0
+            cs[:, j] = np.where(ok, H[:, j, j] / np.where(ok, den, 1.0), 1.0)
+            sn[:, j] = np.where(ok, H[:, j + 1, j] / np.where(ok, den, 1.0), 0.0)
+            H[:, j, j] = den
+            H[:, j + 1, j] = 0.0
+            g[:, j + 1] = -sn[:, j] * g[:, j]
+            g[:, j] = cs[:, j] * g[:, j]
+            total += 1
+            res = np.abs(g[:, j + 1]) / bsafe
+            newly = (stop < 0) & ((res <= tol) | (col[:, -1] == 0.0))
+            stop[newly] = j + 1
+            if (stop >= 0).all() or total >= maxiter:
+                j_end = j + 1
+                break
+        k = np.where(stop < 0, j_end, stop)
+        Y = np.zeros((R, j_end))
+        for r in range(R):
+            if k[r] > 0:
+                Y[r, : k[r]] = np.linalg.solve(np.triu(H[r, : k[r], : k[r]]), g[r, : k[r]])
+        X = X + t.bmm(t.as_tensor(Y, dtype=B.dtype, device=B.device)[:, None, :],
+                      V[:, :j_end])[:, 0]
+        if (stop >= 0).all() or total >= maxiter:
+            final = np.abs(g[np.arange(R), k]) / bsafe
+            return X, np.where(final <= tol, 0, total).astype(np.int64), total
+
+
+class ConstrainedPanelOperator:
+    """V (R, n_free) float64 -> cm^T A cm V for a panel of R vectors.  With an
+    FP32 elasticRH3 operator the farfield runs as one tensor-core panel apply
+    (TriToTriDirectFarfieldOp.dot_panel_device) and the nearfield BSR per
+    vector; other operators apply dot_device vector by vector."""
+
+    def __init__(self, iop, cm, R):
+        t = device.torch()
+        self.iop = iop
+        self.R = R
+        self.ft = device.torch_dtype(getattr(iop, "float_type", np.float64))
+        self.cm = DeviceCSR(cm)
+        self.cmT = DeviceCSR(cm.T)
+        self.n = cm.shape[1]
+        self.n_full_in, self.n_full_out = iop.shape[1], iop.shape[0]
+        self.U = t.zeros((R, self.n_full_in), dtype=t.float64, device="cuda")
+        self.Xf = t.zeros((R, self.n_full_in), dtype=self.ft, device="cuda")
+        self.Yf = t.zeros((R, self.n_full_out), dtype=self.ft, device="cuda")
+        far = getattr(iop, "farfield", None)
+        self.panel = (self.ft == t.float32 and far is not None and
+                      hasattr(far, "panel_supported") and far.panel_supported())
+
+    def _csr_panel(self, mat, X, Y):
+        _lib.check(_lib.lib.tct_csr_matvec_panel(
+            _lib.TCT_F64, mat.shape[0], _lib.tptr(mat.indptr), _lib.tptr(mat.indices),
+            _lib.tptr(mat.data), _lib.tptr(X), X.shape[1], _lib.tptr(Y), Y.shape[1], X.shape[0],
+            0, _lib.stream_ptr()), "tct_csr_matvec_panel")
+        return Y
+
+    def __call__(self, V):
+        t = device.torch()
+        R = V.shape[0]
+        U = self._csr_panel(self.cm, V.contiguous(), self.U[:R])
+        self.Xf[:R].copy_(U)
+        if self.panel:
+            self.iop.farfield.dot_panel_device(self.Xf[:R], self.Yf[:R])
+            for r in range(R):
+                self.iop.nearfield.dot_device(self.Xf[r], self.Yf[r], accumulate=True)
+        else:
+            for r in range(R):
+                self.iop.dot_device(self.Xf[r], self.Yf[r])
+        out = t.empty((R, self.n), dtype=t.float64, device="cuda")
+        return self._csr_panel(self.cmT, self.Yf[:R].to(t.float64), out)
+
+
+def iterative_solve_batch(iop64, iop32, cm, rhs, tol=1e-8, inner_tol=1e-5, restart=200,
+                          max_refine=8):
+    """R constrained solves at once, mixed precision: GMRES on the FP32
+    operator (tensor-core panel farfield) inside FP64 iterative refinement
+    with residuals of the FP64 operator, to ||cm^T (rhs - A u)|| <= tol
+    ||cm^T rhs|| in FP64 for every system.  rhs: (R, n_total) host or device;
+    returns (R, n_total) host float64 and records the refinement history in
+    iterative_solve_batch.last."""
+    t = device.torch()
+    rhs_d = (rhs if device.is_device_tensor(rhs) else
+             device.to_dev(np.asarray(rhs, np.float64))).to(t.float64)
+    R = rhs_d.shape[0]
+    A64 = ConstrainedPanelOperator(iop64, cm, R)
+    A32 = ConstrainedPanelOperator(iop32, cm, R)
+    b = A64._csr_panel(A64.cmT, rhs_d.contiguous(),
+                       t.empty((R, A64.n), dtype=t.float64, device="cuda"))
+    bn = t.linalg.norm(b, dim=1)
+    x = t.zeros_like(b)
+    steps, resid = [], []
+    for _ in range(max_refine):
+        r = b - A64(x) if steps else b.clone()
+        rel = float((t.linalg.norm(r, dim=1) / t.where(bn > 0, bn, t.ones_like(bn))).max())
+        resid.append(rel)
+        if rel <= tol:
+            break
+        d, info, n_it = gmres_batch(A32, r, tol=inner_tol, restart=restart)
+        steps.append(n_it)
+        x = x + d
+    else:
+        r = b - A64(x)
+        resid.append(float((t.linalg.norm(r, dim=1) / t.where(bn > 0, bn, t.ones_like(bn))).max()))
+    iterative_solve_batch.last = dict(gmres_steps=steps, residuals=resid)
+    full = t.empty((R, cm.shape[0]), dtype=t.float64, device="cuda")
+    A64._csr_panel(A64.cm, x.contiguous(), full)
+    return full.cpu().numpy()

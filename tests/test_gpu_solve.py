@@ -84,3 +84,27 @@ def test_fp32_operator_solve_reaches_fp32_accuracy(cuda, orc):
     u32 = iterative_solve(_op(pts, tris, np.float32), cm, rhs, cfg=dict(solver_tol=1e-5))
     u64 = iterative_solve(_op(pts, tris, np.float64), cm, rhs, cfg=dict(solver_tol=1e-10))
     assert np.linalg.norm(u32 - u64) / np.linalg.norm(u64) < 1e-3
+
+
+def test_batched_mixed_precision_solves(cuda, orc):
+    """16 right-hand sides solved together (FP32 tensor-core panel operator
+    inside FP64 refinement) agree with the plain FP64 one-at-a-time solve,
+    reach the FP64 residual bar, and a system's answer does not depend on the
+    batch it is solved in."""
+    from tectosaur_b200.simple_solver import iterative_solve_batch
+    pts, tris = bumpy_mesh(8, seed=3)
+    cm = _cm(tris)
+    op64 = _op(pts, tris, np.float64)
+    op32 = _op(pts, tris, np.float32)
+    rhs = np.random.default_rng(4).standard_normal((16, tris.shape[0] * 9))
+    U = iterative_solve_batch(op64, op32, cm, rhs, tol=1e-9)
+    assert iterative_solve_batch.last["residuals"][-1] <= 1e-9
+    for r in [0, 9]:
+        u64 = iterative_solve(op64, cm, rhs[r], cfg=dict(solver_tol=1e-11))
+        assert np.linalg.norm(U[r] - u64) / np.linalg.norm(u64) < 1e-7
+        res = cm.T @ (_oracle_apply(orc, pts, tris, U[r]) - rhs[r])
+        assert np.linalg.norm(res) / np.linalg.norm(cm.T @ rhs[r]) < 2e-9
+    alone = iterative_solve_batch(op64, op32, cm, rhs[5:6], tol=1e-9)
+    mixed = iterative_solve_batch(op64, op32, cm, np.concatenate([rhs[5:6], rhs[:3]]), tol=1e-9)
+    assert np.linalg.norm(alone[0] - U[5]) / np.linalg.norm(U[5]) < 1e-7
+    assert np.linalg.norm(mixed[0] - U[5]) / np.linalg.norm(U[5]) < 1e-7

@@ -91,3 +91,20 @@ def test_free_edges_and_fixed_vertices():
     corner_vert = np.repeat(tris.reshape(-1), 3)
     assert np.all(rows_hit[np.isin(corner_vert, fv)] == 0)
     assert np.all(rows_hit[~np.isin(corner_vert, fv)] == 1)
+
+
+def test_gmres_batch_matches_single_solves():
+    from tectosaur_b200.simple_solver import gmres_batch
+    rng = np.random.default_rng(7)
+    n, R = 120, 5
+    As = [np.eye(n) + 0.35 * rng.standard_normal((n, n)) / np.sqrt(n) for _ in range(R)]
+    # one operator for all systems (as in the solve), different right-hand sides
+    A = torch.from_numpy(As[0])
+    B = torch.from_numpy(rng.standard_normal((R, n)))
+    B[3] = 0.0  # a zero right-hand side converges at once
+    X, info, n_it = gmres_batch(lambda V: V @ A.T, B, tol=1e-11, restart=20)
+    assert np.all(info == 0)
+    for r in range(R):
+        want = np.linalg.solve(As[0], B[r].numpy())
+        assert np.linalg.norm(X[r].numpy() - want) <= 1e-9 * max(np.linalg.norm(want), 1e-300)
+    assert float(X[3].abs().max()) == 0.0
