@@ -1055,7 +1055,12 @@ def run_batch_workload(args, rank, world, torch, dist):
                                               iterative_solve_batch, shared_vertex_matrix)
     tol = 1e-8
     R = args.rhs if args.rhs != 64 else 16
-    pts, tris = c1_mesh()
+    if args.grid is None:
+        pts, tris = c1_mesh()
+    else:
+        from tectosaur_b200.mesh.mesh_gen import make_rect
+        g = args.grid
+        pts, tris = make_rect(g, g, [[-1, -1, 0], [-1, 1, 0], [1, 1, 0], [1, -1, 0]])
     n = tris.shape[0]
     op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
                                            np.float64, TriToTriDirectFarfieldOp)
@@ -1106,11 +1111,13 @@ def run_batch_workload(args, rank, world, torch, dist):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 tensor-core farfield panel + f64 refinement",
         "data": "synthetic (seeded mesh and right-hand sides)",
-        "config": {"workload": ("%d seeded N(0, 1) tractions on the 722-triangle plain-method "
-                                "mesh (elasticRH3, continuity + free edges) solved together: "
-                                "batched GMRES on the FP32 operator (farfield as one "
-                                "tensor-core panel apply per step) inside FP64 iterative "
-                                "refinement to 1e-8 FP64 residual" % R),
+        "config": {"workload": ("%d seeded N(0, 1) tractions on the %d-triangle planar fault "
+                                "(make_rect over [-1, 1]^2, elasticRH3, continuity + free "
+                                "edges) solved together: batched GMRES on the FP32 operator "
+                                "(farfield as one tensor-core panel apply and nearfield as one "
+                                "BSR panel launch per step) inside FP64 iterative refinement "
+                                "to 1e-8 FP64 residual" % (R, n)),
+                   "n_tris": int(n),
                    "rhs_per_batch": R, "plain_fp64_solves_per_s": R / t_plain,
                    "speedup_vs_plain": value / (R / t_plain),
                    "max_rel_diff_vs_plain_fp64": err,

@@ -162,6 +162,16 @@ int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
                     int64_t data_stride, const void* x, void* y, int accumulate,
                     void* stream);
 
+/* Panel form of tct_bsr9_matvec (an addition: the reference applies its
+ * BSR matrix to one vector at a time, util/sparse.py:44-64): y_v (+)= A x_v
+ * for v < n_vec, x_v = x + v * x_stride, y_v = y + v * y_stride (strides in
+ * Reals; y_stride >= 9 * n_row_blocks).  Each block is read from HBM once
+ * per apply (vector groups of 8 (FP32) / 4 (FP64) re-read it from L2). */
+int tct_bsr9_matvec_panel(int prec, int64_t n_row_blocks, const int32_t* indptr,
+                          const int32_t* indices, const void* data, int64_t data_stride,
+                          const void* x, int64_t x_stride, void* y, int64_t y_stride,
+                          int n_vec, int accumulate, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Measurement utility (no reference counterpart): FP32 FMA throughput probe.
  * Launches n_blocks x 256 threads, each running `iters` steps of 8 independent
@@ -332,25 +342,28 @@ int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
 
 /* ---- multi-RHS farfield on the tensor cores ------------------------------- */
 
-/* Direct farfield of elasticRH3 (FP32, 3-point rule) applied to a panel of R
- * input vectors at once: out[r] (+)= Far in[r] for r < R (R = 16).
+/* Direct farfield of elasticRH3 (FP32; n_q = 3, 4 or 7 point triangle rule,
+ * quad_pts / quad_wts as in tct_farfield_tris_matvec) applied to a panel of
+ * R input vectors at once: out[r] (+)= Far in[r] for r < R (R = 16).
  * The reference applies farfield_tris_to_tris{K} (matrix_free.cl:19-107) to
  * one vector per call; here the per-triangle-pair kernel scalars are
  * generated on the CUDA cores and contracted with the input panel by
  * tcgen05.mma (split TF32, FP32 accumulation in tensor memory folded into
  * a Kahan pair every 4 source tiles).
  * in: R x (9 n_src) floats, out: R x (9 n_obs) floats (device, vector after
- * vector); pts / tris as in tct_farfield_tris_matvec. */
-size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R);
+ * vector); pts / tris as in tct_farfield_tris_matvec.  The workspace size
+ * is 0 for an unsupported R or rule. */
+size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R, int n_q);
 int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
                                  const int32_t* obs_tris, int64_t n_obs,
-                                 const int32_t* src_tris, int64_t n_src, int R,
+                                 const int32_t* src_tris, int64_t n_src, int R, int n_q,
+                                 const double* quad_pts, const double* quad_wts,
                                  const double* params, int accumulate, void* workspace,
                                  size_t workspace_bytes, void* stream);
 /* Reads (synchronising the stream) the error word of the last panel apply
  * with this workspace: 0 = ok, 1 = a bounded wait on the tensor cores gave up. */
 int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
-                                void* stream, int* host_flag);
+                                int n_q, void* stream, int* host_flag);
 
 /* ---- constrained solve -------------------------------------------------- */
 

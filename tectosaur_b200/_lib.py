@@ -59,6 +59,8 @@ _SIGS = {
     "tct_farfield_tris_matvec_noalloc": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i,
                                           c_dp, c_dp, c_dp, c_i, c_p], c_i),
     "tct_bsr9_matvec": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_i, c_p], c_i),
+    "tct_bsr9_matvec_panel": ([c_i, c_i64, c_p, c_p, c_p, c_i64, c_p, c_i64, c_p, c_i64, c_i,
+                               c_i, c_p], c_i),
     "tct_find_near_pairs": ([c_dp, c_dp, c_i64, c_dp, c_dp, c_i64, ctypes.c_double, c_i,
                              ctypes.POINTER(c_p)], c_i),
     "tct_pairs_count": ([c_p], c_i64),
@@ -177,10 +179,10 @@ _SOLVE_SIGS = {
     "tct_csr_matvec_panel": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_p],
                              c_i),
     "tct_fp64_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
-    "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i], c_sz),
-    "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_dp, c_i, c_p,
-                                      c_sz, c_p], c_i),
-    "tct_farfield_rh_panel_error": ([c_p, c_i64, c_i64, c_i, c_p, ctypes.POINTER(c_i)], c_i),
+    "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i, c_i], c_sz),
+    "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_dp, c_dp,
+                                      c_dp, c_i, c_p, c_sz, c_p], c_i),
+    "tct_farfield_rh_panel_error": ([c_p, c_i64, c_i64, c_i, c_i, c_p, ctypes.POINTER(c_i)], c_i),
 }
 for _name, (_args, _res) in _SOLVE_SIGS.items():
     _f = getattr(lib, _name)

@@ -10,6 +10,8 @@
 // (FP32) or 256-byte (FP64) transaction; x is gathered through L1/L2 (it is
 // 9 Reals per triangle and stays cache resident).  Each lane keeps 9 row
 // partial sums, reduced across the warp with shuffles at the end of the row.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace tct {
@@ -87,6 +89,89 @@ int run_bsr(int64_t n_rows, const int32_t* indptr, const int32_t* indices, const
     return launch_status("tct_bsr9_matvec");
 }
 
+
+// Panel form: y_v (+)= A x_v for n_vec vectors (x_v at x + v * x_stride,
+// y_v at y + v * y_stride).  Each block is read once per group of NV
+// vectors: a lane loads column j of its block (9 values) and updates the
+// NV x 9 row sums with x_v[col*9 + j].  The flattened grid puts the NV-vector
+// groups of a row range in consecutive blocks, which run together, so a
+// block row is fetched from HBM once and re-read from L2 by the other groups.
+template <typename R, int NV>
+__global__ void __launch_bounds__(256, 2)
+bsr9_panel_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
+                  const int32_t* __restrict__ indices, const R* __restrict__ data,
+                  int64_t stride, const R* __restrict__ x, int64_t x_stride,
+                  R* __restrict__ y, int64_t y_stride, int n_vec, int n_groups,
+                  int accumulate) {
+    const int lane = threadIdx.x & 31;
+    const int group = (int)(blockIdx.x % (unsigned)n_groups);
+    const int64_t xb = blockIdx.x / (unsigned)n_groups;
+    const int64_t n_xb = gridDim.x / (unsigned)n_groups;
+    const int v0 = group * NV;
+    const int nv = min(NV, n_vec - v0);
+    const int wpb = blockDim.x >> 5;
+    const int64_t warp = xb * wpb + (threadIdx.x >> 5);
+    const int64_t n_warps = n_xb * wpb;
+    const R* xg = x + (int64_t)v0 * x_stride;
+    for (int64_t row = warp; row < n_rows; row += n_warps) {
+        const int32_t start = __ldg(indptr + row), end = __ldg(indptr + row + 1);
+        R acc[NV][9];
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+            for (int i = 0; i < 9; i++) acc[v][i] = 0;
+        for (int32_t s = start + lane; s < end; s += 32) {
+            const int64_t col9 = (int64_t)__ldg(indices + s) * 9;
+#pragma unroll 1
+            for (int j = 0; j < 9; j++) {
+                R a[9];
+#pragma unroll
+                for (int i = 0; i < 9; i++) a[i] = __ldg(data + (int64_t)(i * 9 + j) * stride + s);
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    if (v < nv) {
+                        const R xs = __ldg(xg + v * x_stride + col9 + j);
+#pragma unroll
+                        for (int i = 0; i < 9; i++) acc[v][i] += a[i] * xs;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+#pragma unroll
+            for (int i = 0; i < 9; i++)
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                    acc[v][i] += __shfl_xor_sync(0xffffffffu, acc[v][i], off);
+            if (lane < 9 && v < nv) {
+                R val = acc[v][0];
+#pragma unroll
+                for (int i = 1; i < 9; i++)
+                    if (lane == i) val = acc[v][i];
+                R* yp = y + (int64_t)(v0 + v) * y_stride + row * 9 + lane;
+                *yp = accumulate ? *yp + val : val;
+            }
+        }
+    }
+}
+
+template <typename R, int NV>
+int run_bsr_panel(int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+                  const void* data, int64_t stride, const void* x, int64_t x_stride, void* y,
+                  int64_t y_stride, int n_vec, int accumulate, cudaStream_t st) {
+    const int threads = 256;
+    const int n_groups = (n_vec + NV - 1) / NV;
+    const int64_t max_xb = std::max<int64_t>(1, (int64_t)sm_count() * 4 / n_groups);
+    int64_t xb = (n_rows * 32 + threads - 1) / threads;
+    if (xb > max_xb) xb = max_xb;
+    if (xb < 1) xb = 1;
+    bsr9_panel_kernel<R, NV><<<(unsigned)(xb * n_groups), threads, 0, st>>>(
+        n_rows, indptr, indices, (const R*)data, stride, (const R*)x, x_stride, (R*)y, y_stride,
+        n_vec, n_groups, accumulate);
+    return launch_status("tct_bsr9_matvec_panel");
+}
+
 }  // namespace
 }  // namespace tct
 
@@ -106,5 +191,30 @@ extern "C" int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* in
         return run_bsr<double>(n_row_blocks, indptr, indices, data, data2, data_stride, x, y,
                                accumulate, as_stream(stream));
     set_error("tct_bsr9_matvec: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
+
+extern "C" int tct_bsr9_matvec_panel(int prec, int64_t n_row_blocks, const int32_t* indptr,
+                                     const int32_t* indices, const void* data,
+                                     int64_t data_stride, const void* x, int64_t x_stride,
+                                     void* y, int64_t y_stride, int n_vec, int accumulate,
+                                     void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_row_blocks >= 0 && data_stride >= 0 && n_vec >= 0,
+                  "tct_bsr9_matvec_panel: negative size");
+    if (n_row_blocks == 0 || n_vec == 0) return TCT_OK;
+    TCT_CHECK_ARG(indptr && y && x, "tct_bsr9_matvec_panel: null pointer");
+    TCT_CHECK_ARG(data_stride < (int64_t(1) << 31), "tct_bsr9_matvec_panel: more than 2^31 blocks");
+    TCT_CHECK_ARG(n_vec == 1 || (x_stride >= 0 && y_stride >= 9 * n_row_blocks),
+                  "tct_bsr9_matvec_panel: vector strides overlap");
+    if (prec == TCT_F32)
+        return run_bsr_panel<float, 8>(n_row_blocks, indptr, indices, data, data_stride, x,
+                                       x_stride, y, y_stride, n_vec, accumulate,
+                                       as_stream(stream));
+    if (prec == TCT_F64)
+        return run_bsr_panel<double, 4>(n_row_blocks, indptr, indices, data, data_stride, x,
+                                        x_stride, y, y_stride, n_vec, accumulate,
+                                        as_stream(stream));
+    set_error("tct_bsr9_matvec_panel: unsupported precision %d", prec);
     return TCT_ERR_PREC;
 }

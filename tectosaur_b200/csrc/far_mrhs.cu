@@ -1,10 +1,11 @@
-// Multi-RHS direct farfield for elasticRH3 (FP32, 3-point rule) on the
+// Multi-RHS direct farfield for elasticRH3 (FP32; 3-, 4- and 7-point rules) on the
 // 5th-generation tensor cores: y_r = Far x_r for a panel of R right-hand
 // sides (the reference applies farfield_tris_to_tris once per vector,
 // tectosaur/matrix_free.cl:19-107).
 //
-// For elasticRH3 the 9 point pairs of a triangle pair reduce to the scalar
-// S0 and the symmetric 3x3 T (the direct kernel's factorisation), and the
+// For elasticRH3 the NQ x NQ point pairs of a triangle pair reduce to the
+// scalar S0 and the symmetric 3x3 T (the direct kernel's factorisation:
+// T = sum_q1,q2 w_q1 w_q2 D D^T / r^3 over the point pairs), and the
 // input enters only through per-source 3x3 matrices P and M = -2 ssc:
 //   W_o[d][j] += S0 P_s[d][j] + sum_k T[d][k] M_s[k][j].
 // With R inputs this is a GEMM:
@@ -41,7 +42,7 @@
 // allocating tensor memory.
 #include <algorithm>
 
-#include "common.cuh"
+#include "far_common.cuh"
 
 namespace tct {
 namespace {
@@ -244,6 +245,7 @@ mrhs_prep(Consts<float> c, float w2, const float* __restrict__ pts,
 }
 
 // ---- main: generate A, copy B, tcgen05.mma into TMEM ------------------------
+// Observation quadrature points of the rule (barycentric 1 - x - y, x, y).
 // grid (obs blocks of 128, source chunks); 256 threads: thread (row, half)
 // generates row `row` of A for the half `half` of the tile's 8 source
 // triangles; one thread issues the B tile as a bulk async copy (completing
@@ -263,9 +265,10 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
         : "memory");
 }
 
-template <int R>
+template <int R, int NQ, bool UNIFORM>
 __global__ void __launch_bounds__(MR_THREADS, 1)
-mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, int64_t n_obs,
+mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __restrict__ obs_tris,
+          int64_t n_obs,
           const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
           const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
     constexpr int N = 9 * R;
@@ -314,8 +317,9 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
     const uint32_t barm = smem_u32(&bar_mma);
     const uint32_t barb = smem_u32(&bar_b);
 
-    // obs quadrature points (3-point rule: barycentric 2/3, 1/6, 1/6)
-    float x[3][3];
+    // obs quadrature points of the rule; weight products for non-uniform rules
+    // (a uniform rule's w^2 is folded into B by mrhs_prep)
+    float x[NQ][3];
     {
         TriGeom<float> ot;
         if (valid) {
@@ -326,14 +330,19 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
 #pragma unroll
                 for (int d = 0; d < 3; d++) ot.v[a][d] = 0.f;
         }
-        const float wb[3][3] = {{2.f / 3.f, 1.f / 6.f, 1.f / 6.f},
-                                {1.f / 6.f, 2.f / 3.f, 1.f / 6.f},
-                                {1.f / 6.f, 1.f / 6.f, 2.f / 3.f}};
 #pragma unroll
-        for (int q = 0; q < 3; q++)
+        for (int q = 0; q < NQ; q++) {
+            const float bq[3] = {1.f - rule.x[q] - rule.y[q], rule.x[q], rule.y[q]};
 #pragma unroll
-            for (int d = 0; d < 3; d++)
-                x[q][d] = wb[q][0] * ot.v[0][d] + wb[q][1] * ot.v[1][d] + wb[q][2] * ot.v[2][d];
+            for (int d = 0; d < 3; d++) x[q][d] = bary_point(ot, bq, d);
+        }
+    }
+    float wq[UNIFORM ? 1 : NQ * NQ];
+    if (!UNIFORM) {
+#pragma unroll
+        for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+            for (int q2 = 0; q2 < NQ; q2++) wq[q1 * NQ + q2] = rule.w[q1] * rule.w[q2];
     }
 
     uint32_t phase_m = 0, phase_b = 0;
@@ -374,18 +383,19 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
         float av[MR_K / 2];
 #pragma unroll
         for (int sl = 0; sl < MR_S / 2; sl++) {
-            const float* y = srcy + (t * MR_S + half * (MR_S / 2) + sl) * 9;
+            const float* y = srcy + (t * MR_S + half * (MR_S / 2) + sl) * (3 * NQ);
             float T00 = 0.f, T01 = 0.f, T02 = 0.f, T11 = 0.f, T12 = 0.f, T22 = 0.f;
 #pragma unroll
-            for (int q2 = 0; q2 < 3; q2++) {
+            for (int q2 = 0; q2 < NQ; q2++) {
                 const float y0 = __ldg(y + 3 * q2), y1 = __ldg(y + 3 * q2 + 1),
                             y2 = __ldg(y + 3 * q2 + 2);
 #pragma unroll
-                for (int q1 = 0; q1 < 3; q1++) {
+                for (int q1 = 0; q1 < NQ; q1++) {
                     const float D0 = y0 - x[q1][0], D1 = y1 - x[q1][1], D2 = y2 - x[q1][2];
                     const float r2 = fmaf(D0, D0, fmaf(D1, D1, fmaf(D2, D2, MR_EPS)));
                     const float ir = rsqrtf(r2);
-                    const float g = ir * ir * ir;
+                    float g = ir * ir * ir;
+                    if (!UNIFORM) g *= wq[q1 * NQ + q2];
                     const float g0 = g * D0, g1 = g * D1, g2 = g * D2;
                     T00 = fmaf(g0, D0, T00);
                     T01 = fmaf(g0, D1, T01);
@@ -493,30 +503,30 @@ mrhs_main(const float* __restrict__ pts, const int32_t* __restrict__ obs_tris, i
     }
 }
 
-// Source quadrature points (3 x 3 per source triangle, padded with far-away
+// Source quadrature points (NQ x 3 per source triangle, padded with far-away
 // points that contribute nothing: their A entries are multiplied by zero rows
 // of B).
+template <int NQ>
 __global__ void __launch_bounds__(128)
-mrhs_points(const float* __restrict__ pts, const int32_t* __restrict__ src_tris, int64_t n_src,
-            int64_t n_src_pad, float* __restrict__ srcy) {
+mrhs_points(Rule2D<float> rule, const float* __restrict__ pts,
+            const int32_t* __restrict__ src_tris, int64_t n_src, int64_t n_src_pad,
+            float* __restrict__ srcy) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_src_pad) return;
-    const float wb[3][3] = {{2.f / 3.f, 1.f / 6.f, 1.f / 6.f},
-                            {1.f / 6.f, 2.f / 3.f, 1.f / 6.f},
-                            {1.f / 6.f, 1.f / 6.f, 2.f / 3.f}};
-    float* y = srcy + s * 9;
+    float* y = srcy + s * (3 * NQ);
     if (s >= n_src) {
 #pragma unroll
-        for (int k = 0; k < 9; k++) y[k] = 1e18f;
+        for (int k = 0; k < 3 * NQ; k++) y[k] = 1e18f;
         return;
     }
     TriGeom<float> t;
     load_tri(t, pts, src_tris, s, 0, false, false);
 #pragma unroll
-    for (int q = 0; q < 3; q++)
+    for (int q = 0; q < NQ; q++) {
+        const float bq[3] = {1.f - rule.x[q] - rule.y[q], rule.x[q], rule.y[q]};
 #pragma unroll
-        for (int d = 0; d < 3; d++)
-            y[3 * q + d] = wb[q][0] * t.v[0][d] + wb[q][1] * t.v[1][d] + wb[q][2] * t.v[2][d];
+        for (int d = 0; d < 3; d++) y[3 * q + d] = bary_point(t, bq, d);
+    }
 }
 
 // Sum the chunk partials in a fixed order and apply the obs-side contraction:
@@ -568,32 +578,33 @@ struct MrhsSizes {
     size_t B, y, partial, err;
 };
 
-MrhsSizes mrhs_sizes(int64_t n_obs, int64_t n_src, int R) {
+MrhsSizes mrhs_sizes(int64_t n_obs, int64_t n_src, int R, int nq) {
     const int64_t n_pad = (n_src + MR_S - 1) / MR_S * MR_S;
     const int64_t n_tiles = n_pad / MR_S;
     MrhsSizes s;
     s.B = al256((size_t)n_tiles * 2 * 9 * R * MR_K * 4);
-    s.y = al256((size_t)n_pad * 9 * 4);
+    s.y = al256((size_t)n_pad * 3 * nq * 4);
     s.partial = al256((size_t)mrhs_chunks(n_obs, n_tiles) * R * n_obs * 9 * 4);
     s.err = 256;
     return s;
 }
 
-template <int R>
-int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, const float* pts,
-             const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris, int64_t n_src,
-             int accumulate, unsigned char* ws, cudaStream_t st) {
+template <int R, int NQ, bool UNIFORM>
+int run_mrhs(const Consts<float>& c, const Rule2D<float>& rule, float* out, const float* in,
+             const float* pts, const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris,
+             int64_t n_src, int accumulate, unsigned char* ws, cudaStream_t st) {
     constexpr int N = 9 * R;
     const int64_t n_pad = (n_src + MR_S - 1) / MR_S * MR_S;
     const int64_t n_tiles = n_pad / MR_S;
-    const MrhsSizes sz = mrhs_sizes(n_obs, n_src, R);
+    const MrhsSizes sz = mrhs_sizes(n_obs, n_src, R, NQ);
+    const float w2 = UNIFORM ? rule.w[0] * rule.w[0] : 1.f;
     float* Bg = reinterpret_cast<float*>(ws);
     float* srcy = reinterpret_cast<float*>(ws + sz.B);
     float* partial = reinterpret_cast<float*>(ws + sz.B + sz.y);
     int* err = reinterpret_cast<int*>(ws + sz.B + sz.y + sz.partial);
     if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return launch_status("mrhs memset");
-    mrhs_points<<<(unsigned)((n_pad + 127) / 128), 128, 0, st>>>(pts, src_tris, n_src, n_pad,
-                                                                 srcy);
+    mrhs_points<NQ><<<(unsigned)((n_pad + 127) / 128), 128, 0, st>>>(rule, pts, src_tris, n_src,
+                                                                     n_pad, srcy);
     int rc = launch_status("mrhs points");
     if (rc) return rc;
     mrhs_prep<<<(unsigned)((n_pad * R + 127) / 128), 128, 0, st>>>(c, w2, pts, src_tris, n_src,
@@ -603,12 +614,13 @@ int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, cons
     const int64_t per = (n_tiles + chunks - 1) / chunks;
     const int64_t real = (n_tiles + per - 1) / per;
     const size_t smem = (size_t)2 * MR_M * MR_K * 4 + (size_t)2 * N * MR_K * 4;
-    if (cudaFuncSetAttribute(mrhs_main<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+    auto kfn = mrhs_main<R, NQ, UNIFORM>;
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
         return launch_status("mrhs smem attribute");
     dim3 grid((unsigned)((n_obs + MR_M - 1) / MR_M), (unsigned)real);
-    mrhs_main<R><<<grid, MR_THREADS, smem, st>>>(pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
-                                                 partial, err);
+    kfn<<<grid, MR_THREADS, smem, st>>>(rule, pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
+                                        partial, err);
     if ((rc = launch_status("mrhs main"))) return rc;
     mrhs_reduce<<<(unsigned)((n_obs * R + 127) / 128), 128, 0, st>>>(
         pts, obs_tris, n_obs, R, (int)real, partial, out, accumulate);
@@ -620,17 +632,20 @@ int run_mrhs(const Consts<float>& c, float w2, float* out, const float* in, cons
 
 using namespace tct;
 
-extern "C" size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R) {
-    if (R != 16) return 0;
-    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
+inline bool mrhs_rule_ok(int nq) { return nq == 3 || nq == 4 || nq == 7; }
+
+extern "C" size_t tct_farfield_rh_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R,
+                                                        int n_q) {
+    if (R != 16 || !mrhs_rule_ok(n_q) || n_obs < 0 || n_src < 0) return 0;
+    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R, n_q);
     return s.B + s.y + s.partial + s.err;
 }
 
 extern "C" int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src,
-                                           int R, void* stream, int* host_flag) {
-    TCT_CHECK_ARG(workspace && host_flag && R == 16,
+                                           int R, int n_q, void* stream, int* host_flag) {
+    TCT_CHECK_ARG(workspace && host_flag && R == 16 && mrhs_rule_ok(n_q),
                   "tct_farfield_rh_panel_error: bad arguments");
-    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R);
+    const MrhsSizes s = mrhs_sizes(n_obs, n_src, R, n_q);
     cudaStream_t st = as_stream(stream);
     if (cudaMemcpyAsync(host_flag, reinterpret_cast<const unsigned char*>(workspace) + s.B + s.y +
                                        s.partial,
@@ -643,18 +658,30 @@ extern "C" int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs,
 extern "C" int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
                                             const int32_t* obs_tris, int64_t n_obs,
                                             const int32_t* src_tris, int64_t n_src, int R,
-                                            const double* params, int accumulate, void* workspace,
+                                            int n_q, const double* quad_pts,
+                                            const double* quad_wts, const double* params,
+                                            int accumulate, void* workspace,
                                             size_t workspace_bytes, void* stream) {
     TCT_CHECK_ARG(R == 16, "tct_farfield_rh_panel_matvec: R must be 16 (got %d)", R);
+    TCT_CHECK_ARG(mrhs_rule_ok(n_q),
+                  "tct_farfield_rh_panel_matvec: %d-point rule (supported: 3, 4, 7)", n_q);
     TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_rh_panel_matvec: negative size");
-    TCT_CHECK_ARG(params, "tct_farfield_rh_panel_matvec: null params");
+    TCT_CHECK_ARG(params && quad_pts && quad_wts,
+                  "tct_farfield_rh_panel_matvec: null params or rule");
     if (n_obs == 0) return TCT_OK;
-    const size_t need = tct_farfield_rh_panel_workspace_bytes(n_obs, n_src, R);
+    const size_t need = tct_farfield_rh_panel_workspace_bytes(n_obs, n_src, R, n_q);
     TCT_CHECK_ARG(workspace && workspace_bytes >= need && aligned(workspace, 256),
                   "tct_farfield_rh_panel_matvec: workspace of %zu bytes (256-aligned) required",
                   need);
     const Consts<float> c = make_consts<float>(params);
-    const float w = 1.f / 6.f;  // the 3-point rule's weights
+    Rule2D<float> rule;
+    bool uniform = true;
+    for (int q = 0; q < MAXQ; q++) {
+        rule.x[q] = q < n_q ? (float)quad_pts[2 * q] : 0.f;
+        rule.y[q] = q < n_q ? (float)quad_pts[2 * q + 1] : 0.f;
+        rule.w[q] = q < n_q ? (float)quad_wts[q] : 0.f;
+        if (q < n_q) uniform = uniform && quad_wts[q] == quad_wts[0];
+    }
     unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
     cudaStream_t st = as_stream(stream);
     if (n_src == 0) {
@@ -662,6 +689,18 @@ extern "C" int tct_farfield_rh_panel_matvec(void* out, const void* in, const voi
             return launch_status("tct_farfield_rh_panel_matvec memset");
         return TCT_OK;
     }
-    return run_mrhs<16>(c, w * w, (float*)out, (const float*)in, (const float*)pts, obs_tris,
-                        n_obs, src_tris, n_src, accumulate, ws, st);
+    float* o = (float*)out;
+    const float* x = (const float*)in;
+    const float* p = (const float*)pts;
+#define TCT_MRHS(NQV)                                                                        \
+    return uniform ? run_mrhs<16, NQV, true>(c, rule, o, x, p, obs_tris, n_obs, src_tris, n_src, \
+                                             accumulate, ws, st)                               \
+                   : run_mrhs<16, NQV, false>(c, rule, o, x, p, obs_tris, n_obs, src_tris,       \
+                                              n_src, accumulate, ws, st);
+    switch (n_q) {
+        case 3: TCT_MRHS(3)
+        case 4: TCT_MRHS(4)
+        default: TCT_MRHS(7)
+    }
+#undef TCT_MRHS
 }

@@ -175,6 +175,10 @@ class RegularizedNearfieldIntegralOp:
         """y (+)= Near x on device tensors of float_type."""
         return self.bsr.matvec(x, y, accumulate=accumulate, stream=stream)
 
+    def dot_panel_device(self, X, Y, accumulate=False, stream=None):
+        """Y[r] (+)= Near X[r] for device tensors X (R, n_cols), Y (R, n_rows)."""
+        return self.bsr.matvec_panel(X, Y, accumulate=accumulate, stream=stream)
+
     def _host_or_device(self, v, fn):
         if device.is_device_tensor(v):
             x = v.to(device.torch_dtype(self.float_type)).contiguous()

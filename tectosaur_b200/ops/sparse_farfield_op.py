@@ -67,12 +67,13 @@ class TriToTriDirectFarfieldOp:
 
     # -- many right-hand sides ------------------------------------------------
     def panel_supported(self):
-        """The tensor-core panel path: elasticRH3, FP32, the 3-point rule."""
-        return self.K_name == "elasticRH3" and self.prec == _lib.TCT_F32 and self.n_q == 3
+        """The tensor-core panel path: elasticRH3, FP32, a 3-, 4- or 7-point rule."""
+        return (self.K_name == "elasticRH3" and self.prec == _lib.TCT_F32
+                and self.n_q in (3, 4, 7))
 
     def dot_panel_device(self, X, Y, accumulate=False, stream=None):
         """Y[r] (+)= Far X[r] for device tensors X (R, 9 n_src), Y (R, 9 n_obs).
-        elasticRH3 / FP32 / 3-point rule runs on the tensor cores in panels
+        elasticRH3 / FP32 (3-, 4- or 7-point rule) runs on the tensor cores in panels
         of 16 vectors (split TF32, compensated FP32 accumulation); other
         kernels apply dot_device vector by vector."""
         t = device.torch()
@@ -94,7 +95,8 @@ class TriToTriDirectFarfieldOp:
                 (width, Y.shape[1]), dtype=Y.dtype, device=Y.device)
             if take != width and accumulate:
                 out[:take] = Y[r0:r0 + take]
-            nbytes = _lib.lib.tct_farfield_rh_panel_workspace_bytes(self.n_obs, self.n_src, width)
+            nbytes = _lib.lib.tct_farfield_rh_panel_workspace_bytes(self.n_obs, self.n_src, width,
+                                                                    self.n_q)
             ws = self._panel_ws.get(width)
             if ws is None or ws.numel() < nbytes:
                 ws = device.workspace(nbytes)
@@ -102,7 +104,8 @@ class TriToTriDirectFarfieldOp:
             _lib.check(_lib.lib.tct_farfield_rh_panel_matvec(
                 _lib.tptr(out), _lib.tptr(xin), _lib.tptr(self.gpu_pts),
                 _lib.tptr(self.gpu_obs_tris), self.n_obs, _lib.tptr(self.gpu_src_tris), self.n_src,
-                width, _lib.dptr(self.params), int(bool(accumulate)), _lib.tptr(ws), nbytes,
+                width, self.n_q, _lib.dptr(self.qx), _lib.dptr(self.qw), _lib.dptr(self.params),
+                int(bool(accumulate)), _lib.tptr(ws), nbytes,
                 _lib.stream_ptr(stream)), "tct_farfield_rh_panel_matvec")
             if take != width:
                 Y[r0:r0 + take] = out[:take]
@@ -117,7 +120,7 @@ class TriToTriDirectFarfieldOp:
         if ws is None:
             return 0
         _lib.check(_lib.lib.tct_farfield_rh_panel_error(
-            _lib.tptr(ws), self.n_obs, self.n_src, width, _lib.stream_ptr(stream),
+            _lib.tptr(ws), self.n_obs, self.n_src, width, self.n_q, _lib.stream_ptr(stream),
             ctypes.byref(flag)), "tct_farfield_rh_panel_error")
         return flag.value
 

@@ -43,6 +43,29 @@ class RegularizedSparseIntegralOp:
         self.nearfield.dot_device(x, y, accumulate=True, stream=stream)
         return y
 
+    def dot_panel_device(self, X, Y, stream=None):
+        """Y[r] = (Far + Near) X[r] for device tensors X (R, 9 n_src),
+        Y (R, 9 n_obs) of float_type (an addition: R vectors per apply; the
+        elasticRH3 FP32 farfield runs on the tensor cores, the nearfield BSR
+        in one launch)."""
+        far = self.farfield
+        if hasattr(far, "dot_panel_device"):
+            far.dot_panel_device(X, Y, accumulate=False, stream=stream)
+        else:
+            for r in range(X.shape[0]):
+                far.dot_device(X[r], Y[r], accumulate=False, stream=stream)
+        self.nearfield.dot_panel_device(X, Y, accumulate=True, stream=stream)
+        return Y
+
+    def dot_panel(self, X):
+        """Host (R, 9 n_src) in, host (R, 9 n_obs) out."""
+        t = device.torch()
+        X = np.asarray(X).reshape(-1, self.shape[1])
+        Xd = device.to_dev(np.ascontiguousarray(X, dtype=self.float_type), self.float_type)
+        Yd = t.empty((Xd.shape[0], self.shape[0]), dtype=Xd.dtype, device="cuda")
+        self.dot_panel_device(Xd, Yd)
+        return Yd.cpu().numpy()
+
     def capture_graph(self):
         """Record one full apply (farfield + nearfield) as a CUDA graph on
         private input/output buffers; returns (graph, x, y): fill x, call

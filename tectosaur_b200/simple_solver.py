@@ -303,10 +303,10 @@ def gmres_batch(A, B, tol=1e-8, restart=200, maxiter=None):
 
 
 class ConstrainedPanelOperator:
-    """V (R, n_free) float64 -> cm^T A cm V for a panel of R vectors.  With an
-    FP32 elasticRH3 operator the farfield runs as one tensor-core panel apply
-    (TriToTriDirectFarfieldOp.dot_panel_device) and the nearfield BSR per
-    vector; other operators apply dot_device vector by vector."""
+    """V (R, n_free) float64 -> cm^T A cm V for a panel of R vectors.  An
+    operator with dot_panel_device applies all R vectors at once (FP32
+    elasticRH3: tensor-core farfield panel + one BSR panel launch); other
+    operators apply dot_device vector by vector."""
 
     def __init__(self, iop, cm, R):
         t = device.torch()
@@ -320,9 +320,7 @@ class ConstrainedPanelOperator:
         self.U = t.zeros((R, self.n_full_in), dtype=t.float64, device="cuda")
         self.Xf = t.zeros((R, self.n_full_in), dtype=self.ft, device="cuda")
         self.Yf = t.zeros((R, self.n_full_out), dtype=self.ft, device="cuda")
-        far = getattr(iop, "farfield", None)
-        self.panel = (self.ft == t.float32 and far is not None and
-                      hasattr(far, "panel_supported") and far.panel_supported())
+        self.panel = hasattr(iop, "dot_panel_device")
 
     def _csr_panel(self, mat, X, Y):
         _lib.check(_lib.lib.tct_csr_matvec_panel(
@@ -337,9 +335,7 @@ class ConstrainedPanelOperator:
         U = self._csr_panel(self.cm, V.contiguous(), self.U[:R])
         self.Xf[:R].copy_(U)
         if self.panel:
-            self.iop.farfield.dot_panel_device(self.Xf[:R], self.Yf[:R])
-            for r in range(R):
-                self.iop.nearfield.dot_device(self.Xf[r], self.Yf[r], accumulate=True)
+            self.iop.dot_panel_device(self.Xf[:R], self.Yf[:R])
         else:
             for r in range(R):
                 self.iop.dot_device(self.Xf[r], self.Yf[r])

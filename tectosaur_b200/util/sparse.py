@@ -69,6 +69,22 @@ class DeviceBSR9:
             "tct_bsr9_matvec")
         return y
 
+    def matvec_panel(self, X, Y, accumulate=False, stream=None):
+        """Y[v] (+)= A X[v] for device tensors X (R, n_cols), Y (R, n_rows)
+        (row strides may exceed the lengths); one launch, each block read
+        from HBM once."""
+        R = X.shape[0]
+        if Y.shape[0] != R:
+            raise ValueError("matvec_panel: %d input vs %d output vectors" % (R, Y.shape[0]))
+        if X.stride(1) != 1 or Y.stride(1) != 1:
+            raise ValueError("matvec_panel: rows must be contiguous")
+        _lib.check(_lib.lib.tct_bsr9_matvec_panel(
+            _lib.prec_of(self.float_type), self.n_row_blocks, _lib.tptr(self.indptr),
+            _lib.tptr(self.indices), _lib.tptr(self.data), max(self.nnzb, 1), _lib.tptr(X),
+            X.stride(0), _lib.tptr(Y), Y.stride(0), R, int(bool(accumulate)),
+            _lib.stream_ptr(stream)), "tct_bsr9_matvec_panel")
+        return Y
+
     def blocks_host(self, data=None):
         """(nnzb, 9, 9) host array of the blocks in BSR order."""
         d = (self.data if data is None else data)[:81 * self.nnzb]

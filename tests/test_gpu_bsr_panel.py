@@ -1,0 +1,72 @@
+"""The BSR nearfield matvec applied to a panel of vectors in one launch
+(tct_bsr9_matvec_panel) against the single-vector kernel, and the operator's
+panel apply (RegularizedSparseIntegralOp.dot_panel) against dot per vector."""
+import numpy as np
+import pytest
+import torch
+
+import tectosaur_b200 as tct
+from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+from tectosaur_b200.util.sparse import DeviceBSR9, make_bsr_index
+
+from helpers import PARAMS, bumpy_mesh, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_bsr(n_rows, n_cols, nnz, ft, seed):
+    rng = np.random.default_rng(seed)
+    rows = rng.integers(0, n_rows, nnz)
+    cols = rng.integers(0, n_cols, nnz)
+    # one empty row and one long row (more than 32 blocks: several lane passes)
+    rows[rows == 1] = 0
+    rows[:70] = 2
+    indptr, indices, slot = make_bsr_index(n_rows, rows, cols)
+    m = DeviceBSR9((9 * n_rows, 9 * n_cols), indptr, indices, ft)
+    blocks = rng.standard_normal((nnz, 81))
+    m.data.copy_(torch.from_numpy(np.ascontiguousarray(blocks.T).ravel()).to(m.data.dtype))
+    return m
+
+
+@pytest.mark.parametrize("ft", [np.float32, np.float64])
+@pytest.mark.parametrize("R", [1, 3, 8, 13, 16])
+def test_bsr_panel_matches_single(cuda, ft, R):
+    m = _random_bsr(300, 250, 6000, ft, seed=R)
+    tdt = torch.float32 if ft == np.float32 else torch.float64
+    X = torch.randn((R, 9 * 250), dtype=torch.float64, device="cuda").to(tdt)
+    Y = torch.empty((R, 9 * 300), dtype=tdt, device="cuda")
+    m.matvec_panel(X, Y)
+    want = torch.empty_like(Y)
+    for r in range(R):
+        m.matvec(X[r], want[r])
+    tol = 1e-6 if ft == np.float32 else 1e-14
+    assert rel(Y.cpu().numpy(), want.cpu().numpy()) < tol
+    assert np.all(Y[:, 9:18].cpu().numpy() == 0)  # the empty row
+
+
+def test_bsr_panel_strides_and_accumulate(cuda):
+    m = _random_bsr(200, 200, 3000, np.float32, seed=9)
+    R = 10
+    Xbig = torch.randn((R, 9 * 200 + 37), device="cuda")
+    Ybig = torch.randn((R, 9 * 200 + 5), device="cuda")
+    X, Y = Xbig[:, :9 * 200], Ybig[:, :9 * 200]
+    Y0 = Y.clone()
+    tail = Ybig[:, 9 * 200:].clone()
+    m.matvec_panel(X, Y, accumulate=True)
+    want = Y0.clone()
+    for r in range(R):
+        m.matvec(X[r].contiguous(), want[r], accumulate=True)
+    assert rel(Y.cpu().numpy(), want.cpu().numpy()) < 1e-6
+    assert torch.equal(Ybig[:, 9 * 200:], tail)  # nothing written past a row
+
+
+@pytest.mark.parametrize("ft", [np.float32, np.float64])
+def test_operator_panel_matches_dot(cuda, ft):
+    pts, tris = bumpy_mesh(10, seed=4)
+    op = tct.RegularizedSparseIntegralOp(3, 3, 3, 1, 3, 2.5, "elasticRH3", "elasticRH3", PARAMS,
+                                         pts, tris, ft, TriToTriDirectFarfieldOp)
+    X = np.random.default_rng(2).standard_normal((5, op.shape[1])).astype(ft)
+    got = op.dot_panel(X)
+    want = np.stack([op.dot(X[r]) for r in range(5)])
+    tol = 1e-5 if ft == np.float32 else 1e-13
+    assert rel(got, want) < tol

@@ -12,12 +12,12 @@ from helpers import PARAMS, bumpy_mesh
 pytestmark = pytest.mark.gpu
 
 
-def _setup(n, R, seed=0, obs=None):
+def _setup(n, R, seed=0, obs=None, nq_far=1):
     pts, tris = bumpy_mesh(n, seed=seed)
     nt = tris.shape[0]
     idx = np.arange(nt)
     obs = idx if obs is None else obs
-    op = TriToTriDirectFarfieldOp(1, "elasticRH3", PARAMS, pts, tris, np.float32, obs, idx)
+    op = TriToTriDirectFarfieldOp(nq_far, "elasticRH3", PARAMS, pts, tris, np.float32, obs, idx)
     X = np.random.default_rng(seed + 1).standard_normal((R, 9 * nt)).astype(np.float32)
     return pts, tris, op, X
 
@@ -41,12 +41,25 @@ def test_panel_matches_per_vector(cuda, n, R):
     assert np.all(err < 1e-5), err
 
 
-def test_panel_vs_fp64_oracle(cuda, orc):
+@pytest.mark.parametrize("nq_far", [2, 3])
+def test_panel_rules_match_per_vector(cuda, nq_far):
+    # the 4-point (negative centre weight) and 7-point rules
+    pts, tris, op, X = _setup(13, 20, seed=7, nq_far=nq_far)
+    assert op.panel_supported() and op.n_q == {2: 4, 3: 7}[nq_far]
+    got = op.dot_panel(X)
+    want = _per_vector(op, X)
+    assert op.panel_error(16) == 0
+    err = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+    assert np.all(err < 1e-5), err
+
+
+@pytest.mark.parametrize("nq_far", [1, 2])
+def test_panel_vs_fp64_oracle(cuda, orc, nq_far):
     from tectosaur_b200.util.quadrature import gauss2d_tri
-    pts, tris, op, X = _setup(14, 16, seed=3)
+    pts, tris, op, X = _setup(14, 16, seed=3, nq_far=nq_far)
     got = op.dot_panel(X)
     for r in [0, 7, 15]:
-        want = orc.farfield_tris("elasticRH3", np.float64, gauss2d_tri(1), pts, tris, tris,
+        want = orc.farfield_tris("elasticRH3", np.float64, gauss2d_tri(nq_far), pts, tris, tris,
                                  X[r].astype(np.float64), PARAMS)
         assert np.linalg.norm(got[r] - want) / np.linalg.norm(want) < 1e-5
 
