@@ -1139,6 +1139,173 @@ def run_batch_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def serve_meshes(n_meshes=6, seed=6, lo=2000, hi=20000):
+    """The served stream's meshes: triangle counts log-uniform in [lo, hi]
+    (seeded), cycling through a vertical strike-slip fault, a 30-degree
+    dipping fault and a topographic surface patch with a Gaussian hill."""
+    from tectosaur_b200.mesh.mesh_gen import make_rect
+    rng = np.random.default_rng(seed)
+    out = []
+    dip = np.radians(30.0)
+    for i in range(n_meshes):
+        n_tris = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        g = int(round(np.sqrt(n_tris / 2.0))) + 1
+        kind = ("planar", "dipping", "topo")[i % 3]
+        if kind == "planar":
+            pts, tris = make_rect(g, g, [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]])
+        elif kind == "dipping":
+            pts, tris = make_rect(g, g, [[-1, 0, 0], [1, 0, 0], [1, 2 * np.cos(dip), -2 * np.sin(dip)],
+                                         [-1, 2 * np.cos(dip), -2 * np.sin(dip)]])
+        else:
+            pts, tris = make_rect(g, g, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
+            pts = pts.copy()
+            amp, w = rng.uniform(0.1, 0.3), rng.uniform(0.3, 0.6)
+            pts[:, 2] = amp * np.exp(-(pts[:, 0] ** 2 + pts[:, 1] ** 2) / (2 * w * w))
+        out.append(("%s-%d" % (kind, tris.shape[0]), np.asarray(pts), np.asarray(tris)))
+    return out
+
+
+def run_serve_workload(args, rank, world, torch, dist):
+    """The served stream: solve requests on several resident meshes arriving
+    as a Poisson stream, served with continuous batching (tectosaur_b200.
+    serve) against the plain FP64 one-solve-at-a-time GPU path."""
+    import tectosaur_b200 as tct
+    from tectosaur_b200 import _lib, serve
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    from tectosaur_b200.simple_solver import (free_edge_vertices, iterative_solve,
+                                              shared_vertex_matrix)
+    tol = 1e-8
+    n_req = args.requests
+    meshes = serve_meshes()
+    t_build = time.perf_counter()
+    srv = serve.SolveServer(slots=16, restart=64)
+    specs = {}
+    for key, pts, tris in meshes:
+        cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+        op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
+                                               np.float64, TriToTriDirectFarfieldOp,
+                                               keep_uncorrected=False)
+        srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64)
+        specs[key] = (op64, cm, tris.shape[0])
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
+    rng = np.random.default_rng(7 + rank)
+    keys = [m[0] for m in meshes]
+    stream = []
+    for i in range(n_req):
+        k = keys[int(rng.integers(len(keys)))]
+        stream.append((k, rng.standard_normal(9 * specs[k][2])))
+
+    def replay(offsets):
+        return srv.replay([(off, k, b, tol) for off, (k, b) in zip(offsets, stream)])
+
+    zeros = [0.0] * n_req
+    for _ in range(args.warmup):
+        replay(zeros)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    l0 = _lib.launch_count()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    applies0 = sum(r.engine.n_vector_applies for r in srv.resident.values())
+    torch.cuda.synchronize()
+    a.record()
+    sat = []
+    for _ in range(args.steps):
+        sat = replay(zeros)
+    torch.cuda.synchronize()
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = _lib.launch_count() - l0
+    applies = sum(r.engine.n_vector_applies for r in srv.resident.values()) - applies0
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    served_rate = n_req * args.steps / (total_ms * 1e-3)
+    sat_lat = np.array([r.latency for r in sat])
+    # the plain path: FP64 operator, one solve at a time, in arrival order
+    iterative_solve(specs[keys[0]][0], specs[keys[0]][1], stream[0][1], cfg=dict(solver_tol=tol))
+    torch.cuda.synchronize()
+    service, plain_x, plain_steps = [], [], []
+    for k, rhs in stream:
+        t0 = time.perf_counter()
+        plain_x.append(iterative_solve(specs[k][0], specs[k][1], rhs, cfg=dict(solver_tol=tol)))
+        service.append(time.perf_counter() - t0)
+        plain_steps.append(iterative_solve.last["n_iter"])
+    plain_rate = n_req / sum(service)
+    err = max(float(np.linalg.norm(r.x - px) / np.linalg.norm(px))
+              for r, px in zip(sat, plain_x))
+    # latency under Poisson arrivals at fractions of the served saturation rate;
+    # the plain path's latency at the same arrivals is its FIFO queue over
+    # the measured service times
+    sweep = []
+    for frac in (0.5, 0.9):
+        lam = frac * served_rate / world
+        gaps = np.random.default_rng(11).exponential(1.0 / lam, n_req)
+        offs = np.cumsum(gaps) - gaps[0]
+        reqs = replay(list(offs))
+        lat = np.array([r.latency for r in reqs])
+        fin, plat = 0.0, []
+        for off, sv in zip(offs, service):
+            fin = max(fin, off) + sv
+            plat.append(fin - off)
+        sweep.append({"arrival_rate_per_s": lam, "fraction_of_served_saturation": frac,
+                      "served_p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                      "served_p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                      "plain_p50_ms": 1e3 * float(np.percentile(plat, 50)),
+                      "plain_p99_ms": 1e3 * float(np.percentile(plat, 99))})
+    if rank != 0:
+        return
+    ms = total_ms / args.steps
+    line = {
+        "metric": "BEM solves/s: served (continuous batching, mixed precision) vs plain FP64",
+        "value": served_rate, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 operator (tensor-core farfield panel) + f64 residual refinement",
+        "data": "synthetic (seeded meshes, arrivals and right-hand sides)",
+        "config": {"workload": ("%d solve requests (seeded N(0, 1) tractions, FP64 residual "
+                                "1e-8) on %d resident meshes of %s triangles (log-uniform "
+                                "2k-20k: vertical, 30-degree dipping faults, topographic "
+                                "patch; elasticRH3 RegularizedSparseIntegralOp(6,6,6,2,5,2.5), "
+                                "continuity + free-edge constraints), all arriving at once "
+                                "(saturation); one step = the whole stream"
+                                % (n_req, len(meshes), [m[2].shape[0] for m in meshes])),
+                   "meshes": [m[0] for m in meshes], "requests": n_req,
+                   "slots_per_mesh": srv.slots, "restart": srv.restart,
+                   "plain_fp64_solves_per_s": plain_rate,
+                   "speedup_vs_plain": served_rate / plain_rate,
+                   "max_rel_diff_vs_plain_fp64": err,
+                   "saturation_latency_ms_p50": 1e3 * float(np.percentile(sat_lat, 50)),
+                   "saturation_latency_ms_p99": 1e3 * float(np.percentile(sat_lat, 99)),
+                   "latency_sweep": sweep,
+                   "served_matvecs_per_s": applies / (total_ms * 1e-3),
+                   "plain_gmres_steps_mean": float(np.mean(plain_steps)),
+                   "served_gmres_steps_mean": float(np.mean([r.gmres_steps for r in sat])),
+                   "mesh_build_s": t_build, "resident_bytes": srv.resident_bytes,
+                   "l2": "operators and Krylov bases of 6 meshes resident (GBs, beyond L2)",
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "whole served stream (see the batch and panel workloads for "
+                               "the kernels)",
+                     "bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s",
+                     "frac": None, "traffic": None},
+        "e2e": {"value": served_rate, "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(b.nbytes for _, b in stream)),
+                "d2h_bytes_per_step": int(sum(r.x.nbytes for r in sat)),
+                "api": "serve.SolveServer.replay(stream of (t, mesh, rhs numpy, tol)) -> "
+                       "numpy solutions"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def config_block(n_tris, nnzb):
     return {
         "workload": ("direct-farfield 60k-triangle topographic surface (174x174 grid over "
@@ -1162,7 +1329,7 @@ def main():
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch"],
+                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -1170,6 +1337,8 @@ def main():
                          "batched mixed-precision solves vs the plain FP64 solve")
     ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--pairs", type=int, default=400_000)
+    ap.add_argument("--requests", type=int, default=48,
+                    help="solve requests in the served stream (serve workload)")
     ap.add_argument("--fmm-order", type=int, default=None)
     ap.add_argument("--fmm-ppc", type=int, default=None)
     ap.add_argument("--fmm-mode", default=None, choices=["fmm", "treecode"])
@@ -1193,9 +1362,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs", "panel", "batch"):
+    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
-         "panel": run_panel_workload, "batch": run_batch_workload}[args.workload](
+         "panel": run_panel_workload, "batch": run_batch_workload,
+         "serve": run_serve_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()

@@ -172,6 +172,10 @@ int tct_bsr9_matvec_panel(int prec, int64_t n_row_blocks, const int32_t* indptr,
                           const void* x, int64_t x_stride, void* y, int64_t y_stride,
                           int n_vec, int accumulate, void* stream);
 
+/* Number of kernels this library has launched in the process (a measurement
+ * aid with no reference counterpart; host). */
+uint64_t tct_launch_count(void);
+
 /* ------------------------------------------------------------------------ */
 /* Measurement utility (no reference counterpart): FP32 FMA throughput probe.
  * Launches n_blocks x 256 threads, each running `iters` steps of 8 independent
@@ -240,6 +244,17 @@ int tct_split_adjacent_close(const int64_t* pairs, int64_t n_pairs,
  * from the 6-column edge-adjacent rows (nearfield/nearfield_op.py:44-62). Host. */
 int tct_resolve_ea_rotation(const int64_t* tris, const int64_t* ea, int64_t n,
                             int64_t* out);
+
+/* Host update of one GMRES step for several systems at once (Givens QR
+ * of each system's Hessenberg matrix; the reference runs scipy's gmres,
+ * examples/solve.py:25-61): system s = sys[i] puts its new column
+ * cols[i * col_stride + 0 .. j[s] + 1] into column j[s] of H_s
+ * (H + s (m+1) m, column-major), applies its rotations cs/sn (m per system),
+ * adds rotation j[s], updates g (m + 1 per system) and writes the residual
+ * estimate |g_s[j[s] + 1]| to res[i].  Host. */
+int tct_gmres_givens(int64_t n_active, const int64_t* sys, const int64_t* j, int64_t m,
+                     const double* cols, int64_t col_stride, double* H, double* cs, double* sn,
+                     double* g, double* res);
 
 /* BSR index build (util/fast_sparse.cpp:14-68 semantics: stable counting
  * sort by block row, duplicates kept).  slot[i] = position of input block i

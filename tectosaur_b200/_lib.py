@@ -70,6 +70,8 @@ _SIGS = {
                                   c_i64p, c_i64p], c_i),
     "tct_resolve_ea_rotation": ([c_i64p, c_i64p, c_i64, c_i64p], c_i),
     "tct_make_bsr_index": ([c_i64, c_i64, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p], c_i),
+    "tct_gmres_givens": ([c_i64, c_i64p, c_i64p, c_i64, c_dp, c_i64, c_dp, c_dp, c_dp, c_dp,
+                          c_dp], c_i),
 }
 
 for _name, (_args, _res) in _SIGS.items():
@@ -179,6 +181,7 @@ _SOLVE_SIGS = {
     "tct_csr_matvec_panel": ([c_i, c_i64, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_p],
                              c_i),
     "tct_fp64_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
+    "tct_launch_count": ([], ctypes.c_uint64),
     "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i, c_i], c_sz),
     "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_dp, c_dp,
                                       c_dp, c_i, c_p, c_sz, c_p], c_i),
@@ -189,3 +192,8 @@ for _name, (_args, _res) in _SOLVE_SIGS.items():
     _f.argtypes = _args
     _f.restype = _res
 EXPORTED = sorted(set(EXPORTED) | set(_SOLVE_SIGS))
+
+
+def launch_count():
+    """Kernels launched by libtct_b200.so so far in this process."""
+    return int(lib.tct_launch_count())

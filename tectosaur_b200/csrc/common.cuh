@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -22,12 +23,17 @@ void set_error(const char* fmt, ...);
         }                                   \
     } while (0)
 
+// Kernels launched by the library (every launch is followed by
+// launch_status; read by tct_launch_count).
+extern std::atomic<unsigned long long> g_launches;
+
 inline int launch_status(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("%s: %s", what, cudaGetErrorString(e));
         return TCT_ERR_CUDA;
     }
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     return TCT_OK;
 }
 

@@ -12,6 +12,34 @@ namespace {
 
 constexpr int MAXQ = 13;
 
+// Packed FP32 pairs (add/mul/fma.rn.f32x2: two lanes of work per instruction).
+typedef unsigned long long f2_t;
+
+__device__ __forceinline__ f2_t pk(float x, float y) {
+    f2_t d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(x), "f"(y));
+    return d;
+}
+__device__ __forceinline__ void upk(f2_t d, float& x, float& y) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(d));
+}
+__device__ __forceinline__ f2_t add2(f2_t a, f2_t b) {
+    f2_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) {
+    f2_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) {
+    f2_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+
 template <typename R>
 struct Rule2D {
     R x[MAXQ], y[MAXQ], w[MAXQ];

@@ -246,14 +246,14 @@ mrhs_prep(Consts<float> c, float w2, const float* __restrict__ pts,
 
 // ---- main: generate A, copy B, tcgen05.mma into TMEM ------------------------
 // Observation quadrature points of the rule (barycentric 1 - x - y, x, y).
-// grid (obs blocks of 128, source chunks); 256 threads: thread (row, half)
-// generates row `row` of A for the half `half` of the tile's 8 source
-// triangles; one thread issues the B tile as a bulk async copy (completing
-// on bar_b) before the generation starts, so the copy overlaps it, and then
-// the MMAs (completing on bar_mma).  The two warp groups split the tensor-
-// memory columns of the fold and the epilogue.  Dynamic smem: A hi/lo
-// (2 x 128 x 56 x 4), B hi/lo (2 x N x 56 x 4).
-constexpr int MR_THREADS = 256;
+// grid (obs blocks of 128, source chunks); G x 128 threads: thread
+// (row, group) generates row `row` of A for the group's 8 / G of the tile's 8
+// source triangles (G = 4 keeps 16 warps in flight where the registers allow,
+// G = 2 for the 7-point rule); one thread issues the B tiles as bulk async
+// copies (completing on bar_b[buffer]) and the MMAs (completing on
+// bar_mma).  The G warp groups split the tensor-memory columns of the fold
+// and the epilogue.  Dynamic smem: A hi/lo (2 x 128 x 56 x 4), two B
+// buffers of hi/lo (2 x 2 x N x 56 x 4).
 constexpr int MR_COPIES = 4;  // bulk copies per B tile
 
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
@@ -265,25 +265,27 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
         : "memory");
 }
 
-template <int R, int NQ, bool UNIFORM>
-__global__ void __launch_bounds__(MR_THREADS, 1)
+template <int R, int NQ, bool UNIFORM, int G>
+__global__ void __launch_bounds__(128 * G, 1)
 mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __restrict__ obs_tris,
           int64_t n_obs,
           const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
           const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
     constexpr int N = 9 * R;
-    constexpr int NH = N / 2;  // tensor-memory columns per warp group
+    constexpr int SG = MR_S / G;  // source triangles per thread group
+    constexpr int KG = 7 * SG;    // A values per thread and tile
     static_assert(3 * N <= 512, "D, S and C must fit the 512 tensor-memory columns");
-    static_assert(NH % 8 == 0, "column halves must be whole 8-column groups");
+    static_assert(N % 8 == 0 && MR_S % G == 0 && KG % 2 == 0, "tile split");
     constexpr int NCOL = 512;
     constexpr uint32_t B_BYTES = 2u * N * MR_K * 4;
     static_assert(B_BYTES % (16 * MR_COPIES) == 0, "bulk copies must be 16-byte multiples");
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* Ah = smem;
     unsigned char* Al = Ah + MR_M * MR_K * 4;
-    unsigned char* Bs = Al + MR_M * MR_K * 4;  // hi then lo, 2 * N * MR_K * 4
+    // two B buffers (tile t and t + 1), each hi then lo, 2 * N * MR_K * 4
+    unsigned char* Bs0 = Al + MR_M * MR_K * 4;
     __shared__ __align__(8) uint64_t bar_mma;
-    __shared__ __align__(8) uint64_t bar_b;
+    __shared__ __align__(8) uint64_t bar_b[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
@@ -293,7 +295,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     if (abort_flag) return;  // an earlier CTA timed out: no tensor memory taken yet
     const int warp = tid >> 5;
     const int row = tid & (MR_M - 1);
-    const int half = tid >> 7;
+    const int grp = tid >> 7;  // thread group: A sources and tensor-memory columns
     const int64_t o = (int64_t)blockIdx.x * MR_M + row;
     const bool valid = o < n_obs;
     const int64_t t0 = (int64_t)blockIdx.y * tiles_per_chunk;
@@ -307,7 +309,8 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_mma)), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b)), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b[0])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b[1])), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -315,7 +318,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_slot;
     const uint32_t barm = smem_u32(&bar_mma);
-    const uint32_t barb = smem_u32(&bar_b);
+    const uint32_t barb0 = smem_u32(&bar_b[0]), barb1 = smem_u32(&bar_b[1]);
 
     // obs quadrature points of the rule; weight products for non-uniform rules
     // (a uniform rule's w^2 is folded into B by mrhs_prep)
@@ -337,22 +340,107 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
             for (int d = 0; d < 3; d++) x[q][d] = bary_point(ot, bq, d);
         }
     }
-    float wq[UNIFORM ? 1 : NQ * NQ];
-    if (!UNIFORM) {
+    // packed (the same point in both lanes, negated): D = y_pair + negx
+    f2_t negx[NQ][3];
 #pragma unroll
-        for (int q1 = 0; q1 < NQ; q1++)
+    for (int q = 0; q < NQ; q++)
 #pragma unroll
-            for (int q2 = 0; q2 < NQ; q2++) wq[q1 * NQ + q2] = rule.w[q1] * rule.w[q2];
-    }
+        for (int d = 0; d < 3; d++) negx[q][d] = pk(-x[q][d], -x[q][d]);
+    // weight products of a non-uniform rule (packed where the registers allow)
+    constexpr bool WPACK = !UNIFORM && NQ <= 4;
+    f2_t wq2[WPACK ? NQ * NQ : 1];
+    float wq[(!UNIFORM && !WPACK) ? NQ * NQ : 1];
+#pragma unroll
+    for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+        for (int q2 = 0; q2 < NQ; q2++) {
+            const float w = rule.w[q1] * rule.w[q2];
+            if constexpr (WPACK) wq2[q1 * NQ + q2] = pk(w, w);
+            else if constexpr (!UNIFORM) wq[q1 * NQ + q2] = w;
+        }
+    const f2_t eps2 = pk(MR_EPS, MR_EPS);
 
-    uint32_t phase_m = 0, phase_b = 0;
+    // Pipeline per tile t: the A values of tile t are generated in registers
+    // while the MMAs of tile t - 1 run on the tensor cores and the B tile of t
+    // (issued one tile ahead) is in flight; then, once the MMAs of t - 1 have
+    // completed, A is stored to shared memory, the B tile of t + 1 is issued
+    // into the buffer the MMAs of t - 1 read, and the MMAs of t are issued.
+    // (per-buffer state in scalars: a runtime-indexed array would live in local memory)
+    uint32_t phase_m = 0, phase_b0 = 0, phase_b1 = 0;
+    bool pend0 = false, pend1 = false;  // CTA-uniform: B copies issued, not waited for
     bool ok = true;            // CTA-uniform
     bool mma_pending = false;  // CTA-uniform: a commit not yet waited for
-    bool copy_timeout = false;
     const uint32_t idesc = mr_instr_desc(N);
     const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const int col0 = half * NH;
+    // this warp's tensor-memory columns: whole 8-column groups, split over G
+    const int col0 = (grp * (N / 8) / G) * 8, col1 = ((grp + 1) * (N / 8) / G) * 8;
+    auto issue_b = [&](int64_t tile, int buf) {
+        const uint32_t bar = buf ? barb1 : barb0;
+        if (tid == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"(B_BYTES)
+                         : "memory");
+            const unsigned char* src =
+                reinterpret_cast<const unsigned char*>(Bg) + tile * (int64_t)B_BYTES;
+            const uint32_t dst = smem_u32(Bs0) + (uint32_t)buf * B_BYTES;
+#pragma unroll
+            for (int cpy = 0; cpy < MR_COPIES; cpy++)
+                bulk_g2s(dst + cpy * (B_BYTES / MR_COPIES), src + cpy * (B_BYTES / MR_COPIES),
+                         B_BYTES / MR_COPIES, bar);
+        }
+        if (buf) pend1 = true;
+        else pend0 = true;
+    };
+    if (t0 < t1) issue_b(t0, 0);
     for (int64_t t = t0; t < t1; t++) {
+        const int buf = (int)((t - t0) & 1);
+        // A: this thread's SG source triangles of the tile, KG values, two
+        // source triangles per packed instruction
+        float av[KG];
+#pragma unroll
+        for (int sp = 0; sp < SG / 2; sp++) {
+            const f2_t* y = reinterpret_cast<const f2_t*>(srcy) +
+                            ((t * MR_S + grp * SG) / 2 + sp) * (3 * NQ);
+            f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
+#pragma unroll
+            for (int q2 = 0; q2 < NQ; q2++) {
+                const f2_t y0 = __ldg(y + 3 * q2), y1 = __ldg(y + 3 * q2 + 1),
+                           y2 = __ldg(y + 3 * q2 + 2);
+#pragma unroll
+                for (int q1 = 0; q1 < NQ; q1++) {
+                    const f2_t D0 = add2(y0, negx[q1][0]);
+                    const f2_t D1 = add2(y1, negx[q1][1]);
+                    const f2_t D2 = add2(y2, negx[q1][2]);
+                    f2_t r2 = fma2(D0, D0, eps2);
+                    r2 = fma2(D1, D1, r2);
+                    r2 = fma2(D2, D2, r2);
+                    float ra, rb;
+                    upk(r2, ra, rb);
+                    const f2_t ir = pk(rsqrtf(ra), rsqrtf(rb));
+                    f2_t g = mul2(mul2(ir, ir), ir);
+                    if constexpr (WPACK) g = mul2(g, wq2[q1 * NQ + q2]);
+                    else if constexpr (!UNIFORM)
+                        g = mul2(g, pk(wq[q1 * NQ + q2], wq[q1 * NQ + q2]));
+                    const f2_t g0 = mul2(g, D0), g1 = mul2(g, D1), g2 = mul2(g, D2);
+                    T00 = fma2(g0, D0, T00);
+                    T01 = fma2(g0, D1, T01);
+                    T02 = fma2(g0, D2, T02);
+                    T11 = fma2(g1, D1, T11);
+                    T12 = fma2(g1, D2, T12);
+                    T22 = fma2(g2, D2, T22);
+                }
+            }
+            const f2_t S0 = add2(add2(T00, T11), T22);
+            const f2_t Tc[7] = {S0, T00, T01, T02, T11, T12, T22};
+#pragma unroll
+            for (int c = 0; c < 7; c++) {
+                float va, vb;
+                upk(Tc[c], va, vb);
+                av[7 * (2 * sp) + c] = valid ? va : 0.f;
+                av[7 * (2 * sp + 1) + c] = valid ? vb : 0.f;
+            }
+        }
+        // the MMAs of tile t - 1 have read A and B buffer buf ^ 1
         if (mma_pending) {
             const bool w = mbar_wait(barm, phase_m);
             if (!__syncthreads_and(w)) {
@@ -363,86 +451,61 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
             mma_pending = false;
             if ((t - t0) % MR_FLUSH == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                tmem_fold<N>(lane_base, col0, col0 + NH, t - t0 == MR_FLUSH);
+                tmem_fold<N>(lane_base, col0, col1, t - t0 == MR_FLUSH);
                 asm volatile("tcgen05.fence::before_thread_sync;");
             }
         }
-        // B tile: bulk async copy issued first, overlapping the generation
-        if (tid == 0) {
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barb),
-                         "r"(B_BYTES)
-                         : "memory");
-            const unsigned char* src =
-                reinterpret_cast<const unsigned char*>(Bg) + t * (int64_t)B_BYTES;
+        if (t + 1 < t1) issue_b(t + 1, buf ^ 1);
+        if constexpr (KG % 4 == 0) {
 #pragma unroll
-            for (int cpy = 0; cpy < MR_COPIES; cpy++)
-                bulk_g2s(smem_u32(Bs) + cpy * (B_BYTES / MR_COPIES),
-                         src + cpy * (B_BYTES / MR_COPIES), B_BYTES / MR_COPIES, barb);
-        }
-        // A: this thread's half of the tile, 4 source triangles = 28 values
-        float av[MR_K / 2];
-#pragma unroll
-        for (int sl = 0; sl < MR_S / 2; sl++) {
-            const float* y = srcy + (t * MR_S + half * (MR_S / 2) + sl) * (3 * NQ);
-            float T00 = 0.f, T01 = 0.f, T02 = 0.f, T11 = 0.f, T12 = 0.f, T22 = 0.f;
-#pragma unroll
-            for (int q2 = 0; q2 < NQ; q2++) {
-                const float y0 = __ldg(y + 3 * q2), y1 = __ldg(y + 3 * q2 + 1),
-                            y2 = __ldg(y + 3 * q2 + 2);
-#pragma unroll
-                for (int q1 = 0; q1 < NQ; q1++) {
-                    const float D0 = y0 - x[q1][0], D1 = y1 - x[q1][1], D2 = y2 - x[q1][2];
-                    const float r2 = fmaf(D0, D0, fmaf(D1, D1, fmaf(D2, D2, MR_EPS)));
-                    const float ir = rsqrtf(r2);
-                    float g = ir * ir * ir;
-                    if (!UNIFORM) g *= wq[q1 * NQ + q2];
-                    const float g0 = g * D0, g1 = g * D1, g2 = g * D2;
-                    T00 = fmaf(g0, D0, T00);
-                    T01 = fmaf(g0, D1, T01);
-                    T02 = fmaf(g0, D2, T02);
-                    T11 = fmaf(g1, D1, T11);
-                    T12 = fmaf(g1, D2, T12);
-                    T22 = fmaf(g2, D2, T22);
-                }
+            for (int ch = 0; ch < KG / 4; ch++) {
+                float4 h, l;
+                h.x = tf32_round(av[4 * ch + 0]);
+                h.y = tf32_round(av[4 * ch + 1]);
+                h.z = tf32_round(av[4 * ch + 2]);
+                h.w = tf32_round(av[4 * ch + 3]);
+                l.x = tf32_round(av[4 * ch + 0] - h.x);
+                l.y = tf32_round(av[4 * ch + 1] - h.y);
+                l.z = tf32_round(av[4 * ch + 2] - h.z);
+                l.w = tf32_round(av[4 * ch + 3] - h.w);
+                const uint32_t off = mr_off(row, grp * KG + 4 * ch, MR_M);
+                *reinterpret_cast<float4*>(Ah + off) = h;
+                *reinterpret_cast<float4*>(Al + off) = l;
             }
-            av[7 * sl + 0] = valid ? T00 + T11 + T22 : 0.f;
-            av[7 * sl + 1] = valid ? T00 : 0.f;
-            av[7 * sl + 2] = valid ? T01 : 0.f;
-            av[7 * sl + 3] = valid ? T02 : 0.f;
-            av[7 * sl + 4] = valid ? T11 : 0.f;
-            av[7 * sl + 5] = valid ? T12 : 0.f;
-            av[7 * sl + 6] = valid ? T22 : 0.f;
-        }
+        } else {  // KG = 14: the group's k range starts at an even k
 #pragma unroll
-        for (int ch = 0; ch < MR_K / 8; ch++) {
-            float4 h, l;
-            h.x = tf32_round(av[4 * ch + 0]);
-            h.y = tf32_round(av[4 * ch + 1]);
-            h.z = tf32_round(av[4 * ch + 2]);
-            h.w = tf32_round(av[4 * ch + 3]);
-            l.x = tf32_round(av[4 * ch + 0] - h.x);
-            l.y = tf32_round(av[4 * ch + 1] - h.y);
-            l.z = tf32_round(av[4 * ch + 2] - h.z);
-            l.w = tf32_round(av[4 * ch + 3] - h.w);
-            const uint32_t off = mr_off(row, 4 * (half * (MR_K / 8) + ch), MR_M);
-            *reinterpret_cast<float4*>(Ah + off) = h;
-            *reinterpret_cast<float4*>(Al + off) = l;
+            for (int ch = 0; ch < KG / 2; ch++) {
+                float2 h, l;
+                h.x = tf32_round(av[2 * ch + 0]);
+                h.y = tf32_round(av[2 * ch + 1]);
+                l.x = tf32_round(av[2 * ch + 0] - h.x);
+                l.y = tf32_round(av[2 * ch + 1] - h.y);
+                const uint32_t off = mr_off(row, grp * KG + 2 * ch, MR_M);
+                *reinterpret_cast<float2*>(Ah + off) = h;
+                *reinterpret_cast<float2*>(Al + off) = l;
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         {
-            const bool wb = mbar_wait(barb, phase_b);
+            const bool wb = mbar_wait(buf ? barb1 : barb0, buf ? phase_b1 : phase_b0);
             if (!__syncthreads_and(wb)) {
                 ok = false;
-                copy_timeout = true;
                 break;
             }
-            phase_b ^= 1;
+            if (buf) {
+                phase_b1 ^= 1;
+                pend1 = false;
+            } else {
+                phase_b0 ^= 1;
+                pend0 = false;
+            }
         }
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t lboA = MR_M / 8 * 128, lboB = N / 8 * 128;
-            const uint32_t aH = smem_u32(Ah), aL = smem_u32(Al), bH = smem_u32(Bs),
-                           bL = smem_u32(Bs + N * MR_K * 4);
+            const uint32_t aH = smem_u32(Ah), aL = smem_u32(Al),
+                           bH = smem_u32(Bs0) + (uint32_t)buf * B_BYTES,
+                           bL = bH + N * MR_K * 4;
 #pragma unroll
             for (int ks = 0; ks < MR_KSTEPS; ks++) {
                 const uint64_t dAh = mr_smem_desc(aH + 2 * ks * lboA, lboA, 128);
@@ -465,12 +528,14 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     if (ok && mma_pending) {
         const bool w = mbar_wait(barm, phase_m);
         if (!__syncthreads_and(w)) ok = false;
+        else mma_pending = false;
     }
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
         // one more bounded wait for whatever is still in flight
-        if (copy_timeout) mbar_wait(barb, phase_b);
-        else mbar_wait(barm, phase_m);
+        if (mma_pending) mbar_wait(barm, phase_m);
+        if (pend0) mbar_wait(barb0, phase_b0);
+        if (pend1) mbar_wait(barb1, phase_b1);
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
 
@@ -478,9 +543,9 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     // column half -> partial[chunk][r][o][9] (the obs-side contraction
     // out[b][d] = J_o sum_j sc_o[b][j] W[d][j] is done by the reduce kernel)
     if (ok && t1 > t0) {
-        tmem_fold<N>(lane_base, col0, col0 + NH, t1 - t0 <= MR_FLUSH);
+        tmem_fold<N>(lane_base, col0, col1, t1 - t0 <= MR_FLUSH);
 #pragma unroll 1
-        for (int c0 = col0; c0 < col0 + NH; c0 += 8) {
+        for (int c0 = col0; c0 < col1; c0 += 8) {
             float sv[8], cv[8];
             tmem_ld8(lane_base + N + c0, sv);
             tmem_ld8(lane_base + 2 * N + c0, cv);
@@ -503,9 +568,11 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     }
 }
 
-// Source quadrature points (NQ x 3 per source triangle, padded with far-away
-// points that contribute nothing: their A entries are multiplied by zero rows
-// of B).
+// Source quadrature points, padded with far-away points that contribute
+// nothing (their A entries are multiplied by zero rows of B).  Layout: pairs
+// of consecutive source triangles interleaved, value (q, d) of triangle s at
+// srcy[(s / 2) * 6 NQ + 2 (3 q + d) + s % 2], so that one 8-byte load gives
+// the packed pair.
 template <int NQ>
 __global__ void __launch_bounds__(128)
 mrhs_points(Rule2D<float> rule, const float* __restrict__ pts,
@@ -513,10 +580,10 @@ mrhs_points(Rule2D<float> rule, const float* __restrict__ pts,
             float* __restrict__ srcy) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_src_pad) return;
-    float* y = srcy + s * (3 * NQ);
+    float* y = srcy + (s / 2) * (6 * NQ) + (s % 2);
     if (s >= n_src) {
 #pragma unroll
-        for (int k = 0; k < 3 * NQ; k++) y[k] = 1e18f;
+        for (int k = 0; k < 3 * NQ; k++) y[2 * k] = 1e18f;
         return;
     }
     TriGeom<float> t;
@@ -525,7 +592,7 @@ mrhs_points(Rule2D<float> rule, const float* __restrict__ pts,
     for (int q = 0; q < NQ; q++) {
         const float bq[3] = {1.f - rule.x[q] - rule.y[q], rule.x[q], rule.y[q]};
 #pragma unroll
-        for (int d = 0; d < 3; d++) y[3 * q + d] = bary_point(t, bq, d);
+        for (int d = 0; d < 3; d++) y[2 * (3 * q + d)] = bary_point(t, bq, d);
     }
 }
 
@@ -613,13 +680,14 @@ int run_mrhs(const Consts<float>& c, const Rule2D<float>& rule, float* out, cons
     const int64_t chunks = mrhs_chunks(n_obs, n_tiles);
     const int64_t per = (n_tiles + chunks - 1) / chunks;
     const int64_t real = (n_tiles + per - 1) / per;
-    const size_t smem = (size_t)2 * MR_M * MR_K * 4 + (size_t)2 * N * MR_K * 4;
-    auto kfn = mrhs_main<R, NQ, UNIFORM>;
+    const size_t smem = (size_t)2 * MR_M * MR_K * 4 + (size_t)2 * 2 * N * MR_K * 4;
+    constexpr int G = 2;  // 8 warps (16 were measured no faster)
+    auto kfn = mrhs_main<R, NQ, UNIFORM, G>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return launch_status("mrhs smem attribute");
     dim3 grid((unsigned)((n_obs + MR_M - 1) / MR_M), (unsigned)real);
-    kfn<<<grid, MR_THREADS, smem, st>>>(rule, pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
+    kfn<<<grid, 128 * G, smem, st>>>(rule, pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
                                         partial, err);
     if ((rc = launch_status("mrhs main"))) return rc;
     mrhs_reduce<<<(unsigned)((n_obs * R + 127) / 128), 128, 0, st>>>(

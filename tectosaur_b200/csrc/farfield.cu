@@ -132,32 +132,6 @@ far_main(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
 // folded into P and -2 ssc by the prep kernel.
 constexpr float RH2_EPS = 1e-24f;
 
-typedef unsigned long long f2_t;
-
-__device__ __forceinline__ f2_t pk(float x, float y) {
-    f2_t d;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(x), "f"(y));
-    return d;
-}
-__device__ __forceinline__ void upk(f2_t d, float& x, float& y) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(d));
-}
-__device__ __forceinline__ f2_t add2(f2_t a, f2_t b) {
-    f2_t d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) {
-    f2_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) {
-    f2_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
 // Record of one source triangle for the packed kernel, every value stored
 // twice (an f32x2 operand): y[q][d] (3 NQ pairs), P (9), M = -2 ssc (9).
 template <int NQ>

@@ -635,4 +635,51 @@ int tct_make_bsr_index(int64_t n_row_blocks, int64_t n_blocks, const int64_t* ro
     return TCT_OK;
 }
 
+
+// One Arnoldi step's host update for a set of GMRES systems (the Givens
+// QR of the Hessenberg matrix, as in the reference's solver, scipy's gmres
+// driven by examples/solve.py:25-61).  System s = sys[i] takes its new
+// column cols[i * col_stride + 0 .. j[s] + 1] (h_0..h_j, ||w||) into column
+// j[s] of H_s ((m + 1) x m, column-major per system), applies its previous
+// rotations, forms rotation j[s], updates g_s and writes |g_s[j + 1]| to
+// res[i].
+int tct_gmres_givens(int64_t n_active, const int64_t* sys, const int64_t* j, int64_t m,
+                     const double* cols, int64_t col_stride, double* H, double* cs, double* sn,
+                     double* g, double* res) {
+    if (n_active < 0 || m < 1 || (n_active > 0 && (!sys || !j || !cols || !H || !cs || !sn ||
+                                                   !g || !res))) {
+        tct::set_error("tct_gmres_givens: bad arguments");
+        return TCT_ERR_ARG;
+    }
+    for (int64_t i = 0; i < n_active; i++) {
+        const int64_t s = sys[i], js = j[s];
+        if (s < 0 || js < 0 || js >= m || js + 2 > col_stride) {
+            tct::set_error("tct_gmres_givens: step %lld of system %lld out of range",
+                           (long long)js, (long long)s);
+            return TCT_ERR_ARG;
+        }
+        double* h = H + s * (m + 1) * m + js * (m + 1);
+        double* c = cs + s * m;
+        double* sv = sn + s * m;
+        double* gs = g + s * (m + 1);
+        const double* col = cols + i * col_stride;
+        for (int64_t k = 0; k < js + 2; k++) h[k] = col[k];
+        for (int64_t k = js + 2; k < m + 1; k++) h[k] = 0.0;
+        for (int64_t k = 0; k < js; k++) {
+            const double a = h[k], b = h[k + 1];
+            h[k] = c[k] * a + sv[k] * b;
+            h[k + 1] = -sv[k] * a + c[k] * b;
+        }
+        const double den = std::hypot(h[js], h[js + 1]);
+        c[js] = den > 0 ? h[js] / den : 1.0;
+        sv[js] = den > 0 ? h[js + 1] / den : 0.0;
+        h[js] = den;
+        h[js + 1] = 0.0;
+        gs[js + 1] = -sv[js] * gs[js];
+        gs[js] = c[js] * gs[js];
+        res[i] = std::fabs(gs[js + 1]);
+    }
+    return TCT_OK;
+}
+
 }  // extern "C"

@@ -93,3 +93,11 @@ extern "C" int tct_fp32x2_fma_probe(void* out, int64_t n_blocks, int iters, void
     fma2_probe<<<(unsigned)n_blocks, 256, 0, as_stream(stream)>>>((float*)out, iters, 1.0f);
     return launch_status("tct_fp32x2_fma_probe");
 }
+
+namespace tct {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+extern "C" uint64_t tct_launch_count(void) {
+    return tct::g_launches.load(std::memory_order_relaxed);
+}

@@ -199,6 +199,21 @@ class RegularizedNearfieldIntegralOp:
         return self._host_or_device(
             v, lambda x, y: self.bsr.matvec(x, y, extra=self.correction))
 
+    def astype(self, float_type, keep_uncorrected=True):
+        """The same nearfield in another precision: the block structure is
+        shared and the blocks are cast (not re-integrated)."""
+        import copy
+        twin = copy.copy(self)
+        twin.float_type = np.dtype(float_type)
+        tdt = device.torch_dtype(float_type)
+        twin.bsr = copy.copy(self.bsr)
+        twin.bsr.float_type = twin.float_type
+        twin.bsr.data = self.bsr.data.to(tdt)
+        twin.correction = (self.correction.to(tdt)
+                           if keep_uncorrected and self.correction is not None else None)
+        twin._mats = None
+        return twin
+
     # -- host views (reference attributes) --------------------------------
     def _build_mats(self):
         D = self.bsr.blocks_host()

@@ -30,8 +30,25 @@ class RegularizedSparseIntegralOp:
             keep_uncorrected=keep_uncorrected)
         self.farfield = farfield_op_type(
             nq_far, K_far_name, params, pts, tris, float_type, obs_subset, src_subset)
+        self._far_args = (farfield_op_type, nq_far, K_far_name, params, pts, tris, obs_subset,
+                          src_subset)
         self.shape = self.nearfield.shape
         self._graph = None
+
+    def astype(self, float_type, keep_uncorrected=True):
+        """The same operator in another precision (an addition, for mixed-
+        precision solves): the nearfield blocks are cast from this operator's
+        (structure shared, no re-integration), the farfield is set up anew in
+        float_type."""
+        import copy
+        twin = copy.copy(self)
+        twin.float_type = np.dtype(float_type)
+        twin.nearfield = self.nearfield.astype(float_type, keep_uncorrected)
+        factory, nq_far, K_far, params, pts, tris, obs_subset, src_subset = self._far_args
+        twin.farfield = factory(nq_far, K_far, params, pts, tris, float_type, obs_subset,
+                                src_subset)
+        twin._graph = None
+        return twin
 
     # -- device apply -------------------------------------------------------
     def dot_device(self, x, y, stream=None):

@@ -1,0 +1,76 @@
+"""The continuous-batching solve server on the device: served results
+against the plain FP64 one-solve-at-a-time path (simple_solver.
+iterative_solve), and a request's result alone against the same request in
+a mix of meshes and right-hand sides."""
+import numpy as np
+import pytest
+
+from tectosaur_b200 import _lib, serve
+from tectosaur_b200.mesh.mesh_gen import make_rect
+from tectosaur_b200.simple_solver import (free_edge_vertices, iterative_solve,
+                                          shared_vertex_matrix)
+
+from helpers import PARAMS, bumpy_mesh
+
+pytestmark = pytest.mark.gpu
+
+NQ = (6, 6, 6, 2, 5, 2.5)
+
+
+def _meshes():
+    a = make_rect(10, 10, [[-1, -1, 0], [-1, 1, 0], [1, 1, 0], [1, -1, 0]])
+    b = bumpy_mesh(9, seed=2)
+    return {k: (np.asarray(p), np.asarray(t)) for k, (p, t) in {"fault": a, "surface": b}.items()}
+
+
+def _server(meshes):
+    srv = serve.SolveServer(slots=16, restart=64)
+    for k, (pts, tris) in meshes.items():
+        cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+        srv.add_mesh(k, pts, tris, cm, nq=NQ, params=PARAMS)
+    return srv
+
+
+def test_served_matches_plain_fp64(cuda):
+    meshes = _meshes()
+    srv = _server(meshes)
+    rng = np.random.default_rng(0)
+    reqs = []
+    for i in range(6):
+        k = "fault" if i % 2 == 0 else "surface"
+        reqs.append(srv.submit(k, rng.standard_normal(9 * meshes[k][1].shape[0]), tol=1e-8))
+    n0 = _lib.launch_count()
+    srv.run_until_idle(max_ticks=20_000)
+    assert _lib.launch_count() > n0  # the library's kernels ran
+    for k in meshes:
+        r = srv.resident[k]
+        assert r.op32.farfield.panel_supported()  # the tensor-core panel path
+    for r in reqs:
+        assert r.converged and r.residual <= 1e-8, (r.residual, r.error)
+        op64 = srv.resident[r.key].op64
+        pts, tris = meshes[r.key]
+        cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+        want = iterative_solve(op64, cm, r.rhs, cfg=dict(solver_tol=1e-10))
+        assert np.linalg.norm(r.x - want) / np.linalg.norm(want) < 1e-6
+
+
+def test_same_alone_and_in_mix(cuda):
+    meshes = _meshes()
+    rng = np.random.default_rng(1)
+    target = rng.standard_normal(9 * meshes["fault"][1].shape[0])
+    alone = _server(meshes)
+    r0 = alone.submit("fault", target, tol=1e-8)
+    alone.run_until_idle(max_ticks=20_000)
+    mixed = _server(meshes)
+    for _ in range(5):
+        mixed.submit("surface", rng.standard_normal(9 * meshes["surface"][1].shape[0]), 1e-8)
+    mixed.step()
+    mixed.submit("fault", rng.standard_normal(target.shape[0]), 1e-6)
+    mixed.step()
+    r1 = mixed.submit("fault", target, tol=1e-8)
+    for _ in range(4):
+        mixed.submit("fault", rng.standard_normal(target.shape[0]), 1e-7)
+    mixed.run_until_idle(max_ticks=20_000)
+    assert r0.converged and r1.converged
+    assert all(r.converged for r in mixed.completed)
+    assert np.linalg.norm(r1.x - r0.x) / np.linalg.norm(r0.x) < 1e-9
