@@ -364,7 +364,7 @@ int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
  * one vector per call; here the per-triangle-pair kernel scalars are
  * generated on the CUDA cores and contracted with the input panel by
  * tcgen05.mma (split TF32, FP32 accumulation in tensor memory folded into
- * a Kahan pair every 4 source tiles).
+ * a Kahan pair every 8 source tiles).
  * in: R x (9 n_src) floats, out: R x (9 n_obs) floats (device, vector after
  * vector); pts / tris as in tct_farfield_tris_matvec.  The workspace size
  * is 0 for an unsupported R or rule. */

@@ -52,7 +52,7 @@ constexpr int MR_S = 8;              // source triangles per tile
 constexpr int MR_K = 7 * MR_S;       // 56: GEMM K per tile
 constexpr int MR_KSTEPS = MR_K / 8;  // tf32 MMA K = 8
 constexpr float MR_EPS = 1e-24f;     // r^2 offset (see far_main_rh2)
-constexpr int MR_FLUSH = 4;          // tiles per tensor-memory accumulation
+constexpr int MR_FLUSH = 8;          // tiles per tensor-memory accumulation
 constexpr unsigned long long MRHS_WAIT_NS = 200000000ull;  // 0.2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -266,7 +266,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 }
 
 template <int R, int NQ, bool UNIFORM, int G>
-__global__ void __launch_bounds__(128 * G, 1)
+__global__ void __launch_bounds__(128 * G + 32, 1)
 mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __restrict__ obs_tris,
           int64_t n_obs,
           const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
@@ -296,6 +296,11 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     const int warp = tid >> 5;
     const int row = tid & (MR_M - 1);
     const int grp = tid >> 7;  // thread group: A sources and tensor-memory columns
+    // The last warp issues the B copies and the MMAs and polls their
+    // barriers, so that the A generators never stall behind the tensor
+    // core's instruction queue.
+    const bool mma_warp = warp == 4 * G;
+    const bool mma_lead = tid == 128 * G;
     const int64_t o = (int64_t)blockIdx.x * MR_M + row;
     const bool valid = o < n_obs;
     const int64_t t0 = (int64_t)blockIdx.y * tiles_per_chunk;
@@ -376,7 +381,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     const int col0 = (grp * (N / 8) / G) * 8, col1 = ((grp + 1) * (N / 8) / G) * 8;
     auto issue_b = [&](int64_t tile, int buf) {
         const uint32_t bar = buf ? barb1 : barb0;
-        if (tid == 0) {
+        if (mma_lead) {
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                          "r"(B_BYTES)
                          : "memory");
@@ -395,10 +400,10 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     for (int64_t t = t0; t < t1; t++) {
         const int buf = (int)((t - t0) & 1);
         // A: this thread's SG source triangles of the tile, KG values, two
-        // source triangles per packed instruction
+        // source triangles per packed instruction (the MMA warp has no rows)
         float av[KG];
 #pragma unroll
-        for (int sp = 0; sp < SG / 2; sp++) {
+        for (int sp = 0; sp < (mma_warp ? 0 : SG / 2); sp++) {
             const f2_t* y = reinterpret_cast<const f2_t*>(srcy) +
                             ((t * MR_S + grp * SG) / 2 + sp) * (3 * NQ);
             f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
@@ -442,7 +447,8 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
         }
         // the MMAs of tile t - 1 have read A and B buffer buf ^ 1
         if (mma_pending) {
-            const bool w = mbar_wait(barm, phase_m);
+            // the MMA warp polls; the others wait at the CTA barrier
+            const bool w = mma_warp ? mbar_wait(barm, phase_m) : true;
             if (!__syncthreads_and(w)) {
                 ok = false;  // the MMAs of the previous tile did not complete in time
                 break;
@@ -451,12 +457,13 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
             mma_pending = false;
             if ((t - t0) % MR_FLUSH == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                tmem_fold<N>(lane_base, col0, col1, t - t0 == MR_FLUSH);
+                if (!mma_warp) tmem_fold<N>(lane_base, col0, col1, t - t0 == MR_FLUSH);
                 asm volatile("tcgen05.fence::before_thread_sync;");
             }
         }
         if (t + 1 < t1) issue_b(t + 1, buf ^ 1);
-        if constexpr (KG % 4 == 0) {
+        if (mma_warp) {
+        } else if constexpr (KG % 4 == 0) {
 #pragma unroll
             for (int ch = 0; ch < KG / 4; ch++) {
                 float4 h, l;
@@ -487,7 +494,8 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         {
-            const bool wb = mbar_wait(buf ? barb1 : barb0, buf ? phase_b1 : phase_b0);
+            const bool wb = mma_warp ? mbar_wait(buf ? barb1 : barb0, buf ? phase_b1 : phase_b0)
+                                     : true;
             if (!__syncthreads_and(wb)) {
                 ok = false;
                 break;
@@ -500,7 +508,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
                 pend0 = false;
             }
         }
-        if (tid == 0) {
+        if (mma_lead) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t lboA = MR_M / 8 * 128, lboB = N / 8 * 128;
             const uint32_t aH = smem_u32(Ah), aL = smem_u32(Al),
@@ -526,7 +534,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
         mma_pending = true;
     }
     if (ok && mma_pending) {
-        const bool w = mbar_wait(barm, phase_m);
+        const bool w = mma_warp ? mbar_wait(barm, phase_m) : true;
         if (!__syncthreads_and(w)) ok = false;
         else mma_pending = false;
     }
@@ -542,7 +550,7 @@ mrhs_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __re
     // epilogue: fold the last group, then S - C of this thread's row and
     // column half -> partial[chunk][r][o][9] (the obs-side contraction
     // out[b][d] = J_o sum_j sc_o[b][j] W[d][j] is done by the reduce kernel)
-    if (ok && t1 > t0) {
+    if (ok && t1 > t0 && !mma_warp) {
         tmem_fold<N>(lane_base, col0, col1, t1 - t0 <= MR_FLUSH);
 #pragma unroll 1
         for (int c0 = col0; c0 < col1; c0 += 8) {
@@ -681,13 +689,13 @@ int run_mrhs(const Consts<float>& c, const Rule2D<float>& rule, float* out, cons
     const int64_t per = (n_tiles + chunks - 1) / chunks;
     const int64_t real = (n_tiles + per - 1) / per;
     const size_t smem = (size_t)2 * MR_M * MR_K * 4 + (size_t)2 * 2 * N * MR_K * 4;
-    constexpr int G = 2;  // 8 warps (16 were measured no faster)
+    constexpr int G = 2;  // 8 A-generating warps (16 measured slower: 266 vs 277 applies/s)
     auto kfn = mrhs_main<R, NQ, UNIFORM, G>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return launch_status("mrhs smem attribute");
     dim3 grid((unsigned)((n_obs + MR_M - 1) / MR_M), (unsigned)real);
-    kfn<<<grid, 128 * G, smem, st>>>(rule, pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
+    kfn<<<grid, 128 * G + 32, smem, st>>>(rule, pts, obs_tris, n_obs, srcy, n_tiles, per, Bg,
                                         partial, err);
     if ((rc = launch_status("mrhs main"))) return rc;
     mrhs_reduce<<<(unsigned)((n_obs * R + 127) / 128), 128, 0, st>>>(
