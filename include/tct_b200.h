@@ -380,6 +380,42 @@ int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
 int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
                                 int n_q, void* stream, int* host_flag);
 
+/* ---- quasidynamic (rate-and-state) stepper, FP64 --------------------------- */
+
+/* Per DOF: slip velocity from the rate-state Newton solve of
+ * qd/newton.cpp:107-150 (rate_state_solver; shear-magnitude form, or
+ * per-component with separate_dims).  traction, velocity: (n_tris *
+ * basis_dim, 3); tri_normals (n_tris, 3); state, a, normal_stress: per DOF.
+ * *n_failed (device int, caller-zeroed) counts DOFs whose Newton iteration
+ * did not converge in maxiter steps; they keep the last iterate, as in the
+ * reference, whose convergence assert is compiled out (NDEBUG). */
+int tct_qd_rate_state(int64_t n_tris, int basis_dim, const double* tri_normals,
+                      const double* traction, const double* state, const double* a, double eta,
+                      double V0, double C, const double* normal_stress, double tol, int maxiter,
+                      int separate_dims, double* velocity, int* n_failed, void* stream);
+
+/* Per DOF: vertex average of v_newton (qd/pt_average.cpp:10-35; vertex p's
+ * DOFs are vert_dofs[vert_start[p] .. vert_start[p+1]) in increasing order,
+ * dof_vert[dof] = p), the optional no-backslip filter, plus plate_rate x
+ * field_edges (qd/model_helpers.py:79-119), and the aging-law derivative
+ * dstatedt = (b V0 / Dc)(exp((f0 - state) / b) - |V| / V0)
+ * (model_helpers.py:122-130).  velocity: (n_dofs, 3), dstatedt: n_dofs. */
+int tct_qd_velocity_state(int64_t n_dofs, const int32_t* vert_start, const int32_t* vert_dofs,
+                          const int32_t* dof_vert, const double* v_newton,
+                          const double* field_edges, const double* field_interior,
+                          double plate_rate, int no_backslip, const double* state,
+                          const double* b, double V0, double Dc, double f0, double* velocity,
+                          double* dstatedt, void* stream);
+
+/* Conjugate gradients on a CSR matrix (int64 indices, double values) in one
+ * CTA, x0 = 0, stopping when ||r|| < max(atol, rtol ||b||) or after maxiter
+ * iterations: the scipy.sparse.linalg.cg solve of the constrained mass
+ * system in qd/full_model.py:160-176.  work: 3 n doubles; *iters (device)
+ * receives the iteration count. */
+int tct_cg_csr(int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
+               const double* b, double* x, double* work, double rtol, double atol, int maxiter,
+               int* iters, void* stream);
+
 /* ---- constrained solve -------------------------------------------------- */
 
 /* y (+)= A x for a CSR matrix with double values (device): the constraint

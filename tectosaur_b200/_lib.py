@@ -182,6 +182,13 @@ _SOLVE_SIGS = {
                              c_i),
     "tct_fp64_fma_probe": ([c_p, c_i64, c_i, c_p], c_i),
     "tct_launch_count": ([], ctypes.c_uint64),
+    "tct_qd_rate_state": ([c_i64, c_i, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_double,
+                           ctypes.c_double, c_p, ctypes.c_double, c_i, c_i, c_p, c_p, c_p], c_i),
+    "tct_qd_velocity_state": ([c_i64, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_double, c_i, c_p,
+                               c_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, c_p, c_p,
+                               c_p], c_i),
+    "tct_cg_csr": ([c_i64, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_double, c_i,
+                    c_p, c_p], c_i),
     "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i, c_i], c_sz),
     "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_dp, c_dp,
                                       c_dp, c_i, c_p, c_sz, c_p], c_i),

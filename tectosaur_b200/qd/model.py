@@ -1,0 +1,219 @@
+"""Quasidynamic full-space fault model with its state on the device
+(reference: tectosaur/qd/full_model.py:19-197 and qd/model_helpers.py).
+
+derivs(t, y), y = (slip (9 n_tris), state (3 n_tris)), runs as in the
+reference, every step on the GPU and without host synchronisation:
+  slip deficit = ones_interior (t plate_rate slipdir - slip)
+  traction     = sm cm (cm^T M cm)^-1 cm^T (-H slip_deficit)
+                 H: RegularizedSparseIntegralOp elasticRH3 (its dot_device),
+                 the mass solve: conjugate gradients in one CTA (tct_cg_csr,
+                 rtol 1e-5, atol 1e-12 as the reference's scipy cg call)
+  V            = rate-state Newton solve per DOF (tct_qd_rate_state), vertex
+                 average, plate rate on the free edges (tct_qd_velocity_state)
+  dstate/dt    = aging law (same kernel)
+A y with non-finite entries or a state outside [0, 1.2], or a non-finite V,
+gives inf * y (the reference's signal to its time stepper to shrink the
+step); it is selected on the device.  Newton solves that stop at maxiter
+are counted on the device (newton_failures()).
+"""
+import numpy as np
+
+from .. import _lib
+from ..ops.mass_op import MassOp, unscaled_normals
+from ..simple_solver import DeviceCSR, free_edge_vertices, shared_vertex_matrix
+from ..util import device
+
+
+def calc_derived_constants(cfg):
+    """model_helpers.py:60-73: shear wave speed and radiation damping."""
+    out = dict(cfg)
+    out["cs"] = np.sqrt(out["sm"] / out["density"])
+    out["eta"] = out["sm"] / (2 * out["cs"])
+    return out
+
+
+def aging_law(cfg, V, state):
+    """model_helpers.py:122-125 (host form)."""
+    return (cfg["b"] * cfg["V0"] / cfg["Dc"]) * (
+        np.exp((cfg["f0"] - state) / cfg["b"]) - (V / cfg["V0"]))
+
+
+def build_elastic_op(pts, tris, cfg, K="H", float_type=None):
+    """model_helpers.py:23-42: the regularized elastic operator of the qd
+    model (direct or FMM farfield per tectosaur_cfg)."""
+    from ..ops.sparse_farfield_op import FMMFarfieldOp, TriToTriDirectFarfieldOp
+    from ..ops.sparse_integral_op import RegularizedSparseIntegralOp
+    op_cfg = cfg["tectosaur_cfg"]
+    name = "elastic" + K + "3" if K == "U" else "elasticR" + K + "3"
+    if op_cfg.get("use_fmm", False):
+        far = FMMFarfieldOp(op_cfg["fmm_mac"], op_cfg["pts_per_cell"], op_cfg["fmm_order"])
+    else:
+        far = TriToTriDirectFarfieldOp
+    return RegularizedSparseIntegralOp(
+        op_cfg["quad_coincident_order"], op_cfg["quad_edgeadj_order"],
+        op_cfg["quad_vertadj_order"], op_cfg["quad_far_order"], op_cfg["quad_near_order"],
+        op_cfg["quad_near_threshold"], name, name, [1.0, cfg["pr"]], pts, tris,
+        float_type or op_cfg["float_type"], far)
+
+
+def edge_ones_interior(tris):
+    """1 at every slip DOF (9 per triangle) not held by the free-edge
+    constraints, 0 at those held: cm.dot(ones) for the constraint matrix of
+    free_edge_constraints (full_model.py:119-124, constraint_builders.py:
+    74-135), i.e. the DOFs of triangle corners at free-edge vertices."""
+    tris = np.asarray(tris)
+    interior_dof = ~np.isin(tris.reshape(-1), free_edge_vertices(tris))
+    return np.repeat(interior_dof.astype(np.float64), 3)
+
+
+def _per_dof(v, n):
+    return np.ascontiguousarray(np.broadcast_to(np.asarray(v, np.float64), (n,)))
+
+
+class FullspaceModel:
+    """FullspaceModel(m, cfg) of qd/full_model.py:19-150 for a fault-only
+    mesh m = (pts, tris).  H: an already built elastic operator (default:
+    build_elastic_op from cfg['tectosaur_cfg'])."""
+
+    def __init__(self, m, cfg, H=None):
+        t = device.require_cuda()
+        self.cfg = calc_derived_constants(cfg)
+        pts, tris = np.asarray(m[0], np.float64), np.asarray(m[1], np.int64)
+        self.m = (pts, tris)
+        # setup_mesh (full_model.py:105-117)
+        self.unscaled_tri_normals = unscaled_normals(pts[tris])
+        self.tri_size = np.linalg.norm(self.unscaled_tri_normals, axis=1)
+        self.tri_normals = self.unscaled_tri_normals / self.tri_size[:, None]
+        self.n_tris = tris.shape[0]
+        self.basis_dim = 3
+        self.n_dofs = self.basis_dim * self.n_tris
+        # setup_edge_bcs (full_model.py:119-135): DOFs at free-edge vertices
+        fixed = free_edge_vertices(tris)
+        self.ones_interior = edge_ones_interior(tris)
+        sd = self.cfg.get("slipdir", (1.0, 0.0, 0.0))
+        self.field_inslipdir_interior = self.ones_interior.copy()
+        self.field_inslipdir = self.ones_interior.copy()
+        for d in range(3):
+            self.field_inslipdir_interior.reshape(-1, 3)[:, d] *= sd[d]
+            self.field_inslipdir.reshape(-1, 3)[:, d] = sd[d]
+        self.field_inslipdir_edges = self.field_inslipdir - self.field_inslipdir_interior
+        # slip -> traction (full_model.py:152-176): continuity + free edges
+        self.H = H if H is not None else build_elastic_op(pts, tris, self.cfg)
+        self.H_dtype = device.torch_dtype(getattr(self.H, "float_type", np.float64))
+        self.mass = MassOp(self.cfg["tectosaur_cfg"]["quad_mass_order"], pts, tris)
+        self.cm_host = shared_vertex_matrix(tris, fixed_vertices=fixed)
+        self.cm, self.cmT = DeviceCSR(self.cm_host), DeviceCSR(self.cm_host.T)
+        mc = (self.cm_host.T @ self.mass.mat @ self.cm_host).tocsr()
+        mc.sort_indices()
+        self.n_free = mc.shape[0]
+        self.mass_c = (device.to_dev(mc.indptr.astype(np.int64)),
+                       device.to_dev(mc.indices.astype(np.int64)),
+                       device.to_dev(mc.data.astype(np.float64)))
+        # vertex averaging: the DOFs at each vertex in increasing order
+        dof_vert = tris.reshape(-1)
+        order = np.argsort(dof_vert, kind="stable")
+        counts = np.bincount(dof_vert, minlength=pts.shape[0])
+        self.vert_start = device.to_dev(np.concatenate([[0], np.cumsum(counts)]), np.int32)
+        self.vert_dofs = device.to_dev(order, np.int32)
+        self.dof_vert = device.to_dev(dof_vert, np.int32)
+        # device copies of the per-DOF fields and parameters
+        f64 = t.float64
+        self.d_normals = device.to_dev(self.tri_normals)
+        self.d_interior = device.to_dev(self.ones_interior)
+        self.d_inslipdir = device.to_dev(self.field_inslipdir)
+        self.d_edges = device.to_dev(self.field_inslipdir_edges)
+        self.d_int_dir = device.to_dev(self.field_inslipdir_interior)
+        self.d_a = device.to_dev(_per_dof(self.cfg["a"], self.n_dofs))
+        self.d_b = device.to_dev(_per_dof(self.cfg["b"], self.n_dofs))
+        self.d_sigma = device.to_dev(np.full(self.n_dofs, float(self.cfg["additional_normal_stress"])))
+        n9 = 9 * self.n_tris
+        self._x = t.zeros(n9, dtype=self.H_dtype, device="cuda")
+        self._y = t.zeros(n9, dtype=self.H_dtype, device="cuda")
+        self._rhs_c = t.zeros(self.n_free, dtype=f64, device="cuda")
+        self._soln = t.zeros(self.n_free, dtype=f64, device="cuda")
+        self._cg_work = t.zeros(3 * max(self.n_free, 1), dtype=f64, device="cuda")
+        self._cg_iters = t.zeros(1, dtype=t.int32, device="cuda")
+        self._vn = t.zeros(n9, dtype=f64, device="cuda")
+        self.n_failed = t.zeros(1, dtype=t.int32, device="cuda")
+        self.n_evals = 0
+
+    # -- pieces ---------------------------------------------------------------
+    def slip_to_traction(self, slip):
+        """sm cm (cm^T M cm)^-1 cm^T (-H slip) on device FP64 vectors."""
+        t = device.torch()
+        self._x.copy_(slip)
+        self.H.dot_device(self._x, self._y)
+        rhs = -self._y.to(t.float64)
+        self.cmT.dot_device(rhs, self._rhs_c)
+        ip, ix, dv = self.mass_c
+        _lib.check(_lib.lib.tct_cg_csr(
+            self.n_free, _lib.tptr(ip), _lib.tptr(ix), _lib.tptr(dv), _lib.tptr(self._rhs_c),
+            _lib.tptr(self._soln), _lib.tptr(self._cg_work), 1e-5, 1e-12, 10 * self.n_free,
+            _lib.tptr(self._cg_iters), _lib.stream_ptr()), "tct_cg_csr")
+        out = t.empty(9 * self.n_tris, dtype=t.float64, device="cuda")
+        self.cm.dot_device(self._soln, out)
+        out *= self.cfg["sm"]
+        if self.cfg.get("only_x", False):
+            out.view(-1, 3)[:, 1:] = 0.0
+        return out
+
+    def rate_state_solve(self, traction, state):
+        """(V, dstate/dt): model_helpers.py:79-119 and the aging law."""
+        t = device.torch()
+        cfg = self.cfg
+        _lib.check(_lib.lib.tct_qd_rate_state(
+            self.n_tris, 3, _lib.tptr(self.d_normals), _lib.tptr(traction), _lib.tptr(state),
+            _lib.tptr(self.d_a), float(cfg["eta"]), float(cfg["V0"]), float(cfg.get("C", 0.0)),
+            _lib.tptr(self.d_sigma), 1e-12, 50, int(bool(cfg.get("rs_separate_dims", False))),
+            _lib.tptr(self._vn), _lib.tptr(self.n_failed), _lib.stream_ptr()),
+            "tct_qd_rate_state")
+        V = t.empty(9 * self.n_tris, dtype=t.float64, device="cuda")
+        dstate = t.empty(self.n_dofs, dtype=t.float64, device="cuda")
+        _lib.check(_lib.lib.tct_qd_velocity_state(
+            self.n_dofs, _lib.tptr(self.vert_start), _lib.tptr(self.vert_dofs),
+            _lib.tptr(self.dof_vert), _lib.tptr(self._vn), _lib.tptr(self.d_edges),
+            _lib.tptr(self.d_int_dir), float(cfg["plate_rate"]),
+            int(bool(cfg.get("no_backslip", False))), _lib.tptr(state), _lib.tptr(self.d_b),
+            float(cfg["V0"]), float(cfg["Dc"]), float(cfg["f0"]), _lib.tptr(V), _lib.tptr(dstate),
+            _lib.stream_ptr()), "tct_qd_velocity_state")
+        return V, dstate
+
+    def solve_for_full_state(self, t_, y):
+        """full_model.py:42-85 on device tensors: (slip, slip_deficit,
+        state, traction, V, dstatedt, bad) with bad a device bool."""
+        t = device.torch()
+        n_slip = y.shape[0] // 4 * 3
+        slip, state = y[:n_slip], y[n_slip:].contiguous()
+        plate_motion = (t_ * self.cfg["plate_rate"]) * self.d_inslipdir
+        slip_deficit = self.d_interior * (plate_motion - slip)
+        traction = self.slip_to_traction(slip_deficit)
+        V, dstate = self.rate_state_solve(traction, state)
+        bad = (~t.isfinite(y).all()) | (state < 0).any() | (state > 1.2).any() | \
+            (~t.isfinite(V).all())
+        return slip, slip_deficit, state, traction, V, dstate, bad
+
+    def make_derivs(self):
+        t = device.torch()
+
+        def derivs(t_, y):
+            self.n_evals += 1
+            *_, V, dstate, bad = self.solve_for_full_state(t_, y)
+            out = t.cat((V, dstate))
+            return t.where(bad, y * float("inf"), out)
+
+        return derivs
+
+    def newton_failures(self, reset=True):
+        """DOFs whose Newton iteration stopped at maxiter since the last call
+        (a host sync).  The reference's assert on them is compiled out
+        (extension builds define NDEBUG), so such a DOF keeps its last
+        iterate there too; an attempted step that meets them is normally
+        rejected by the error control."""
+        n = int(self.n_failed.item())
+        if reset and n:
+            self.n_failed.zero_()
+        return n
+
+    @property
+    def last_cg_iterations(self):
+        return int(self._cg_iters.item())

@@ -22,6 +22,12 @@ Outputs (all small, committed):
   near_split.npz    reference find_close_or_touching + split_adjacent_close +
                     resolve_ea_rotation on two meshes (lexsorted).
   mass_op.npz       reference MassOp matrix (dense) on a small mesh.
+  qd.npz            the reference's quasidynamic pieces on seeded inputs:
+                    qd/newton.cpp rate_state_solver (shear-magnitude and
+                    separate-dimension forms, zero-shear DOFs included),
+                    qd/pt_average.cpp pt_averageD, and free_edge_constraints
+                    + build_constraint_matrix of the qd model's edge
+                    conditions (the DOFs it holds at zero).
 """
 import hashlib
 import os
@@ -151,7 +157,49 @@ def mass_op():
     np.savez_compressed(os.path.join(HERE, "mass_op.npz"), **out)
 
 
+def qd_inputs(seed=12, n_tris=40):
+    """Seeded rate-state inputs in the units of the reference's qd runs
+    (Pa, m/s; sm 3e10, density 2670 -> eta = sm / (2 cs))."""
+    rng = np.random.default_rng(seed)
+    n = rng.standard_normal((n_tris, 3))
+    n /= np.linalg.norm(n, axis=1)[:, None]
+    traction = rng.standard_normal((n_tris * 3, 3)) * rng.uniform(1e5, 3e7, (n_tris * 3, 1))
+    traction[::7] = 0.0  # zero shear: the solver returns zero velocity
+    state = rng.uniform(0.5, 0.85, n_tris * 3)
+    a = rng.uniform(0.008, 0.012, n_tris * 3)
+    sm, density = 3e10, 2670.0
+    eta = sm / (2 * np.sqrt(sm / density))
+    normal_stress = np.full(n_tris * 3, 50e6)
+    return dict(tri_normals=n, traction=traction, state=state, a=a, eta=eta, V0=1e-6, C=0.0,
+                normal_stress=normal_stress)
+
+
+def qd():
+    import tectosaur.mesh.mesh_gen as mesh_gen
+    from tectosaur.constraint_builders import free_edge_constraints
+    from tectosaur.constraints import build_constraint_matrix
+    newton = refshim._load_ext("newton")
+    pt_average = refshim._load_ext("pt_average")
+    inp = qd_inputs()
+    out = {"in_" + k: np.asarray(v) for k, v in inp.items()}
+    for sep in (False, True):
+        V = np.zeros_like(inp["traction"])
+        newton.rate_state_solver(inp["tri_normals"], inp["traction"], inp["state"], V, inp["a"],
+                                 inp["eta"], inp["V0"], inp["C"], inp["normal_stress"], 1e-12,
+                                 50, 3, sep)
+        out["V_sep%d" % int(sep)] = V
+    m = mesh_gen.make_rect(5, 4, [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]])
+    field = np.random.default_rng(13).standard_normal(m[1].size)
+    out["avg_pts"], out["avg_tris"], out["avg_field"] = m[0], m[1], field
+    out["avg_out"] = pt_average.pt_averageD(m[0], m[1].astype(np.int64), field)
+    cs = free_edge_constraints(m[1])
+    cm, _, _ = build_constraint_matrix(cs, m[1].shape[0] * 9)
+    out["edge_ones_interior"] = cm.dot(np.ones(cm.shape[1]))
+    np.savez_compressed(os.path.join(HERE, "qd.npz"), **out)
+
+
 if __name__ == "__main__":
+    qd()
     ref_goldens()
     quad_rules()
     kernel_values()
