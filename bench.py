@@ -1139,6 +1139,149 @@ def run_batch_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def qd_mesh(n=25):
+    """The reference's quasidynamic example fault: make_rect(25, 25) over a
+    2 x 2 vertical square (1,152 triangles)."""
+    from tectosaur_b200.mesh.mesh_gen import make_rect
+    return make_rect(n, n, [[-1, 0, 1], [-1, 0, -1], [1, 0, -1], [1, 0, 1]])
+
+
+def qd_config(n_tris, float_type=np.float32):
+    """The configuration of the reference's quasidynamic example run
+    (shear modulus 3e10, density 2670, a 0.010, b 0.015, Dc 2e-6, f0 0.6,
+    V0 1e-6, plate rate 1e-9, 50 MPa normal stress, time-step tolerance 1e-4,
+    the 722-triangle plain method's operator rules, mass rule order 4)."""
+    return dict(sm=3e10, pr=0.25, density=2670.0, Dc=2e-6, f0=0.6, V0=1e-6,
+                a=np.full(n_tris * 3, 0.010), b=np.full(n_tris * 3, 0.015), plate_rate=1e-9,
+                additional_normal_stress=50e6, timestep_tol=1e-4,
+                tectosaur_cfg=dict(quad_coincident_order=6, quad_edgeadj_order=6,
+                                   quad_vertadj_order=6, quad_near_order=5,
+                                   quad_near_threshold=2.5, quad_far_order=2, quad_mass_order=4,
+                                   float_type=float_type, use_fmm=False))
+
+
+def qd_initial(n_tris, seed=9):
+    """Zero slip, state 0.7 with a seeded perturbation (which perturbs the
+    initial slip rate)."""
+    rng = np.random.default_rng(seed)
+    return np.concatenate([np.zeros(9 * n_tris), 0.7 + 0.01 * rng.standard_normal(3 * n_tris)])
+
+
+def cpu_qd_baseline(pts, tris, cfg, y0, n_steps):
+    """The oracle (qd_oracle.FullspaceModel: oracle operator composition,
+    scipy cg, the rate-state Newton restatement) stepped by scipy's RK23,
+    as the reference's Integrator does; nearfield blocks integrated before
+    the timing."""
+    from scipy.integrate import RK23
+    from oracle import qd_oracle
+    from tectosaur_b200.ops.mass_op import MassOp, unscaled_normals
+    from tectosaur_b200.qd.model import edge_ones_interior
+    from tectosaur_b200.simple_solver import free_edge_vertices, shared_vertex_matrix
+    import scipy.sparse
+    op = cfg["tectosaur_cfg"]
+    H = qd_oracle.sparse_op(op["quad_coincident_order"], op["quad_edgeadj_order"],
+                            op["quad_vertadj_order"], op["quad_far_order"],
+                            op["quad_near_order"], op["quad_near_threshold"], "elasticRH3",
+                            [1.0, cfg["pr"]], pts, tris, op["float_type"])
+    ones = edge_ones_interior(tris)
+    cm_edges = scipy.sparse.diags(ones).tocsc()[:, ones > 0]
+    cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+    un = unscaled_normals(pts[tris])
+    normals = un / np.linalg.norm(un, axis=1)[:, None]
+    om = qd_oracle.FullspaceModel(pts, tris, cfg, H, MassOp(4, pts, tris).mat, cm, cm_edges,
+                                  normals)
+    rk = RK23(om.derivs, 0.0, y0, 1e50, atol=cfg["timestep_tol"], rtol=cfg["timestep_tol"])
+    rk.h_abs = 365.25 * 24 * 3600 / 10.0
+    t0 = time.perf_counter()
+    for _ in range(n_steps):
+        rk.step()
+    dt = time.perf_counter() - t0
+    return {"value": n_steps / dt, "unit": "qd steps/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": ("%d RK23 steps of the oracle model (oracle operator, scipy cg, Newton "
+                       "restatement) from the same initial state, %.1f s" % (n_steps, dt))}
+
+
+def run_qd_workload(args, rank, world, torch, dist):
+    """Quasidynamic rate-and-state time stepping of the reference's example
+    fault, the whole state on the device."""
+    from tectosaur_b200 import _lib, qd
+    pts, tris = qd_mesh()
+    n = tris.shape[0]
+    cfg = qd_config(n)
+    t_build = time.perf_counter()
+    model = qd.FullspaceModel((pts, tris), cfg)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
+    y0 = qd_initial(n, seed=9 + rank)
+    n_steps = args.qd_steps
+
+    def run():
+        integ = qd.Integrator(model, (0.0, y0))
+        integ.integrate(n_steps)
+        y_end = integ.h_y[-1].cpu().numpy()
+        return integ, y_end
+
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    l0 = _lib.launch_count()
+    e0 = model.n_evals
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        integ, y_end = run()
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = _lib.launch_count() - l0
+    evals = (model.n_evals - e0) / args.steps
+    total_ms = a.elapsed_time(b)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n_steps * args.steps / (total_ms * 1e-3)
+    if rank != 0:
+        return
+    line = {
+        "metric": "quasidynamic time steps/s (RK23 with rate-state friction, device-resident)",
+        "value": value, "unit": "qd steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 state, f32 elastic operator", "data": "synthetic (seeded initial state)",
+        "config": {"workload": ("%d RK23 steps (one bench step = the whole integration from "
+                                "the seeded state) of the reference's quasidynamic example: "
+                                "make_rect(25, 25) vertical fault, %d triangles, elasticRH3 "
+                                "RegularizedSparseIntegralOp(6,6,6,2,5,2.5) FP32, mass order 4, "
+                                "a 0.010, b 0.015, Dc 2e-6, V0 1e-6, timestep_tol 1e-4"
+                                % (n_steps, n)),
+                   "n_tris": n, "qd_steps": n_steps, "rejected_steps": integ.rk23.n_rejected,
+                   "derivs_per_run": evals, "t_end_years": integ.h_t[-1] / qd.siay,
+                   "last_cg_iterations": model.last_cg_iterations,
+                   "newton_failures": model.newton_failures(),
+                   "model_build_s": t_build, "l2": "small problem: working set in L2",
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "whole stepper (latency-bound at this size)", "bound": "hbm",
+                     "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
+                     "traffic": None},
+        "e2e": {"value": value, "unit": "qd steps/s", "h2d_bytes_per_step": int(y0.nbytes),
+                "d2h_bytes_per_step": int(y_end.nbytes),
+                "api": "qd.Integrator(model, (0, y0 numpy)).integrate(n); h_y[-1] -> numpy"},
+        "gpu_launches": int(launches // args.steps),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_qd_baseline(pts, tris, cfg, y0, 3)
+    print(json.dumps(line), flush=True)
+
+
 def serve_meshes(n_meshes=6, seed=6, lo=2000, hi=20000):
     """The served stream's meshes: triangle counts log-uniform in [lo, hi]
     (seeded), cycling through a vertical strike-slip fault, a 30-degree
@@ -1329,7 +1472,7 @@ def main():
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve"],
+                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -1337,6 +1480,8 @@ def main():
                          "batched mixed-precision solves vs the plain FP64 solve")
     ap.add_argument("--rhs", type=int, default=64)
     ap.add_argument("--pairs", type=int, default=400_000)
+    ap.add_argument("--qd-steps", type=int, default=200,
+                    help="RK23 steps per quasidynamic integration (qd workload)")
     ap.add_argument("--requests", type=int, default=48,
                     help="solve requests in the served stream (serve workload)")
     ap.add_argument("--fmm-order", type=int, default=None)
@@ -1362,10 +1507,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve"):
+    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
          "panel": run_panel_workload, "batch": run_batch_workload,
-         "serve": run_serve_workload}[args.workload](
+         "serve": run_serve_workload, "qd": run_qd_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()

@@ -82,34 +82,6 @@ def oracle_sparse_op(orc, nq_co, nq_ea, nq_va, nq_far, nq_near, thr, K, params, 
                      float_type):
     """v -> the oracle composition of RegularizedSparseIntegralOp.dot with the
     corrected nearfield blocks integrated once (for repeated applies)."""
-    from tectosaur_b200.nearfield import triangle_rules as tr
-    from tectosaur_b200.nearfield.nearfield_op import nearfield_pairs
-    from tectosaur_b200.util.quadrature import gauss2d_tri, gauss4d_tri
-    tris = np.asarray(tris)
-    idx = np.arange(tris.shape[0])
-    classes = nearfield_pairs(pts, tris, idx, idx, thr)
-    far_rule = gauss4d_tri(nq_far, nq_far)
-    rules = {"co": (tr.coincident_quad(nq_co), False, True),
-             "ea": (tr.edge_adj_quad(nq_ea), True, True),
-             "va": (tr.vertex_adj_quad(nq_va, nq_va, nq_va), True, True),
-             "near": (gauss4d_tri(nq_near, nq_near), False, False)}
-    ft = np.dtype(float_type)
-    near = []
-    for c, (rule, adj, check0) in rules.items():
-        recs, dofs = classes[c]
-        if dofs.shape[0] == 0:
-            continue
-        blocks = orc.pairs(K, float_type, rule, pts, tris, recs[:, :5 if adj else 2], params,
-                           adj=adj, check0=check0).astype(ft)
-        corr = orc.pairs(K, float_type, far_rule, pts, tris, recs[:, :2], params, adj=False,
-                         check0=(c == "co")).astype(ft)
-        near.append((dofs, (blocks - corr).reshape(-1, 9, 9).astype(np.float64)))
-    q2 = gauss2d_tri(nq_far)
-
-    def dot(v):
-        y = orc.farfield_tris(K, float_type, q2, pts, tris, tris, v, params)
-        for dofs, blocks in near:
-            y = y + orc.bcoo_matvec(float_type, dofs[:, 0], dofs[:, 1], blocks, v, y.shape[0])
-        return y
-
-    return dot
+    from oracle import qd_oracle
+    return qd_oracle.sparse_op(nq_co, nq_ea, nq_va, nq_far, nq_near, thr, K, params, pts, tris,
+                               float_type)
