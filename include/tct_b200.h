@@ -380,6 +380,41 @@ int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
 int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
                                 int n_q, void* stream, int* host_flag);
 
+/* ---- interior evaluation (tectosaur/interior.py InteriorOp) --------------- */
+
+/* Triangle sources to observation points (matrix_free.cl:109-194,
+ * farfield_tris_to_pts{K}; kernels U/T/A/H): out[i] (3 per point) = sum over
+ * source triangles and rule points of J_s w_q K(x_i, y_q; n_i, n_s) .
+ * (sum_b in_b phi_b(q)), r2 == 0 skipped.  in: 9 per source triangle; the
+ * rule (n_q <= 13 points) and params on the host; workspace sized by
+ * tct_farfield_tris_to_pts_workspace_bytes. */
+size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_src, int n_q);
+int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const void* in,
+                             const void* obs_pts, const void* obs_ns, int64_t n_obs,
+                             const void* pts, const int32_t* src_tris, int64_t n_src, int n_q,
+                             const double* quad_pts, const double* quad_wts,
+                             const double* params, void* workspace, size_t workspace_bytes,
+                             void* stream);
+
+/* Point-triangle integrals (assemble.cl:140-186 interior_pairs, kernels
+ * U/T/A/H): per pair (obs point, src triangle, clicks) (int32 x3) the 27
+ * entries [d_obs][b_src][d_src] of J_s sum_q w_q phi_b K, Kahan-summed, the
+ * source triangle rotated by clicks and the basis de-rotated.  qp (2 n_q),
+ * qw (n_q): device arrays in the working precision.  finite_part keeps only
+ * basis b = clicks. */
+int tct_interior_pairs(int kernel, int prec, void* result, int n_q, const void* qp,
+                       const void* qw, const void* obs_pts, const void* obs_ns, const void* pts,
+                       const int32_t* tris, const int32_t* pairs, int64_t n_pairs,
+                       const double* params, int finite_part, void* stream);
+
+/* Observation point at vertex `clicks` of the source triangle
+ * (interior_corners.cl, elasticH3): 27 entries per pair as above; qt, qw:
+ * device arrays of an angle rule on [0, pi/2]. */
+int tct_interior_corners(int prec, void* result, int n_q, const void* qt, const void* qw,
+                         const void* obs_ns, const void* pts, const int32_t* tris,
+                         const int32_t* pairs, int64_t n_pairs, const double* params,
+                         void* stream);
+
 /* ---- quasidynamic (rate-and-state) stepper, FP64 --------------------------- */
 
 /* Per DOF: slip velocity from the rate-state Newton solve of

@@ -636,6 +636,197 @@ int bcoo_impl(long nb, int bs, const long* rows, const long* cols,
 
 }  // namespace
 
+// ---- interior evaluation (interior.py, assemble.cl:140-186,
+// matrix_free.cl:109-194, interior_corners.cl) --------------------------------
+
+// Point-triangle integrals (interior_pairs + integrate_pt_tri,
+// integral_primitives.cl:216-258): per pair (obs point, src tri, clicks) the
+// 27 entries [d_obs][b_src][d_src] = J_s sum_q w_q phi_b(q) K(x, y_q)
+// (Kahan-summed, no r2 == 0 skip), de-rotated by the clicks.
+template <typename R>
+int interior_pairs_impl(int kernel, double* result, int n_q, const double* qp_d,
+                        const double* qw_d, const double* obs_pts_d, const double* obs_ns_d,
+                        int n_obs, const double* pts_d, int n_pts, const int* tris,
+                        const int* pairs, long n_pairs, const double* params_d,
+                        int finite_part, int n_threads) {
+    auto op = cast<R>(obs_pts_d, 3 * (size_t)n_obs);
+    auto on = cast<R>(obs_ns_d, 3 * (size_t)n_obs);
+    auto pts = cast<R>(pts_d, 3 * (size_t)n_pts);
+    auto qp = cast<R>(qp_d, 2 * (size_t)n_q);
+    auto qw = cast<R>(qw_d, n_q);
+    R params[2] = {R(params_d[0]), R(params_d[1])};
+    Consts<R> c(params);
+#pragma omp parallel for num_threads(n_threads) schedule(static)
+    for (long i = 0; i < n_pairs; i++) {
+        const int obs = pairs[3 * i], src = pairs[3 * i + 1], clicks = pairs[3 * i + 2];
+        TriInfo<R> s;
+        tri_info(s, pts.data(), tris, src, clicks, false);
+        const R* x = &op[(size_t)obs * 3];
+        const R* nobs = &on[(size_t)obs * 3];
+        R rt[27], kc[27];
+        for (int k = 0; k < 27; k++) rt[k] = kc[k] = 0;
+        for (int iq = 0; iq < n_q; iq++) {
+            R sx = qp[iq * 2], sy = qp[iq * 2 + 1], quadw = qw[iq];
+            R srcb[3] = {1 - sx - sy, sx, sy};
+            R y[3];
+            for (int d = 0; d < 3; d++) {
+                y[d] = 0;
+                for (int b = 0; b < 3; b++) y[d] += srcb[b] * s.tri[b][d];
+            }
+            R D[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
+            R r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+            R Karr[9];
+            tensor_UTAH(kernel, c, D[0], D[1], D[2], r2, nobs, s.n, Karr);
+            R obsb0 = R(1) * quadw;
+            int idx = 0;
+            for (int dob = 0; dob < 3; dob++)
+                for (int bs = 0; bs < 3; bs++)
+                    for (int ds = 0; ds < 3; ds++, idx++) {
+                        R val = obsb0 * srcb[bs] * Karr[dob * 3 + ds];
+                        R yk = val - kc[idx];
+                        R t = rt[idx] + yk;
+                        kc[idx] = (t - rt[idx]) - yk;
+                        rt[idx] = t;
+                    }
+        }
+        int derot[3];
+        for (int b = 0; b < 3; b++) derot[b] = positive_mod(-clicks + b, 3);
+        double* out = result + i * 27;
+        for (int d1 = 0; d1 < 3; d1++)
+            for (int b2 = 0; b2 < 3; b2++) {
+                if (finite_part && b2 != clicks) continue;
+                for (int d2 = 0; d2 < 3; d2++)
+                    out[d1 * 9 + b2 * 3 + d2] = s.jacobian * rt[d1 * 9 + derot[b2] * 3 + d2];
+            }
+    }
+    return 0;
+}
+
+// Observation point at a vertex of the source triangle (interior_corners.cl,
+// elasticH3): the radial integral from the vertex done in closed form, a
+// Gauss rule over the angle t in [0, pi/2].  In the reference kernel the
+// log-term tensor I4 is scaled by the integer quotient 1/3, which is 0, so
+// only the 1/r^3 tensor I3 and the scalar terms I1, I2 contribute; that is
+// restated as is.
+template <typename R>
+int interior_corners_impl(double* result, int n_q, const double* qp_d, const double* qw_d,
+                          const double* obs_ns_d, int n_obs, const double* pts_d, int n_pts,
+                          const int* tris, const int* pairs, long n_pairs,
+                          const double* params_d, int n_threads) {
+    auto on = cast<R>(obs_ns_d, 3 * (size_t)n_obs);
+    auto pts = cast<R>(pts_d, 3 * (size_t)n_pts);
+    auto qp = cast<R>(qp_d, n_q);
+    auto qw = cast<R>(qw_d, n_q);
+    R params[2] = {R(params_d[0]), R(params_d[1])};
+    Consts<R> c(params);
+#pragma omp parallel for num_threads(n_threads) schedule(static)
+    for (long i = 0; i < n_pairs; i++) {
+        const int obs = pairs[3 * i], src = pairs[3 * i + 1], clicks = pairs[3 * i + 2];
+        TriInfo<R> s;
+        tri_info(s, pts.data(), tris, src, clicks, false);
+        const R* nobs = &on[(size_t)obs * 3];
+        R rt[27], kc[27];
+        for (int k = 0; k < 27; k++) rt[k] = kc[k] = 0;
+        R v1[3], v2[3];
+        for (int d = 0; d < 3; d++) {
+            v1[d] = s.tri[1][d] - s.tri[0][d];
+            v2[d] = s.tri[2][d] - s.tri[0][d];
+        }
+        const R mn = nobs[0] * s.n[0] + nobs[1] * s.n[1] + nobs[2] * s.n[2];
+        for (int iq = 0; iq < n_q; iq++) {
+            const R t = qp[iq], quadw = qw[iq];
+            const R ct = std::cos(t), st = std::sin(t);
+            const R rhomax = R(1.0) / (ct + st);
+            R a[3];
+            for (int d = 0; d < 3; d++) a[d] = v1[d] * ct + v2[d] * st;
+            const R A2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+            const R A = std::sqrt(A2);
+            const R A3 = A2 * A;
+            const R A5 = (A3 * A) * A;
+            const R I1 = R(-1) / (A3 * rhomax);
+            const R I2 = (std::log(R(2.0)) + std::log(A) + std::log(rhomax) - 1) / A3;
+            const R T0[3] = {-I2 * ct - I2 * st + I1, I2 * ct, I2 * st};
+            for (int b = 0; b < 3; b++)
+                for (int dob = 0; dob < 3; dob++)
+                    for (int ds = 0; ds < 3; ds++) {
+                        // I3 enters through basis 0 only (the I4 terms vanish)
+                        const R I3 = (-a[dob]) * a[ds] / (A5 * rhomax);
+                        const R T1 = b == 0 ? I3 : R(0);
+                        R Kval = 0.0;
+                        Kval += c.CsH0 * c.CsH3 * T1 * mn;
+                        if (dob == ds) Kval += c.CsH0 * c.CsH1 * mn * T0[b];
+                        const int idx = dob * 9 + b * 3 + ds;
+                        const R val = quadw * Kval;
+                        const R yk = val - kc[idx];
+                        const R tt = rt[idx] + yk;
+                        kc[idx] = (tt - rt[idx]) - yk;
+                        rt[idx] = tt;
+                    }
+        }
+        int derot[3];
+        for (int b = 0; b < 3; b++) derot[b] = positive_mod(-clicks + b, 3);
+        double* out = result + i * 27;
+        for (int d1 = 0; d1 < 3; d1++)
+            for (int b2 = 0; b2 < 3; b2++)
+                for (int d2 = 0; d2 < 3; d2++)
+                    out[d1 * 9 + b2 * 3 + d2] = s.jacobian * rt[d1 * 9 + derot[b2] * 3 + d2];
+    }
+    return 0;
+}
+
+// Triangle sources to observation points (matrix_free.cl:109-194
+// farfield_tris_to_pts{K}): per point the sum over all source triangles
+// and quadrature points of J_s w_q K(x, y_q) . (sum_b in_b phi_b), r2 == 0
+// skipped.
+template <typename R>
+int farfield_tris_to_pts_impl(int kernel, double* out, const double* in_d,
+                              const double* obs_pts_d, const double* obs_ns_d, int n_obs,
+                              const double* pts_d, int n_pts, const int* src_tris, int n_src,
+                              int n_q, const double* qp_d, const double* qw_d,
+                              const double* params_d, int n_threads) {
+    auto op = cast<R>(obs_pts_d, 3 * (size_t)n_obs);
+    auto on = cast<R>(obs_ns_d, 3 * (size_t)n_obs);
+    auto pts = cast<R>(pts_d, 3 * (size_t)n_pts);
+    auto input = cast<R>(in_d, 9 * (size_t)n_src);
+    auto qp = cast<R>(qp_d, 2 * (size_t)n_q);
+    auto qw = cast<R>(qw_d, n_q);
+    R params[2] = {R(params_d[0]), R(params_d[1])};
+    Consts<R> c(params);
+    std::vector<TriInfo<R>> src(n_src);
+    for (int j = 0; j < n_src; j++) tri_info(src[j], pts.data(), src_tris, j, 0, false);
+#pragma omp parallel for num_threads(n_threads) schedule(static)
+    for (int i = 0; i < n_obs; i++) {
+        const R* x = &op[(size_t)i * 3];
+        R sum[3] = {0, 0, 0};
+        for (int j = 0; j < n_src; j++) {
+            const TriInfo<R>& s = src[j];
+            const R* in9 = &input[(size_t)j * 9];
+            for (int iq = 0; iq < n_q; iq++) {
+                R sx = qp[iq * 2], sy = qp[iq * 2 + 1], quadw = qw[iq];
+                R srcb[3] = {1 - sx - sy, sx, sy};
+                R y[3];
+                for (int d = 0; d < 3; d++) {
+                    y[d] = 0;
+                    for (int b = 0; b < 3; b++) y[d] += srcb[b] * s.tri[b][d];
+                }
+                R D[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
+                R r2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+                if (r2 == 0.0) continue;
+                R factor = s.jacobian * quadw;
+                R inv[3] = {0, 0, 0};
+                for (int d = 0; d < 3; d++)
+                    for (int b = 0; b < 3; b++) inv[d] += in9[b * 3 + d] * srcb[b];
+                R sum3[3] = {0, 0, 0};
+                vector_code<R>(kernel, c, D, r2, &on[(size_t)i * 3], s.n, inv, in9, nullptr,
+                               nullptr, R(1), sum3, nullptr);
+                for (int d = 0; d < 3; d++) sum[d] += factor * sum3[d];
+            }
+        }
+        for (int d = 0; d < 3; d++) out[(size_t)i * 3 + d] = sum[d];
+    }
+    return 0;
+}
+
 extern "C" {
 
 int orc_pairs(int kernel, int prec, int adj, int check0, double* result,
@@ -686,6 +877,45 @@ int orc_farfield_tris_dense(int kernel, int prec, double* out, int n_quad,
                                           n_obs, src_tris, n_src, params, n_threads);
     return farfield_dense_impl<double>(kernel, out, n_quad, quad_pts, quad_wts, pts, obs_tris,
                                        n_obs, src_tris, n_src, params, n_threads);
+}
+
+int orc_interior_pairs(int kernel, int prec, double* result, int n_q, const double* qp,
+                       const double* qw, const double* obs_pts, const double* obs_ns, int n_obs,
+                       const double* pts, int n_pts, const int* tris, const int* pairs,
+                       long n_pairs, const double* params, int finite_part, int n_threads) {
+    if (kernel < 0 || kernel > 3) return 2;
+    if (prec == 0)
+        return interior_pairs_impl<float>(kernel, result, n_q, qp, qw, obs_pts, obs_ns, n_obs,
+                                          pts, n_pts, tris, pairs, n_pairs, params, finite_part,
+                                          n_threads);
+    return interior_pairs_impl<double>(kernel, result, n_q, qp, qw, obs_pts, obs_ns, n_obs, pts,
+                                       n_pts, tris, pairs, n_pairs, params, finite_part,
+                                       n_threads);
+}
+
+int orc_interior_corners(int prec, double* result, int n_q, const double* qp,
+                         const double* qw, const double* obs_ns, int n_obs, const double* pts,
+                         int n_pts, const int* tris, const int* pairs, long n_pairs,
+                         const double* params, int n_threads) {
+    if (prec == 0)
+        return interior_corners_impl<float>(result, n_q, qp, qw, obs_ns, n_obs, pts, n_pts, tris,
+                                            pairs, n_pairs, params, n_threads);
+    return interior_corners_impl<double>(result, n_q, qp, qw, obs_ns, n_obs, pts, n_pts, tris,
+                                         pairs, n_pairs, params, n_threads);
+}
+
+int orc_farfield_tris_to_pts(int kernel, int prec, double* out, const double* in,
+                             const double* obs_pts, const double* obs_ns, int n_obs,
+                             const double* pts, int n_pts, const int* src_tris, int n_src,
+                             int n_q, const double* qp, const double* qw,
+                             const double* params, int n_threads) {
+    if (kernel < 0 || kernel > 3) return 2;
+    if (prec == 0)
+        return farfield_tris_to_pts_impl<float>(kernel, out, in, obs_pts, obs_ns, n_obs, pts,
+                                                n_pts, src_tris, n_src, n_q, qp, qw, params,
+                                                n_threads);
+    return farfield_tris_to_pts_impl<double>(kernel, out, in, obs_pts, obs_ns, n_obs, pts, n_pts,
+                                             src_tris, n_src, n_q, qp, qw, params, n_threads);
 }
 
 int orc_make_bsr(long n_row_blocks, long n_blocks, int bs, const long* rows,

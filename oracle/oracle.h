@@ -39,6 +39,27 @@ int orc_farfield_pts(int kernel, int prec, double* out, const double* obs_pts,
                      const double* src_ns, int n_src, const double* in,
                      const double* params, int n_threads);
 
+/* Interior evaluation (tectosaur/interior.py).  interior_pairs:
+ * assemble.cl:140-186 with integrate_pt_tri (integral_primitives.cl:216-258),
+ * kernels 0-3; pairs (obs pt, src tri, clicks) int32; result (n, 3, 3, 3)
+ * [d_obs][b_src][d_src]. */
+int orc_interior_pairs(int kernel, int prec, double* result, int n_q, const double* qp,
+                       const double* qw, const double* obs_pts, const double* obs_ns, int n_obs,
+                       const double* pts, int n_pts, const int* tris, const int* pairs,
+                       long n_pairs, const double* params, int finite_part, int n_threads);
+/* interior_corners.cl (elasticH3, observation point at source vertex
+ * `clicks`); qp: n_q angles in [0, pi/2]. */
+int orc_interior_corners(int prec, double* result, int n_q, const double* qp,
+                         const double* qw, const double* obs_ns, int n_obs, const double* pts,
+                         int n_pts, const int* tris, const int* pairs, long n_pairs,
+                         const double* params, int n_threads);
+/* farfield_tris_to_pts{K}: matrix_free.cl:109-194, kernels 0-3. */
+int orc_farfield_tris_to_pts(int kernel, int prec, double* out, const double* in,
+                             const double* obs_pts, const double* obs_ns, int n_obs,
+                             const double* pts, int n_pts, const int* src_tris, int n_src,
+                             int n_q, const double* qp, const double* qw,
+                             const double* params, int n_threads);
+
 /* farfield_tris (dense 9x9 blocks): tectosaur/assemble.cl:105-138.
  * out layout (n_obs, 3, 3, n_src, 3, 3). */
 int orc_farfield_tris_dense(int kernel, int prec, double* out, int n_quad,

@@ -122,6 +122,68 @@ def farfield_pts(kernel, float_type, obs_pts, obs_ns, src_pts, src_ns, v, params
     return out
 
 
+def interior_pairs(kernel, float_type, quad2d, obs_pts, obs_ns, pts, tris, pair_list, params,
+                   finite_part=False, n_threads=None):
+    """(n, 3, 3, 3) point-triangle integrals (assemble.cl interior_pairs)."""
+    pair_list = np.asarray(pair_list).reshape(-1, 3)
+    n = pair_list.shape[0]
+    out = np.zeros((n, 27))
+    qp, qpp = _d(quad2d[0])
+    qw, qwp = _d(quad2d[1])
+    a, ap = _d(obs_pts)
+    b, bp = _d(obs_ns)
+    p, pp = _d(pts)
+    t, tp = _i(tris)
+    pl, plp = _i(pair_list)
+    pr, prp = _d(params)
+    _, op = _d(out)
+    rc = lib().orc_interior_pairs(KERNEL_IDS[kernel], _prec(float_type), op, qp.shape[0], qpp,
+                                  qwp, ap, bp, a.shape[0], pp, p.shape[0], tp, plp, ctypes.c_long(n), prp,
+                                  int(bool(finite_part)), _threads(n_threads))
+    _check(rc, "interior_pairs")
+    return out.reshape((n, 3, 3, 3))
+
+
+def interior_corners(float_type, quad1d, obs_ns, pts, tris, pair_list, params, n_threads=None):
+    """(n, 3, 3, 3) vertex integrals of elasticH3 (interior_corners.cl)."""
+    pair_list = np.asarray(pair_list).reshape(-1, 3)
+    n = pair_list.shape[0]
+    out = np.zeros((n, 27))
+    qp, qpp = _d(quad1d[0])
+    qw, qwp = _d(quad1d[1])
+    b, bp = _d(obs_ns)
+    p, pp = _d(pts)
+    t, tp = _i(tris)
+    pl, plp = _i(pair_list)
+    pr, prp = _d(params)
+    _, op = _d(out)
+    rc = lib().orc_interior_corners(_prec(float_type), op, qp.shape[0], qpp, qwp, bp,
+                                    b.shape[0], pp, p.shape[0], tp, plp, ctypes.c_long(n), prp,
+                                    _threads(n_threads))
+    _check(rc, "interior_corners")
+    return out.reshape((n, 3, 3, 3))
+
+
+def farfield_tris_to_pts(kernel, float_type, quad2d, obs_pts, obs_ns, pts, src_tris, v, params,
+                         n_threads=None):
+    """Triangle sources -> points (matrix_free.cl farfield_tris_to_pts{K})."""
+    out = np.zeros(np.asarray(obs_pts).shape[0] * 3)
+    qp, qpp = _d(quad2d[0])
+    qw, qwp = _d(quad2d[1])
+    a, ap = _d(obs_pts)
+    b, bp = _d(obs_ns)
+    p, pp = _d(pts)
+    t, tp = _i(src_tris)
+    vin, vp = _d(v)
+    pr, prp = _d(params)
+    _, op = _d(out)
+    rc = lib().orc_farfield_tris_to_pts(KERNEL_IDS[kernel], _prec(float_type), op, vp, ap, bp,
+                                        a.shape[0], pp, p.shape[0], tp, t.shape[0], qp.shape[0],
+                                        qpp, qwp, prp, _threads(n_threads))
+    _check(rc, "farfield_tris_to_pts")
+    return out
+
+
 def farfield_tris_dense(kernel, float_type, quad4d, pts, obs_tris, src_tris, params,
                         n_threads=None):
     """Dense (n_obs, 3, 3, n_src, 3, 3) farfield blocks (assemble.cl farfield_tris)."""

@@ -15,10 +15,11 @@ from .ops.sparse_integral_op import RegularizedSparseIntegralOp
 from .ops.sparse_farfield_op import TriToTriDirectFarfieldOp
 from .ops.dense_integral_op import RegularizedDenseIntegralOp, farfield_tris
 from .farfield import farfield_pts_direct
+from .interior import InteriorOp
 from .kernels import kernels
 
 __all__ = [
     "make_rect", "MassOp", "SumOp", "NegOp", "MultOp", "CompositeOp", "DenseOp",
     "RegularizedSparseIntegralOp", "TriToTriDirectFarfieldOp", "RegularizedDenseIntegralOp",
-    "farfield_tris", "farfield_pts_direct", "kernels",
+    "farfield_tris", "farfield_pts_direct", "InteriorOp", "kernels",
 ]

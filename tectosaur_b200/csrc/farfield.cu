@@ -614,6 +614,35 @@ pts_kernel(Consts<R> c, R* __restrict__ out, const R* __restrict__ obs_pts,
     }
 }
 
+// Source records of the triangle-to-point farfield (matrix_free.cl:109-194):
+// per (source triangle, quadrature point) the point y_q, the normal and the
+// interpolated input scaled by J_s w_q; the point-to-point kernel then sums
+// them in (triangle, point) order, skipping r2 == 0 as the reference does.
+template <typename R>
+__global__ void __launch_bounds__(128)
+tris_to_pts_prep(Rule2D<R> rule, int n_q, const R* __restrict__ pts,
+                 const int32_t* __restrict__ tris, int64_t n_src, const R* __restrict__ in,
+                 R* __restrict__ yq, R* __restrict__ nq, R* __restrict__ vq) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_src * n_q) return;
+    const int64_t j = g / n_q;
+    const int q = (int)(g - j * n_q);
+    TriGeom<R> t;
+    load_tri(t, pts, tris, j, 0, false, false);
+    const R x = rule.x[q], y = rule.y[q];
+    const R b[3] = {1 - x - y, x, y};
+    const R f = t.J * rule.w[q];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        yq[g * 3 + d] = bary_point(t, b, d);
+        nq[g * 3 + d] = t.n[d];
+        R v = 0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) v += in[j * 9 + k * 3 + d] * b[k];
+        vq[g * 3 + d] = f * v;
+    }
+}
+
 template <typename R>
 int pts_dispatch(int kernel, const double* params, void* out, const void* op, const void* on,
                  int64_t n_obs, const void* sp, const void* sn, int64_t n_src, const void* in,
@@ -781,6 +810,57 @@ extern "C" int tct_farfield_pts(int kernel, int prec, void* out, const void* obs
         return pts_dispatch<double>(kernel, params, out, obs_pts, obs_ns, n_obs, src_pts, src_ns,
                                     n_src, in, as_stream(stream));
     set_error("tct_farfield_pts: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
+
+extern "C" size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_src, int n_q) {
+    const size_t r = prec == TCT_F32 ? 4 : 8;
+    return ((size_t)n_src * n_q * 9 * r + 255) / 256 * 256 + 256;
+}
+
+extern "C" int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const void* in,
+                                        const void* obs_pts, const void* obs_ns, int64_t n_obs,
+                                        const void* pts, const int32_t* src_tris, int64_t n_src,
+                                        int n_q, const double* quad_pts, const double* quad_wts,
+                                        const double* params, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_tris_to_pts: negative size");
+    TCT_CHECK_ARG(n_q >= 1 && n_q <= MAXQ, "tct_farfield_tris_to_pts: %d-point rule (1..%d)",
+                  n_q, MAXQ);
+    if (n_obs == 0) return TCT_OK;
+    TCT_CHECK_ARG(out && obs_pts && obs_ns && params && quad_pts && quad_wts,
+                  "tct_farfield_tris_to_pts: null pointer");
+    const size_t need = tct_farfield_tris_to_pts_workspace_bytes(prec, n_src, n_q);
+    TCT_CHECK_ARG(n_src == 0 || (workspace && workspace_bytes >= need && aligned(workspace, 256)),
+                  "tct_farfield_tris_to_pts: workspace of %zu bytes (256-aligned) required", need);
+    cudaStream_t st = as_stream(stream);
+    const int64_t m = n_src * n_q;
+    const unsigned blocks = (unsigned)((m + 127) / 128);
+#define TCT_T2P(R, PREC)                                                                    \
+    if (prec == PREC) {                                                                     \
+        Rule2D<R> rule;                                                                     \
+        for (int q = 0; q < MAXQ; q++) {                                                    \
+            rule.x[q] = q < n_q ? (R)quad_pts[2 * q] : R(0);                                \
+            rule.y[q] = q < n_q ? (R)quad_pts[2 * q + 1] : R(0);                            \
+            rule.w[q] = q < n_q ? (R)quad_wts[q] : R(0);                                    \
+        }                                                                                   \
+        R* yq = reinterpret_cast<R*>(workspace);                                            \
+        R* nq = yq + 3 * m;                                                                 \
+        R* vq = nq + 3 * m;                                                                 \
+        if (m > 0) {                                                                        \
+            tris_to_pts_prep<R><<<blocks, 128, 0, st>>>(rule, n_q, (const R*)pts, src_tris, \
+                                                        n_src, (const R*)in, yq, nq, vq);   \
+            int rc = launch_status("tct_farfield_tris_to_pts prep");                        \
+            if (rc) return rc;                                                              \
+        }                                                                                   \
+        return pts_dispatch<R>(kernel, params, out, obs_pts, obs_ns, n_obs, yq, nq, m, vq,  \
+                               st);                                                         \
+    }
+    TCT_T2P(float, TCT_F32)
+    TCT_T2P(double, TCT_F64)
+#undef TCT_T2P
+    set_error("tct_farfield_tris_to_pts: unsupported precision %d", prec);
     return TCT_ERR_PREC;
 }
 

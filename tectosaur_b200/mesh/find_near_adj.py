@@ -61,3 +61,27 @@ def split_adjacent_close(close_pairs, tris_a, tris_b):
         _lib.i64ptr(va), ctypes.byref(nv), _lib.i64ptr(ea), ctypes.byref(ne)),
         "tct_split_adjacent_close")
     return near[:nn.value].copy(), va[:nv.value].copy(), ea[:ne.value].copy()
+
+
+def split_vertex_nearfield(close_pairs, obs_pts, src_pts, src_tris):
+    """(vertex_pairs, near_pairs) of point-triangle pairs
+    (fast_find_nearfield.cpp:184-215): a pair whose observation point lies
+    within 1e-9 of a source vertex d becomes (obs, tri, d) (the last such d),
+    any other (obs, tri, 0); input order kept."""
+    close_pairs = np.asarray(close_pairs, dtype=np.int64).reshape(-1, 2)
+    obs_pts = np.asarray(obs_pts, dtype=np.float64)
+    src_pts = np.asarray(src_pts, dtype=np.float64)
+    src_tris = np.asarray(src_tris, dtype=np.int64)
+    if close_pairs.shape[0] == 0:
+        e = np.empty((0, 3), dtype=np.int64)
+        return e, e.copy()
+    o = obs_pts[close_pairs[:, 0]]
+    corner = np.full(close_pairs.shape[0], -1, dtype=np.int64)
+    for d in range(3):
+        v = src_pts[src_tris[close_pairs[:, 1], d]]
+        dist = np.sqrt(np.sum((o - v) ** 2, axis=1))
+        corner[dist < 1e-9] = d
+    isv = corner >= 0
+    vertex = np.column_stack([close_pairs[isv], corner[isv]])
+    near = np.column_stack([close_pairs[~isv], np.zeros((~isv).sum(), dtype=np.int64)])
+    return vertex, near

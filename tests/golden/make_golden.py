@@ -8,9 +8,10 @@ built by ``make -C oracle ref``:
 
 Outputs (all small, committed):
   ref_goldens.npz   the reference's own golden masters for the near-pair
-                    finder and the two-triangle farfield (copied verbatim from
-                    tests/golden_masters/*.npy), plus the sphere mesh
-                    test_find_adjacency is computed on.
+                    finder, the two-triangle farfield and the interior
+                    evaluation (copied verbatim from tests/golden_masters/
+                    *.npy), plus the sphere mesh test_find_adjacency is
+                    computed on.
   quad_rules.npz    reference quadrature rules: small ones in full, larger
                     ones as SHA-256 digests of their FP64 bytes.
   kernel_values.npz pointwise U/T/A/H values of the reference's sympy
@@ -55,7 +56,7 @@ def ref_goldens():
     out = {}
     for name in ["test_close_or_touching", "test_find_nearfield_real",
                  "test_find_adjacency", "test_find_close_notself",
-                 "test_farfield_two_tris"]:
+                 "test_farfield_two_tris", "test_interior"]:
         out[name] = np.load(os.path.join(GM, name + ".npy"))
     sphere = mesh_gen.make_sphere([0, 0, 0], 1.0, 3)
     out["sphere_pts"] = sphere[0]
