@@ -1282,6 +1282,102 @@ def run_qd_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_interior_workload(args, rank, world, torch, dist):
+    """Interior evaluation (InteriorOp.dot) on the reference's interior
+    nearfield test configuration, scaled: a make_rect(n, n) fault in the
+    z = 0 plane and a 50 x 50 grid of observation points on the y = 0 plane
+    through it (tests/test_integral_op.py:219-248 of the reference)."""
+    import tectosaur_b200 as tct
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.util.quadrature import gauss2d_tri
+    n = args.grid or 30
+    src = tct.make_rect(n, n, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
+    xs = np.linspace(-3, 3, 50)
+    X, Z = np.meshgrid(xs, xs)
+    obs = np.array([e.flatten() for e in [X, np.zeros_like(X), Z]]).T.copy()
+    ns = np.zeros(obs.shape)
+    ns[:, 2] = 1.0
+    K, nq_vertex, nq_far, nq_near = "elasticT3", 8, 2, 5
+    t_build = time.perf_counter()
+    op = tct.InteriorOp(obs, ns, src, K, 4, nq_vertex, nq_far, nq_near, PARAMS, np.float32)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
+    v = np.zeros(src[1].shape[0] * 9)
+    v.reshape((-1, 3))[:, 0] = 1.0
+    vd = torch.from_numpy(v).cuda()
+    y = torch.empty(op.shape[0], dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        op.dot_device(vd, y)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    l0 = _lib.launch_count()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        op.dot_device(vd, y)
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = (_lib.launch_count() - l0) // args.steps
+    ms = a.elapsed_time(b) / args.steps
+    n_obs = obs.shape[0]
+    value = world * n_obs / (ms * 1e-3)
+    # e2e: host vector in, host values out
+    op.dot(v)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = op.dot(v)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    # point-pair work of the farfield kernel (the dominant term)
+    nq2 = gauss2d_tri(nq_far)[0].shape[0]
+    pairs = n_obs * src[1].shape[0] * nq2
+    if rank != 0:
+        return
+    line = {
+        "metric": "interior evaluation points/s (InteriorOp.dot)",
+        "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 farfield, f64 pair terms", "data": "synthetic",
+        "config": {"workload": ("InteriorOp(elasticT3, nq_vertex 8, nq_far 2, nq_near 5) of a "
+                                "make_rect(%d, %d) fault (%d triangles) at a 50 x 50 grid of "
+                                "points through it, the reference's interior nearfield test "
+                                "case" % (n, n, src[1].shape[0])),
+                   "n_obs": n_obs, "n_src_tris": int(src[1].shape[0]),
+                   "near_pairs": int(op.near_pairs.shape[0]),
+                   "vertex_pairs": int(op.vertex_pairs.shape[0]),
+                   "point_pairs_per_apply": pairs, "build_s": t_build,
+                   "l2": "small problem: working set in L2", "parallelism": "replicas"},
+        "roofline": {"kernel": "pts_kernel (triangle-to-point farfield)", "bound": "fp32",
+                     "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
+                     "traffic": None},
+        "e2e": {"value": world * n_obs / (e2e_ms * 1e-3), "unit": "points/s",
+                "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": int(out.nbytes),
+                "api": "InteriorOp.dot(numpy) -> numpy"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        M = op.near_mat - op.near_mat_correction + op.vertex_mat
+        reps, t0 = 0, time.perf_counter()
+        while reps == 0 or time.perf_counter() - t0 < 2.0:
+            orc.farfield_tris_to_pts(K, np.float32, gauss2d_tri(nq_far), obs, ns, src[0],
+                                     src[1], v, PARAMS)
+            M.dot(v)
+            reps += 1
+        dt = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {
+            "value": n_obs / dt, "unit": "points/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": "the whole apply: oracle triangle-to-point farfield of all %d points "
+                      "(FP32, all host threads) plus the pair terms' host sparse product, "
+                      "%d repetitions, %.3f s each" % (n_obs, reps, dt)}
+    print(json.dumps(line), flush=True)
+
+
 def serve_meshes(n_meshes=6, seed=6, lo=2000, hi=20000):
     """The served stream's meshes: triangle counts log-uniform in [lo, hi]
     (seeded), cycling through a vertical strike-slip fault, a 30-degree
@@ -1472,7 +1568,8 @@ def main():
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd"],
+                    choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd",
+                             "interior"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -1507,10 +1604,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd"):
+    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd", "interior"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
          "panel": run_panel_workload, "batch": run_batch_workload,
-         "serve": run_serve_workload, "qd": run_qd_workload}[args.workload](
+         "serve": run_serve_workload, "qd": run_qd_workload,
+         "interior": run_interior_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()
