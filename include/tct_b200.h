@@ -387,8 +387,9 @@ int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_
  * source triangles and rule points of J_s w_q K(x_i, y_q; n_i, n_s) .
  * (sum_b in_b phi_b(q)), r2 == 0 skipped.  in: 9 per source triangle; the
  * rule (n_q <= 13 points) and params on the host; workspace sized by
- * tct_farfield_tris_to_pts_workspace_bytes. */
-size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_src, int n_q);
+ * tct_farfield_tris_to_pts_workspace_bytes.  Small point sets split the
+ * sources over blocks (partial sums reduced in a fixed order). */
+size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_obs, int64_t n_src, int n_q);
 int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const void* in,
                              const void* obs_pts, const void* obs_ns, int64_t n_obs,
                              const void* pts, const int32_t* src_tris, int64_t n_src, int n_q,

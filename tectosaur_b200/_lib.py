@@ -187,7 +187,7 @@ _SOLVE_SIGS = {
     "tct_qd_velocity_state": ([c_i64, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_double, c_i, c_p,
                                c_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, c_p, c_p,
                                c_p], c_i),
-    "tct_farfield_tris_to_pts_workspace_bytes": ([c_i, c_i64, c_i], c_sz),
+    "tct_farfield_tris_to_pts_workspace_bytes": ([c_i, c_i64, c_i64, c_i], c_sz),
     "tct_farfield_tris_to_pts": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_i64, c_i,
                                   c_dp, c_dp, c_dp, c_p, c_sz, c_p], c_i),
     "tct_interior_pairs": ([c_i, c_i, c_p, c_i, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_dp,

@@ -567,9 +567,14 @@ template <typename R, int K>
 __global__ void __launch_bounds__(128)
 pts_kernel(Consts<R> c, R* __restrict__ out, const R* __restrict__ obs_pts,
            const R* __restrict__ obs_ns, int64_t n_obs, const R* __restrict__ src_pts,
-           const R* __restrict__ src_ns, int64_t n_src, const R* __restrict__ in) {
+           const R* __restrict__ src_ns, int64_t n_src, const R* __restrict__ in,
+           int64_t src_per_chunk) {
+    // grid.y splits the sources into chunks; chunk c writes out + c n_obs 3
     __shared__ R sh[128 * 9];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t s_begin = (int64_t)blockIdx.y * src_per_chunk;
+    const int64_t s_end = min(n_src, s_begin + src_per_chunk);
+    out += (int64_t)blockIdx.y * n_obs * 3;
     const bool valid = i < n_obs;
     R xo[3] = {0, 0, 0}, no[3] = {0, 0, 0};
     if (valid) {
@@ -580,8 +585,8 @@ pts_kernel(Consts<R> c, R* __restrict__ out, const R* __restrict__ obs_pts,
         }
     }
     R sum[3] = {0, 0, 0};
-    for (int64_t t0 = 0; t0 < n_src; t0 += 128) {
-        const int n_tile = (int)min((int64_t)128, n_src - t0);
+    for (int64_t t0 = s_begin; t0 < s_end; t0 += 128) {
+        const int n_tile = (int)min((int64_t)128, s_end - t0);
         __syncthreads();
         if (threadIdx.x < n_tile) {
             const int64_t j = t0 + threadIdx.x;
@@ -646,14 +651,15 @@ tris_to_pts_prep(Rule2D<R> rule, int n_q, const R* __restrict__ pts,
 template <typename R>
 int pts_dispatch(int kernel, const double* params, void* out, const void* op, const void* on,
                  int64_t n_obs, const void* sp, const void* sn, int64_t n_src, const void* in,
-                 cudaStream_t st) {
+                 cudaStream_t st, int64_t n_chunks = 1) {
     Consts<R> c = make_consts<R>(params);
-    unsigned blocks = (unsigned)((n_obs + 127) / 128);
+    const int64_t per = n_chunks > 1 ? (n_src + n_chunks - 1) / n_chunks : n_src;
+    dim3 blocks((unsigned)((n_obs + 127) / 128), (unsigned)std::max<int64_t>(n_chunks, 1));
 #define TCT_PTS_CASE(KID)                                                                 \
     case KID:                                                                             \
         pts_kernel<R, KID><<<blocks, 128, 0, st>>>(c, (R*)out, (const R*)op, (const R*)on, \
                                                    n_obs, (const R*)sp, (const R*)sn,     \
-                                                   n_src, (const R*)in);                  \
+                                                   n_src, (const R*)in, per);             \
         break;
     switch (kernel) {
         TCT_PTS_CASE(kU)
@@ -813,9 +819,27 @@ extern "C" int tct_farfield_pts(int kernel, int prec, void* out, const void* obs
     return TCT_ERR_PREC;
 }
 
-extern "C" size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_src, int n_q) {
+namespace tct {
+namespace {
+// Source chunks of the triangle-to-point farfield: about two blocks per SM
+// over the observation blocks, at least 512 source points per chunk, at
+// most 64 chunks.
+int64_t t2p_chunks(int64_t n_obs, int64_t n_src_pts) {
+    const int64_t obs_blocks = std::max<int64_t>((n_obs + 127) / 128, 1);
+    int64_t want = (2 * 148 + obs_blocks - 1) / obs_blocks;
+    want = std::min<int64_t>(want, std::max<int64_t>(n_src_pts / 512, 1));
+    return std::max<int64_t>(1, std::min<int64_t>(want, 64));
+}
+}  // namespace
+}  // namespace tct
+
+extern "C" size_t tct_farfield_tris_to_pts_workspace_bytes(int prec, int64_t n_obs,
+                                                           int64_t n_src, int n_q) {
     const size_t r = prec == TCT_F32 ? 4 : 8;
-    return ((size_t)n_src * n_q * 9 * r + 255) / 256 * 256 + 256;
+    const int64_t chunks = tct::t2p_chunks(n_obs, n_src * n_q);
+    const size_t recs = ((size_t)n_src * n_q * 9 * r + 255) / 256 * 256;
+    const size_t part = chunks > 1 ? ((size_t)chunks * n_obs * 3 * r + 255) / 256 * 256 : 0;
+    return recs + part + 256;
 }
 
 extern "C" int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const void* in,
@@ -831,7 +855,7 @@ extern "C" int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const v
     if (n_obs == 0) return TCT_OK;
     TCT_CHECK_ARG(out && obs_pts && obs_ns && params && quad_pts && quad_wts,
                   "tct_farfield_tris_to_pts: null pointer");
-    const size_t need = tct_farfield_tris_to_pts_workspace_bytes(prec, n_src, n_q);
+    const size_t need = tct_farfield_tris_to_pts_workspace_bytes(prec, n_obs, n_src, n_q);
     TCT_CHECK_ARG(n_src == 0 || (workspace && workspace_bytes >= need && aligned(workspace, 256)),
                   "tct_farfield_tris_to_pts: workspace of %zu bytes (256-aligned) required", need);
     cudaStream_t st = as_stream(stream);
@@ -854,8 +878,19 @@ extern "C" int tct_farfield_tris_to_pts(int kernel, int prec, void* out, const v
             int rc = launch_status("tct_farfield_tris_to_pts prep");                        \
             if (rc) return rc;                                                              \
         }                                                                                   \
-        return pts_dispatch<R>(kernel, params, out, obs_pts, obs_ns, n_obs, yq, nq, m, vq,  \
-                               st);                                                         \
+        const int64_t chunks = t2p_chunks(n_obs, m);                                        \
+        if (chunks <= 1)                                                                    \
+            return pts_dispatch<R>(kernel, params, out, obs_pts, obs_ns, n_obs, yq, nq, m,  \
+                                   vq, st);                                                 \
+        R* part = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(workspace) +      \
+                                       ((size_t)m * 9 * sizeof(R) + 255) / 256 * 256);       \
+        int rc = pts_dispatch<R>(kernel, params, part, obs_pts, obs_ns, n_obs, yq, nq, m,   \
+                                 vq, st, chunks);                                           \
+        if (rc) return rc;                                                                  \
+        const int64_t n3 = n_obs * 3;                                                       \
+        chunk_reduce<R><<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(part, (int)chunks, n3, \
+                                                                     (R*)out, 0);           \
+        return launch_status("tct_farfield_tris_to_pts reduce");                            \
     }
     TCT_T2P(float, TCT_F32)
     TCT_T2P(double, TCT_F64)

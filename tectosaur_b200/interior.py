@@ -65,7 +65,7 @@ class TriToPtDirectFarfieldOp:
         self.gpu_src_tris = device.to_dev(np.asarray(src_mesh[1]), np.int32)
         self.params = np.ascontiguousarray(np.asarray(params, np.float64)[:2])
         self.ws_bytes = _lib.lib.tct_farfield_tris_to_pts_workspace_bytes(
-            self.prec, self.n_src, self.qx.shape[0])
+            self.prec, self.n_obs, self.n_src, self.qx.shape[0])
         self.workspace = device.workspace(self.ws_bytes)
 
     def dot_device(self, x, y, stream=None):
