@@ -1282,6 +1282,134 @@ def run_qd_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def c4_free_surface_problem(pts, tris, n_surf):
+    """The C4 free-surface problem: surface displacement unknown (continuity,
+    held at zero on the surface's outer edges), fault slip prescribed (unit
+    thrust slip up dip: (0, cos 30, -sin 30) in the fault's dip plane).
+    Returns (cm, c_rhs) as examples/solve.py:iterative_solve uses them: the
+    solution is cm x + c_rhs."""
+    from tectosaur_b200.simple_solver import free_edge_vertices, shared_vertex_matrix
+    n = tris.shape[0]
+    fixed = np.concatenate([free_edge_vertices(tris[:n_surf]), np.unique(tris[n_surf:])])
+    cm = shared_vertex_matrix(tris, fixed_vertices=fixed)
+    slip = np.zeros((n, 3, 3))
+    slip[n_surf:, :, 1] = np.cos(np.radians(30.0))
+    slip[n_surf:, :, 2] = -np.sin(np.radians(30.0))
+    return cm, slip.reshape(-1)
+
+
+def run_c4solve_workload(args, rank, world, torch, dist):
+    """The FMM-accelerated free-surface solve of the 1M-triangle C4 mesh:
+    GMRES on the FP32 operator (FMM farfield, order 8, mac 3, 128 triangles
+    per leaf) inside FP64-residual iterative refinement to 1e-6, against the
+    plain FP64 GMRES solve."""
+    import tectosaur_b200 as tct
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.fmm.tsfmm import FMMFarfieldOp
+    from tectosaur_b200.simple_solver import iterative_solve, iterative_solve_batch
+    tol = 1e-6
+    grid = args.grid or 707
+    pts, tris = c4_mesh(grid)
+    n = tris.shape[0]
+    n_surf = (grid - 1) ** 2 * 2
+    cfg = dict(FMM_CFG)
+    t0 = time.perf_counter()
+    op64 = tct.RegularizedSparseIntegralOp(*[NQ[k] for k in ("nq_co", "nq_ea", "nq_va",
+                                                               "nq_far", "nq_near", "thr")],
+                                           K_NAME, K_NAME, PARAMS, pts, tris, np.float64,
+                                           FMMFarfieldOp(cfg["mac"], cfg["pts_per_cell"],
+                                                         cfg["order"], mode=cfg["mode"]),
+                                           keep_uncorrected=False)
+    op32 = op64.astype(np.float32, keep_uncorrected=False)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    cm, c_rhs = c4_free_surface_problem(pts, tris, n_surf)
+    rhs = -op64.dot(c_rhs)
+    mem_gb = torch.cuda.memory_allocated() / 1e9
+
+    def solve():
+        return iterative_solve_batch(op64, op32, cm, rhs[None, :], tol=tol, restart=200)[0]
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    l0 = _lib.launch_count()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        u = solve()
+    b.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    hist = iterative_solve_batch.last
+    launches = (_lib.launch_count() - l0) // args.steps
+    ms = a.elapsed_time(b) / args.steps
+    value = world / (ms * 1e-3)
+    # the plain path: FP64 GMRES on the FP64 operator, one solve
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    u64 = iterative_solve(op64, cm, rhs, cfg=dict(solver_tol=tol))
+    t_plain = time.perf_counter() - t1
+    plain_steps = iterative_solve.last["n_iter"]
+    diff = float(np.linalg.norm(u - u64) / np.linalg.norm(u64))
+    # matvec timings (device)
+    x32 = torch.randn(9 * n, device="cuda")
+    y32 = torch.empty_like(x32)
+    op32.dot_device(x32, y32)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    op32.dot_device(x32, y32)
+    torch.cuda.synchronize()
+    t_mv32 = time.perf_counter() - t2
+    if rank != 0:
+        return
+    line = {
+        "metric": "BEM solves/s: FMM solve, FP32 GMRES + FP64 refinement vs plain FP64",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 operator + f64 refinement",
+        "data": "synthetic (seeded hills; prescribed uniform fault slip)",
+        "config": {"workload": ("free-surface displacement solve of the C4 mesh (%d x %d "
+                                "topographic surface over [-50, 50]^2 with three seeded hills "
+                                "+ a 30-degree dipping 20 x 10 thrust fault, %d triangles): "
+                                "surface DOFs unknown (continuity, zero on the outer edges), "
+                                "unit thrust slip prescribed on the fault; elasticRH3 "
+                                "RegularizedSparseIntegralOp(6,6,6,1,5,2.5) with the FMM "
+                                "farfield (order 8, mac 3, 128 per leaf); FP32 GMRES inside "
+                                "FP64-residual refinement to 1e-6" % (grid, grid, n)),
+                   "n_tris": n, "n_free": int(cm.shape[1]),
+                   "nearfield_blocks": int(op64.nearfield.bsr.nnzb),
+                   "gmres_steps": hist["gmres_steps"], "residuals": hist["residuals"],
+                   "plain_fp64_solves_per_s": 1.0 / t_plain,
+                   "plain_fp64_gmres_steps": int(plain_steps),
+                   "speedup_vs_plain": value / (1.0 / t_plain),
+                   "rel_diff_vs_plain_fp64": diff, "fp32_matvec_s": t_mv32,
+                   "build_s": t_build, "hbm_gb": mem_gb,
+                   "l2": "operator of %.0f GB (FP64 + FP32 nearfield blocks), beyond L2"
+                         % mem_gb,
+                   "parallelism": "replicas"},
+        "roofline": {"kernel": "whole solve (FMM matvecs: see the fmm workload)",
+                     "bound": "fp32", "achieved": None, "peak": None, "unit": "TFLOP/s",
+                     "frac": None, "traffic": None},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": int(rhs.nbytes),
+                "d2h_bytes_per_step": int(u.nbytes),
+                "api": "simple_solver.iterative_solve_batch(op64, op32, cm, rhs) -> numpy"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        cb = cpu_direct_far_baseline(pts, tris, target_s=10.0)
+        steps = sum(hist["gmres_steps"])
+        cb = dict(cb, value=cb["value"] / max(steps, 1), unit="solves/s",
+                  sample=cb["sample"] + "; one solve = %d such applies" % steps)
+        line["cpu_baseline"] = cb
+    print(json.dumps(line), flush=True)
+
+
 def run_interior_workload(args, rank, world, torch, dist):
     """Interior evaluation (InteriorOp.dot) on the reference's interior
     nearfield test configuration, scaled: a make_rect(n, n) fault in the
@@ -1569,7 +1697,7 @@ def main():
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
                     choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd",
-                             "interior"],
+                             "interior", "c4solve"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -1604,11 +1732,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
 
-    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd", "interior"):
+    if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd", "interior",
+                         "c4solve"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
          "panel": run_panel_workload, "batch": run_batch_workload,
          "serve": run_serve_workload, "qd": run_qd_workload,
-         "interior": run_interior_workload}[args.workload](
+         "interior": run_interior_workload, "c4solve": run_c4solve_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()

@@ -348,7 +348,9 @@ def iterative_solve_batch(iop64, iop32, cm, rhs, tol=1e-8, inner_tol=1e-5, resta
     """R constrained solves at once, mixed precision: GMRES on the FP32
     operator (tensor-core panel farfield) inside FP64 iterative refinement
     with residuals of the FP64 operator, to ||cm^T (rhs - A u)|| <= tol
-    ||cm^T rhs|| in FP64 for every system.  rhs: (R, n_total) host or device;
+    ||cm^T rhs|| in FP64 for every system; each correction solve stops at
+    max(inner_tol, tol / (2 r)) relative, r the current relative residual.
+    rhs: (R, n_total) host or device;
     returns (R, n_total) host float64 and records the refinement history in
     iterative_solve_batch.last."""
     t = device.torch()
@@ -368,7 +370,9 @@ def iterative_solve_batch(iop64, iop32, cm, rhs, tol=1e-8, inner_tol=1e-5, resta
         resid.append(rel)
         if rel <= tol:
             break
-        d, info, n_it = gmres_batch(A32, r, tol=inner_tol, restart=restart)
+        # no more accurate than the outer tolerance needs
+        eta = max(inner_tol, 0.5 * tol / rel) if rel > 0 else inner_tol
+        d, info, n_it = gmres_batch(A32, r, tol=eta, restart=restart)
         steps.append(n_it)
         x = x + d
     else:
