@@ -1533,16 +1533,20 @@ def serve_meshes(n_meshes=6, seed=6, lo=2000, hi=20000):
 
 
 def run_serve_workload(args, rank, world, torch, dist):
-    """The served stream: solve requests on several resident meshes arriving
-    as a Poisson stream, served with continuous batching (tectosaur_b200.
-    serve) against the plain FP64 one-solve-at-a-time GPU path."""
+    """The served stream (C5): solve requests on several resident meshes and
+    quasidynamic requests (qd_steps RK23 steps of the reference's example
+    fault from seeded states), served with continuous batching
+    (tectosaur_b200.serve), against the plain one-request-at-a-time GPU
+    paths (FP64 GMRES solve; single-state qd Integrator)."""
     import tectosaur_b200 as tct
-    from tectosaur_b200 import _lib, serve
+    from tectosaur_b200 import _lib, qd, serve
     from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
     from tectosaur_b200.simple_solver import (free_edge_vertices, iterative_solve,
                                               shared_vertex_matrix)
     tol = 1e-8
     n_req = args.requests
+    n_qd = args.qd_requests
+    qd_steps = args.qd_steps
     meshes = serve_meshes()
     t_build = time.perf_counter()
     srv = serve.SolveServer(slots=16, restart=64)
@@ -1554,6 +1558,12 @@ def run_serve_workload(args, rank, world, torch, dist):
                                                keep_uncorrected=False)
         srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64)
         specs[key] = (op64, cm, tris.shape[0])
+    qpts, qtris = qd_mesh()
+    nq_tris = qtris.shape[0]
+    qcfg = qd_config(nq_tris)
+    qmodel = qd.FullspaceModel((qpts, qtris), qcfg) if n_qd else None
+    if n_qd:
+        srv.add_qd_mesh("qd-fault", qpts, qtris, qcfg, model=qmodel)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
     rng = np.random.default_rng(7 + rank)
@@ -1561,12 +1571,20 @@ def run_serve_workload(args, rank, world, torch, dist):
     stream = []
     for i in range(n_req):
         k = keys[int(rng.integers(len(keys)))]
-        stream.append((k, rng.standard_normal(9 * specs[k][2])))
+        stream.append(("solve", k, rng.standard_normal(9 * specs[k][2])))
+    for i in range(n_qd):
+        stream.insert(int(rng.integers(len(stream) + 1)),
+                      ("qd", "qd-fault", qd_initial(nq_tris, seed=100 + i)))
+    n_all = len(stream)
 
     def replay(offsets):
-        return srv.replay([(off, k, b, tol) for off, (k, b) in zip(offsets, stream)])
+        arr = []
+        for off, (kind, k, payload) in zip(offsets, stream):
+            arr.append((off, "qd", k, payload, qd_steps) if kind == "qd" else
+                       (off, k, payload, tol))
+        return srv.replay(arr)
 
-    zeros = [0.0] * n_req
+    zeros = [0.0] * n_all
     for _ in range(args.warmup):
         replay(zeros)
     torch.cuda.synchronize()
@@ -1577,96 +1595,106 @@ def run_serve_workload(args, rank, world, torch, dist):
     l0 = _lib.launch_count()
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
-    applies0 = sum(r.engine.n_vector_applies for r in srv.resident.values())
     torch.cuda.synchronize()
     a.record()
-    sat = []
     for _ in range(args.steps):
         sat = replay(zeros)
-    torch.cuda.synchronize()
     b.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = _lib.launch_count() - l0
-    applies = sum(r.engine.n_vector_applies for r in srv.resident.values()) - applies0
     total_ms = a.elapsed_time(b)
     if dist is not None:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    served_rate = n_req * args.steps / (total_ms * 1e-3)
-    sat_lat = np.array([r.latency for r in sat])
-    # the plain path: FP64 operator, one solve at a time, in arrival order
-    iterative_solve(specs[keys[0]][0], specs[keys[0]][1], stream[0][1], cfg=dict(solver_tol=tol))
+    served_rate = n_all * args.steps / (total_ms * 1e-3)
+    kinds = [k for k, _, _ in stream]
+    sat_lat = {kd: np.array([r.latency for r, k in zip(sat, kinds) if k == kd])
+               for kd in ("solve", "qd") if kd in kinds}
+    assert all(r.error is None for r in sat), [r.error for r in sat if r.error]
+    # the plain paths, one request at a time in arrival order
+    iterative_solve(specs[keys[0]][0], specs[keys[0]][1], stream[0][2] if kinds[0] == "solve"
+                    else np.ones(9 * specs[keys[0]][2]), cfg=dict(solver_tol=tol))
     torch.cuda.synchronize()
-    service, plain_x, plain_steps = [], [], []
-    for k, rhs in stream:
+    service, err_solve, err_qd = [], [], []
+    for (kind, k, payload), r in zip(stream, sat):
         t0 = time.perf_counter()
-        plain_x.append(iterative_solve(specs[k][0], specs[k][1], rhs, cfg=dict(solver_tol=tol)))
+        if kind == "solve":
+            x = iterative_solve(specs[k][0], specs[k][1], payload, cfg=dict(solver_tol=tol))
+            err_solve.append(float(np.linalg.norm(r.x - x) / np.linalg.norm(x)))
+        else:
+            integ = qd.Integrator(qmodel, (0.0, payload))
+            integ.integrate(qd_steps)
+            y = integ.h_y[-1].cpu().numpy()
+            err_qd.append(float(np.linalg.norm(r.y - y) / np.linalg.norm(y)))
+        torch.cuda.synchronize()
         service.append(time.perf_counter() - t0)
-        plain_steps.append(iterative_solve.last["n_iter"])
-    plain_rate = n_req / sum(service)
-    err = max(float(np.linalg.norm(r.x - px) / np.linalg.norm(px))
-              for r, px in zip(sat, plain_x))
-    # latency under Poisson arrivals at fractions of the served saturation rate;
-    # the plain path's latency at the same arrivals is its FIFO queue over
-    # the measured service times
+    plain_rate = n_all / sum(service)
     sweep = []
     for frac in (0.5, 0.9):
         lam = frac * served_rate / world
-        gaps = np.random.default_rng(11).exponential(1.0 / lam, n_req)
+        gaps = np.random.default_rng(11).exponential(1.0 / lam, n_all)
         offs = np.cumsum(gaps) - gaps[0]
         reqs = replay(list(offs))
-        lat = np.array([r.latency for r in reqs])
         fin, plat = 0.0, []
         for off, sv in zip(offs, service):
             fin = max(fin, off) + sv
             plat.append(fin - off)
-        sweep.append({"arrival_rate_per_s": lam, "fraction_of_served_saturation": frac,
-                      "served_p50_ms": 1e3 * float(np.percentile(lat, 50)),
-                      "served_p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                      "plain_p50_ms": 1e3 * float(np.percentile(plat, 50)),
-                      "plain_p99_ms": 1e3 * float(np.percentile(plat, 99))})
+        entry = {"arrival_rate_per_s": lam, "fraction_of_served_saturation": frac}
+        for kd in sat_lat:
+            lat = np.array([r.latency for r, k in zip(reqs, kinds) if k == kd])
+            pl = np.array([v for v, k in zip(plat, kinds) if k == kd])
+            entry.update({"served_%s_p50_ms" % kd: 1e3 * float(np.percentile(lat, 50)),
+                          "served_%s_p99_ms" % kd: 1e3 * float(np.percentile(lat, 99)),
+                          "plain_%s_p50_ms" % kd: 1e3 * float(np.percentile(pl, 50)),
+                          "plain_%s_p99_ms" % kd: 1e3 * float(np.percentile(pl, 99))})
+        sweep.append(entry)
     if rank != 0:
         return
     ms = total_ms / args.steps
+    plain_by = {kd: sum(sv for sv, k in zip(service, kinds) if k == kd) for kd in sat_lat}
     line = {
-        "metric": "BEM solves/s: served (continuous batching, mixed precision) vs plain FP64",
-        "value": served_rate, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "metric": "BEM requests/s: served (continuous batching, mixed precision) vs plain",
+        "value": served_rate, "unit": "requests/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 operator (tensor-core farfield panel) + f64 residual refinement",
-        "data": "synthetic (seeded meshes, arrivals and right-hand sides)",
+        "dtype": "f32 operator (tensor-core farfield panel) + f64 residual refinement / f64 "
+                 "qd state",
+        "data": "synthetic (seeded meshes, arrivals, right-hand sides and qd states)",
         "config": {"workload": ("%d solve requests (seeded N(0, 1) tractions, FP64 residual "
                                 "1e-8) on %d resident meshes of %s triangles (log-uniform "
                                 "2k-20k: vertical, 30-degree dipping faults, topographic "
                                 "patch; elasticRH3 RegularizedSparseIntegralOp(6,6,6,2,5,2.5), "
-                                "continuity + free-edge constraints), all arriving at once "
+                                "continuity + free-edge constraints) and %d quasidynamic "
+                                "requests (%d RK23 steps of the reference's example fault, "
+                                "%d triangles, from seeded states), all arriving at once "
                                 "(saturation); one step = the whole stream"
-                                % (n_req, len(meshes), [m[2].shape[0] for m in meshes])),
-                   "meshes": [m[0] for m in meshes], "requests": n_req,
+                                % (n_req, len(meshes), [m[2].shape[0] for m in meshes], n_qd,
+                                   qd_steps, nq_tris)),
+                   "meshes": [m[0] for m in meshes] + (["qd-fault"] if n_qd else []),
+                   "requests": {"solve": n_req, "qd": n_qd}, "qd_steps": qd_steps,
                    "slots_per_mesh": srv.slots, "restart": srv.restart,
-                   "plain_fp64_solves_per_s": plain_rate,
+                   "plain_requests_per_s": plain_rate,
                    "speedup_vs_plain": served_rate / plain_rate,
-                   "max_rel_diff_vs_plain_fp64": err,
-                   "saturation_latency_ms_p50": 1e3 * float(np.percentile(sat_lat, 50)),
-                   "saturation_latency_ms_p99": 1e3 * float(np.percentile(sat_lat, 99)),
+                   "plain_seconds_by_kind": plain_by,
+                   "max_rel_diff_solve_vs_plain_fp64": max(err_solve) if err_solve else None,
+                   "max_rel_diff_qd_vs_plain_integrator": max(err_qd) if err_qd else None,
+                   "saturation_latency_ms": {kd: {"p50": 1e3 * float(np.percentile(v, 50)),
+                                                  "p99": 1e3 * float(np.percentile(v, 99))}
+                                             for kd, v in sat_lat.items()},
                    "latency_sweep": sweep,
-                   "served_matvecs_per_s": applies / (total_ms * 1e-3),
-                   "plain_gmres_steps_mean": float(np.mean(plain_steps)),
-                   "served_gmres_steps_mean": float(np.mean([r.gmres_steps for r in sat])),
                    "mesh_build_s": t_build, "resident_bytes": srv.resident_bytes,
-                   "l2": "operators and Krylov bases of 6 meshes resident (GBs, beyond L2)",
+                   "l2": "operators and Krylov bases of the resident meshes (GBs, beyond L2)",
                    "parallelism": "replicas"},
-        "roofline": {"kernel": "whole served stream (see the batch and panel workloads for "
-                               "the kernels)",
+        "roofline": {"kernel": "whole served stream (see the batch, panel and qd workloads)",
                      "bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s",
                      "frac": None, "traffic": None},
-        "e2e": {"value": served_rate, "unit": "solves/s",
-                "h2d_bytes_per_step": int(sum(b.nbytes for _, b in stream)),
-                "d2h_bytes_per_step": int(sum(r.x.nbytes for r in sat)),
-                "api": "serve.SolveServer.replay(stream of (t, mesh, rhs numpy, tol)) -> "
-                       "numpy solutions"},
+        "e2e": {"value": served_rate, "unit": "requests/s",
+                "h2d_bytes_per_step": int(sum(p.nbytes for _, _, p in stream)),
+                "d2h_bytes_per_step": int(sum((r.x if k == "solve" else r.y).nbytes
+                                              for r, k in zip(sat, kinds))),
+                "api": "serve.SolveServer.replay(stream of solve and qd requests) -> numpy"},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -1707,6 +1735,8 @@ def main():
     ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--qd-steps", type=int, default=200,
                     help="RK23 steps per quasidynamic integration (qd workload)")
+    ap.add_argument("--qd-requests", type=int, default=8,
+                    help="quasidynamic requests in the served stream (serve workload)")
     ap.add_argument("--requests", type=int, default=48,
                     help="solve requests in the served stream (serve workload)")
     ap.add_argument("--fmm-order", type=int, default=None)

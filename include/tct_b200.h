@@ -443,6 +443,25 @@ int tct_qd_velocity_state(int64_t n_dofs, const int32_t* vert_start, const int32
                           const double* b, double V0, double Dc, double f0, double* velocity,
                           double* dstatedt, void* stream);
 
+/* Batched forms: n_sys systems on the same mesh, system k's traction /
+ * state / velocity / Newton velocity / derivative at base + k * stride (in
+ * doubles); the mesh fields (normals, a, b, normal_stress, fields, vertex
+ * lists) are shared. */
+int tct_qd_rate_state_batch(int64_t n_tris, int basis_dim, int n_sys, const double* tri_normals,
+                            const double* traction, int64_t traction_stride, const double* state,
+                            int64_t state_stride, const double* a, double eta, double V0,
+                            double C, const double* normal_stress, double tol, int maxiter,
+                            int separate_dims, double* velocity, int64_t velocity_stride,
+                            int* n_failed, void* stream);
+int tct_qd_velocity_state_batch(int64_t n_dofs, int n_sys, const int32_t* vert_start,
+                                const int32_t* vert_dofs, const int32_t* dof_vert,
+                                const double* v_newton, int64_t vn_stride,
+                                const double* field_edges, const double* field_interior,
+                                double plate_rate, int no_backslip, const double* state,
+                                int64_t state_stride, const double* b, double V0, double Dc,
+                                double f0, double* velocity, int64_t velocity_stride,
+                                double* dstatedt, int64_t dstate_stride, void* stream);
+
 /* Conjugate gradients on a CSR matrix (int64 indices, double values) in one
  * CTA, x0 = 0, stopping when ||r|| < max(atol, rtol ||b||) or after maxiter
  * iterations: the scipy.sparse.linalg.cg solve of the constrained mass
@@ -451,6 +470,12 @@ int tct_qd_velocity_state(int64_t n_dofs, const int32_t* vert_start, const int32
 int tct_cg_csr(int64_t n, const int64_t* indptr, const int64_t* indices, const double* data,
                const double* b, double* x, double* work, double rtol, double atol, int maxiter,
                int* iters, void* stream);
+/* n_sys systems with the same matrix, one CTA each: b_k = b + k b_stride,
+ * x_k = x + k x_stride, work: 3 n n_sys doubles, iters: n_sys ints. */
+int tct_cg_csr_batch(int64_t n, int n_sys, const int64_t* indptr, const int64_t* indices,
+                     const double* data, const double* b, int64_t b_stride, double* x,
+                     int64_t x_stride, double* work, double rtol, double atol, int maxiter,
+                     int* iters, void* stream);
 
 /* ---- constrained solve -------------------------------------------------- */
 

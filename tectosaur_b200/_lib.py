@@ -194,6 +194,15 @@ _SOLVE_SIGS = {
                             c_i, c_p], c_i),
     "tct_interior_corners": ([c_i, c_p, c_i, c_p, c_p, c_p, c_p, c_p, c_p, c_i64, c_dp, c_p],
                              c_i),
+    "tct_qd_rate_state_batch": ([c_i64, c_i, c_i, c_p, c_p, c_i64, c_p, c_i64, c_p,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_double, c_p,
+                                 ctypes.c_double, c_i, c_i, c_p, c_i64, c_p, c_p], c_i),
+    "tct_qd_velocity_state_batch": ([c_i64, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_p,
+                                     ctypes.c_double, c_i, c_p, c_i64, c_p, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, c_p, c_i64, c_p, c_i64,
+                                     c_p], c_i),
+    "tct_cg_csr_batch": ([c_i64, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_p,
+                          ctypes.c_double, ctypes.c_double, c_i, c_p, c_p], c_i),
     "tct_cg_csr": ([c_i64, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_double, c_i,
                     c_p, c_p], c_i),
     "tct_farfield_rh_panel_workspace_bytes": ([c_i64, c_i64, c_i, c_i], c_sz),

@@ -53,16 +53,20 @@ __device__ double newton_rs(double tau, double eta, double sn, double st, double
 }
 
 __global__ void __launch_bounds__(128)
-qd_rate_state(int64_t n_dofs, int basis_dim, const double* __restrict__ normals,
-              const double* __restrict__ traction, const double* __restrict__ state,
+qd_rate_state(int64_t n_dofs, int n_sys, int basis_dim, const double* __restrict__ normals,
+              const double* __restrict__ traction, int64_t traction_stride,
+              const double* __restrict__ state, int64_t state_stride,
               const double* __restrict__ a, double eta, double V0, double C,
               const double* __restrict__ normal_stress, double tol, int maxiter, int separate,
-              double* __restrict__ velocity, int* __restrict__ n_failed) {
-    const int64_t dof = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (dof >= n_dofs) return;
-    const double* t = traction + dof * 3;
-    double* v = velocity + dof * 3;
-    const double st = state[dof], ad = a[dof], extra = normal_stress[dof];
+              double* __restrict__ velocity, int64_t velocity_stride,
+              int* __restrict__ n_failed) {
+    // one thread per (system, DOF); the mesh fields are shared by the systems
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_dofs * n_sys) return;
+    const int64_t sys = g / n_dofs, dof = g - sys * n_dofs;
+    const double* t = traction + sys * traction_stride + dof * 3;
+    double* v = velocity + sys * velocity_stride + dof * 3;
+    const double st = state[sys * state_stride + dof], ad = a[dof], extra = normal_stress[dof];
     bool ok = true;
     if (separate) {
         for (int k = 0; k < 3; k++) {
@@ -92,14 +96,21 @@ qd_rate_state(int64_t n_dofs, int basis_dim, const double* __restrict__ normals,
 }
 
 __global__ void __launch_bounds__(128)
-qd_velocity(int64_t n_dofs, const int32_t* __restrict__ vert_start,
+qd_velocity(int64_t n_dofs, int n_sys, const int32_t* __restrict__ vert_start,
             const int32_t* __restrict__ vert_dofs, const int32_t* __restrict__ dof_vert,
-            const double* __restrict__ v_newton, const double* __restrict__ field_edges,
-            const double* __restrict__ field_interior, double plate_rate, int no_backslip,
-            const double* __restrict__ state, const double* __restrict__ b, double V0, double Dc,
-            double f0, double* __restrict__ velocity, double* __restrict__ dstatedt) {
-    const int64_t dof = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (dof >= n_dofs) return;
+            const double* __restrict__ v_newton, int64_t vn_stride,
+            const double* __restrict__ field_edges, const double* __restrict__ field_interior,
+            double plate_rate, int no_backslip, const double* __restrict__ state,
+            int64_t state_stride, const double* __restrict__ b, double V0, double Dc, double f0,
+            double* __restrict__ velocity, int64_t velocity_stride, double* __restrict__ dstatedt,
+            int64_t dstate_stride) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_dofs * n_sys) return;
+    const int64_t sys = g / n_dofs, dof = g - sys * n_dofs;
+    v_newton += sys * vn_stride;
+    state += sys * state_stride;
+    velocity += sys * velocity_stride;
+    dstatedt += sys * dstate_stride;
     const int32_t p = dof_vert[dof];
     const int32_t s = vert_start[p], e = vert_start[p + 1];
     double avg[3];
@@ -138,12 +149,18 @@ __device__ double block_sum(double v, double* red) {
 
 __global__ void __launch_bounds__(CG_THREADS)
 cg_csr_block(int64_t n, const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
-             const double* __restrict__ data, const double* __restrict__ bvec,
-             double* __restrict__ x, double* __restrict__ r, double* __restrict__ p,
-             double* __restrict__ q, double rtol, double atol_in, int maxiter,
-             int* __restrict__ iters) {
+             const double* __restrict__ data, const double* __restrict__ bvec, int64_t b_stride,
+             double* __restrict__ x, int64_t x_stride, double* __restrict__ work, double rtol,
+             double atol_in, int maxiter, int* __restrict__ iters) {
+    // one CTA per system (blockIdx.x), all with the same matrix
     __shared__ double red[32];
     const int tid = threadIdx.x;
+    bvec += blockIdx.x * b_stride;
+    x += blockIdx.x * x_stride;
+    double* __restrict__ r = work + (int64_t)blockIdx.x * 3 * n;
+    double* __restrict__ p = r + n;
+    double* __restrict__ q = p + n;
+    iters += blockIdx.x;
     double bb = 0.0;
     for (int64_t i = tid; i < n; i += blockDim.x) bb += bvec[i] * bvec[i];
     const double bnrm2 = sqrt(block_sum(bb, red));
@@ -191,20 +208,58 @@ cg_csr_block(int64_t n, const int64_t* __restrict__ indptr, const int64_t* __res
 
 using namespace tct;
 
+extern "C" int tct_qd_rate_state_batch(int64_t n_tris, int basis_dim, int n_sys,
+                                       const double* tri_normals, const double* traction,
+                                       int64_t traction_stride, const double* state,
+                                       int64_t state_stride, const double* a, double eta,
+                                       double V0, double C, const double* normal_stress,
+                                       double tol, int maxiter, int separate_dims,
+                                       double* velocity, int64_t velocity_stride, int* n_failed,
+                                       void* stream) {
+    TCT_CHECK_ARG(n_tris >= 0 && basis_dim >= 1 && maxiter >= 0 && n_sys >= 0,
+                  "tct_qd_rate_state: bad sizes");
+    const int64_t n = n_tris * basis_dim;
+    if (n == 0 || n_sys == 0) return TCT_OK;
+    TCT_CHECK_ARG(tri_normals && traction && state && a && normal_stress && velocity && n_failed,
+                  "tct_qd_rate_state: null pointer");
+    const int64_t m = n * n_sys;
+    qd_rate_state<<<(unsigned)((m + 127) / 128), 128, 0, as_stream(stream)>>>(
+        n, n_sys, basis_dim, tri_normals, traction, traction_stride, state, state_stride, a, eta,
+        V0, C, normal_stress, tol, maxiter, separate_dims, velocity, velocity_stride, n_failed);
+    return launch_status("tct_qd_rate_state");
+}
+
 extern "C" int tct_qd_rate_state(int64_t n_tris, int basis_dim, const double* tri_normals,
                                  const double* traction, const double* state, const double* a,
                                  double eta, double V0, double C, const double* normal_stress,
                                  double tol, int maxiter, int separate_dims, double* velocity,
                                  int* n_failed, void* stream) {
-    TCT_CHECK_ARG(n_tris >= 0 && basis_dim >= 1 && maxiter >= 0, "tct_qd_rate_state: bad sizes");
-    const int64_t n = n_tris * basis_dim;
-    if (n == 0) return TCT_OK;
-    TCT_CHECK_ARG(tri_normals && traction && state && a && normal_stress && velocity && n_failed,
-                  "tct_qd_rate_state: null pointer");
-    qd_rate_state<<<(unsigned)((n + 127) / 128), 128, 0, as_stream(stream)>>>(
-        n, basis_dim, tri_normals, traction, state, a, eta, V0, C, normal_stress, tol, maxiter,
-        separate_dims, velocity, n_failed);
-    return launch_status("tct_qd_rate_state");
+    return tct_qd_rate_state_batch(n_tris, basis_dim, 1, tri_normals, traction, 0, state, 0, a,
+                                   eta, V0, C, normal_stress, tol, maxiter, separate_dims,
+                                   velocity, 0, n_failed, stream);
+}
+
+extern "C" int tct_qd_velocity_state_batch(int64_t n_dofs, int n_sys, const int32_t* vert_start,
+                                           const int32_t* vert_dofs, const int32_t* dof_vert,
+                                           const double* v_newton, int64_t vn_stride,
+                                           const double* field_edges,
+                                           const double* field_interior, double plate_rate,
+                                           int no_backslip, const double* state,
+                                           int64_t state_stride, const double* b, double V0,
+                                           double Dc, double f0, double* velocity,
+                                           int64_t velocity_stride, double* dstatedt,
+                                           int64_t dstate_stride, void* stream) {
+    TCT_CHECK_ARG(n_dofs >= 0 && n_sys >= 0, "tct_qd_velocity_state: negative size");
+    if (n_dofs == 0 || n_sys == 0) return TCT_OK;
+    TCT_CHECK_ARG(vert_start && vert_dofs && dof_vert && v_newton && field_edges &&
+                      field_interior && state && b && velocity && dstatedt,
+                  "tct_qd_velocity_state: null pointer");
+    const int64_t m = n_dofs * n_sys;
+    qd_velocity<<<(unsigned)((m + 127) / 128), 128, 0, as_stream(stream)>>>(
+        n_dofs, n_sys, vert_start, vert_dofs, dof_vert, v_newton, vn_stride, field_edges,
+        field_interior, plate_rate, no_backslip, state, state_stride, b, V0, Dc, f0, velocity,
+        velocity_stride, dstatedt, dstate_stride);
+    return launch_status("tct_qd_velocity_state");
 }
 
 extern "C" int tct_qd_velocity_state(int64_t n_dofs, const int32_t* vert_start,
@@ -214,25 +269,27 @@ extern "C" int tct_qd_velocity_state(int64_t n_dofs, const int32_t* vert_start,
                                      int no_backslip, const double* state, const double* b,
                                      double V0, double Dc, double f0, double* velocity,
                                      double* dstatedt, void* stream) {
-    TCT_CHECK_ARG(n_dofs >= 0, "tct_qd_velocity_state: negative size");
-    if (n_dofs == 0) return TCT_OK;
-    TCT_CHECK_ARG(vert_start && vert_dofs && dof_vert && v_newton && field_edges &&
-                      field_interior && state && b && velocity && dstatedt,
-                  "tct_qd_velocity_state: null pointer");
-    qd_velocity<<<(unsigned)((n_dofs + 127) / 128), 128, 0, as_stream(stream)>>>(
-        n_dofs, vert_start, vert_dofs, dof_vert, v_newton, field_edges, field_interior,
-        plate_rate, no_backslip, state, b, V0, Dc, f0, velocity, dstatedt);
-    return launch_status("tct_qd_velocity_state");
+    return tct_qd_velocity_state_batch(n_dofs, 1, vert_start, vert_dofs, dof_vert, v_newton, 0,
+                                       field_edges, field_interior, plate_rate, no_backslip,
+                                       state, 0, b, V0, Dc, f0, velocity, 0, dstatedt, 0, stream);
+}
+
+extern "C" int tct_cg_csr_batch(int64_t n, int n_sys, const int64_t* indptr,
+                                const int64_t* indices, const double* data, const double* b,
+                                int64_t b_stride, double* x, int64_t x_stride, double* work,
+                                double rtol, double atol, int maxiter, int* iters, void* stream) {
+    TCT_CHECK_ARG(n >= 0 && maxiter >= 0 && n_sys >= 0, "tct_cg_csr: bad sizes");
+    if (n == 0 || n_sys == 0) return TCT_OK;
+    TCT_CHECK_ARG(indptr && indices && data && b && x && work && iters,
+                  "tct_cg_csr: null pointer");
+    cg_csr_block<<<(unsigned)n_sys, CG_THREADS, 0, as_stream(stream)>>>(
+        n, indptr, indices, data, b, b_stride, x, x_stride, work, rtol, atol, maxiter, iters);
+    return launch_status("tct_cg_csr");
 }
 
 extern "C" int tct_cg_csr(int64_t n, const int64_t* indptr, const int64_t* indices,
                           const double* data, const double* b, double* x, double* work,
                           double rtol, double atol, int maxiter, int* iters, void* stream) {
-    TCT_CHECK_ARG(n >= 0 && maxiter >= 0, "tct_cg_csr: bad sizes");
-    if (n == 0) return TCT_OK;
-    TCT_CHECK_ARG(indptr && indices && data && b && x && work && iters,
-                  "tct_cg_csr: null pointer");
-    cg_csr_block<<<1, CG_THREADS, 0, as_stream(stream)>>>(
-        n, indptr, indices, data, b, x, work, work + n, work + 2 * n, rtol, atol, maxiter, iters);
-    return launch_status("tct_cg_csr");
+    return tct_cg_csr_batch(n, 1, indptr, indices, data, b, 0, x, 0, work, rtol, atol, maxiter,
+                            iters, stream);
 }

@@ -203,6 +203,90 @@ class FullspaceModel:
 
         return derivs
 
+    # -- several states at once (the served form) ----------------------------------
+    def _panel(self, X, Y):
+        """Y = H X for (R, 9 n) panels of H's float type."""
+        if hasattr(self.H, "dot_panel_device"):
+            return self.H.dot_panel_device(X, Y)
+        for r in range(X.shape[0]):
+            self.H.dot_device(X[r], Y[r])
+        return Y
+
+    def _csr_panel(self, mat, X, Y):
+        _lib.check(_lib.lib.tct_csr_matvec_panel(
+            _lib.TCT_F64, mat.shape[0], _lib.tptr(mat.indptr), _lib.tptr(mat.indices),
+            _lib.tptr(mat.data), _lib.tptr(X), X.stride(0), _lib.tptr(Y), Y.stride(0),
+            X.shape[0], 0, _lib.stream_ptr()), "tct_csr_matvec_panel")
+        return Y
+
+    def slip_to_traction_batch(self, D):
+        """slip_to_traction for the rows of D (R, 9 n): one panel apply of H,
+        one CG launch with a CTA per row."""
+        t = device.torch()
+        R = D.shape[0]
+        X = D.to(self.H_dtype).contiguous()
+        Yh = t.empty_like(X)
+        self._panel(X, Yh)
+        rhs = (-Yh).to(t.float64)
+        rc = t.empty((R, self.n_free), dtype=t.float64, device="cuda")
+        self._csr_panel(self.cmT, rhs, rc)
+        soln = t.empty_like(rc)
+        work = t.empty(3 * max(self.n_free, 1) * R, dtype=t.float64, device="cuda")
+        iters = t.empty(R, dtype=t.int32, device="cuda")
+        ip, ix, dv = self.mass_c
+        _lib.check(_lib.lib.tct_cg_csr_batch(
+            self.n_free, R, _lib.tptr(ip), _lib.tptr(ix), _lib.tptr(dv), _lib.tptr(rc),
+            rc.stride(0), _lib.tptr(soln), soln.stride(0), _lib.tptr(work), 1e-5, 1e-12,
+            10 * self.n_free, _lib.tptr(iters), _lib.stream_ptr()), "tct_cg_csr_batch")
+        out = t.empty((R, 9 * self.n_tris), dtype=t.float64, device="cuda")
+        self._csr_panel(self.cm, soln, out)
+        out *= self.cfg["sm"]
+        if self.cfg.get("only_x", False):
+            out.view(R, -1, 3)[:, :, 1:] = 0.0
+        return out
+
+    def rate_state_solve_batch(self, traction, state):
+        """(V, dstate/dt) for the rows of traction (R, 9 n) and state
+        (R, 3 n; any row stride)."""
+        t = device.torch()
+        cfg = self.cfg
+        R = traction.shape[0]
+        n9 = 9 * self.n_tris
+        vn = t.empty((R, n9), dtype=t.float64, device="cuda")
+        _lib.check(_lib.lib.tct_qd_rate_state_batch(
+            self.n_tris, 3, R, _lib.tptr(self.d_normals), _lib.tptr(traction),
+            traction.stride(0), _lib.tptr(state), state.stride(0), _lib.tptr(self.d_a),
+            float(cfg["eta"]), float(cfg["V0"]), float(cfg.get("C", 0.0)),
+            _lib.tptr(self.d_sigma), 1e-12, 50, int(bool(cfg.get("rs_separate_dims", False))),
+            _lib.tptr(vn), vn.stride(0), _lib.tptr(self.n_failed), _lib.stream_ptr()),
+            "tct_qd_rate_state_batch")
+        V = t.empty((R, n9), dtype=t.float64, device="cuda")
+        dstate = t.empty((R, self.n_dofs), dtype=t.float64, device="cuda")
+        _lib.check(_lib.lib.tct_qd_velocity_state_batch(
+            self.n_dofs, R, _lib.tptr(self.vert_start), _lib.tptr(self.vert_dofs),
+            _lib.tptr(self.dof_vert), _lib.tptr(vn), vn.stride(0), _lib.tptr(self.d_edges),
+            _lib.tptr(self.d_int_dir), float(cfg["plate_rate"]),
+            int(bool(cfg.get("no_backslip", False))), _lib.tptr(state), state.stride(0),
+            _lib.tptr(self.d_b), float(cfg["V0"]), float(cfg["Dc"]), float(cfg["f0"]),
+            _lib.tptr(V), V.stride(0), _lib.tptr(dstate), dstate.stride(0), _lib.stream_ptr()),
+            "tct_qd_velocity_state_batch")
+        return V, dstate
+
+    def derivs_batch(self, ts, Y):
+        """derivs for R states at once: ts (R,) device float64, Y (R, n_y)."""
+        t = device.torch()
+        self.n_evals += Y.shape[0]
+        n9 = 9 * self.n_tris
+        slip, state = Y[:, :n9], Y[:, n9:]
+        plate = (ts[:, None] * self.cfg["plate_rate"]) * self.d_inslipdir[None, :]
+        deficit = self.d_interior[None, :] * (plate - slip)
+        traction = self.slip_to_traction_batch(deficit)
+        V, dstate = self.rate_state_solve_batch(traction, state)
+        bad = (~t.isfinite(Y).all(dim=1)) | (state < 0).any(dim=1) | (state > 1.2).any(dim=1) | \
+            (~t.isfinite(V).all(dim=1))
+        out = t.cat((V, dstate), dim=1)
+        return t.where(bad[:, None], Y * float("inf"), out)
+
     def newton_failures(self, reset=True):
         """DOFs whose Newton iteration stopped at maxiter since the last call
         (a host sync).  The reference's assert on them is compiled out

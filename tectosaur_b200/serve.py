@@ -314,6 +314,187 @@ class SolveEngine:
         return finished
 
 
+class QdRequest:
+    """n_steps quasidynamic RK23 steps of a fault model from (t0, y0)."""
+
+    _ids = itertools.count()
+
+    def __init__(self, key, y0, n_steps, t0=0.0, first_step=None, t_submit=None):
+        self.id = next(QdRequest._ids)
+        self.key = key
+        self.y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1)
+        self.n_steps = int(n_steps)
+        self.t0 = float(t0)
+        self.first_step = first_step
+        self.t_submit = time.perf_counter() if t_submit is None else t_submit
+        self.t_admit = None
+        self.t_done = None
+        self.y = None
+        self.ts = []
+        self.steps = 0
+        self.rejected = 0
+        self.error = None
+        self.converged = False
+
+    @property
+    def done(self):
+        return self.t_done is not None
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_submit
+
+
+class QdEngine:
+    """S quasidynamic integrations on one fault model, advancing together:
+    each tick every occupied slot makes one RK23 attempt (scipy's RK23 step
+    control per slot, restated in qd/rk23.py), its three derivative
+    evaluations batched over the slots (one panel apply of H, one CG launch,
+    one Newton launch, one averaging launch per evaluation); slots are
+    refilled between ticks."""
+
+    def __init__(self, model, slots=16, stream=None):
+        t = device.torch()
+        from .qd import rk23 as rk
+        self.t, self.rk = t, rk
+        self.model = model
+        self.derivs = model.derivs_batch
+        self.S = int(slots)
+        self.stream = stream
+        self.n_y = 12 * model.n_tris
+        self.tol = float(model.cfg["timestep_tol"])
+        self.Y = t.zeros((self.S, self.n_y), dtype=t.float64, device="cuda")
+        self.F = t.zeros_like(self.Y)
+        self.tv = np.zeros(self.S)
+        self.h = np.zeros(self.S)
+        self.rejected_now = np.zeros(self.S, bool)
+        self.req = [None] * self.S
+        self._norms = t.zeros(self.S, dtype=t.float64, pin_memory=True)
+        self._tpin = t.zeros((4, self.S), dtype=t.float64, pin_memory=True)
+        self._tdev = t.zeros((4, self.S), dtype=t.float64, device="cuda")
+        self._ipin = t.zeros(self.S, dtype=t.int64, pin_memory=True)
+        self._idev = t.zeros(self.S, dtype=t.int64, device="cuda")
+        self._event = t.cuda.Event()
+        self._pending = None
+        self.last_used = time.perf_counter()
+
+    def _ctx(self):
+        if self.stream is None:
+            return contextlib.nullcontext()
+        return self.t.cuda.stream(self.stream)
+
+    @property
+    def free_slots(self):
+        return sum(r is None for r in self.req)
+
+    @property
+    def busy(self):
+        return any(r is not None for r in self.req)
+
+    def admit(self, req):
+        free = [s for s in range(self.S) if self.req[s] is None]
+        if not free:
+            return False
+        if req.y0.shape[0] != self.n_y:
+            req.error = "state of %d values, the model has %d" % (req.y0.shape[0], self.n_y)
+            req.t_done = time.perf_counter()
+            return True
+        s = free[0]
+        t = self.t
+        with self._ctx():
+            self.Y[s] = t.from_numpy(req.y0).to("cuda")
+            ts = t.full((1,), req.t0, dtype=t.float64, device="cuda")
+            self.F[s] = self.derivs(ts, self.Y[s:s + 1])[0]
+        self.tv[s] = req.t0
+        self.h[s] = req.first_step if req.first_step is not None else 3.15576e6
+        self.rejected_now[s] = False
+        self.req[s] = req
+        req.t_admit = time.perf_counter()
+        if req.n_steps <= 0:
+            self._finish(s)
+        return True
+
+    def _finish(self, s, error=None):
+        req = self.req[s]
+        with self._ctx():
+            req.y = self.Y[s].cpu().numpy()
+        req.error = error
+        req.converged = error is None
+        req.t_done = time.perf_counter()
+        self.req[s] = None
+        return req
+
+    def launch(self):
+        t, rk = self.t, self.rk
+        act = [s for s in range(self.S) if self.req[s] is not None]
+        self._pending = None
+        if not act:
+            return
+        k = len(act)
+        h = np.array([self.h[s] for s in act])
+        tv = np.array([self.tv[s] for s in act])
+        tp = self._tpin.numpy()
+        tp[0, :k] = h
+        tp[1, :k] = tv + rk.C[1] * h
+        tp[2, :k] = tv + rk.C[2] * h
+        tp[3, :k] = tv + h
+        self._ipin.numpy()[:k] = act
+        with self._ctx():
+            self._tdev.copy_(self._tpin, non_blocking=True)
+            self._idev.copy_(self._ipin, non_blocking=True)
+            idx = self._idev[:k]
+            hd = self._tdev[0, :k][:, None]
+            y, K0 = self.Y[idx], self.F[idx]
+            K1 = self.derivs(self._tdev[1, :k], y + (K0 * rk.A[1][0]) * hd)
+            K2 = self.derivs(self._tdev[2, :k], y + (K0 * rk.A[2][0] + K1 * rk.A[2][1]) * hd)
+            y_new = y + hd * (K0 * rk.B[0] + K1 * rk.B[1] + K2 * rk.B[2])
+            f_new = self.derivs(self._tdev[3, :k], y_new)
+            err = (K0 * rk.E[0] + K1 * rk.E[1] + K2 * rk.E[2] + f_new * rk.E[3]) * hd
+            scale = self.tol + t.maximum(y.abs(), y_new.abs()) * self.tol
+            self._norms[:k].copy_(t.linalg.norm(err / scale, dim=1), non_blocking=True)
+            self._event.record()
+        self._pending = (act, h, y_new, f_new)
+
+    def complete(self):
+        if self._pending is None:
+            return []
+        rk = self.rk
+        act, h, y_new, f_new = self._pending
+        self._pending = None
+        self._event.synchronize()
+        norms = self._norms.numpy()[: len(act)] / np.sqrt(self.n_y)
+        self.last_used = time.perf_counter()
+        done = []
+        for i, s in enumerate(act):
+            req = self.req[s]
+            en = float(norms[i])
+            t_old = self.tv[s]
+            min_step = 10 * abs(np.nextafter(t_old, np.inf) - t_old)
+            if en < 1:
+                factor = rk.MAX_FACTOR if en == 0 else min(rk.MAX_FACTOR,
+                                                           rk.SAFETY * en ** rk.ERROR_EXPONENT)
+                if self.rejected_now[s]:
+                    factor = min(1.0, factor)
+                with self._ctx():
+                    self.Y[s] = y_new[i]
+                    self.F[s] = f_new[i]
+                self.tv[s] = t_old + h[i]
+                self.h[s] = h[i] * factor
+                self.rejected_now[s] = False
+                req.steps += 1
+                req.ts.append(self.tv[s])
+                if req.steps >= req.n_steps:
+                    done.append(self._finish(s))
+            else:
+                shrink = rk.SAFETY * en ** rk.ERROR_EXPONENT if en == en else 0.0
+                self.h[s] = h[i] * max(rk.MIN_FACTOR, shrink)
+                self.rejected_now[s] = True
+                req.rejected += 1
+                if self.h[s] < min_step:
+                    done.append(self._finish(s, error="step size below the spacing of t"))
+        return done
+
+
 def _back_substitute(R, g):
     k = g.shape[0]
     y = np.zeros(k)
@@ -349,6 +530,8 @@ class MeshSpec:
         triangle in FP64 + FP32, the panel farfield operand, the Krylov
         bases of the slots."""
         n = self.n_tris
+        if getattr(self, "kind", "solve") == "qd":
+            return int(n * 100 * 648 + n * 8100 + slots * 4 * 12 * n * 8)
         n_free = self.cm.shape[1] if self.cm is not None else 9 * n
         return int(n * 100 * (648 + 324) + n * 8100 + slots * (restart + 4) * n_free * 8)
 
@@ -401,6 +584,15 @@ class SolveServer:
         self.n_evictions = 0
 
     # -- meshes ------------------------------------------------------------------
+    def add_qd_mesh(self, key, pts, tris, cfg, model=None):
+        """A fault for quasidynamic requests (qd.FullspaceModel(m, cfg))."""
+        spec = MeshSpec(key, pts, tris)
+        spec.kind = "qd"
+        spec.qd_cfg = cfg
+        spec.model = model
+        self.specs[key] = spec
+        return spec
+
     def add_mesh(self, key, pts, tris, cm=None, **op_args):
         from .ops.sparse_farfield_op import TriToTriDirectFarfieldOp
         op_args.setdefault("farfield_op_type", TriToTriDirectFarfieldOp)
@@ -431,6 +623,8 @@ class SolveServer:
 
     @staticmethod
     def _build(self, spec):
+        if getattr(spec, "kind", "solve") == "qd":
+            return SolveServer._build_qd(self, spec)
         from .ops.sparse_integral_op import RegularizedSparseIntegralOp
         from .simple_solver import ConstrainedPanelOperator, DeviceCSR
         t = device.torch()
@@ -470,6 +664,29 @@ class SolveServer:
         self.n_builds += 1
         return _Resident(spec, op64, op32, engine, spec.measured_bytes)
 
+    @staticmethod
+    def _build_qd(self, spec):
+        from .qd import FullspaceModel
+        t = device.torch()
+        t.cuda.synchronize()
+        before = t.cuda.memory_allocated()
+        model = spec.model or FullspaceModel((spec.pts, spec.tris), spec.qd_cfg)
+        engine = QdEngine(model, self.slots, t.cuda.Stream())
+        t.cuda.synchronize()
+        spec.measured_bytes = max(t.cuda.memory_allocated() - before, 1)
+        self.n_builds += 1
+        return _Resident(spec, None, None, engine, spec.measured_bytes)
+
+    def submit_qd(self, key, y0, n_steps, t0=0.0, first_step=None, t_submit=None):
+        """A quasidynamic request: n_steps RK23 steps from (t0, y0) on a
+        fault registered with add_qd_mesh; its result is req.y (host) and
+        req.ts (the accepted step times)."""
+        if getattr(self.specs.get(key), "kind", None) != "qd":
+            raise KeyError("no quasidynamic mesh %r" % (key,))
+        req = QdRequest(key, y0, n_steps, t0, first_step, t_submit)
+        self.queue.append(req)
+        return req
+
     def _engine_for(self, key):
         if key in self.resident:
             self.resident.move_to_end(key)
@@ -506,6 +723,8 @@ class SolveServer:
                 continue
             if eng is None or not eng.admit(req):
                 waiting.append(req)
+            elif req.done:  # refused by the engine (e.g. a state of the wrong size)
+                self.completed.append(req)
         self.queue = waiting
 
     @property
@@ -535,9 +754,11 @@ class SolveServer:
         return self.completed
 
     def replay(self, arrivals):
-        """Serve a timed stream: arrivals = [(t_offset_s, key, rhs, tol)],
-        each submitted once the wall clock passes its offset (its latency is
-        counted from the offset).  Returns the requests in arrival order."""
+        """Serve a timed stream: arrivals = [(t_offset_s, key, rhs, tol)] for
+        solves and [(t_offset_s, "qd", key, y0, n_steps)] for quasidynamic
+        integrations, each submitted once the wall clock passes its offset
+        (its latency is counted from the offset).  Returns the requests in
+        arrival order."""
         arrivals = sorted(arrivals, key=lambda a: a[0])
         t0 = time.perf_counter()
         reqs = []
@@ -545,8 +766,13 @@ class SolveServer:
         while i < len(arrivals) or not self.idle:
             now = time.perf_counter() - t0
             while i < len(arrivals) and arrivals[i][0] <= now:
-                off, key, rhs, tol = arrivals[i]
-                reqs.append(self.submit(key, rhs, tol, t_submit=t0 + off))
+                a = arrivals[i]
+                if len(a) == 5 and a[1] == "qd":
+                    off, _, key, y0, n_steps = a
+                    reqs.append(self.submit_qd(key, y0, n_steps, t_submit=t0 + off))
+                else:
+                    off, key, rhs, tol = a
+                    reqs.append(self.submit(key, rhs, tol, t_submit=t0 + off))
                 i += 1
             if self.idle:
                 if i < len(arrivals):

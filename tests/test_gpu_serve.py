@@ -74,3 +74,58 @@ def test_same_alone_and_in_mix(cuda):
     assert r0.converged and r1.converged
     assert all(r.converged for r in mixed.completed)
     assert np.linalg.norm(r1.x - r0.x) / np.linalg.norm(r0.x) < 1e-9
+
+
+def _qd_setup(ft=np.float64, n=6):
+    from tectosaur_b200 import qd
+    pts, tris = make_rect(n, n, [[-1, 0, 1], [-1, 0, -1], [1, 0, -1], [1, 0, 1]])
+    nt = tris.shape[0]
+    cfg = dict(sm=3e10, pr=0.25, density=2670.0, Dc=2e-6, f0=0.6, V0=1e-6,
+               a=np.full(nt * 3, 0.010), b=np.full(nt * 3, 0.015), plate_rate=1e-9,
+               additional_normal_stress=50e6, timestep_tol=1e-4,
+               tectosaur_cfg=dict(quad_coincident_order=6, quad_edgeadj_order=6,
+                                  quad_vertadj_order=6, quad_near_order=5,
+                                  quad_near_threshold=2.5, quad_far_order=2,
+                                  quad_mass_order=4, float_type=ft, use_fmm=False))
+    model = qd.FullspaceModel((pts, tris), cfg)
+    rng = np.random.default_rng(3)
+    y0s = [np.concatenate([np.zeros(9 * nt), 0.7 + 0.01 * rng.standard_normal(3 * nt)])
+           for _ in range(3)]
+    return pts, tris, cfg, model, y0s
+
+
+def test_qd_served_matches_integrator(cuda):
+    from tectosaur_b200 import qd
+    pts, tris, cfg, model, y0s = _qd_setup()
+    steps = 15
+    integ = qd.Integrator(model, (0.0, y0s[0]))
+    integ.integrate(steps)
+    srv = serve.SolveServer(slots=4)
+    srv.add_qd_mesh("fault", pts, tris, cfg, model=model)
+    req = srv.submit_qd("fault", y0s[0], steps)
+    n0 = _lib.launch_count()
+    srv.run_until_idle(max_ticks=10_000)
+    assert _lib.launch_count() > n0
+    assert req.converged and req.steps == steps and req.error is None
+    np.testing.assert_allclose(req.ts, integ.h_t, rtol=1e-10)
+    want = integ.h_y[-1].cpu().numpy()
+    assert np.linalg.norm(req.y - want) / np.linalg.norm(want) < 1e-10
+
+
+def test_qd_same_alone_and_in_mix(cuda):
+    pts, tris, cfg, model, y0s = _qd_setup(np.float32)
+    alone = serve.SolveServer(slots=4)
+    alone.add_qd_mesh("fault", pts, tris, cfg, model=model)
+    r0 = alone.submit_qd("fault", y0s[0], 12)
+    alone.run_until_idle(max_ticks=10_000)
+    mixed = serve.SolveServer(slots=4)
+    mixed.add_qd_mesh("fault", pts, tris, cfg, model=model)
+    others = [mixed.submit_qd("fault", y0s[1], 20)]
+    mixed.step()
+    r1 = mixed.submit_qd("fault", y0s[0], 12)
+    others.append(mixed.submit_qd("fault", y0s[2], 5))
+    mixed.run_until_idle(max_ticks=10_000)
+    assert r0.converged and r1.converged and all(o.converged for o in others)
+    assert r1.steps == r0.steps == 12
+    np.testing.assert_allclose(r1.ts, r0.ts, rtol=1e-9)
+    assert np.linalg.norm(r1.y - r0.y) / np.linalg.norm(r0.y) < 1e-9
