@@ -499,14 +499,8 @@ fmm_m2p(int p, Rule2D<R> rule, int nq, const int64_t* __restrict__ obs_nodes,
 // Written as L_b = (s_o/rho)^|b| / (rho b!) sum_a f_|a| Dc_(a+b) Nt_a with
 // Dc_c = c! D_c(R0 / rho), f_n = (-1)^n (s_s/rho)^n and Nt_a = N_a / a! (the
 // moments are divided by a! once, after M2M, by fmm_moment_factorials), so a
-// pair's source moments are used as stored.  One warp per obs node walks its
-// M2L list; per pair the lanes copy the source node's moments into the warp's
-// shared memory and build Dc level by level there (warp syncs only), then
-// lane l contracts the local terms b dealt to it in snake order (b = 32k + l,
-// 32k + 31 - l, ... balances the trip counts, which fall with |b|), reading
-// the moment rows as shared-memory broadcasts.  The
-// pair's sums get the Yl correction (- R0_d times the m channel) and the b
-// scaling, and are added to the warp's local expansion in shared memory.
+// pair's source moments are used as stored; the Yl correction (- R0_d times
+// the m channel) is linear in the moments and applied to each source row.
 template <typename R>
 __global__ void __launch_bounds__(128)
 fmm_moment_factorials(int p, int nchp, int64_t n_nodes, R* __restrict__ mom) {
@@ -522,73 +516,6 @@ fmm_moment_factorials(int p, int nchp, int64_t n_nodes, R* __restrict__ mom) {
     mom[e] /= f;
 }
 
-// Lane plan of the M2L contraction for order p (one warp, written to the
-// workspace each call).  The work of local term b is n_terms(p - |b|)
-// source terms; terms are cut into chunks of at most CH = ceil(total / 32)
-// iterations and the chunks are dealt, in order, to the lane with the least
-// work so far (ties to the lowest lane), so every lane runs about CH
-// iterations.  A term cut into several chunks gets consecutive partial slots,
-// summed in a fixed order after the contraction (deterministic results).
-constexpr int M2L_MAXI = 32;   // chunks per lane (15 at most for p <= 12)
-constexpr int M2L_SLOTS = 32;  // partial slots (31 at most for p <= 12)
-struct M2LPlan {
-    int item[32][M2L_MAXI][4];  // b, first, end (graded source-term range), slot or -1
-    int cnt[32];
-    int split[M2L_SLOTS][3];    // b, first slot, end slot
-    int nsplit;
-};
-
-__global__ void __launch_bounds__(32) fmm_m2l_plan(int p, M2LPlan* __restrict__ plan) {
-    const int lane = threadIdx.x;
-    const int NT = n_terms(p);
-    const int CH = (n_terms6(p) + 31) / 32;
-    int load = 0, cnt = 0, slot = 0, nsplit = 0;
-    for (int b = 0; b < NT; b++) {
-        int b0, b1, b2;
-        decode(b, b0, b1, b2);
-        const int t = n_terms(p - (b0 + b1 + b2));
-        const int nch = (t + CH - 1) / CH;
-        const bool split = nch > 1 && slot + nch <= M2L_SLOTS;
-        const int step = split ? CH : t;
-        for (int c = 0, g0 = 0; g0 < t; c++, g0 += step) {
-            const int g1 = min(t, g0 + step);
-            const unsigned key = ((unsigned)load << 5) | (unsigned)lane;
-            const unsigned win = __reduce_min_sync(0xffffffffu, key) & 31u;
-            if ((unsigned)lane == win && cnt < M2L_MAXI) {
-                plan->item[lane][cnt][0] = b;
-                plan->item[lane][cnt][1] = g0;
-                plan->item[lane][cnt][2] = g1;
-                plan->item[lane][cnt][3] = split ? slot + c : -1;
-                cnt++;
-                load += g1 - g0;
-            }
-        }
-        if (split) {
-            if (lane == 0) {
-                plan->split[nsplit][0] = b;
-                plan->split[nsplit][1] = slot;
-                plan->split[nsplit][2] = slot + nch;
-            }
-            slot += nch;
-            nsplit++;
-        }
-    }
-    plan->cnt[lane] = cnt;
-    if (lane == 0) plan->nsplit = nsplit;
-}
-
-template <typename R, int K>
-__device__ __forceinline__ void m2l_flush(R (&acc)[Chan<K>::NCH], const R R0[3], R sc, R* lrow) {
-    using C = Chan<K>;
-    // Yl = Y - R0_d m; scaled add into the warp's local expansion
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-        for (int j = 0; j < C::J; j++) acc[C::CH_Y + d * C::J + j] -= R0[d] * acc[C::CH_M + j];
-#pragma unroll
-    for (int k = 0; k < C::NCH; k++) lrow[k] += sc * acc[k];
-}
-
 template <typename R>
 __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
     R f = 1;
@@ -598,167 +525,296 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
     return f;
 }
 
+// ---- M2L, one CTA per observation node ------------------------------------
+// The same L_b as fmm_m2l, organised for throughput: the CTA keeps its local
+// expansion in registers across its whole M2L list.  Warp 0 is the producer:
+// for source node k + 1 it computes rho, f_n, (s_o/rho)^n / rho and Dc level
+// by level into the second of two shared-memory buffers, while the other
+// seven warps contract source node k; every thread copies its share of node
+// k + 1's moments into the second moment buffer with cp.async.  A
+// contraction thread owns up to M2L2_MAXIT work items (local term b, a range
+// of source terms a in graded order), the same items for every pair; per
+// pair an item's sum (coef = (s_o/rho)^|b| / rho * f_|a| * Dc_(a+b) times
+// the source row with the Yl correction folded in, Y_dj - R0_d m_j) is
+// accumulated in registers and added to the item's slot in shared memory,
+// which only that thread touches.  At the end the slots of each b are summed
+// in a fixed order and scaled by 1 / b!.  One barrier per pair; registers
+// stay under 80 so that three CTAs share an SM.
+constexpr int M2L2_THREADS = 256;
+constexpr int M2L2_TC = M2L2_THREADS - 32;  // contraction threads
+constexpr int M2L2_MAXIT = 3;
+constexpr int M2L2_MAXITEMS = M2L2_TC * M2L2_MAXIT;
+constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
+struct M2LPlan2 {
+    int n_items;
+    int item[M2L2_MAXITEMS][8];   // b, g0, g1, a0, a2, |a| at g0, b0, b2
+    int bstart[FMM_NTMAX + 1];    // items of term b: [bstart[b], bstart[b + 1])
+    int tcnt[M2L2_TC];
+    int titem[M2L2_TC][M2L2_MAXIT];
+    int rec[FMM_NTMAX][8];        // Dc recurrence: a0, a1, a2 and the 5 used indices
+};
+
+// The plan: items cut term b's n_terms(p - |b|) source terms into near-equal
+// chunks of at most CH = ceil(total / M2L2_TC) terms; the items, largest
+// first, are dealt to the contraction threads in snake order.  One thread,
+// written to the workspace each call.
+__global__ void __launch_bounds__(32) fmm_m2l2_plan(int p, M2LPlan2* __restrict__ plan, int* err) {
+    if (threadIdx.x != 0) return;
+    const int NT = n_terms(p);
+    const int total = n_terms6(p);
+    const int CH = (total + M2L2_TC - 1) / M2L2_TC;
+    int n = 0;
+    for (int b = 0; b < NT; b++) {
+        int b0, b1, b2;
+        decode(b, b0, b1, b2);
+        const int t = n_terms(p - (b0 + b1 + b2));
+        const int nch = (t + CH - 1) / CH;
+        plan->bstart[b] = n;
+        for (int c = 0; c < nch; c++) {
+            if (n >= M2L2_MAXITEMS) {
+                *err = 1;
+                return;
+            }
+            const int g0 = (int)((int64_t)t * c / nch), g1 = (int)((int64_t)t * (c + 1) / nch);
+            int a0, a1, a2;
+            decode(g0, a0, a1, a2);
+            int* it = plan->item[n];
+            it[0] = b; it[1] = g0; it[2] = g1; it[3] = a0; it[4] = a2; it[5] = a0 + a1 + a2;
+            it[6] = b0; it[7] = b2;
+            n++;
+        }
+    }
+    plan->bstart[NT] = n;
+    plan->n_items = n;
+    // deal items by size, largest first (counting sort on sizes 1..CH), snake order
+    for (int t = 0; t < M2L2_TC; t++) plan->tcnt[t] = 0;
+    int dealt = 0;
+    for (int sz = CH; sz >= 1; sz--)
+        for (int i = 0; i < n; i++) {
+            if (plan->item[i][2] - plan->item[i][1] != sz) continue;
+            const int round = dealt / M2L2_TC, pos = dealt % M2L2_TC;
+            const int th = (round & 1) ? M2L2_TC - 1 - pos : pos;
+            if (plan->tcnt[th] >= M2L2_MAXIT) {
+                *err = 1;
+                return;
+            }
+            plan->titem[th][plan->tcnt[th]++] = i;
+            dealt++;
+        }
+    // the Dc recurrence table
+    for (int g = 0; g < NT; g++) {
+        int a0, a1, a2;
+        decode(g, a0, a1, a2);
+        int* r = plan->rec[g];
+        r[0] = a0; r[1] = a1; r[2] = a2;
+        r[3] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
+        r[4] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
+        r[5] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
+        r[6] = a0 > 1 ? midx(a0 - 2, a1, a2) : 0;
+        r[7] = 0;  // the a1 - 2 and a2 - 2 indices are recomputed (rare)
+    }
+}
+
+// Number of plan items for order p (host mirror of fmm_m2l2_plan's cut).
+inline int m2l2_items(int p) {
+    const int total = n_terms6(p), CH = (total + M2L2_TC - 1) / M2L2_TC;
+    int n = 0;
+    for (int m = 0; m <= p; m++) {
+        const int t = n_terms(p - m), cnt = (m + 1) * (m + 2) / 2;
+        n += cnt * ((t + CH - 1) / CH);
+    }
+    return n;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename R, int K>
-__global__ void __launch_bounds__(128)
-fmm_m2l(int p, int wpb, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
-        const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
-        const R* __restrict__ ocent, const R* __restrict__ orad, const R* __restrict__ scent,
-        const R* __restrict__ srad, const R* __restrict__ mom, const M2LPlan* __restrict__ plan,
-        R* __restrict__ loc) {
+__global__ void __launch_bounds__(M2L2_THREADS, 3)
+fmm_m2l2(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
+         const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
+         const R* __restrict__ ocent, const R* __restrict__ orad, const R* __restrict__ scent,
+         const R* __restrict__ srad, const R* __restrict__ mom, const M2LPlan2* __restrict__ plan,
+         R* __restrict__ loc) {
     using C = Chan<K>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NT = n_terms(p);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t oi = (int64_t)blockIdx.x * wpb + warp;
-    if (warp >= wpb || oi >= n_obs_nodes) return;  // whole warps only: no block barriers below
-    // per-warp segment: Lw, Ns (NT x NCHP each), partial slots, Dc, fw, pw;
-    // padded to 4 Reals so that every warp's Ns stays 16-byte aligned
-    const int seg = (2 * NT + M2L_SLOTS) * C::NCHP + (NT + 32 + 3) / 4 * 4;
-    R* Lw = reinterpret_cast<R*>(smem_raw) + (size_t)warp * seg;
-    R* Ns = Lw + NT * C::NCHP;        // the current source node's moments
-    R* Ps = Ns + NT * C::NCHP;        // partial sums of split terms
-    R* Dc = Ps + M2L_SLOTS * C::NCHP;  // NT
-    R* fw = Dc + NT;                  // f_n, n <= p
-    R* pw = fw + 16;                  // (s_o/rho)^n / rho
-    for (int e = lane; e < NT * C::NCHP; e += 32) Lw[e] = 0;
-    const int mycnt = plan->cnt[lane];
-    const int nsplit = plan->nsplit;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t oi = blockIdx.x;
+    if (oi >= n_obs_nodes) return;
+    const int rowsz = NT * C::NCHP;
+    R* Nb = reinterpret_cast<R*>(smem_raw);  // 2 x NT x NCHP moments
+    R* Db = Nb + 2 * rowsz;                  // 2 x NT Dc
+    R* Sb = Db + 2 * ((NT + 3) / 4 * 4);     // 2 x 40: f_n [0, 16), pw_n [16, 32), R0 [32, 35)
+    R* slots = Sb + 80;                      // n_items x NCHP item sums
     const int64_t node = obs_nodes[oi];
     const R co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
     const R so = orad[node];
-    for (int64_t l = starts[oi]; l < starts[oi + 1]; l++) {
+    const int64_t l0 = starts[oi], l1 = starts[oi + 1];
+    const int64_t npair = l1 - l0;
+
+    auto issue_copy = [&](int64_t l, int buf) {
+        const R* src = mom + srcs[l] * (int64_t)rowsz;
+        R* dst = Nb + buf * rowsz;
+        constexpr int PER = 16 / sizeof(R);
+        for (int k = tid; k < rowsz / PER; k += M2L2_THREADS)
+            cp_async16(dst + k * PER, src + k * PER);
+        cp_async_commit();
+    };
+    auto produce = [&](int64_t l, int buf) {  // warp 0
         const int64_t sn = srcs[l];
-        const R R0[3] = {co[0] - scent[3 * sn], co[1] - scent[3 * sn + 1], co[2] - scent[3 * sn + 2]};
+        const R R0[3] = {co[0] - scent[3 * sn], co[1] - scent[3 * sn + 1],
+                         co[2] - scent[3 * sn + 2]};
         const R rho = sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
         const R inv_rho = R(1) / rho;
         const R Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
-        __syncwarp();  // the previous pair's readers are done
+        R* S = Sb + buf * 40;
+        R* D = Db + buf * ((NT + 3) / 4 * 4);
         if (lane <= p) {
-            fw[lane] = ((lane & 1) ? R(-1) : R(1)) * ipow(srad[sn] * inv_rho, lane);
-            pw[lane] = ipow(so * inv_rho, lane) * inv_rho;
-        } else if (lane < 16) {
-            fw[lane] = 0;
-            pw[lane] = 0;
+            S[lane] = ((lane & 1) ? R(-1) : R(1)) * ipow(srad[sn] * inv_rho, lane);
+            S[16 + lane] = ipow(so * inv_rho, lane) * inv_rho;
         }
-        if (lane == 0) Dc[0] = 1;
-        {
-            const R* Ms = mom + sn * (int64_t)C::NCHP * NT;
-            if (sizeof(R) == 4) {
-                const float4* sv = reinterpret_cast<const float4*>(Ms);
-                float4* dv = reinterpret_cast<float4*>(Ns);
-                for (int k = lane; k < NT * C::NCHP / 4; k += 32) dv[k] = __ldg(sv + k);
-            } else {
-                const double2* sv = reinterpret_cast<const double2*>(Ms);
-                double2* dv = reinterpret_cast<double2*>(Ns);
-                for (int k = lane; k < NT * C::NCHP / 2; k += 32) dv[k] = __ldg(sv + k);
-            }
-        }
+        if (lane < 3) S[32 + lane] = R0[lane];
+        if (lane == 0) D[0] = 1;
         __syncwarp();
         for (int n = 1; n <= p; n++) {
-            const int lsz = (n + 1) * (n + 2) / 2;
+            const int lsz = (n + 1) * (n + 2) / 2, base = n_terms(n - 1);
             const R cA = -(R)(2 * n - 1) / (R)n, cB = -(R)(n - 1) / (R)n;
             for (int w = lane; w < lsz; w += 32) {
-                int a0 = n, off = 0;
-                while (off + (n - a0 + 1) <= w) {
-                    off += n - a0 + 1;
-                    a0--;
-                }
-                const int a2 = w - off, a1 = n - a0 - a2;
+                const int* rr = plan->rec[base + w];
+                const int a0 = rr[0], a1 = rr[1], a2 = rr[2];
                 R s1 = 0, s2 = 0;
-                if (a0 > 0) s1 += Rh[0] * (R)a0 * Dc[midx(a0 - 1, a1, a2)];
-                if (a1 > 0) s1 += Rh[1] * (R)a1 * Dc[midx(a0, a1 - 1, a2)];
-                if (a2 > 0) s1 += Rh[2] * (R)a2 * Dc[midx(a0, a1, a2 - 1)];
-                if (a0 > 1) s2 += (R)(a0 * (a0 - 1)) * Dc[midx(a0 - 2, a1, a2)];
-                if (a1 > 1) s2 += (R)(a1 * (a1 - 1)) * Dc[midx(a0, a1 - 2, a2)];
-                if (a2 > 1) s2 += (R)(a2 * (a2 - 1)) * Dc[midx(a0, a1, a2 - 2)];
-                Dc[n_terms(n - 1) + w] = cA * s1 + cB * s2;
+                if (a0 > 0) s1 += Rh[0] * (R)a0 * D[rr[3]];
+                if (a1 > 0) s1 += Rh[1] * (R)a1 * D[rr[4]];
+                if (a2 > 0) s1 += Rh[2] * (R)a2 * D[rr[5]];
+                if (a0 > 1) s2 += (R)(a0 * (a0 - 1)) * D[rr[6]];
+                if (a1 > 1) s2 += (R)(a1 * (a1 - 1)) * D[midx(a0, a1 - 2, a2)];
+                if (a2 > 1) s2 += (R)(a2 * (a2 - 1)) * D[midx(a0, a1, a2 - 2)];
+                D[base + w] = cA * s1 + cB * s2;
             }
             __syncwarp();
         }
-        // flat loop over this lane's chunks: every lane runs ~CH iterations
-        int k = 0;
-        int b = 0, b0 = 0, b1 = 0, b2 = 0, g = 0, g1 = 0, slot = -1, na = 0, a0 = 0, a2 = 0,
-            n = 0, rowbase = 0;
-        R f = 0;
-        R acc[C::NCH];
-        while (k < mycnt) {
-            if (g == g1) {  // start chunk k
-                b = plan->item[lane][k][0];
-                g = plan->item[lane][k][1];
-                g1 = plan->item[lane][k][2];
-                slot = plan->item[lane][k][3];
-                decode(b, b0, b1, b2);
-                int a1;
-                decode(g, a0, a1, a2);
-                na = a0 + a1 + a2;
-                n = na + b0 + b1 + b2;
-                rowbase = n_terms(n - 1) + (n - a0 - b0) * (n - a0 - b0 + 1) / 2 + b2;
-                f = fw[na];
+    };
+
+    // this thread's work items
+    const int ct = tid - 32;
+    int my_n = 0;
+    int itid[M2L2_MAXIT], itg0[M2L2_MAXIT], itg1[M2L2_MAXIT], ita0[M2L2_MAXIT],
+        ita2[M2L2_MAXIT], itna[M2L2_MAXIT], itb0[M2L2_MAXIT], itb2[M2L2_MAXIT],
+        itnb[M2L2_MAXIT];
+    if (warp > 0) {
+        my_n = plan->tcnt[ct];
 #pragma unroll
-                for (int c = 0; c < C::NCH; c++) acc[c] = 0;
-            }
-            const R coef = f * Dc[rowbase + a2];
-            const R* nrow = Ns + g * C::NCHP;
-            if (sizeof(R) == 4) {
-#pragma unroll
-                for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
-                    const float4 v = reinterpret_cast<const float4*>(nrow)[k4];
-                    const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (int u = 0; u < 4; u++)
-                        if (4 * k4 + u < C::NCH) acc[4 * k4 + u] += coef * (R)vv[u];
-                }
-            } else {
-#pragma unroll
-                for (int k2 = 0; k2 < C::NCHP / 2; k2++) {
-                    const double2 v = reinterpret_cast<const double2*>(nrow)[k2];
-                    if (2 * k2 < C::NCH) acc[2 * k2] += coef * (R)v.x;
-                    if (2 * k2 + 1 < C::NCH) acc[2 * k2 + 1] += coef * (R)v.y;
-                }
-            }
-            // next source term in graded order
-            g++;
-            a2++;
-            if (a2 > na - a0) {
-                a2 = 0;
-                a0--;
-                if (a0 < 0) {
-                    na++;
-                    a0 = na;
-                    n++;
-                    f = fw[na];
-                }
-                rowbase = n_terms(n - 1) + (n - a0 - b0) * (n - a0 - b0 + 1) / 2 + b2;
-            }
-            if (g == g1) {  // end of chunk k
-                if (slot < 0) {
-                    m2l_flush<R, K>(acc, R0, pw[b0 + b1 + b2] / mfact<R>(b0, b1, b2),
-                                    Lw + b * C::NCHP);
-                } else {
-#pragma unroll
-                    for (int c = 0; c < C::NCH; c++) Ps[slot * C::NCHP + c] = acc[c];
-                }
-                k++;
-            }
-        }
-        __syncwarp();
-        for (int j = lane; j < nsplit; j += 32) {
-            const int bs = plan->split[j][0];
-            int c0, c1, c2;
-            decode(bs, c0, c1, c2);
-            R sacc[C::NCH];
-#pragma unroll
-            for (int c = 0; c < C::NCH; c++) sacc[c] = 0;
-            for (int sl = plan->split[j][1]; sl < plan->split[j][2]; sl++)
-#pragma unroll
-                for (int c = 0; c < C::NCH; c++) sacc[c] += Ps[sl * C::NCHP + c];
-            m2l_flush<R, K>(sacc, R0, pw[c0 + c1 + c2] / mfact<R>(c0, c1, c2), Lw + bs * C::NCHP);
+        for (int i = 0; i < M2L2_MAXIT; i++) {
+            itid[i] = i < my_n ? plan->titem[ct][i] : 0;
+            const int* it = plan->item[itid[i]];
+            itg0[i] = it[1]; itg1[i] = it[2]; ita0[i] = it[3];
+            ita2[i] = it[4]; itna[i] = it[5]; itb0[i] = it[6]; itb2[i] = it[7];
+            int b0, b1, b2;
+            decode(it[0], b0, b1, b2);
+            itnb[i] = b0 + b1 + b2;
         }
     }
-    __syncwarp();
-    R* Lg = loc + node * (int64_t)C::NCHP * NT;
-    for (int e = lane; e < NT * C::NCHP; e += 32) Lg[e] = Lw[e];
+    const int n_items = plan->n_items;
+    for (int e = tid; e < n_items * C::NCHP; e += M2L2_THREADS) slots[e] = 0;
+
+    if (npair > 0) {
+        issue_copy(l0, 0);
+        if (warp == 0) produce(l0, 0);
+    }
+    for (int64_t k = 0; k < npair; k++) {
+        const int buf = (int)(k & 1);
+        cp_async_wait_all();
+        __syncthreads();  // pair k's moments and Dc are complete; pair k - 1 is done
+        if (k + 1 < npair) {
+            issue_copy(l0 + k + 1, buf ^ 1);
+            if (warp == 0) produce(l0 + k + 1, buf ^ 1);
+        }
+        if (warp == 0) continue;
+        const R* S = Sb + buf * 40;
+        const R* D = Db + buf * ((NT + 3) / 4 * 4);
+        const R* N = Nb + buf * rowsz;
+        const R R0[3] = {S[32], S[33], S[34]};
+#pragma unroll 1
+        for (int i = 0; i < M2L2_MAXIT; i++) {
+            if (i >= my_n) break;
+            R acc[C::NCH];
+#pragma unroll
+            for (int c = 0; c < C::NCH; c++) acc[c] = 0;
+            const R sb = S[16 + itnb[i]];
+            const int b0 = itb0[i], b2 = itb2[i];
+            int a0 = ita0[i], a2 = ita2[i], na = itna[i];
+            int nn = na + itnb[i];
+            int rowbase = n_terms(nn - 1) + (nn - a0 - b0) * (nn - a0 - b0 + 1) / 2 + b2;
+            R f = sb * S[na];
+            for (int g = itg0[i]; g < itg1[i]; g++) {
+                const R coef = f * D[rowbase + a2];
+                const R* row = N + g * C::NCHP;
+                R v[C::NCHP];
+                if (sizeof(R) == 4) {
+#pragma unroll
+                    for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
+                        const float4 q = reinterpret_cast<const float4*>(row)[k4];
+                        v[4 * k4] = (R)q.x; v[4 * k4 + 1] = (R)q.y;
+                        v[4 * k4 + 2] = (R)q.z; v[4 * k4 + 3] = (R)q.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int k2 = 0; k2 < C::NCHP / 2; k2++) {
+                        const double2 q = reinterpret_cast<const double2*>(row)[k2];
+                        v[2 * k2] = (R)q.x; v[2 * k2 + 1] = (R)q.y;
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+#pragma unroll
+                    for (int j = 0; j < C::J; j++)
+                        v[C::CH_Y + d * C::J + j] -= R0[d] * v[C::CH_M + j];
+#pragma unroll
+                for (int c = 0; c < C::NCH; c++) acc[c] += coef * v[c];
+                // next source term in graded order
+                a2++;
+                if (a2 > na - a0) {
+                    a2 = 0;
+                    a0--;
+                    if (a0 < 0) {
+                        na++;
+                        a0 = na;
+                        nn++;
+                        f = sb * S[na];
+                    }
+                    rowbase = n_terms(nn - 1) + (nn - a0 - b0) * (nn - a0 - b0 + 1) / 2 + b2;
+                }
+            }
+            R* sl = slots + itid[i] * C::NCHP;
+#pragma unroll
+            for (int c = 0; c < C::NCH; c++) sl[c] += acc[c];
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    R* Lg = loc + node * (int64_t)rowsz;
+    for (int b = tid; b < NT; b += M2L2_THREADS) {
+        int b0, b1, b2;
+        decode(b, b0, b1, b2);
+        const R inv = R(1) / mfact<R>(b0, b1, b2);
+        R sum[C::NCH];
+#pragma unroll
+        for (int c = 0; c < C::NCH; c++) sum[c] = 0;
+        for (int it = plan->bstart[b]; it < plan->bstart[b + 1]; it++)
+#pragma unroll
+            for (int c = 0; c < C::NCH; c++) sum[c] += slots[it * C::NCHP + c];
+#pragma unroll
+        for (int c = 0; c < C::NCHP; c++) Lg[b * C::NCHP + c] = c < C::NCH ? sum[c] * inv : R(0);
+    }
 }
+
 
 // ---- L2L (FMM) -------------------------------------------------------------
 // One block per obs node of one depth (parents final): loc[child] += shift of
@@ -936,7 +992,7 @@ Sizes sizes_for(size_t rs, int mode, int order, int64_t n_obs, int64_t n_src, in
     s.rec = al256(rs * Rec<K, NQ>::LEN * (size_t)n_src);
     s.mom = al256(rs * C::NCHP * (size_t)n_terms(order) * n_src_nodes);
     s.loc = mode == 1 ? al256(rs * C::NCHP * (size_t)n_terms(order) * n_obs_nodes) : 0;
-    s.plan = mode == 1 ? al256(sizeof(M2LPlan)) : 0;
+    s.plan = mode == 1 ? al256(sizeof(M2LPlan2) + 256) : 0;
     s.W = al256(rs * NAcc<K, NQ>::n * (size_t)n_obs);
     s.F = al256(rs * C::NO * (size_t)NQ * n_obs);
     return s;
@@ -989,7 +1045,7 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
     R* rec = reinterpret_cast<R*>(ws);
     R* mom = reinterpret_cast<R*>(ws + sz.rec);
     R* loc = reinterpret_cast<R*>(ws + sz.rec + sz.mom);
-    M2LPlan* plan = reinterpret_cast<M2LPlan*>(ws + sz.rec + sz.mom + sz.loc);
+    unsigned char* plan = ws + sz.rec + sz.mom + sz.loc;
     R* W = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan);
     R* F = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan + sz.W);
     const R* scent = (const R*)stt.centers;
@@ -1041,16 +1097,21 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, st>>>(
                 p, C::NCHP, stt.n_nodes, mom);
             if ((rc = launch_status("fmm moment factorials"))) return rc;
-            fmm_m2l_plan<<<1, 32, 0, st>>>(p, plan);
+            if (m2l2_items(p) > M2L2_MAXITEMS) {
+                set_error("tct_fmm_matvec: FMM order %d exceeds the M2L plan's capacity", p);
+                return TCT_ERR_ARG;
+            }
+            M2LPlan2* plan2 = reinterpret_cast<M2LPlan2*>(plan);
+            int* plan_err = reinterpret_cast<int*>(plan + al256(sizeof(M2LPlan2)));
+            fmm_m2l2_plan<<<1, 32, 0, st>>>(p, plan2, plan_err);
             if ((rc = launch_status("fmm m2l plan"))) return rc;
-            const size_t per_warp =
-                sizeof(R) * ((2 * (size_t)NT + M2L_SLOTS) * C::NCHP + (NT + 32 + 3) / 4 * 4);
-            const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (200 * 1024) / per_warp));
-            const size_t smem = per_warp * wpb;
-            if ((rc = set_smem(fmm_m2l<R, K>, smem))) return rc;
-            fmm_m2l<R, K><<<(unsigned)((far.n_obs + wpb - 1) / wpb), 32 * wpb, smem, st>>>(
-                p, wpb, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
-                plan, loc);
+            const size_t smem_all = sizeof(R) * (2 * (size_t)NT * C::NCHP +
+                                                 2 * (size_t)((NT + 3) / 4 * 4) + 80 +
+                                                 (size_t)m2l2_items(p) * C::NCHP);
+            if ((rc = set_smem(fmm_m2l2<R, K>, smem_all))) return rc;
+            fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, st>>>(
+                p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom, plan2,
+                loc);
             if ((rc = launch_status("fmm m2l"))) return rc;
         }
         const size_t smem_l2l =
