@@ -343,5 +343,133 @@ __device__ __forceinline__ void far_epilogue(const Rule2D<R>& rule, const TriGeo
     }
 }
 
+// ---- packed-FP32 elasticRH3 pair sums (direct farfield and treecode P2P) -----
+// Two observation triangles per thread, one in each half of an f32x2 register
+// pair, so every point-pair operation is one fma/mul/add.rn.f32x2 instruction
+// for both.  Per point pair (both halves): D = y - x, r2e = |D|^2 + EPS,
+// invr = rsqrt(r2e) (two MUFU ops), g = invr^3, T += g D D^T; per triangle
+// pair S0 = trace(T) (= sum of 1/r, since trace(D D^T) / r^3 = 1/r) and
+// W += S0 P + T (-2 ssc).  EPS = 1e-24 keeps invr^3 finite at r2 == 0, where
+// D == 0 makes the point pair contribute exactly nothing -- the reference's
+// "skip r^2 == 0" (matrix_free.cl:79-81) without a per-pair select.  EPS is
+// below the FP32 rounding of any r2 above ~1e-17 (point separations above
+// ~3e-9 in mesh units).  J_s * CsRH0 (and, for equal-weight rules, w^2) are
+// folded into P and -2 ssc by the prep kernel.
+constexpr float RH2_EPS = 1e-24f;
+
+// Record of one source triangle for the packed kernel, every value stored
+// twice (an f32x2 operand): y[q][d] (3 NQ pairs), P (9), M = -2 ssc (9).
+template <int NQ>
+struct RecRH2 {
+    static constexpr int Y = 0;
+    static constexpr int P = 3 * NQ;
+    static constexpr int M = 3 * NQ + 9;
+    static constexpr int PAIRS = 3 * NQ + 18;
+    static constexpr int LEN = (2 * PAIRS + 3) / 4 * 4;  // floats
+};
+
+template <int NQ, bool UNIFORM>
+__global__ void __launch_bounds__(128)
+far_prep_rh2(Consts<float> c, Rule2D<float> rule, const float* __restrict__ pts,
+             const int32_t* __restrict__ src_tris, int64_t n_src, const float* __restrict__ in,
+             const int64_t* __restrict__ src_orig, float* __restrict__ rec) {
+    using L = RecRH2<NQ>;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_src) return;
+    TriGeom<float> s;
+    load_tri(s, pts, src_tris, i, 0, false, true);
+    const int64_t ii = src_orig ? src_orig[i] : i;  // input row of tree-ordered sources
+    float in9[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) in9[k] = in[ii * 9 + k];
+    float* r = rec + i * L::LEN;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+        const float sx = rule.x[q], sy = rule.y[q];
+        const float sb[3] = {1 - sx - sy, sx, sy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const float y = bary_point(s, sb, d);
+            r[2 * (L::Y + 3 * q + d)] = y;
+            r[2 * (L::Y + 3 * q + d) + 1] = y;
+        }
+    }
+    float ssc[3][3];
+#pragma unroll
+    for (int Ij = 0; Ij < 3; Ij++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            float a = 0;
+#pragma unroll
+            for (int b = 0; b < 3; b++) a += s.sc[b][Ij] * in9[b * 3 + d];
+            ssc[d][Ij] = a;
+        }
+    float scale = s.J * c.CsRH0;
+    if (UNIFORM) scale *= rule.w[0] * rule.w[0];
+    const float B = (ssc[0][0] + ssc[1][1] + ssc[2][2]) * c.CsRH1;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float p = scale * ((d == j ? B : 0.f) + c.CsRH2 * ssc[j][d] - 2 * ssc[d][j]);
+            const float m = scale * (-2.f * ssc[d][j]);
+            r[2 * (L::P + 3 * d + j)] = p;
+            r[2 * (L::P + 3 * d + j) + 1] = p;
+            r[2 * (L::M + 3 * d + j)] = m;
+            r[2 * (L::M + 3 * d + j) + 1] = m;
+        }
+#pragma unroll
+    for (int k = 2 * L::PAIRS; k < L::LEN; k++) r[k] = 0;
+}
+
+// One packed source record r against this thread's two observation
+// triangles (negated target points negx, pair weights wq for unequal-weight
+// rules): W[3 d + j] += S0 P[d][j] + sum_k T[d][k] M[k][j], both halves.
+template <int NQ, bool UNIFORM>
+__device__ __forceinline__ void rh2_pair(const f2_t* __restrict__ r, const f2_t (&negx)[NQ][3],
+                                         const f2_t (&wq)[UNIFORM ? 1 : NQ * NQ], f2_t eps,
+                                         f2_t (&W)[9]) {
+    using L = RecRH2<NQ>;
+    f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
+#pragma unroll
+    for (int q2 = 0; q2 < NQ; q2++) {
+        const f2_t y0 = r[L::Y + 3 * q2 + 0], y1 = r[L::Y + 3 * q2 + 1],
+                   y2 = r[L::Y + 3 * q2 + 2];
+#pragma unroll
+        for (int q1 = 0; q1 < NQ; q1++) {
+            const f2_t D0 = add2(y0, negx[q1][0]);
+            const f2_t D1 = add2(y1, negx[q1][1]);
+            const f2_t D2 = add2(y2, negx[q1][2]);
+            f2_t r2 = fma2(D0, D0, eps);
+            r2 = fma2(D1, D1, r2);
+            r2 = fma2(D2, D2, r2);
+            float ra, rb;
+            upk(r2, ra, rb);
+            const f2_t invr = pk(rsqrtf(ra), rsqrtf(rb));
+            f2_t g = mul2(mul2(invr, invr), invr);
+            if (!UNIFORM) g = mul2(g, wq[q1 * NQ + q2]);
+            const f2_t g0 = mul2(g, D0), g1 = mul2(g, D1), g2 = mul2(g, D2);
+            T00 = fma2(g0, D0, T00);
+            T01 = fma2(g0, D1, T01);
+            T02 = fma2(g0, D2, T02);
+            T11 = fma2(g1, D1, T11);
+            T12 = fma2(g1, D2, T12);
+            T22 = fma2(g2, D2, T22);
+        }
+    }
+    const f2_t S0 = add2(add2(T00, T11), T22);
+    const f2_t T[3][3] = {{T00, T01, T02}, {T01, T11, T12}, {T02, T12, T22}};
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+            f2_t w = fma2(S0, r[L::P + 3 * d + jj], W[3 * d + jj]);
+            w = fma2(T[d][0], r[L::M + 0 * 3 + jj], w);
+            w = fma2(T[d][1], r[L::M + 1 * 3 + jj], w);
+            w = fma2(T[d][2], r[L::M + 2 * 3 + jj], w);
+            W[3 * d + jj] = w;
+        }
+}
+
 }  // namespace
 }  // namespace tct

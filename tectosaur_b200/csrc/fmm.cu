@@ -341,10 +341,24 @@ fmm_m2m(int p, const int64_t* __restrict__ parents, const int64_t* __restrict__ 
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ---- P2P -------------------------------------------------------------------
 // One block per obs leaf with a non-empty P2P list.  The leaf's m obs
-// triangles take m threads; the block's 128 threads form 128 / m groups that
-// take the listed source leaves round-robin, each thread running the direct
+// triangles take m threads; the block's 128 threads form G = 128 / m groups,
+// and group g takes the g-th of G equal slices of the list's source
+// triangles (concatenated in list order), each thread running the direct
 // farfield's pair loop over its group's source triangles (records read
 // through L1 as broadcasts within a group).  Group sums are added in a fixed
 // order, so the result is deterministic.  W[t] = per-obs-triangle sums in the
@@ -365,6 +379,11 @@ fmm_p2p(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
     const int64_t node = obs_nodes[blockIdx.x];
     const int64_t l0 = starts[blockIdx.x], l1 = starts[blockIdx.x + 1];
     const int64_t ob0 = o_start[node], n_o = o_end[node] - ob0;
+    int64_t n_s = 0;  // source triangles over the whole list
+    for (int64_t l = l0; l < l1; l++) {
+        const int64_t sn = srcs[l];
+        n_s += s_end[sn] - s_start[sn];
+    }
     for (int64_t cb = 0; cb < n_o; cb += blockDim.x) {
         const int m = (int)min((int64_t)blockDim.x, n_o - cb);
         const int G = blockDim.x / m;
@@ -382,14 +401,23 @@ fmm_p2p(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
             R x[NQ][3];
 #pragma unroll
             for (int q = 0; q < NQ; q++) target_point(o, rule, q, x[q]);
-            for (int64_t l = l0 + grp; l < l1; l += G) {
+            // group grp takes source positions [p0, p1) of the list's
+            // concatenated source triangles
+            const int p0 = (int)(n_s * grp / G), p1 = (int)(n_s * (grp + 1) / G);
+            int cpos = 0;
+            for (int64_t l = l0; l < l1 && cpos < p1; l++) {
                 const int64_t sn = srcs[l];
+                const int64_t a = s_start[sn];
+                const int n = (int)(s_end[sn] - a);
+                const int lo = max(p0, cpos), hi = min(p1, cpos + n);
+                const R* rp = rec + (a + (lo - cpos)) * L::LEN;
+                cpos += n;
+                if (lo >= hi) continue;
                 R acc[NA];
 #pragma unroll
                 for (int k = 0; k < NA; k++) acc[k] = 0;
-                const int64_t e = s_end[sn];
-                for (int64_t s = s_start[sn]; s < e; s++)
-                    far_pair<R, K, NQ>(c, rule, o, x, rec + s * L::LEN, acc);
+                for (int j = lo; j < hi; j++, rp += L::LEN)
+                    far_pair<R, K, NQ>(c, rule, o, x, rp, acc);
 #pragma unroll
                 for (int k = 0; k < NA; k++) fold<R, KAHAN>(tot[k], cmp[k], acc[k]);
             }
@@ -405,6 +433,182 @@ fmm_p2p(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
             for (int k = 0; k < NA; k++) {
                 R sacc = 0;
                 for (int g = 0; g < G; g++) sacc += red[(g * m + threadIdx.x) * NA + k];
+                w[k] = sacc;
+            }
+        }
+    }
+}
+
+// ---- P2P, packed elasticRH3 in FP32 ------------------------------------------
+// fmm_p2p with the direct farfield's packed pair sums (rh2_pair).  The block's
+// four warps split a chunk of m <= 128 obs triangles of the leaf into T =
+// ceil(m / 64) teams of 64 (a lane takes triangles lane and lane + 32 of its
+// team, one in each f32x2 half) and the list's source triangles, concatenated
+// in list order, into S = 4 / T equal slices; warp w is team w % T, slice
+// w / T.  A warp streams its slice through its own two shared-memory buffers
+// of P2P_CH packed records (cp.async, the next chunk in flight while the
+// current one is summed; records read as broadcasts), and Kahan-folds the
+// packed sums of each chunk into its totals.  Slice totals are added in a
+// fixed order.  W[t] = the 9 sums of obs triangle t in the NAcc layout
+// (overwritten).
+constexpr int P2P_CH = 16;
+
+template <int NQ>
+constexpr size_t p2p_rh2_smem() {
+    return sizeof(float) * (128 * 18 + 4 * 2 * P2P_CH * RecRH2<NQ>::LEN);
+}
+
+template <int NQ, bool UNIFORM>
+__global__ void __launch_bounds__(128, NQ == 3 ? 4 : 3)
+fmm_p2p_rh2(Rule2D<float> rule, const float* __restrict__ pts,
+            const int32_t* __restrict__ obs_tris, const int64_t* __restrict__ obs_nodes,
+            const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
+            const int64_t* __restrict__ o_start, const int64_t* __restrict__ o_end,
+            const int64_t* __restrict__ s_start, const int64_t* __restrict__ s_end,
+            const float* __restrict__ rec, float* __restrict__ W) {
+    using L = RecRH2<NQ>;
+    constexpr int V4 = L::LEN / 4;  // float4s per record
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* red = reinterpret_cast<float*>(smem_raw);  // 128 x 18 slice totals
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* buf = red + 128 * 18 + warp * 2 * P2P_CH * L::LEN;  // this warp's two buffers
+    const int64_t node = obs_nodes[blockIdx.x];
+    const int64_t l0 = starts[blockIdx.x], l1 = starts[blockIdx.x + 1];
+    const int64_t ob0 = o_start[node], n_o = o_end[node] - ob0;
+    f2_t wq[UNIFORM ? 1 : NQ * NQ];
+    wq[0] = 0ull;
+    if (!UNIFORM) {
+#pragma unroll
+        for (int q1 = 0; q1 < NQ; q1++)
+#pragma unroll
+            for (int q2 = 0; q2 < NQ; q2++) {
+                const float w = rule.w[q1] * rule.w[q2];
+                wq[q1 * NQ + q2] = pk(w, w);
+            }
+    }
+    const f2_t eps = pk(RH2_EPS, RH2_EPS);
+    int n_s = 0;  // source triangles over the whole list (warp reduction)
+    for (int64_t l = l0 + lane; l < l1; l += 32) {
+        const int64_t sn = srcs[l];
+        n_s += (int)(s_end[sn] - s_start[sn]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_s += __shfl_xor_sync(0xffffffffu, n_s, o);
+
+    for (int64_t cb = 0; cb < n_o; cb += 128) {
+        const int m = (int)min((int64_t)128, n_o - cb);
+        const int T = m > 64 ? 2 : 1, S = 4 / T;
+        const int team = warp % T, slice = warp / T;
+        const int ta = team * 64 + lane, tb = ta + 32;
+        const bool va = ta < m, vb = tb < m;
+        float tot[2][9], cmp[2][9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            tot[0][k] = tot[1][k] = 0.f;
+            cmp[0][k] = cmp[1][k] = 0.f;
+        }
+        f2_t negx[NQ][3];
+        {
+            TriGeom<float> oa, ob;
+            if (va) load_tri(oa, pts, obs_tris, ob0 + cb + ta, 0, false, true);
+            if (vb) load_tri(ob, pts, obs_tris, ob0 + cb + tb, 0, false, true);
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const float ox = rule.x[q], oy = rule.y[q];
+                const float bq[3] = {1 - ox - oy, ox, oy};
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                    negx[q][d] = pk(va ? -bary_point(oa, bq, d) : 0.f,
+                                    vb ? -bary_point(ob, bq, d) : 0.f);
+            }
+        }
+        // the slice [p0, p1) of the concatenated sources; the stream cursor
+        // (list entry l, its first record a, offset off, records left rem)
+        const int p0 = (int)((int64_t)n_s * slice / S), p1 = (int)((int64_t)n_s * (slice + 1) / S);
+        int64_t l = l0, a = 0;
+        int off = 0, rem = 0, skip = p0;
+        while (l < l1) {  // find the entry holding position p0
+            const int64_t sn = srcs[l];
+            a = s_start[sn];
+            rem = (int)(s_end[sn] - a);
+            if (skip < rem) break;
+            skip -= rem;
+            l++;
+        }
+        off = skip;
+        rem -= skip;
+        // copy the next `need` stream records into buffer b (one commit group)
+        auto issue = [&](int need, int b) {
+            int64_t gidx = 0;
+            int r_base = 0;
+            while (r_base < need) {
+                while (rem == 0 && l + 1 < l1) {
+                    l++;
+                    const int64_t sn = srcs[l];
+                    a = s_start[sn];
+                    rem = (int)(s_end[sn] - a);
+                    off = 0;
+                }
+                const int take = min(rem, need - r_base);
+                if (take <= 0) break;  // unreachable: the slice never outruns the list
+                if (lane >= r_base && lane < r_base + take) gidx = a + off + (lane - r_base);
+                r_base += take;
+                off += take;
+                rem -= take;
+            }
+            float* dst = buf + b * P2P_CH * L::LEN;
+            for (int e0 = 0; e0 < need * V4; e0 += 32) {  // warp-uniform trip count
+                const int e = e0 + lane;
+                const int r = min(e / V4, need - 1), part = e - r * V4;
+                const int64_t g = __shfl_sync(0xffffffffu, gidx, r);
+                if (e < need * V4)
+                    cp_async16(dst + r * L::LEN + part * 4, rec + g * L::LEN + part * 4);
+            }
+            cp_async_commit();
+        };
+        const int n_mine = p1 - p0;
+        if (n_mine > 0) issue(min(P2P_CH, n_mine), 0);
+        for (int c0 = 0; c0 < n_mine; c0 += P2P_CH) {
+            const int cur = (c0 / P2P_CH) & 1;
+            const int need = min(P2P_CH, n_mine - c0);
+            if (c0 + P2P_CH < n_mine) {
+                issue(min(P2P_CH, n_mine - c0 - P2P_CH), cur ^ 1);
+                cp_async_wait_group<1>();
+            } else {
+                cp_async_wait_group<0>();
+            }
+            __syncwarp();
+            const float* rb = buf + cur * P2P_CH * L::LEN;
+            f2_t Wp[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) Wp[k] = 0ull;
+#pragma unroll 2
+            for (int j = 0; j < need; j++)
+                rh2_pair<NQ, UNIFORM>(reinterpret_cast<const f2_t*>(rb + j * L::LEN), negx, wq,
+                                      eps, Wp);
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                float wa, wb;
+                upk(Wp[k], wa, wb);
+                fold<float, true>(tot[0][k], cmp[0][k], wa);
+                fold<float, true>(tot[1][k], cmp[1][k], wb);
+            }
+            __syncwarp();  // buffer cur is free for the chunk after next
+        }
+        __syncthreads();  // the previous chunk's reads of red are done
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            red[threadIdx.x * 18 + k] = tot[0][k];
+            red[threadIdx.x * 18 + 9 + k] = tot[1][k];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < m; t += blockDim.x) {
+            const int tm = t / 64, within = t % 64, ln = within % 32, half = within / 32;
+            float* w = W + (ob0 + cb + t) * 9;
+            for (int k = 0; k < 9; k++) {
+                float sacc = 0.f;
+                for (int sl = 0; sl < S; sl++)
+                    sacc += red[((sl * T + tm) * 32 + ln) * 18 + half * 9 + k];
                 w[k] = sacc;
             }
         }
@@ -626,14 +830,6 @@ inline int m2l2_items(int p) {
     return n;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                     (uint32_t)__cvta_generic_to_shared(smem_dst)),
-                 "l"(gsrc)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename R, int K>
 __global__ void __launch_bounds__(M2L2_THREADS, 3)
@@ -981,8 +1177,14 @@ fmm_finish(Rule2D<R> rule, const R* __restrict__ pts, const int32_t* __restrict_
 inline size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 
 struct Sizes {
-    size_t rec, mom, loc, plan, W, F;
+    size_t rec, mom, loc, plan, W, F, rec2;
 };
+
+// The packed P2P runs for elasticRH3 in FP32 with the 3-, 4- and 7-point rules.
+template <typename R, int K, int NQ>
+constexpr bool p2p_packed() {
+    return sizeof(R) == 4 && K == kRH && (NQ == 3 || NQ == 4 || NQ == 7);
+}
 
 template <int K, int NQ>
 Sizes sizes_for(size_t rs, int mode, int order, int64_t n_obs, int64_t n_src, int64_t n_obs_nodes,
@@ -995,6 +1197,9 @@ Sizes sizes_for(size_t rs, int mode, int order, int64_t n_obs, int64_t n_src, in
     s.plan = mode == 1 ? al256(sizeof(M2LPlan2) + 256) : 0;
     s.W = al256(rs * NAcc<K, NQ>::n * (size_t)n_obs);
     s.F = al256(rs * C::NO * (size_t)NQ * n_obs);
+    s.rec2 = (rs == 4 && K == kRH && (NQ == 3 || NQ == 4 || NQ == 7))
+                 ? al256(4 * (size_t)RecRH2<NQ>::LEN * n_src)
+                 : 0;
     return s;
 }
 
@@ -1019,7 +1224,7 @@ Sizes sizes_dispatch(int kernel, int prec, int mode, int order, int nq, int64_t 
     TCT_SZ_K(kRH)
 #undef TCT_SZ_K
 #undef TCT_SZ_NQ
-    return Sizes{0, 0, 0, 0, 0, 0};
+    return Sizes{0, 0, 0, 0, 0, 0, 0};
 }
 
 template <typename KF>
@@ -1048,6 +1253,9 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
     unsigned char* plan = ws + sz.rec + sz.mom + sz.loc;
     R* W = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan);
     R* F = reinterpret_cast<R*>(ws + sz.rec + sz.mom + sz.loc + sz.plan + sz.W);
+    float* rec2 = reinterpret_cast<float*>(ws + sz.rec + sz.mom + sz.loc + sz.plan + sz.W + sz.F);
+    bool uniform = true;
+    for (int q = 1; q < NQ; q++) uniform = uniform && (rule.w[q] == rule.w[0]);
     const R* scent = (const R*)stt.centers;
     const R* srad = (const R*)stt.radii;
     const R* ocent = (const R*)ot.centers;
@@ -1074,12 +1282,39 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
         if ((rc = launch_status("fmm m2m"))) return rc;
     }
     if (near.n_obs > 0) {
-        const size_t smem = sizeof(R) * 128 * NA;
-        if ((rc = set_smem(fmm_p2p<R, K, NQ>, smem))) return rc;
-        fmm_p2p<R, K, NQ><<<(unsigned)near.n_obs, 128, smem, st>>>(
-            c, rule, obs_pts, obs_tris, near.obs, near.start, near.src, ot.start, ot.end,
-            stt.start, stt.end, rec, W);
-        if ((rc = launch_status("fmm p2p"))) return rc;
+        if constexpr (p2p_packed<R, K, NQ>()) {
+            const Rule2D<float>& rf = rule;
+            const unsigned pb = (unsigned)((n_src + 127) / 128);
+            const size_t smem = p2p_rh2_smem<NQ>();
+            if ((rc = set_smem(fmm_p2p_rh2<NQ, true>, smem)) ||
+                (rc = set_smem(fmm_p2p_rh2<NQ, false>, smem)))
+                return rc;
+            if (uniform) {
+                far_prep_rh2<NQ, true><<<pb, 128, 0, st>>>(c, rf, (const float*)src_pts,
+                                                            src_tris, n_src, (const float*)in,
+                                                            stt.orig, rec2);
+                if ((rc = launch_status("fmm prep (packed)"))) return rc;
+                fmm_p2p_rh2<NQ, true><<<(unsigned)near.n_obs, 128, smem, st>>>(
+                    rf, (const float*)obs_pts, obs_tris, near.obs, near.start, near.src, ot.start,
+                    ot.end, stt.start, stt.end, rec2, (float*)W);
+            } else {
+                far_prep_rh2<NQ, false><<<pb, 128, 0, st>>>(c, rf, (const float*)src_pts,
+                                                             src_tris, n_src, (const float*)in,
+                                                             stt.orig, rec2);
+                if ((rc = launch_status("fmm prep (packed)"))) return rc;
+                fmm_p2p_rh2<NQ, false><<<(unsigned)near.n_obs, 128, smem, st>>>(
+                    rf, (const float*)obs_pts, obs_tris, near.obs, near.start, near.src, ot.start,
+                    ot.end, stt.start, stt.end, rec2, (float*)W);
+            }
+            if ((rc = launch_status("fmm p2p (packed)"))) return rc;
+        } else {
+            const size_t smem = sizeof(R) * 128 * NA;
+            if ((rc = set_smem(fmm_p2p<R, K, NQ>, smem))) return rc;
+            fmm_p2p<R, K, NQ><<<(unsigned)near.n_obs, 128, smem, st>>>(
+                c, rule, obs_pts, obs_tris, near.obs, near.start, near.src, ot.start, ot.end,
+                stt.start, stt.end, rec, W);
+            if ((rc = launch_status("fmm p2p"))) return rc;
+        }
     }
     if (mode == 0) {
         if (far.n_obs > 0) {
@@ -1150,7 +1385,7 @@ extern "C" size_t tct_fmm_workspace_bytes(int kernel, int prec, int mode, int or
         return 0;
     const Sizes s = sizes_dispatch(kernel, prec, mode, order, n_q, n_obs, n_src, n_obs_nodes,
                                    n_src_nodes);
-    return s.rec + s.mom + s.loc + s.plan + s.W + s.F;
+    return s.rec + s.mom + s.loc + s.plan + s.W + s.F + s.rec2;
 }
 
 extern "C" int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q,
