@@ -37,6 +37,7 @@
 // P2P runs the direct farfield's triangle-level pair loop (far_common.cuh) on
 // the listed leaf pairs, from the same per-source records the P2M reads.
 #include <algorithm>
+#include <vector>
 
 #include "far_common.cuh"
 
@@ -51,14 +52,14 @@ __host__ __device__ constexpr int n_terms(int p) { return (p + 1) * (p + 2) * (p
 __host__ __device__ constexpr int n_terms6(int p) {
     return (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) / 720;
 }
-__device__ __forceinline__ int midx(int a0, int a1, int a2) {
+__host__ __device__ __forceinline__ int midx(int a0, int a1, int a2) {
     const int n = a0 + a1 + a2;
     return n * (n + 1) * (n + 2) / 6 + (n - a0) * (n - a0 + 1) / 2 + a2;
 }
 // position of (a0, ., a2) within level n
 __device__ __forceinline__ int lidx(int n, int a0, int a2) { return (n - a0) * (n - a0 + 1) / 2 + a2; }
 
-__device__ __forceinline__ void decode(int g, int& a0, int& a1, int& a2) {
+__host__ __device__ __forceinline__ void decode(int g, int& a0, int& a1, int& a2) {
     int n = 0;
     while (n_terms(n) <= g) n++;
     int rem = n > 0 ? g - n_terms(n - 1) : 0;
@@ -730,8 +731,415 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 }
 
 // ---- M2L, one CTA per observation node ------------------------------------
-// The same L_b as fmm_m2l, organised for throughput: the CTA keeps its local
-// expansion in registers across its whole M2L list.  Warp 0 is the producer:
+// L_b = 1/b! sum over the node's M2L list of (s_o/rho)^|b| / rho *
+// sum_a f_|a| Dc_(a+b) (N_a with the Yl correction Y_dj - R0_d m_j), |a| + |b|
+// <= p (ts_kernels.cl's m2l restated as a contraction over the pair's Dc
+// tensor).  Organised for throughput:
+//  * warp 0 is the producer: for source node k + 1 it computes rho, f_n,
+//    (s_o/rho)^n / rho and Dc level by level, and scatters Dc into a dense
+//    (p+1)^3 cube, so that Dc_(a+b) = cube[lin(a) + lin(b)] is one indexed
+//    load; every thread copies its share of node k + 1's moments into the
+//    second row buffer with cp.async while node k is contracted;
+//  * each of the 224 contraction lanes owns a fixed tuple of NB consecutive
+//    local terms b (all channels, accumulated in registers across the whole
+//    list) and a contiguous chunk of source terms a, the same chunk for the
+//    tuples that share it, so lanes of a warp mostly read the same source
+//    row (shared-memory broadcasts); pairs with |a| + |b| > p are masked;
+//  * at the end the lanes' partial sums go through shared memory in rounds
+//    and each b sums its chunks in a fixed lane order and scales by 1 / b!.
+// The plan (tuples, chunk length, lane tables) depends only on p and NB.
+constexpr int M2L3_THREADS = 256;
+constexpr int M2L3_LANES = M2L3_THREADS - 32;
+constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
+struct M2LPlan3 {
+    int p, nb, L, n_lanes, n_k;
+    int lane_k[M2L3_LANES];    // tuple of the lane (b = k NB + j), -1 for none
+    int lane_a0[M2L3_LANES];   // first source term (graded) and chunk length
+    int lane_cnt[M2L3_LANES];
+    int warp_steps[M2L3_LANES / 32];
+    int kstart[FMM_NTMAX + 1];  // lanes of tuple k: klane[kstart[k] .. kstart[k + 1])
+    int klane[M2L3_LANES];
+    int ainfo[FMM_NTMAX];      // lin(a) | |a| << 16
+    int clin[FMM_NTMAX];       // lin(c) of graded c
+    alignas(16) int rec[FMM_NTMAX][8];  // Dc recurrence: a0, a1, a2 and the used indices
+};
+
+__host__ __device__ inline int cube_lin(int p, int a0, int a1, int a2) {
+    return (a0 * (p + 1) + a1) * (p + 1) + a2;
+}
+
+// Builds the plan; returns 0, or 1 when the tuples do not fit the lanes.
+// Tuples k = 0 .. ceil(NT / nb) - 1 take the b's k nb .. k nb + nb - 1; tuple
+// k's source range is [0, A_k), A_k = n_terms(p - |k nb|) (its lowest b), cut
+// into chunks of L terms, L the smallest length whose chunks fit the lanes;
+// lanes are dealt chunk-major (every tuple's first chunk, then every second
+// chunk, ...), so the lanes of one chunk index are adjacent.
+__host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
+    const int NT = n_terms(p);
+    const int nk = (NT + nb - 1) / nb;
+    plan->p = p;
+    plan->nb = nb;
+    plan->n_k = nk;
+    auto A = [&](int k) {
+        int b0, b1, b2;
+        decode(k * nb, b0, b1, b2);
+        return n_terms(p - (b0 + b1 + b2));
+    };
+    int total = 0;
+    for (int k = 0; k < nk; k++) total += A(k);
+    int L = (total + M2L3_LANES - 1) / M2L3_LANES;
+    if (L < 1) L = 1;
+    for (;; L++) {
+        int cnt = 0;
+        for (int k = 0; k < nk; k++) cnt += (A(k) + L - 1) / L;
+        if (cnt <= M2L3_LANES) break;
+        if (L > NT) return 1;
+    }
+    plan->L = L;
+    int lane = 0;
+    for (int c = 0;; c++) {
+        bool any = false;
+        for (int k = 0; k < nk; k++) {
+            const int ak = A(k);
+            if (c * L >= ak) continue;
+            plan->lane_k[lane] = k;
+            plan->lane_a0[lane] = c * L;
+            plan->lane_cnt[lane] = (ak - c * L < L) ? ak - c * L : L;
+            lane++;
+            any = true;
+        }
+        if (!any) break;
+    }
+    plan->n_lanes = lane;
+    for (int l = lane; l < M2L3_LANES; l++) {
+        plan->lane_k[l] = -1;
+        plan->lane_a0[l] = 0;
+        plan->lane_cnt[l] = 0;
+    }
+    for (int w = 0; w < M2L3_LANES / 32; w++) {
+        int m = 0;
+        for (int l = 32 * w; l < 32 * w + 32; l++) m = plan->lane_cnt[l] > m ? plan->lane_cnt[l] : m;
+        plan->warp_steps[w] = m;
+    }
+    int pos = 0;
+    for (int k = 0; k < nk; k++) {
+        plan->kstart[k] = pos;
+        for (int l = 0; l < lane; l++)
+            if (plan->lane_k[l] == k) plan->klane[pos++] = l;
+    }
+    plan->kstart[nk] = pos;
+    for (int g = 0; g < NT; g++) {
+        int a0, a1, a2;
+        decode(g, a0, a1, a2);
+        plan->ainfo[g] = cube_lin(p, a0, a1, a2) | ((a0 + a1 + a2) << 16);
+        plan->clin[g] = cube_lin(p, a0, a1, a2);
+        int* r = plan->rec[g];
+        r[0] = a0; r[1] = a1; r[2] = a2;
+        r[3] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
+        r[4] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
+        r[5] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
+        r[6] = a0 > 1 ? midx(a0 - 2, a1, a2) : 0;
+        r[7] = a1 > 1 ? midx(a0, a1 - 2, a2) : 0;  // the a2 - 2 index is recomputed
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(32) fmm_m2l3_plan(int p, int nb, M2LPlan3* __restrict__ plan,
+                                                    int* err) {
+    if (threadIdx.x != 0) return;
+    if (m2l3_make_plan(p, nb, plan)) *err = 1;
+}
+
+// Terms b per lane: the accumulators (NB x NCH values) stay near 64 FP32 or
+// 32 FP64 registers.
+template <typename R, int K>
+struct M2L3Cfg {
+    static constexpr int NCH = Chan<K>::NCH;
+    static constexpr int NB = sizeof(R) == 4 ? (K == kRH ? 3 : 64 / NCH)
+                                             : (32 / NCH > 1 ? 32 / NCH : 1);
+};
+
+// Shared-memory layout (units of R): row buffers 2 x NT x NCHP, cubes 2 x
+// CUBEP (these two double as the reduction area, at least 32 lanes' slots),
+// graded Dc scratch NTP, 2 x 40 scalars, 4 x M2L3_CAP pair geometry, then
+// ainfo (NTP ints) and M2L3_CAP source node ids.
+constexpr int M2L3_CAP = 512;  // pairs whose source node and geometry are staged
+struct M2L3Smem {
+    int NT, NTP, CUBE, CUBEP, area, dg, sb, pg, ai, total_bytes;
+};
+template <typename R, int K>
+__host__ __device__ inline M2L3Smem m2l3_smem(int p) {
+    using C = Chan<K>;
+    M2L3Smem m;
+    m.NT = n_terms(p);
+    m.NTP = (m.NT + 3) / 4 * 4;
+    m.CUBE = (p + 1) * (p + 1) * (p + 1);
+    m.CUBEP = (m.CUBE + 3) / 4 * 4;
+    const int need = 2 * m.NT * C::NCHP + 2 * m.CUBEP;
+    const int slots32 = 32 * M2L3Cfg<R, K>::NB * C::NCH;
+    m.area = need > slots32 ? need : (slots32 + 3) / 4 * 4;
+    m.dg = m.area;
+    m.sb = m.dg + m.NTP;
+    m.pg = m.sb + 80;
+    m.ai = m.pg + 4 * M2L3_CAP;
+    m.total_bytes = (int)(sizeof(R) * m.ai + sizeof(int) * (m.NTP + M2L3_CAP));
+    return m;
+}
+
+
+template <typename R, int K>
+__global__ void __launch_bounds__(M2L3_THREADS, 2)
+fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
+         const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
+         const R* __restrict__ ocent, const R* __restrict__ orad, const R* __restrict__ scent,
+         const R* __restrict__ srad, const R* __restrict__ mom, const M2LPlan3* __restrict__ plan,
+         R* __restrict__ loc) {
+    using C = Chan<K>;
+    constexpr int NB = M2L3Cfg<R, K>::NB;
+    constexpr int NCH = C::NCH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const M2L3Smem sm = m2l3_smem<R, K>(p);
+    const int NT = sm.NT;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t oi = blockIdx.x;
+    if (oi >= n_obs_nodes) return;
+    const int rowsz = NT * C::NCHP;
+    R* base = reinterpret_cast<R*>(smem_raw);
+    R* Nb = base;                    // 2 x NT x NCHP source rows
+    R* Cb = base + 2 * rowsz;        // 2 x CUBEP Dc cubes
+    R* Dg = base + sm.dg;            // graded Dc (producer scratch)
+    R* Sb = base + sm.sb;            // 2 x 40: f_n [0, 16), pw_n [16, 32), R0 [32, 35)
+    R* pgeo = base + sm.pg;          // first M2L3_CAP pairs: source center and radius
+    int* ainfo = reinterpret_cast<int*>(base + sm.ai);
+    int* psrc = ainfo + sm.NTP;      // first M2L3_CAP pairs: source node
+    for (int g = tid; g < NT; g += M2L3_THREADS) ainfo[g] = plan->ainfo[g];
+
+    const int64_t node = obs_nodes[oi];
+    const R co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
+    const R so = orad[node];
+    const int64_t l0 = starts[oi], l1 = starts[oi + 1];
+    const int64_t npair = l1 - l0;
+    // the list's source nodes and geometry, staged once (the pipeline below
+    // would otherwise wait on dependent global loads every pair)
+    for (int64_t i = tid; i < npair && i < M2L3_CAP; i += M2L3_THREADS) {
+        const int64_t sn = srcs[l0 + i];
+        psrc[i] = (int)sn;
+        pgeo[4 * i] = scent[3 * sn];
+        pgeo[4 * i + 1] = scent[3 * sn + 1];
+        pgeo[4 * i + 2] = scent[3 * sn + 2];
+        pgeo[4 * i + 3] = srad[sn];
+    }
+    __syncthreads();
+
+    auto issue_copy = [&](int64_t l, int buf) {
+        const int64_t sn = l - l0 < M2L3_CAP ? (int64_t)psrc[l - l0] : srcs[l];
+        const R* src = mom + sn * (int64_t)rowsz;
+        R* dst = Nb + buf * rowsz;
+        constexpr int PER = 16 / sizeof(R);
+        for (int k = tid; k < rowsz / PER; k += M2L3_THREADS)
+            cp_async16(dst + k * PER, src + k * PER);
+        cp_async_commit();
+    };
+    auto produce = [&](int64_t l, int buf) {  // warp 0
+        R cs[3], rs;
+        if (l - l0 < M2L3_CAP) {
+            const R* g = pgeo + 4 * (l - l0);
+            cs[0] = g[0]; cs[1] = g[1]; cs[2] = g[2]; rs = g[3];
+        } else {
+            const int64_t sn = srcs[l];
+            cs[0] = scent[3 * sn]; cs[1] = scent[3 * sn + 1]; cs[2] = scent[3 * sn + 2];
+            rs = srad[sn];
+        }
+        const R R0[3] = {co[0] - cs[0], co[1] - cs[1], co[2] - cs[2]};
+        const R rho = sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
+        const R inv_rho = R(1) / rho;
+        const R Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
+        R* S = Sb + buf * 40;
+        R* Dc = Cb + buf * sm.CUBEP;
+        if (lane <= p) {
+            S[lane] = ((lane & 1) ? R(-1) : R(1)) * ipow(rs * inv_rho, lane);
+            S[16 + lane] = ipow(so * inv_rho, lane) * inv_rho;
+        }
+        if (lane < 3) S[32 + lane] = R0[lane];
+        if (lane == 0) {
+            Dg[0] = 1;
+            Dc[0] = 1;
+        }
+        __syncwarp();
+        // level n from levels n - 1 and n - 2; a lane takes entries lane and
+        // lane + 32 of the level, loads first so both chains overlap
+        for (int n = 1; n <= p; n++) {
+            const int lsz = (n + 1) * (n + 2) / 2, b0 = n_terms(n - 1);
+            const R cA = -(R)(2 * n - 1) / (R)n, cB = -(R)(n - 1) / (R)n;
+            R v[2];
+            int dst[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int w = lane + 32 * h;
+                dst[h] = -1;
+                v[h] = 0;
+                if (w >= lsz) continue;
+                const int4 r0 = *reinterpret_cast<const int4*>(plan->rec[b0 + w]);
+                const int4 r1 = *reinterpret_cast<const int4*>(plan->rec[b0 + w] + 4);
+                const int a0 = r0.x, a1 = r0.y, a2 = r0.z;
+                const R d3 = a0 > 0 ? Dg[r0.w] : R(0), d4 = a1 > 0 ? Dg[r1.x] : R(0);
+                const R d5 = a2 > 0 ? Dg[r1.y] : R(0), d6 = a0 > 1 ? Dg[r1.z] : R(0);
+                const R d7 = a1 > 1 ? Dg[r1.w] : R(0);
+                const R d8 = a2 > 1 ? Dg[midx(a0, a1, a2 - 2)] : R(0);
+                const R s1 = Rh[0] * (R)a0 * d3 + Rh[1] * (R)a1 * d4 + Rh[2] * (R)a2 * d5;
+                const R s2 = (R)(a0 * (a0 - 1)) * d6 + (R)(a1 * (a1 - 1)) * d7 +
+                             (R)(a2 * (a2 - 1)) * d8;
+                v[h] = cA * s1 + cB * s2;
+                dst[h] = b0 + w;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (dst[h] >= 0) {
+                    Dg[dst[h]] = v[h];
+                    Dc[plan->clin[dst[h]]] = v[h];
+                }
+            __syncwarp();
+        }
+    };
+
+    // this lane's tuple and source chunk
+    const int ct = tid - 32;
+    int kk = -1, a_first = 0, cnt = 0, wsteps = 0;
+    int blin[NB], nbl[NB];
+    if (warp > 0) {
+        kk = plan->lane_k[ct];
+        a_first = plan->lane_a0[ct];
+        cnt = plan->lane_cnt[ct];
+        wsteps = plan->warp_steps[warp - 1];
+    }
+#pragma unroll
+    for (int j = 0; j < NB; j++) {
+        const int b = kk * NB + j;
+        if (kk >= 0 && b < NT) {
+            int b0, b1, b2;
+            decode(b, b0, b1, b2);
+            blin[j] = cube_lin(p, b0, b1, b2);
+            nbl[j] = b0 + b1 + b2;
+        } else {
+            blin[j] = 0;
+            nbl[j] = p + 1;  // never valid
+        }
+    }
+    R acc[NB][NCH];
+#pragma unroll
+    for (int j = 0; j < NB; j++)
+#pragma unroll
+        for (int c = 0; c < NCH; c++) acc[j][c] = 0;
+
+    if (npair > 0) {
+        issue_copy(l0, 0);
+        if (warp == 0) produce(l0, 0);
+    }
+    for (int64_t k = 0; k < npair; k++) {
+        const int buf = (int)(k & 1);
+        cp_async_wait_all();
+        __syncthreads();  // pair k's rows, cube and scalars are complete; pair k - 1 is done
+        if (k + 1 < npair) {
+            issue_copy(l0 + k + 1, buf ^ 1);
+            if (warp == 0) produce(l0 + k + 1, buf ^ 1);
+        }
+        if (warp == 0) continue;
+        const R* S = Sb + buf * 40;
+        const R* Dc = Cb + buf * sm.CUBEP;
+        const R* N = Nb + buf * rowsz;
+        const R R0[3] = {S[32], S[33], S[34]};
+        R pw[NB];
+#pragma unroll
+        for (int j = 0; j < NB; j++) pw[j] = nbl[j] <= p ? S[16 + nbl[j]] : R(0);
+#pragma unroll 1
+        for (int s = 0; s < wsteps; s++) {
+            const bool on = s < cnt;
+            const int a = a_first + (on ? s : 0);
+            const int e = ainfo[a];
+            const int alin = e & 0xffff, la = e >> 16;
+            const R fa = on ? S[la] : R(0);
+            R cf[NB];
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+                const int ci = min(alin + blin[j], sm.CUBE - 1);
+                const R dv = Dc[ci];
+                cf[j] = (la + nbl[j] <= p) ? dv * (fa * pw[j]) : R(0);
+            }
+            const R* row = N + a * C::NCHP;
+            R v[C::NCHP];
+            if (sizeof(R) == 4) {
+#pragma unroll
+                for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
+                    const float4 q = reinterpret_cast<const float4*>(row)[k4];
+                    v[4 * k4] = (R)q.x; v[4 * k4 + 1] = (R)q.y;
+                    v[4 * k4 + 2] = (R)q.z; v[4 * k4 + 3] = (R)q.w;
+                }
+            } else {
+#pragma unroll
+                for (int k2 = 0; k2 < C::NCHP / 2; k2++) {
+                    const double2 q = reinterpret_cast<const double2*>(row)[k2];
+                    v[2 * k2] = (R)q.x; v[2 * k2 + 1] = (R)q.y;
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int j = 0; j < C::J; j++)
+                    v[C::CH_Y + d * C::J + j] -= R0[d] * v[C::CH_M + j];
+#pragma unroll
+            for (int j = 0; j < NB; j++)
+#pragma unroll
+                for (int c = 0; c < NCH; c++) acc[j][c] += cf[j] * v[c];
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // reduction in rounds through the row/cube area
+    constexpr int PER = NB * NCH;
+    const int lpr = sm.area / PER;
+    R* Lg = loc + node * (int64_t)rowsz;
+    for (int lo = 0; lo < M2L3_LANES; lo += lpr) {
+        const int hi = lo + lpr < M2L3_LANES ? lo + lpr : M2L3_LANES;
+        if (warp > 0 && ct >= lo && ct < hi) {
+            R* sl = base + (ct - lo) * PER;
+#pragma unroll
+            for (int j = 0; j < NB; j++)
+#pragma unroll
+                for (int c = 0; c < NCH; c++) sl[j * NCH + c] = acc[j][c];
+        }
+        __syncthreads();
+        for (int b = tid; b < NT; b += M2L3_THREADS) {
+            const int k = b / NB, j = b - k * NB;
+            R sum[NCH];
+#pragma unroll
+            for (int c = 0; c < NCH; c++) sum[c] = 0;
+            for (int i = plan->kstart[k]; i < plan->kstart[k + 1]; i++) {
+                const int l = plan->klane[i];
+                if (l < lo || l >= hi) continue;
+                const R* sl = base + (l - lo) * PER + j * NCH;
+#pragma unroll
+                for (int c = 0; c < NCH; c++) sum[c] += sl[c];
+            }
+            int b0, b1, b2;
+            decode(b, b0, b1, b2);
+            const R inv = R(1) / mfact<R>(b0, b1, b2);
+            R* out = Lg + b * C::NCHP;
+            if (lo == 0) {
+#pragma unroll
+                for (int c = 0; c < C::NCHP; c++) out[c] = c < NCH ? sum[c] * inv : R(0);
+            } else {
+#pragma unroll
+                for (int c = 0; c < NCH; c++) out[c] += sum[c] * inv;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+// ---- M2L, item form (FP64, and FP32 when the lane plan does not fit) -------
+// The same L_b as fmm_m2l3 above.  Warp 0 is the producer:
 // for source node k + 1 it computes rho, f_n, (s_o/rho)^n / rho and Dc level
 // by level into the second of two shared-memory buffers, while the other
 // seven warps contract source node k; every thread copies its share of node
@@ -748,7 +1156,6 @@ constexpr int M2L2_THREADS = 256;
 constexpr int M2L2_TC = M2L2_THREADS - 32;  // contraction threads
 constexpr int M2L2_MAXIT = 3;
 constexpr int M2L2_MAXITEMS = M2L2_TC * M2L2_MAXIT;
-constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
 struct M2LPlan2 {
     int n_items;
     int item[M2L2_MAXITEMS][8];   // b, g0, g1, a0, a2, |a| at g0, b0, b2
@@ -1180,6 +1587,10 @@ struct Sizes {
     size_t rec, mom, loc, plan, W, F, rec2;
 };
 
+inline size_t m2l_plan_bytes() {
+    return sizeof(M2LPlan2) > sizeof(M2LPlan3) ? sizeof(M2LPlan2) : sizeof(M2LPlan3);
+}
+
 // The packed P2P runs for elasticRH3 in FP32 with the 3-, 4- and 7-point rules.
 template <typename R, int K, int NQ>
 constexpr bool p2p_packed() {
@@ -1194,7 +1605,7 @@ Sizes sizes_for(size_t rs, int mode, int order, int64_t n_obs, int64_t n_src, in
     s.rec = al256(rs * Rec<K, NQ>::LEN * (size_t)n_src);
     s.mom = al256(rs * C::NCHP * (size_t)n_terms(order) * n_src_nodes);
     s.loc = mode == 1 ? al256(rs * C::NCHP * (size_t)n_terms(order) * n_obs_nodes) : 0;
-    s.plan = mode == 1 ? al256(sizeof(M2LPlan2) + 256) : 0;
+    s.plan = mode == 1 ? al256(m2l_plan_bytes()) + 256 : 0;
     s.W = al256(rs * NAcc<K, NQ>::n * (size_t)n_obs);
     s.F = al256(rs * C::NO * (size_t)NQ * n_obs);
     s.rec2 = (rs == 4 && K == kRH && (NQ == 3 || NQ == 4 || NQ == 7))
@@ -1332,21 +1743,38 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, st>>>(
                 p, C::NCHP, stt.n_nodes, mom);
             if ((rc = launch_status("fmm moment factorials"))) return rc;
-            if (m2l2_items(p) > M2L2_MAXITEMS) {
-                set_error("tct_fmm_matvec: FMM order %d exceeds the M2L plan's capacity", p);
-                return TCT_ERR_ARG;
+            bool lanes = sizeof(R) == 4;  // the lane plan (fmm_m2l3) for FP32
+            if (lanes) {
+                M2LPlan3 host_plan;
+                lanes = m2l3_make_plan(p, M2L3Cfg<R, K>::NB, &host_plan) == 0 &&
+                        m2l3_smem<R, K>(p).total_bytes <= 227 * 1024;
             }
-            M2LPlan2* plan2 = reinterpret_cast<M2LPlan2*>(plan);
-            int* plan_err = reinterpret_cast<int*>(plan + al256(sizeof(M2LPlan2)));
-            fmm_m2l2_plan<<<1, 32, 0, st>>>(p, plan2, plan_err);
-            if ((rc = launch_status("fmm m2l plan"))) return rc;
-            const size_t smem_all = sizeof(R) * (2 * (size_t)NT * C::NCHP +
-                                                 2 * (size_t)((NT + 3) / 4 * 4) + 80 +
-                                                 (size_t)m2l2_items(p) * C::NCHP);
-            if ((rc = set_smem(fmm_m2l2<R, K>, smem_all))) return rc;
-            fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, st>>>(
-                p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom, plan2,
-                loc);
+            int* plan_err = reinterpret_cast<int*>(plan + al256(m2l_plan_bytes()));
+            if (lanes) {
+                M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
+                fmm_m2l3_plan<<<1, 32, 0, st>>>(p, M2L3Cfg<R, K>::NB, plan3, plan_err);
+                if ((rc = launch_status("fmm m2l plan"))) return rc;
+                const size_t smem_all = (size_t)m2l3_smem<R, K>(p).total_bytes;
+                if ((rc = set_smem(fmm_m2l3<R, K>, smem_all))) return rc;
+                fmm_m2l3<R, K><<<(unsigned)far.n_obs, M2L3_THREADS, smem_all, st>>>(
+                    p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
+                    plan3, loc);
+            } else {
+                if (m2l2_items(p) > M2L2_MAXITEMS) {
+                    set_error("tct_fmm_matvec: FMM order %d exceeds the M2L plan's capacity", p);
+                    return TCT_ERR_ARG;
+                }
+                M2LPlan2* plan2 = reinterpret_cast<M2LPlan2*>(plan);
+                fmm_m2l2_plan<<<1, 32, 0, st>>>(p, plan2, plan_err);
+                if ((rc = launch_status("fmm m2l plan"))) return rc;
+                const size_t smem_all = sizeof(R) * (2 * (size_t)NT * C::NCHP +
+                                                     2 * (size_t)((NT + 3) / 4 * 4) + 80 +
+                                                     (size_t)m2l2_items(p) * C::NCHP);
+                if ((rc = set_smem(fmm_m2l2<R, K>, smem_all))) return rc;
+                fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, st>>>(
+                    p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
+                    plan2, loc);
+            }
             if ((rc = launch_status("fmm m2l"))) return rc;
         }
         const size_t smem_l2l =
@@ -1457,3 +1885,53 @@ extern "C" int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q
     set_error("tct_fmm_matvec: unsupported kernel %d / n_q %d", kernel, n_q);
     return TCT_ERR_ARG;
 }
+
+// Host-side check of the M2L work plan for order p and nb terms b per lane:
+// out[0] = valid (a, b) pairs covered, out[1] = pairs covered more than once
+// or invalid and unmasked, out[2] = the chunk length L, out[3] = lanes used,
+// out[4] = the sum over warps of their step counts.  Returns 0, or 1 when the
+// plan does not fit.
+extern "C" int tct_fmm_m2l_plan_stats(int order, int nb, int64_t* out) {
+    if (order < 0 || order > FMM_MAXP || nb < 1 || !out) return TCT_ERR_ARG;
+    M2LPlan3* plan = new M2LPlan3();
+    const int rc = m2l3_make_plan(order, nb, plan);
+    if (rc) {
+        delete plan;
+        return 1;
+    }
+    const int NT = n_terms(order);
+    std::vector<int> seen((size_t)NT * NT, 0);
+    int64_t covered = 0, bad = 0;
+    for (int l = 0; l < M2L3_LANES; l++) {
+        const int k = plan->lane_k[l];
+        if (k < 0) continue;
+        for (int s = 0; s < plan->lane_cnt[l]; s++) {
+            const int a = plan->lane_a0[l] + s;
+            const int la = plan->ainfo[a] >> 16;
+            for (int j = 0; j < nb; j++) {
+                const int b = k * nb + j;
+                if (b >= NT) continue;
+                int b0, b1, b2;
+                decode(b, b0, b1, b2);
+                if (la + b0 + b1 + b2 > order) continue;  // masked in the kernel
+                if (seen[(size_t)a * NT + b]++) bad++;
+                else covered++;
+            }
+        }
+    }
+    // a lane's steps may not exceed its warp's count
+    int64_t steps = 0;
+    for (int w = 0; w < M2L3_LANES / 32; w++) {
+        steps += plan->warp_steps[w];
+        for (int l = 32 * w; l < 32 * w + 32; l++)
+            if (plan->lane_cnt[l] > plan->warp_steps[w]) bad++;
+    }
+    out[0] = covered;
+    out[1] = bad;
+    out[2] = plan->L;
+    out[3] = plan->n_lanes;
+    out[4] = steps;
+    delete plan;
+    return 0;
+}
+

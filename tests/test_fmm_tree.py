@@ -117,43 +117,23 @@ def test_fmm_abi_rejects_bad_arguments():
     assert ws(6, 1, 1, 8, 3, 10, 10, 5, 5) > ws(6, 1, 0, 8, 3, 10, 10, 5, 5)  # locals
 
 
-def _m2l_plan(p, maxi=32, slots=32):
-    """Python mirror of fmm_m2l_plan (csrc/fmm.cu): chunking of the M2L
-    contraction over 32 lanes."""
-    nt = lambda q: (q + 1) * (q + 2) * (q + 3) // 6 if q >= 0 else 0
-
-    def level(b):
-        n = 0
-        while nt(n) <= b:
-            n += 1
-        return n
-
-    total = (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) // 720
-    CH = -(-total // 32)
-    load, cnt = [0] * 32, [0] * 32
-    slot, cover = 0, {}
-    for b in range(nt(p)):
-        t = nt(p - level(b))
-        nch = -(-t // CH)
-        split = nch > 1 and slot + nch <= slots
-        step = CH if split else t
-        g0 = 0
-        while g0 < t:
-            g1 = min(t, g0 + step)
-            lane = min(range(32), key=lambda i: ((load[i] << 5) | i))
-            cnt[lane] += 1
-            load[lane] += g1 - g0
-            cover[b] = cover.get(b, 0) + (g1 - g0)
-            g0 = g1
-        if split:
-            slot += nch
-    return cnt, load, slot, cover, total, CH
-
-
+@pytest.mark.parametrize("nb", [1, 2, 3, 4, 6, 9])
 @pytest.mark.parametrize("p", range(13))
-def test_m2l_plan_fits_tables(p):
-    cnt, load, slots, cover, total, CH = _m2l_plan(p)
-    assert max(cnt) <= 32 and slots <= 32
-    assert sum(load) == total and sum(cover.values()) == total  # every (a, b) pair once
-    if p >= 6:
-        assert max(load) <= CH + 1  # balanced to within one iteration
+def test_m2l_plan_covers_every_pair(p, nb):
+    """The M2L work plan (csrc/fmm.cu m2l3_make_plan, built on the host here)
+    covers every (a, b) with |a| + |b| <= p exactly once, within the lanes.
+    FP32 uses nb = 3 (elasticRH3), 4 (RA), 6 (RT) or 9 (U) terms per lane."""
+    import ctypes
+    from tectosaur_b200 import _lib
+    out = (ctypes.c_int64 * 5)()
+    rc = _lib.lib.tct_fmm_m2l_plan_stats(p, nb, out)
+    nt = (p + 1) * (p + 2) * (p + 3) // 6
+    if nb < 3 and -(-nt // nb) > 224 - 10:
+        return  # more tuples than lanes: the item form runs instead (rc may be 0 or 1)
+    assert rc == 0  # every FP32 configuration (nb >= 3) fits
+    covered, bad, L, lanes, steps = list(out)
+    total = (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) // 720
+    assert covered == total and bad == 0
+    assert 1 <= lanes <= 224
+    if p == 8 and nb == 3:
+        assert L == 6 and lanes == 209  # 1089 lane steps of 6 or fewer
