@@ -760,8 +760,9 @@ struct M2LPlan3 {
     int kstart[FMM_NTMAX + 1];  // lanes of tuple k: klane[kstart[k] .. kstart[k + 1])
     int klane[M2L3_LANES];
     int ainfo[FMM_NTMAX];      // lin(a) | |a| << 16
-    int clin[FMM_NTMAX];       // lin(c) of graded c
-    alignas(16) int rec[FMM_NTMAX][8];  // Dc recurrence: a0, a1, a2 and the used indices
+    // Dc recurrence per graded c: a0 | a1 << 8 | a2 << 16, the graded indices
+    // of c - e_0, c - e_1, c - e_2, c - 2 e_0, c - 2 e_1, c - 2 e_2, lin(c)
+    alignas(16) int rec[FMM_NTMAX][8];
 };
 
 __host__ __device__ inline int cube_lin(int p, int a0, int a1, int a2) {
@@ -832,14 +833,15 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
         int a0, a1, a2;
         decode(g, a0, a1, a2);
         plan->ainfo[g] = cube_lin(p, a0, a1, a2) | ((a0 + a1 + a2) << 16);
-        plan->clin[g] = cube_lin(p, a0, a1, a2);
         int* r = plan->rec[g];
-        r[0] = a0; r[1] = a1; r[2] = a2;
-        r[3] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
-        r[4] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
-        r[5] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
-        r[6] = a0 > 1 ? midx(a0 - 2, a1, a2) : 0;
-        r[7] = a1 > 1 ? midx(a0, a1 - 2, a2) : 0;  // the a2 - 2 index is recomputed
+        r[0] = a0 | (a1 << 8) | (a2 << 16);
+        r[1] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
+        r[2] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
+        r[3] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
+        r[4] = a0 > 1 ? midx(a0 - 2, a1, a2) : 0;
+        r[5] = a1 > 1 ? midx(a0, a1 - 2, a2) : 0;
+        r[6] = a2 > 1 ? midx(a0, a1, a2 - 2) : 0;
+        r[7] = cube_lin(p, a0, a1, a2);
     }
     return 0;
 }
@@ -850,73 +852,73 @@ __global__ void __launch_bounds__(32) fmm_m2l3_plan(int p, int nb, M2LPlan3* __r
     if (m2l3_make_plan(p, nb, plan)) *err = 1;
 }
 
-// Terms b per lane: the accumulators (NB x NCH values) stay near 64 FP32 or
-// 32 FP64 registers.
-template <typename R, int K>
+// Terms b per lane (FP32): the accumulators (NB x NCH values) stay near 64
+// registers.
+template <int K>
 struct M2L3Cfg {
     static constexpr int NCH = Chan<K>::NCH;
-    static constexpr int NB = sizeof(R) == 4 ? (K == kRH ? 3 : 64 / NCH)
-                                             : (32 / NCH > 1 ? 32 / NCH : 1);
+    static constexpr int NB = K == kRH ? 3 : 64 / NCH;
 };
 
-// Shared-memory layout (units of R): row buffers 2 x NT x NCHP, cubes 2 x
-// CUBEP (these two double as the reduction area, at least 32 lanes' slots),
-// graded Dc scratch NTP, 2 x 40 scalars, 4 x M2L3_CAP pair geometry, then
-// ainfo (NTP ints) and M2L3_CAP source node ids.
+// Shared-memory layout (floats): row buffers 2 x NT x NCHP, cubes 2 x CUBEP
+// (CUBEP >= 2 (p+1)^3, so lin(a) + lin(b) needs no clamp; these two regions
+// double as the reduction area, at least 32 lanes' slots), graded Dc scratch
+// NTP, 2 x 40 scalars, 4 x M2L3_CAP pair geometry, then ainfo (NTP ints) and
+// M2L3_CAP source node ids.
 constexpr int M2L3_CAP = 512;  // pairs whose source node and geometry are staged
 struct M2L3Smem {
-    int NT, NTP, CUBE, CUBEP, area, dg, sb, pg, ai, total_bytes;
+    int NT, NTP, CUBEP, area, dg, sb, pg, ai, total_bytes;
 };
-template <typename R, int K>
+template <int K>
 __host__ __device__ inline M2L3Smem m2l3_smem(int p) {
     using C = Chan<K>;
     M2L3Smem m;
     m.NT = n_terms(p);
     m.NTP = (m.NT + 3) / 4 * 4;
-    m.CUBE = (p + 1) * (p + 1) * (p + 1);
-    m.CUBEP = (m.CUBE + 3) / 4 * 4;
+    m.CUBEP = (2 * (p + 1) * (p + 1) * (p + 1) + 3) / 4 * 4;
     const int need = 2 * m.NT * C::NCHP + 2 * m.CUBEP;
-    const int slots32 = 32 * M2L3Cfg<R, K>::NB * C::NCH;
+    const int slots32 = 32 * M2L3Cfg<K>::NB * C::NCH;
     m.area = need > slots32 ? need : (slots32 + 3) / 4 * 4;
     m.dg = m.area;
     m.sb = m.dg + m.NTP;
     m.pg = m.sb + 80;
     m.ai = m.pg + 4 * M2L3_CAP;
-    m.total_bytes = (int)(sizeof(R) * m.ai + sizeof(int) * (m.NTP + M2L3_CAP));
+    m.total_bytes = (int)(sizeof(float) * m.ai + sizeof(int) * (m.NTP + M2L3_CAP));
     return m;
 }
 
-
-template <typename R, int K>
+template <int K>
 __global__ void __launch_bounds__(M2L3_THREADS, 2)
 fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
          const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
-         const R* __restrict__ ocent, const R* __restrict__ orad, const R* __restrict__ scent,
-         const R* __restrict__ srad, const R* __restrict__ mom, const M2LPlan3* __restrict__ plan,
-         R* __restrict__ loc) {
+         const float* __restrict__ ocent, const float* __restrict__ orad,
+         const float* __restrict__ scent, const float* __restrict__ srad,
+         const float* __restrict__ mom, const M2LPlan3* __restrict__ plan,
+         float* __restrict__ loc) {
     using C = Chan<K>;
-    constexpr int NB = M2L3Cfg<R, K>::NB;
+    constexpr int NB = M2L3Cfg<K>::NB;
     constexpr int NCH = C::NCH;
+    constexpr int NP = (NCH + 1) / 2;  // channel pairs (f32x2)
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const M2L3Smem sm = m2l3_smem<R, K>(p);
+    const M2L3Smem sm = m2l3_smem<K>(p);
     const int NT = sm.NT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t oi = blockIdx.x;
     if (oi >= n_obs_nodes) return;
     const int rowsz = NT * C::NCHP;
-    R* base = reinterpret_cast<R*>(smem_raw);
-    R* Nb = base;                    // 2 x NT x NCHP source rows
-    R* Cb = base + 2 * rowsz;        // 2 x CUBEP Dc cubes
-    R* Dg = base + sm.dg;            // graded Dc (producer scratch)
-    R* Sb = base + sm.sb;            // 2 x 40: f_n [0, 16), pw_n [16, 32), R0 [32, 35)
-    R* pgeo = base + sm.pg;          // first M2L3_CAP pairs: source center and radius
+    float* base = reinterpret_cast<float*>(smem_raw);
+    float* Nb = base;                 // 2 x NT x NCHP source rows
+    float* Cb = base + 2 * rowsz;     // 2 x CUBEP scaled Dc cubes
+    float* Dg = base + sm.dg;         // graded Dc (producer scratch)
+    float* Sb = base + sm.sb;         // 2 x 40: (-s_s/s_o)^n [0, 16), R0 [32, 35)
+    float* pgeo = base + sm.pg;       // first M2L3_CAP pairs: source center and radius
     int* ainfo = reinterpret_cast<int*>(base + sm.ai);
-    int* psrc = ainfo + sm.NTP;      // first M2L3_CAP pairs: source node
+    int* psrc = ainfo + sm.NTP;       // first M2L3_CAP pairs: source node
     for (int g = tid; g < NT; g += M2L3_THREADS) ainfo[g] = plan->ainfo[g];
 
     const int64_t node = obs_nodes[oi];
-    const R co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
-    const R so = orad[node];
+    const float co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
+    const float so = orad[node];
     const int64_t l0 = starts[oi], l1 = starts[oi + 1];
     const int64_t npair = l1 - l0;
     // the list's source nodes and geometry, staged once (the pipeline below
@@ -933,70 +935,72 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
 
     auto issue_copy = [&](int64_t l, int buf) {
         const int64_t sn = l - l0 < M2L3_CAP ? (int64_t)psrc[l - l0] : srcs[l];
-        const R* src = mom + sn * (int64_t)rowsz;
-        R* dst = Nb + buf * rowsz;
-        constexpr int PER = 16 / sizeof(R);
-        for (int k = tid; k < rowsz / PER; k += M2L3_THREADS)
-            cp_async16(dst + k * PER, src + k * PER);
+        const float* src = mom + sn * (int64_t)rowsz;
+        float* dst = Nb + buf * rowsz;
+        for (int k = tid; k < rowsz / 4; k += M2L3_THREADS) cp_async16(dst + k * 4, src + k * 4);
         cp_async_commit();
     };
+    // coef(a, b) = f_|a| (s_o/rho)^|b| / rho Dc_(a+b) = S_|a| Dh_(a+b) with
+    // Dh_c = Dc_c (s_o/rho)^|c| / rho (the cube) and S_n = (-s_s/s_o)^n
     auto produce = [&](int64_t l, int buf) {  // warp 0
-        R cs[3], rs;
+        float cs[3], rs;
         if (l - l0 < M2L3_CAP) {
-            const R* g = pgeo + 4 * (l - l0);
+            const float* g = pgeo + 4 * (l - l0);
             cs[0] = g[0]; cs[1] = g[1]; cs[2] = g[2]; rs = g[3];
         } else {
             const int64_t sn = srcs[l];
             cs[0] = scent[3 * sn]; cs[1] = scent[3 * sn + 1]; cs[2] = scent[3 * sn + 2];
             rs = srad[sn];
         }
-        const R R0[3] = {co[0] - cs[0], co[1] - cs[1], co[2] - cs[2]};
-        const R rho = sqrt(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
-        const R inv_rho = R(1) / rho;
-        const R Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
-        R* S = Sb + buf * 40;
-        R* Dc = Cb + buf * sm.CUBEP;
-        if (lane <= p) {
-            S[lane] = ((lane & 1) ? R(-1) : R(1)) * ipow(rs * inv_rho, lane);
-            S[16 + lane] = ipow(so * inv_rho, lane) * inv_rho;
-        }
+        const float R0[3] = {co[0] - cs[0], co[1] - cs[1], co[2] - cs[2]};
+        const float rho = sqrtf(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
+        const float inv_rho = 1.f / rho;
+        const float Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
+        const float q = so * inv_rho;  // pw_n = q^n / rho
+        float* S = Sb + buf * 40;
+        float* Dc = Cb + buf * sm.CUBEP;
+        if (lane <= p) S[lane] = ipow(-rs / so, lane);
         if (lane < 3) S[32 + lane] = R0[lane];
         if (lane == 0) {
-            Dg[0] = 1;
-            Dc[0] = 1;
+            Dg[0] = 1.f;
+            Dc[0] = inv_rho;
         }
         __syncwarp();
         // level n from levels n - 1 and n - 2; a lane takes entries lane and
         // lane + 32 of the level, loads first so both chains overlap
+        float pwn = inv_rho;
         for (int n = 1; n <= p; n++) {
+            pwn *= q;
             const int lsz = (n + 1) * (n + 2) / 2, b0 = n_terms(n - 1);
-            const R cA = -(R)(2 * n - 1) / (R)n, cB = -(R)(n - 1) / (R)n;
-            R v[2];
-            int dst[2];
+            const float cA = -(float)(2 * n - 1) / (float)n, cB = -(float)(n - 1) / (float)n;
+            float v[2];
+            int dst[2], cl[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int w = lane + 32 * h;
                 dst[h] = -1;
-                v[h] = 0;
+                cl[h] = 0;
+                v[h] = 0.f;
                 if (w >= lsz) continue;
                 const int4 r0 = *reinterpret_cast<const int4*>(plan->rec[b0 + w]);
                 const int4 r1 = *reinterpret_cast<const int4*>(plan->rec[b0 + w] + 4);
-                const int a0 = r0.x, a1 = r0.y, a2 = r0.z;
-                const R d3 = a0 > 0 ? Dg[r0.w] : R(0), d4 = a1 > 0 ? Dg[r1.x] : R(0);
-                const R d5 = a2 > 0 ? Dg[r1.y] : R(0), d6 = a0 > 1 ? Dg[r1.z] : R(0);
-                const R d7 = a1 > 1 ? Dg[r1.w] : R(0);
-                const R d8 = a2 > 1 ? Dg[midx(a0, a1, a2 - 2)] : R(0);
-                const R s1 = Rh[0] * (R)a0 * d3 + Rh[1] * (R)a1 * d4 + Rh[2] * (R)a2 * d5;
-                const R s2 = (R)(a0 * (a0 - 1)) * d6 + (R)(a1 * (a1 - 1)) * d7 +
-                             (R)(a2 * (a2 - 1)) * d8;
+                const int a0 = r0.x & 0xff, a1 = (r0.x >> 8) & 0xff, a2 = r0.x >> 16;
+                const float d1 = a0 > 0 ? Dg[r0.y] : 0.f, d2 = a1 > 0 ? Dg[r0.z] : 0.f;
+                const float d3 = a2 > 0 ? Dg[r0.w] : 0.f, d4 = a0 > 1 ? Dg[r1.x] : 0.f;
+                const float d5 = a1 > 1 ? Dg[r1.y] : 0.f, d6 = a2 > 1 ? Dg[r1.z] : 0.f;
+                const float s1 = Rh[0] * (float)a0 * d1 + Rh[1] * (float)a1 * d2 +
+                                 Rh[2] * (float)a2 * d3;
+                const float s2 = (float)(a0 * (a0 - 1)) * d4 + (float)(a1 * (a1 - 1)) * d5 +
+                                 (float)(a2 * (a2 - 1)) * d6;
                 v[h] = cA * s1 + cB * s2;
                 dst[h] = b0 + w;
+                cl[h] = r1.w;
             }
 #pragma unroll
             for (int h = 0; h < 2; h++)
                 if (dst[h] >= 0) {
                     Dg[dst[h]] = v[h];
-                    Dc[plan->clin[dst[h]]] = v[h];
+                    Dc[cl[h]] = v[h] * pwn;
                 }
             __syncwarp();
         }
@@ -1005,7 +1009,7 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     // this lane's tuple and source chunk
     const int ct = tid - 32;
     int kk = -1, a_first = 0, cnt = 0, wsteps = 0;
-    int blin[NB], nbl[NB];
+    int blin[NB], thr[NB];
     if (warp > 0) {
         kk = plan->lane_k[ct];
         a_first = plan->lane_a0[ct];
@@ -1019,17 +1023,17 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
             int b0, b1, b2;
             decode(b, b0, b1, b2);
             blin[j] = cube_lin(p, b0, b1, b2);
-            nbl[j] = b0 + b1 + b2;
+            thr[j] = p - (b0 + b1 + b2);  // a valid while |a| <= thr
         } else {
             blin[j] = 0;
-            nbl[j] = p + 1;  // never valid
+            thr[j] = -1;  // never valid
         }
     }
-    R acc[NB][NCH];
+    f2_t acc[NB][NP];
 #pragma unroll
     for (int j = 0; j < NB; j++)
 #pragma unroll
-        for (int c = 0; c < NCH; c++) acc[j][c] = 0;
+        for (int i = 0; i < NP; i++) acc[j][i] = 0ull;
 
     if (npair > 0) {
         issue_copy(l0, 0);
@@ -1044,42 +1048,29 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
             if (warp == 0) produce(l0 + k + 1, buf ^ 1);
         }
         if (warp == 0) continue;
-        const R* S = Sb + buf * 40;
-        const R* Dc = Cb + buf * sm.CUBEP;
-        const R* N = Nb + buf * rowsz;
-        const R R0[3] = {S[32], S[33], S[34]};
-        R pw[NB];
-#pragma unroll
-        for (int j = 0; j < NB; j++) pw[j] = nbl[j] <= p ? S[16 + nbl[j]] : R(0);
+        const float* S = Sb + buf * 40;
+        const float* Dc = Cb + buf * sm.CUBEP;
+        const float* N = Nb + buf * rowsz;
+        const float R0[3] = {S[32], S[33], S[34]};
 #pragma unroll 1
         for (int s = 0; s < wsteps; s++) {
             const bool on = s < cnt;
             const int a = a_first + (on ? s : 0);
             const int e = ainfo[a];
             const int alin = e & 0xffff, la = e >> 16;
-            const R fa = on ? S[la] : R(0);
-            R cf[NB];
+            const float fa = on ? S[la] : 0.f;
+            f2_t cf[NB];
 #pragma unroll
             for (int j = 0; j < NB; j++) {
-                const int ci = min(alin + blin[j], sm.CUBE - 1);
-                const R dv = Dc[ci];
-                cf[j] = (la + nbl[j] <= p) ? dv * (fa * pw[j]) : R(0);
+                const float c = la <= thr[j] ? Dc[alin + blin[j]] * fa : 0.f;
+                cf[j] = pk(c, c);
             }
-            const R* row = N + a * C::NCHP;
-            R v[C::NCHP];
-            if (sizeof(R) == 4) {
+            const float4* row = reinterpret_cast<const float4*>(N + a * C::NCHP);
+            float v[C::NCHP];
 #pragma unroll
-                for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
-                    const float4 q = reinterpret_cast<const float4*>(row)[k4];
-                    v[4 * k4] = (R)q.x; v[4 * k4 + 1] = (R)q.y;
-                    v[4 * k4 + 2] = (R)q.z; v[4 * k4 + 3] = (R)q.w;
-                }
-            } else {
-#pragma unroll
-                for (int k2 = 0; k2 < C::NCHP / 2; k2++) {
-                    const double2 q = reinterpret_cast<const double2*>(row)[k2];
-                    v[2 * k2] = (R)q.x; v[2 * k2 + 1] = (R)q.y;
-                }
+            for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
+                const float4 q4 = row[k4];
+                v[4 * k4] = q4.x; v[4 * k4 + 1] = q4.y; v[4 * k4 + 2] = q4.z; v[4 * k4 + 3] = q4.w;
             }
 #pragma unroll
             for (int d = 0; d < 3; d++)
@@ -1087,9 +1078,11 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
                 for (int j = 0; j < C::J; j++)
                     v[C::CH_Y + d * C::J + j] -= R0[d] * v[C::CH_M + j];
 #pragma unroll
-            for (int j = 0; j < NB; j++)
+            for (int i = 0; i < NP; i++) {
+                const f2_t vi = pk(v[2 * i], v[2 * i + 1]);
 #pragma unroll
-                for (int c = 0; c < NCH; c++) acc[j][c] += cf[j] * v[c];
+                for (int j = 0; j < NB; j++) acc[j][i] = fma2(cf[j], vi, acc[j][i]);
+            }
         }
     }
     cp_async_wait_all();
@@ -1098,36 +1091,41 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     // reduction in rounds through the row/cube area
     constexpr int PER = NB * NCH;
     const int lpr = sm.area / PER;
-    R* Lg = loc + node * (int64_t)rowsz;
+    float* Lg = loc + node * (int64_t)rowsz;
     for (int lo = 0; lo < M2L3_LANES; lo += lpr) {
         const int hi = lo + lpr < M2L3_LANES ? lo + lpr : M2L3_LANES;
         if (warp > 0 && ct >= lo && ct < hi) {
-            R* sl = base + (ct - lo) * PER;
+            float* sl = base + (ct - lo) * PER;
 #pragma unroll
             for (int j = 0; j < NB; j++)
 #pragma unroll
-                for (int c = 0; c < NCH; c++) sl[j * NCH + c] = acc[j][c];
+                for (int i = 0; i < NP; i++) {
+                    float x, y;
+                    upk(acc[j][i], x, y);
+                    sl[j * NCH + 2 * i] = x;
+                    if (2 * i + 1 < NCH) sl[j * NCH + 2 * i + 1] = y;
+                }
         }
         __syncthreads();
         for (int b = tid; b < NT; b += M2L3_THREADS) {
             const int k = b / NB, j = b - k * NB;
-            R sum[NCH];
+            float sum[NCH];
 #pragma unroll
-            for (int c = 0; c < NCH; c++) sum[c] = 0;
+            for (int c = 0; c < NCH; c++) sum[c] = 0.f;
             for (int i = plan->kstart[k]; i < plan->kstart[k + 1]; i++) {
                 const int l = plan->klane[i];
                 if (l < lo || l >= hi) continue;
-                const R* sl = base + (l - lo) * PER + j * NCH;
+                const float* sl = base + (l - lo) * PER + j * NCH;
 #pragma unroll
                 for (int c = 0; c < NCH; c++) sum[c] += sl[c];
             }
             int b0, b1, b2;
             decode(b, b0, b1, b2);
-            const R inv = R(1) / mfact<R>(b0, b1, b2);
-            R* out = Lg + b * C::NCHP;
+            const float inv = 1.f / mfact<float>(b0, b1, b2);
+            float* out = Lg + b * C::NCHP;
             if (lo == 0) {
 #pragma unroll
-                for (int c = 0; c < C::NCHP; c++) out[c] = c < NCH ? sum[c] * inv : R(0);
+                for (int c = 0; c < C::NCHP; c++) out[c] = c < NCH ? sum[c] * inv : 0.f;
             } else {
 #pragma unroll
                 for (int c = 0; c < NCH; c++) out[c] += sum[c] * inv;
@@ -1743,23 +1741,24 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, st>>>(
                 p, C::NCHP, stt.n_nodes, mom);
             if ((rc = launch_status("fmm moment factorials"))) return rc;
-            bool lanes = sizeof(R) == 4;  // the lane plan (fmm_m2l3) for FP32
-            if (lanes) {
-                M2LPlan3 host_plan;
-                lanes = m2l3_make_plan(p, M2L3Cfg<R, K>::NB, &host_plan) == 0 &&
-                        m2l3_smem<R, K>(p).total_bytes <= 227 * 1024;
-            }
+            bool lanes = false;  // the lane plan (fmm_m2l3) for FP32
             int* plan_err = reinterpret_cast<int*>(plan + al256(m2l_plan_bytes()));
-            if (lanes) {
-                M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
-                fmm_m2l3_plan<<<1, 32, 0, st>>>(p, M2L3Cfg<R, K>::NB, plan3, plan_err);
-                if ((rc = launch_status("fmm m2l plan"))) return rc;
-                const size_t smem_all = (size_t)m2l3_smem<R, K>(p).total_bytes;
-                if ((rc = set_smem(fmm_m2l3<R, K>, smem_all))) return rc;
-                fmm_m2l3<R, K><<<(unsigned)far.n_obs, M2L3_THREADS, smem_all, st>>>(
-                    p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
-                    plan3, loc);
-            } else {
+            if constexpr (sizeof(R) == 4) {
+                M2LPlan3 host_plan;
+                lanes = m2l3_make_plan(p, M2L3Cfg<K>::NB, &host_plan) == 0 &&
+                        m2l3_smem<K>(p).total_bytes <= 227 * 1024;
+                if (lanes) {
+                    M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
+                    fmm_m2l3_plan<<<1, 32, 0, st>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);
+                    if ((rc = launch_status("fmm m2l plan"))) return rc;
+                    const size_t smem_all = (size_t)m2l3_smem<K>(p).total_bytes;
+                    if ((rc = set_smem(fmm_m2l3<K>, smem_all))) return rc;
+                    fmm_m2l3<K><<<(unsigned)far.n_obs, M2L3_THREADS, smem_all, st>>>(
+                        p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
+                        plan3, loc);
+                }
+            }
+            if (!lanes) {
                 if (m2l2_items(p) > M2L2_MAXITEMS) {
                     set_error("tct_fmm_matvec: FMM order %d exceeds the M2L plan's capacity", p);
                     return TCT_ERR_ARG;
