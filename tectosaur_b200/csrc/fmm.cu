@@ -441,22 +441,24 @@ fmm_p2p(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
 }
 
 // ---- P2P, packed elasticRH3 in FP32 ------------------------------------------
-// fmm_p2p with the direct farfield's packed pair sums (rh2_pair).  The block's
-// four warps split a chunk of m <= 128 obs triangles of the leaf into T =
-// ceil(m / 64) teams of 64 (a lane takes triangles lane and lane + 32 of its
-// team, one in each f32x2 half) and the list's source triangles, concatenated
-// in list order, into S = 4 / T equal slices; warp w is team w % T, slice
-// w / T.  A warp streams its slice through its own two shared-memory buffers
-// of P2P_CH packed records (cp.async, the next chunk in flight while the
-// current one is summed; records read as broadcasts), and Kahan-folds the
-// packed sums of each chunk into its totals.  Slice totals are added in a
-// fixed order.  W[t] = the 9 sums of obs triangle t in the NAcc layout
-// (overwritten).
-constexpr int P2P_CH = 16;
+// fmm_p2p with the direct farfield's packed pair sums (rh2_pair).  A chunk of
+// m <= 128 obs triangles of the leaf is split into T = ceil(m / 64) teams of
+// mt = ceil(m / T) triangles; a group of h = ceil(mt / 2) lanes covers a team
+// (a lane takes triangles li and li + h, one in each f32x2 half), a warp holds
+// Gw = 32 / h groups (at most P2P_CHW), and the block's 4 Gw groups are team
+// g % T and slice g / T of S = 4 Gw / T equal slices of the list's source
+// triangles (concatenated in list order), so that small leaves still fill
+// the lanes.  A group streams its slice through its own two shared-memory
+// buffers of CHg = min(P2P_CHW / Gw, h) packed records (cp.async, the next
+// chunk in flight while the current one is summed; records read as
+// broadcasts within the group), and Kahan-folds its packed sums into its
+// totals every 16 or more records.  Slice totals are added in a fixed order.
+// W[t] = the 9 sums of obs triangle t in the NAcc layout (overwritten).
+constexpr int P2P_CHW = 24;  // staged records per warp and buffer
 
 template <int NQ>
 constexpr size_t p2p_rh2_smem() {
-    return sizeof(float) * (128 * 18 + 4 * 2 * P2P_CH * RecRH2<NQ>::LEN);
+    return sizeof(float) * (128 * 18 + 4 * 2 * P2P_CHW * RecRH2<NQ>::LEN);
 }
 
 template <int NQ, bool UNIFORM>
@@ -472,7 +474,7 @@ fmm_p2p_rh2(Rule2D<float> rule, const float* __restrict__ pts,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* red = reinterpret_cast<float*>(smem_raw);  // 128 x 18 slice totals
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* buf = red + 128 * 18 + warp * 2 * P2P_CH * L::LEN;  // this warp's two buffers
+    float* wbuf = red + 128 * 18 + warp * 2 * P2P_CHW * L::LEN;  // this warp's staging
     const int64_t node = obs_nodes[blockIdx.x];
     const int64_t l0 = starts[blockIdx.x], l1 = starts[blockIdx.x + 1];
     const int64_t ob0 = o_start[node], n_o = o_end[node] - ob0;
@@ -498,103 +500,123 @@ fmm_p2p_rh2(Rule2D<float> rule, const float* __restrict__ pts,
 
     for (int64_t cb = 0; cb < n_o; cb += 128) {
         const int m = (int)min((int64_t)128, n_o - cb);
-        const int T = m > 64 ? 2 : 1, S = 4 / T;
-        const int team = warp % T, slice = warp / T;
-        const int ta = team * 64 + lane, tb = ta + 32;
-        const bool va = ta < m, vb = tb < m;
+        const int T = (m + 63) / 64, mt = (m + T - 1) / T;
+        const int h = (mt + 1) / 2;
+        const int Gw = min(32 / h, P2P_CHW);
+        const int S = 4 * Gw / T;
+        const int gl = lane / h, li = lane - gl * h;
+        const int gi = warp * Gw + gl;
+        const int team = gi % T, slice = gi / T;
+        const bool active = gl < Gw && slice < S;
+        const int tb = team * mt, mteam = min(mt, m - tb);
+        const bool va = active && li < mteam, vb = active && li + h < mteam;
+        const int CHg = min(P2P_CHW / Gw, h);
+        const int gbase = gl * h;
+        const unsigned gmask = (h == 32 ? 0xffffffffu : ((1u << h) - 1u)) << (gbase & 31);
+        float* buf = wbuf + (gl < Gw ? gl : 0) * 2 * CHg * L::LEN;
         float tot[2][9], cmp[2][9];
 #pragma unroll
         for (int k = 0; k < 9; k++) {
             tot[0][k] = tot[1][k] = 0.f;
             cmp[0][k] = cmp[1][k] = 0.f;
         }
-        f2_t negx[NQ][3];
-        {
-            TriGeom<float> oa, ob;
-            if (va) load_tri(oa, pts, obs_tris, ob0 + cb + ta, 0, false, true);
-            if (vb) load_tri(ob, pts, obs_tris, ob0 + cb + tb, 0, false, true);
+        if (active) {
+            f2_t negx[NQ][3];
+            {
+                TriGeom<float> oa, ob;
+                if (va) load_tri(oa, pts, obs_tris, ob0 + cb + tb + li, 0, false, true);
+                if (vb) load_tri(ob, pts, obs_tris, ob0 + cb + tb + li + h, 0, false, true);
 #pragma unroll
-            for (int q = 0; q < NQ; q++) {
-                const float ox = rule.x[q], oy = rule.y[q];
-                const float bq[3] = {1 - ox - oy, ox, oy};
+                for (int q = 0; q < NQ; q++) {
+                    const float ox = rule.x[q], oy = rule.y[q];
+                    const float bq[3] = {1 - ox - oy, ox, oy};
 #pragma unroll
-                for (int d = 0; d < 3; d++)
-                    negx[q][d] = pk(va ? -bary_point(oa, bq, d) : 0.f,
-                                    vb ? -bary_point(ob, bq, d) : 0.f);
-            }
-        }
-        // the slice [p0, p1) of the concatenated sources; the stream cursor
-        // (list entry l, its first record a, offset off, records left rem)
-        const int p0 = (int)((int64_t)n_s * slice / S), p1 = (int)((int64_t)n_s * (slice + 1) / S);
-        int64_t l = l0, a = 0;
-        int off = 0, rem = 0, skip = p0;
-        while (l < l1) {  // find the entry holding position p0
-            const int64_t sn = srcs[l];
-            a = s_start[sn];
-            rem = (int)(s_end[sn] - a);
-            if (skip < rem) break;
-            skip -= rem;
-            l++;
-        }
-        off = skip;
-        rem -= skip;
-        // copy the next `need` stream records into buffer b (one commit group)
-        auto issue = [&](int need, int b) {
-            int64_t gidx = 0;
-            int r_base = 0;
-            while (r_base < need) {
-                while (rem == 0 && l + 1 < l1) {
-                    l++;
-                    const int64_t sn = srcs[l];
-                    a = s_start[sn];
-                    rem = (int)(s_end[sn] - a);
-                    off = 0;
+                    for (int d = 0; d < 3; d++)
+                        negx[q][d] = pk(va ? -bary_point(oa, bq, d) : 0.f,
+                                        vb ? -bary_point(ob, bq, d) : 0.f);
                 }
-                const int take = min(rem, need - r_base);
-                if (take <= 0) break;  // unreachable: the slice never outruns the list
-                if (lane >= r_base && lane < r_base + take) gidx = a + off + (lane - r_base);
-                r_base += take;
-                off += take;
-                rem -= take;
             }
-            float* dst = buf + b * P2P_CH * L::LEN;
-            for (int e0 = 0; e0 < need * V4; e0 += 32) {  // warp-uniform trip count
-                const int e = e0 + lane;
-                const int r = min(e / V4, need - 1), part = e - r * V4;
-                const int64_t g = __shfl_sync(0xffffffffu, gidx, r);
-                if (e < need * V4)
-                    cp_async16(dst + r * L::LEN + part * 4, rec + g * L::LEN + part * 4);
+            // the slice [p0, p1) of the concatenated sources; the stream
+            // cursor (list entry l, its first record a, offset off, records
+            // left rem), the same in every lane of the group
+            const int p0 = (int)((int64_t)n_s * slice / S);
+            const int p1 = (int)((int64_t)n_s * (slice + 1) / S);
+            int64_t l = l0, a = 0;
+            int off = 0, rem = 0, skip = p0;
+            while (l < l1) {  // find the entry holding position p0
+                const int64_t sn = srcs[l];
+                a = s_start[sn];
+                rem = (int)(s_end[sn] - a);
+                if (skip < rem) break;
+                skip -= rem;
+                l++;
             }
-            cp_async_commit();
-        };
-        const int n_mine = p1 - p0;
-        if (n_mine > 0) issue(min(P2P_CH, n_mine), 0);
-        for (int c0 = 0; c0 < n_mine; c0 += P2P_CH) {
-            const int cur = (c0 / P2P_CH) & 1;
-            const int need = min(P2P_CH, n_mine - c0);
-            if (c0 + P2P_CH < n_mine) {
-                issue(min(P2P_CH, n_mine - c0 - P2P_CH), cur ^ 1);
-                cp_async_wait_group<1>();
-            } else {
-                cp_async_wait_group<0>();
-            }
-            __syncwarp();
-            const float* rb = buf + cur * P2P_CH * L::LEN;
+            off = skip;
+            rem -= skip;
+            // copy the next `need` (<= CHg <= h) stream records into buffer b
+            auto issue = [&](int need, int b) {
+                int64_t gidx = 0;
+                int r_base = 0;
+                while (r_base < need) {
+                    while (rem == 0 && l + 1 < l1) {
+                        l++;
+                        const int64_t sn = srcs[l];
+                        a = s_start[sn];
+                        rem = (int)(s_end[sn] - a);
+                        off = 0;
+                    }
+                    const int take = min(rem, need - r_base);
+                    if (take <= 0) break;  // unreachable: the slice never outruns the list
+                    if (li >= r_base && li < r_base + take) gidx = a + off + (li - r_base);
+                    r_base += take;
+                    off += take;
+                    rem -= take;
+                }
+                float* dst = buf + b * CHg * L::LEN;
+                for (int e0 = 0; e0 < need * V4; e0 += h) {  // uniform within the group
+                    const int e = e0 + li;
+                    const int r = min(e / V4, need - 1), part = e - r * V4;
+                    const int64_t g = __shfl_sync(gmask, gidx, gbase + r);
+                    if (e < need * V4)
+                        cp_async16(dst + r * L::LEN + part * 4, rec + g * L::LEN + part * 4);
+                }
+                cp_async_commit();
+            };
+            const int n_mine = p1 - p0;
             f2_t Wp[9];
 #pragma unroll
             for (int k = 0; k < 9; k++) Wp[k] = 0ull;
+            int since = 0;
+            if (n_mine > 0) issue(min(CHg, n_mine), 0);
+            for (int c0 = 0; c0 < n_mine; c0 += CHg) {
+                const int cur = (c0 / CHg) & 1;
+                const int need = min(CHg, n_mine - c0);
+                if (c0 + CHg < n_mine) {
+                    issue(min(CHg, n_mine - c0 - CHg), cur ^ 1);
+                    cp_async_wait_group<1>();
+                } else {
+                    cp_async_wait_group<0>();
+                }
+                __syncwarp(gmask);
+                const float* rb = buf + cur * CHg * L::LEN;
 #pragma unroll 2
-            for (int j = 0; j < need; j++)
-                rh2_pair<NQ, UNIFORM>(reinterpret_cast<const f2_t*>(rb + j * L::LEN), negx, wq,
-                                      eps, Wp);
+                for (int j = 0; j < need; j++)
+                    rh2_pair<NQ, UNIFORM>(reinterpret_cast<const f2_t*>(rb + j * L::LEN), negx,
+                                          wq, eps, Wp);
+                since += need;
+                if (since >= 16 || c0 + CHg >= n_mine) {
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
-                float wa, wb;
-                upk(Wp[k], wa, wb);
-                fold<float, true>(tot[0][k], cmp[0][k], wa);
-                fold<float, true>(tot[1][k], cmp[1][k], wb);
+                    for (int k = 0; k < 9; k++) {
+                        float wa, wb;
+                        upk(Wp[k], wa, wb);
+                        fold<float, true>(tot[0][k], cmp[0][k], wa);
+                        fold<float, true>(tot[1][k], cmp[1][k], wb);
+                        Wp[k] = 0ull;
+                    }
+                    since = 0;
+                }
+                __syncwarp(gmask);  // buffer cur is free for the chunk after next
             }
-            __syncwarp();  // buffer cur is free for the chunk after next
         }
         __syncthreads();  // the previous chunk's reads of red are done
 #pragma unroll
@@ -604,12 +626,15 @@ fmm_p2p_rh2(Rule2D<float> rule, const float* __restrict__ pts,
         }
         __syncthreads();
         for (int t = threadIdx.x; t < m; t += blockDim.x) {
-            const int tm = t / 64, within = t % 64, ln = within % 32, half = within / 32;
+            const int tm = t / mt, within = t - tm * mt;
+            const int half = within / h, ln = within - half * h;
             float* w = W + (ob0 + cb + t) * 9;
             for (int k = 0; k < 9; k++) {
                 float sacc = 0.f;
-                for (int sl = 0; sl < S; sl++)
-                    sacc += red[((sl * T + tm) * 32 + ln) * 18 + half * 9 + k];
+                for (int sl = 0; sl < S; sl++) {
+                    const int g = sl * T + tm, wg = g / Gw, lg = g - wg * Gw;
+                    sacc += red[(wg * 32 + lg * h + ln) * 18 + half * 9 + k];
+                }
                 w[k] = sacc;
             }
         }
