@@ -37,6 +37,7 @@
 // P2P runs the direct farfield's triangle-level pair loop (far_common.cuh) on
 // the listed leaf pairs, from the same per-source records the P2M reads.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "far_common.cuh"
@@ -785,9 +786,12 @@ struct M2LPlan3 {
     int kstart[FMM_NTMAX + 1];  // lanes of tuple k: klane[kstart[k] .. kstart[k + 1])
     int klane[M2L3_LANES];
     int ainfo[FMM_NTMAX];      // lin(a) | |a| << 16
-    // Dc recurrence per graded c: a0 | a1 << 8 | a2 << 16, the graded indices
-    // of c - e_0, c - e_1, c - e_2, c - 2 e_0, c - 2 e_1, c - 2 e_2, lin(c)
-    alignas(16) int rec[FMM_NTMAX][8];
+    // Dc recurrence per graded c (level n): the graded indices of c - e_0,
+    // c - e_1, c - e_2 and lin(c); of c - 2 e_0, c - 2 e_1, c - 2 e_2 and 0;
+    // then as float bits cA c_d (3) and 0, cB c_d (c_d - 1) (3) and 0, with
+    // cA = -(2n - 1) / n, cB = -(n - 1) / n (absent neighbours: index 0,
+    // coefficient 0)
+    alignas(16) int rec[FMM_NTMAX][16];
 };
 
 __host__ __device__ inline int cube_lin(int p, int a0, int a1, int a2) {
@@ -858,15 +862,27 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
         int a0, a1, a2;
         decode(g, a0, a1, a2);
         plan->ainfo[g] = cube_lin(p, a0, a1, a2) | ((a0 + a1 + a2) << 16);
+        const int n = a0 + a1 + a2;
+        const float cA = n > 0 ? -(float)(2 * n - 1) / (float)n : 0.f;
+        const float cB = n > 0 ? -(float)(n - 1) / (float)n : 0.f;
         int* r = plan->rec[g];
-        r[0] = a0 | (a1 << 8) | (a2 << 16);
-        r[1] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
-        r[2] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
-        r[3] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
+        r[0] = a0 > 0 ? midx(a0 - 1, a1, a2) : 0;
+        r[1] = a1 > 0 ? midx(a0, a1 - 1, a2) : 0;
+        r[2] = a2 > 0 ? midx(a0, a1, a2 - 1) : 0;
+        r[3] = cube_lin(p, a0, a1, a2);
         r[4] = a0 > 1 ? midx(a0 - 2, a1, a2) : 0;
         r[5] = a1 > 1 ? midx(a0, a1 - 2, a2) : 0;
         r[6] = a2 > 1 ? midx(a0, a1, a2 - 2) : 0;
-        r[7] = cube_lin(p, a0, a1, a2);
+        r[7] = 0;
+        const float cf[8] = {cA * (float)a0, cA * (float)a1, cA * (float)a2, 0.f,
+                             cB * (float)(a0 * (a0 - 1)), cB * (float)(a1 * (a1 - 1)),
+                             cB * (float)(a2 * (a2 - 1)), 0.f};
+        for (int t = 0; t < 8; t++) {
+            float f = cf[t];
+            int bits;
+            memcpy(&bits, &f, sizeof(int));
+            r[8 + t] = bits;
+        }
     }
     return 0;
 }
@@ -885,34 +901,36 @@ struct M2L3Cfg {
     static constexpr int NB = K == kRH ? 3 : 64 / NCH;
 };
 
-// Shared-memory layout (floats): row buffers 2 x NT x NCHP, cubes 2 x CUBEP
-// (CUBEP >= 2 (p+1)^3, so lin(a) + lin(b) needs no clamp; these two regions
-// double as the reduction area, at least 32 lanes' slots), graded Dc scratch
-// NTP, 2 x 40 scalars, 4 x M2L3_CAP pair geometry, then ainfo (NTP ints) and
-// M2L3_CAP source node ids.
+// Shared-memory layout (floats), B pairs per pipeline stage: row buffers
+// 2 B x NT x NCHP, cubes 2 B x CUBEP (CUBEP >= 2 (p+1)^3, so lin(a) + lin(b)
+// needs no clamp; these two regions double as the reduction area, at least
+// 32 lanes' slots), graded Dc scratch B x NTP, 2 B x 40 scalars, 4 x
+// M2L3_CAP pair geometry, then ainfo (NTP ints), M2L3_CAP source node ids and
+// the recurrence table (NT x 16 ints).
 constexpr int M2L3_CAP = 512;  // pairs whose source node and geometry are staged
 struct M2L3Smem {
     int NT, NTP, CUBEP, area, dg, sb, pg, ai, total_bytes;
 };
 template <int K>
-__host__ __device__ inline M2L3Smem m2l3_smem(int p) {
+__host__ __device__ inline M2L3Smem m2l3_smem(int p, int B) {
     using C = Chan<K>;
     M2L3Smem m;
     m.NT = n_terms(p);
     m.NTP = (m.NT + 3) / 4 * 4;
     m.CUBEP = (2 * (p + 1) * (p + 1) * (p + 1) + 3) / 4 * 4;
-    const int need = 2 * m.NT * C::NCHP + 2 * m.CUBEP;
+    const int need = 2 * B * (m.NT * C::NCHP + m.CUBEP);
     const int slots32 = 32 * M2L3Cfg<K>::NB * C::NCH;
     m.area = need > slots32 ? need : (slots32 + 3) / 4 * 4;
     m.dg = m.area;
-    m.sb = m.dg + m.NTP;
-    m.pg = m.sb + 80;
+    m.sb = m.dg + B * m.NTP;
+    m.pg = m.sb + 2 * B * 40;
     m.ai = m.pg + 4 * M2L3_CAP;
-    m.total_bytes = (int)(sizeof(float) * m.ai + sizeof(int) * (m.NTP + M2L3_CAP));
+    m.total_bytes = (int)(sizeof(float) * m.ai + sizeof(int) * (m.NTP + M2L3_CAP) +
+                          sizeof(int) * 16 * m.NT);
     return m;
 }
 
-template <int K>
+template <int K, int B>
 __global__ void __launch_bounds__(M2L3_THREADS, 2)
 fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
          const int64_t* __restrict__ starts, const int64_t* __restrict__ srcs,
@@ -925,25 +943,29 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     constexpr int NCH = C::NCH;
     constexpr int NP = (NCH + 1) / 2;  // channel pairs (f32x2)
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const M2L3Smem sm = m2l3_smem<K>(p);
+    const M2L3Smem sm = m2l3_smem<K>(p, B);
     const int NT = sm.NT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t oi = blockIdx.x;
     if (oi >= n_obs_nodes) return;
     const int rowsz = NT * C::NCHP;
     float* base = reinterpret_cast<float*>(smem_raw);
-    float* Nb = base;                 // 2 x NT x NCHP source rows
-    float* Cb = base + 2 * rowsz;     // 2 x CUBEP scaled Dc cubes
-    float* Dg = base + sm.dg;         // graded Dc (producer scratch)
-    float* Sb = base + sm.sb;         // 2 x 40: (-s_s/s_o)^n [0, 16), R0 [32, 35)
-    float* pgeo = base + sm.pg;       // first M2L3_CAP pairs: source center and radius
+    float* Nb = base;                     // 2 B x NT x NCHP source rows
+    float* Cb = base + 2 * B * rowsz;     // 2 B x CUBEP scaled Dc cubes
+    float* Dg = base + sm.dg;             // B x NTP graded Dc (producer scratch)
+    float* Sb = base + sm.sb;             // 2 B x 40: (-s_s/s_o)^n [0, 16), R0 [32, 35)
+    float* pgeo = base + sm.pg;           // first M2L3_CAP pairs: source center and radius
     int* ainfo = reinterpret_cast<int*>(base + sm.ai);
-    int* psrc = ainfo + sm.NTP;       // first M2L3_CAP pairs: source node
+    int* psrc = ainfo + sm.NTP;           // first M2L3_CAP pairs: source node
+    int* rtab = psrc + M2L3_CAP;          // recurrence table
     for (int g = tid; g < NT; g += M2L3_THREADS) ainfo[g] = plan->ainfo[g];
+    for (int e = tid; e < NT * 4; e += M2L3_THREADS)
+        reinterpret_cast<int4*>(rtab)[e] = reinterpret_cast<const int4*>(plan->rec)[e];
 
     const int64_t node = obs_nodes[oi];
     const float co[3] = {ocent[3 * node], ocent[3 * node + 1], ocent[3 * node + 2]};
     const float so = orad[node];
+    const float inv_so = 1.f / so;  // node radii are positive
     const int64_t l0 = starts[oi], l1 = starts[oi + 1];
     const int64_t npair = l1 - l0;
     // the list's source nodes and geometry, staged once (the pipeline below
@@ -958,75 +980,89 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     }
     __syncthreads();
 
-    auto issue_copy = [&](int64_t l, int buf) {
-        const int64_t sn = l - l0 < M2L3_CAP ? (int64_t)psrc[l - l0] : srcs[l];
-        const float* src = mom + sn * (int64_t)rowsz;
-        float* dst = Nb + buf * rowsz;
-        for (int k = tid; k < rowsz / 4; k += M2L3_THREADS) cp_async16(dst + k * 4, src + k * 4);
+    // pairs [k0, k0 + B) of the list (those below npair) into stage st
+    auto issue_copy = [&](int64_t k0, int st) {
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int64_t k = k0 + u;
+            if (k >= npair) break;
+            const int64_t sn = k < M2L3_CAP ? (int64_t)psrc[k] : srcs[l0 + k];
+            const float* src = mom + sn * (int64_t)rowsz;
+            float* dst = Nb + (st * B + u) * rowsz;
+            for (int e = tid; e < rowsz / 4; e += M2L3_THREADS) cp_async16(dst + e * 4, src + e * 4);
+        }
         cp_async_commit();
     };
     // coef(a, b) = f_|a| (s_o/rho)^|b| / rho Dc_(a+b) = S_|a| Dh_(a+b) with
-    // Dh_c = Dc_c (s_o/rho)^|c| / rho (the cube) and S_n = (-s_s/s_o)^n
-    auto produce = [&](int64_t l, int buf) {  // warp 0
-        float cs[3], rs;
-        if (l - l0 < M2L3_CAP) {
-            const float* g = pgeo + 4 * (l - l0);
-            cs[0] = g[0]; cs[1] = g[1]; cs[2] = g[2]; rs = g[3];
-        } else {
-            const int64_t sn = srcs[l];
-            cs[0] = scent[3 * sn]; cs[1] = scent[3 * sn + 1]; cs[2] = scent[3 * sn + 2];
-            rs = srad[sn];
-        }
-        const float R0[3] = {co[0] - cs[0], co[1] - cs[1], co[2] - cs[2]};
-        const float rho = sqrtf(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
-        const float inv_rho = 1.f / rho;
-        const float Rh[3] = {R0[0] * inv_rho, R0[1] * inv_rho, R0[2] * inv_rho};
-        const float q = so * inv_rho;  // pw_n = q^n / rho
-        float* S = Sb + buf * 40;
-        float* Dc = Cb + buf * sm.CUBEP;
-        if (lane <= p) S[lane] = ipow(-rs / so, lane);
-        if (lane < 3) S[32 + lane] = R0[lane];
-        if (lane == 0) {
-            Dg[0] = 1.f;
-            Dc[0] = inv_rho;
+    // Dh_c = Dc_c (s_o/rho)^|c| / rho (the cube) and S_n = (-s_s/s_o)^n; the
+    // B pairs' recurrences run interleaved (independent chains)
+    auto produce = [&](int64_t k0, int st) {  // warp 0
+        float Rh[B][3], q[B], pwn[B];
+        bool on[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int64_t k = k0 + u;
+            on[u] = k < npair;
+            float cs[3] = {co[0] + 1.f, co[1], co[2]}, rs = 0.f;  // any distinct point if off
+            if (on[u] && k < M2L3_CAP) {
+                const float* g = pgeo + 4 * k;
+                cs[0] = g[0]; cs[1] = g[1]; cs[2] = g[2]; rs = g[3];
+            } else if (on[u]) {
+                const int64_t sn = srcs[l0 + k];
+                cs[0] = scent[3 * sn]; cs[1] = scent[3 * sn + 1]; cs[2] = scent[3 * sn + 2];
+                rs = srad[sn];
+            }
+            const float R0[3] = {co[0] - cs[0], co[1] - cs[1], co[2] - cs[2]};
+            const float rho = sqrtf(R0[0] * R0[0] + R0[1] * R0[1] + R0[2] * R0[2]);
+            const float inv_rho = 1.f / rho;
+            Rh[u][0] = R0[0] * inv_rho; Rh[u][1] = R0[1] * inv_rho; Rh[u][2] = R0[2] * inv_rho;
+            q[u] = so * inv_rho;  // pw_n = q^n / rho
+            pwn[u] = inv_rho;
+            float* S = Sb + (st * B + u) * 40;
+            if (lane <= p) S[lane] = ipow(-rs * inv_so, lane);
+            if (lane < 3) S[32 + lane] = R0[lane];
+            if (lane == 0) {
+                Dg[u * sm.NTP] = 1.f;
+                Cb[(st * B + u) * sm.CUBEP] = inv_rho;
+            }
         }
         __syncwarp();
         // level n from levels n - 1 and n - 2; a lane takes entries lane and
-        // lane + 32 of the level, loads first so both chains overlap
-        float pwn = inv_rho;
+        // lane + 32 of the level for each pair, loads first so the chains overlap
         for (int n = 1; n <= p; n++) {
-            pwn *= q;
             const int lsz = (n + 1) * (n + 2) / 2, b0 = n_terms(n - 1);
-            const float cA = -(float)(2 * n - 1) / (float)n, cB = -(float)(n - 1) / (float)n;
-            float v[2];
+            float v[B][2];
             int dst[2], cl[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int w = lane + 32 * h;
                 dst[h] = -1;
                 cl[h] = 0;
-                v[h] = 0.f;
                 if (w >= lsz) continue;
-                const int4 r0 = *reinterpret_cast<const int4*>(plan->rec[b0 + w]);
-                const int4 r1 = *reinterpret_cast<const int4*>(plan->rec[b0 + w] + 4);
-                const int a0 = r0.x & 0xff, a1 = (r0.x >> 8) & 0xff, a2 = r0.x >> 16;
-                const float d1 = a0 > 0 ? Dg[r0.y] : 0.f, d2 = a1 > 0 ? Dg[r0.z] : 0.f;
-                const float d3 = a2 > 0 ? Dg[r0.w] : 0.f, d4 = a0 > 1 ? Dg[r1.x] : 0.f;
-                const float d5 = a1 > 1 ? Dg[r1.y] : 0.f, d6 = a2 > 1 ? Dg[r1.z] : 0.f;
-                const float s1 = Rh[0] * (float)a0 * d1 + Rh[1] * (float)a1 * d2 +
-                                 Rh[2] * (float)a2 * d3;
-                const float s2 = (float)(a0 * (a0 - 1)) * d4 + (float)(a1 * (a1 - 1)) * d5 +
-                                 (float)(a2 * (a2 - 1)) * d6;
-                v[h] = cA * s1 + cB * s2;
+                const int4* rt = reinterpret_cast<const int4*>(rtab + 16 * (b0 + w));
+                const int4 i0 = rt[0], i1 = rt[1], f0 = rt[2], f1 = rt[3];
+#pragma unroll
+                for (int u = 0; u < B; u++) {
+                    const float* D = Dg + u * sm.NTP;
+                    v[u][h] = __int_as_float(f0.x) * Rh[u][0] * D[i0.x] +
+                              __int_as_float(f0.y) * Rh[u][1] * D[i0.y] +
+                              __int_as_float(f0.z) * Rh[u][2] * D[i0.z] +
+                              __int_as_float(f1.x) * D[i1.x] + __int_as_float(f1.y) * D[i1.y] +
+                              __int_as_float(f1.z) * D[i1.z];
+                }
                 dst[h] = b0 + w;
-                cl[h] = r1.w;
+                cl[h] = i0.w;
             }
 #pragma unroll
-            for (int h = 0; h < 2; h++)
-                if (dst[h] >= 0) {
-                    Dg[dst[h]] = v[h];
-                    Dc[cl[h]] = v[h] * pwn;
-                }
+            for (int u = 0; u < B; u++) {
+                pwn[u] *= q[u];
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                    if (dst[h] >= 0) {
+                        Dg[u * sm.NTP + dst[h]] = v[u][h];
+                        Cb[(st * B + u) * sm.CUBEP + cl[h]] = v[u][h] * pwn[u];
+                    }
+            }
             __syncwarp();
         }
     };
@@ -1060,53 +1096,59 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
 #pragma unroll
         for (int i = 0; i < NP; i++) acc[j][i] = 0ull;
 
-    if (npair > 0) {
-        issue_copy(l0, 0);
-        if (warp == 0) produce(l0, 0);
+    const int64_t nst = (npair + B - 1) / B;  // pipeline stages of B pairs
+    if (nst > 0) {
+        issue_copy(0, 0);
+        if (warp == 0) produce(0, 0);
     }
-    for (int64_t k = 0; k < npair; k++) {
-        const int buf = (int)(k & 1);
+    for (int64_t st = 0; st < nst; st++) {
+        const int buf = (int)(st & 1);
         cp_async_wait_all();
-        __syncthreads();  // pair k's rows, cube and scalars are complete; pair k - 1 is done
-        if (k + 1 < npair) {
-            issue_copy(l0 + k + 1, buf ^ 1);
-            if (warp == 0) produce(l0 + k + 1, buf ^ 1);
+        __syncthreads();  // stage st's rows, cubes and scalars are complete; st - 1 is done
+        if (st + 1 < nst) {
+            issue_copy((st + 1) * B, buf ^ 1);
+            if (warp == 0) produce((st + 1) * B, buf ^ 1);
         }
         if (warp == 0) continue;
-        const float* S = Sb + buf * 40;
-        const float* Dc = Cb + buf * sm.CUBEP;
-        const float* N = Nb + buf * rowsz;
-        const float R0[3] = {S[32], S[33], S[34]};
 #pragma unroll 1
-        for (int s = 0; s < wsteps; s++) {
-            const bool on = s < cnt;
-            const int a = a_first + (on ? s : 0);
-            const int e = ainfo[a];
-            const int alin = e & 0xffff, la = e >> 16;
-            const float fa = on ? S[la] : 0.f;
-            f2_t cf[NB];
+        for (int u = 0; u < B; u++) {
+            if (st * B + u >= npair) break;
+            const float* S = Sb + (buf * B + u) * 40;
+            const float* Dc = Cb + (buf * B + u) * sm.CUBEP;
+            const float* N = Nb + (buf * B + u) * rowsz;
+            const float R0[3] = {S[32], S[33], S[34]};
+#pragma unroll 1
+            for (int s = 0; s < wsteps; s++) {
+                const bool on = s < cnt;
+                const int a = a_first + (on ? s : 0);
+                const int e = ainfo[a];
+                const int alin = e & 0xffff, la = e >> 16;
+                const float fa = on ? S[la] : 0.f;
+                f2_t cf[NB];
 #pragma unroll
-            for (int j = 0; j < NB; j++) {
-                const float c = la <= thr[j] ? Dc[alin + blin[j]] * fa : 0.f;
-                cf[j] = pk(c, c);
-            }
-            const float4* row = reinterpret_cast<const float4*>(N + a * C::NCHP);
-            float v[C::NCHP];
+                for (int j = 0; j < NB; j++) {
+                    const float c = la <= thr[j] ? Dc[alin + blin[j]] * fa : 0.f;
+                    cf[j] = pk(c, c);
+                }
+                const float4* row = reinterpret_cast<const float4*>(N + a * C::NCHP);
+                float v[C::NCHP];
 #pragma unroll
-            for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
-                const float4 q4 = row[k4];
-                v[4 * k4] = q4.x; v[4 * k4 + 1] = q4.y; v[4 * k4 + 2] = q4.z; v[4 * k4 + 3] = q4.w;
-            }
+                for (int k4 = 0; k4 < C::NCHP / 4; k4++) {
+                    const float4 q4 = row[k4];
+                    v[4 * k4] = q4.x; v[4 * k4 + 1] = q4.y; v[4 * k4 + 2] = q4.z;
+                    v[4 * k4 + 3] = q4.w;
+                }
 #pragma unroll
-            for (int d = 0; d < 3; d++)
+                for (int d = 0; d < 3; d++)
 #pragma unroll
-                for (int j = 0; j < C::J; j++)
-                    v[C::CH_Y + d * C::J + j] -= R0[d] * v[C::CH_M + j];
+                    for (int j = 0; j < C::J; j++)
+                        v[C::CH_Y + d * C::J + j] -= R0[d] * v[C::CH_M + j];
 #pragma unroll
-            for (int i = 0; i < NP; i++) {
-                const f2_t vi = pk(v[2 * i], v[2 * i + 1]);
+                for (int i = 0; i < NP; i++) {
+                    const f2_t vi = pk(v[2 * i], v[2 * i + 1]);
 #pragma unroll
-                for (int j = 0; j < NB; j++) acc[j][i] = fma2(cf[j], vi, acc[j][i]);
+                    for (int j = 0; j < NB; j++) acc[j][i] = fma2(cf[j], vi, acc[j][i]);
+                }
             }
         }
     }
@@ -1770,17 +1812,25 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             int* plan_err = reinterpret_cast<int*>(plan + al256(m2l_plan_bytes()));
             if constexpr (sizeof(R) == 4) {
                 M2LPlan3 host_plan;
-                lanes = m2l3_make_plan(p, M2L3Cfg<K>::NB, &host_plan) == 0 &&
-                        m2l3_smem<K>(p).total_bytes <= 227 * 1024;
+                const int smem1 = m2l3_smem<K>(p, 1).total_bytes;
+                const int smem2 = m2l3_smem<K>(p, 2).total_bytes;
+                lanes = m2l3_make_plan(p, M2L3Cfg<K>::NB, &host_plan) == 0 && smem1 <= 227 * 1024;
                 if (lanes) {
                     M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
                     fmm_m2l3_plan<<<1, 32, 0, st>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);
                     if ((rc = launch_status("fmm m2l plan"))) return rc;
-                    const size_t smem_all = (size_t)m2l3_smem<K>(p).total_bytes;
-                    if ((rc = set_smem(fmm_m2l3<K>, smem_all))) return rc;
-                    fmm_m2l3<K><<<(unsigned)far.n_obs, M2L3_THREADS, smem_all, st>>>(
-                        p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
-                        plan3, loc);
+                    // two pairs per stage while two CTAs still fit an SM
+                    if (smem2 + 1024 <= 113 * 1024) {
+                        if ((rc = set_smem(fmm_m2l3<K, 2>, (size_t)smem2))) return rc;
+                        fmm_m2l3<K, 2><<<(unsigned)far.n_obs, M2L3_THREADS, smem2, st>>>(
+                            p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad,
+                            mom, plan3, loc);
+                    } else {
+                        if ((rc = set_smem(fmm_m2l3<K, 1>, (size_t)smem1))) return rc;
+                        fmm_m2l3<K, 1><<<(unsigned)far.n_obs, M2L3_THREADS, smem1, st>>>(
+                            p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad,
+                            mom, plan3, loc);
+                    }
                 }
             }
             if (!lanes) {
