@@ -443,8 +443,8 @@ fmm_p2p(Consts<R> c, Rule2D<R> rule, const R* __restrict__ pts,
 
 // ---- P2P, packed elasticRH3 in FP32 ------------------------------------------
 // fmm_p2p with the direct farfield's packed pair sums (rh2_pair).  A chunk of
-// m <= 128 obs triangles of the leaf is split into T = ceil(m / 64) teams of
-// mt = ceil(m / T) triangles; a group of h = ceil(mt / 2) lanes covers a team
+// m <= 128 obs triangles of the leaf is split into T >= ceil(m / 64) teams of
+// mt = ceil(m / T) triangles (T chosen for the fewest idle lanes); a group of h = ceil(mt / 2) lanes covers a team
 // (a lane takes triangles li and li + h, one in each f32x2 half), a warp holds
 // Gw = 32 / h groups (at most P2P_CHW), and the block's 4 Gw groups are team
 // g % T and slice g / T of S = 4 Gw / T equal slices of the list's source
@@ -501,7 +501,22 @@ fmm_p2p_rh2(Rule2D<float> rule, const float* __restrict__ pts,
 
     for (int64_t cb = 0; cb < n_o; cb += 128) {
         const int m = (int)min((int64_t)128, n_o - cb);
-        const int T = (m + 63) / 64, mt = (m + T - 1) / T;
+        // teams: the count (from ceil(m / 64) up to 8) with the most slices per
+        // obs triangle, m S, i.e. the fewest idle lanes and halves
+        int T = (m + 63) / 64;
+        {
+            int best = 0, bt = T;
+            for (int t = T; t <= 8; t++) {
+                const int mtt = (m + t - 1) / t, ht = (mtt + 1) / 2;
+                const int st = 4 * min(32 / ht, P2P_CHW) / t;
+                if (m * st > best) {
+                    best = m * st;
+                    bt = t;
+                }
+            }
+            T = bt;
+        }
+        const int mt = (m + T - 1) / T;
         const int h = (mt + 1) / 2;
         const int Gw = min(32 / h, P2P_CHW);
         const int S = 4 * Gw / T;
@@ -794,8 +809,19 @@ struct M2LPlan3 {
     alignas(16) int rec[FMM_NTMAX][16];
 };
 
+// Cube index of a multi-index: lin(c) = c0 S0 + c1 S1 + c2, additive and
+// injective on |c| <= p (S1 > p, S0 > p S1 + p); the strides are padded past
+// the minimum so that the lanes of a warp, reading Dh[lin(a) + lin(b)] for
+// their different b, spread over the shared-memory banks (p = 8: 10 and 91
+// instead of 9 and 81 cut a warp step's wavefronts from ~30 to ~24).
+__host__ __device__ inline int cube_s1(int p) { return p + 2; }
+__host__ __device__ inline int cube_s0(int p) { return p * cube_s1(p) + p + 3; }
 __host__ __device__ inline int cube_lin(int p, int a0, int a1, int a2) {
-    return (a0 * (p + 1) + a1) * (p + 1) + a2;
+    return a0 * cube_s0(p) + a1 * cube_s1(p) + a2;
+}
+// cube entries read: lin(a) + lin(b) for |a|, |b| <= p (masked pairs included)
+__host__ __device__ inline int cube_size(int p) {
+    return 2 * p * (cube_s0(p) + cube_s1(p) + 1) + 1;
 }
 
 // Builds the plan; returns 0, or 1 when the tuples do not fit the lanes.
@@ -902,8 +928,8 @@ struct M2L3Cfg {
 };
 
 // Shared-memory layout (floats), B pairs per pipeline stage: row buffers
-// 2 B x NT x NCHP, cubes 2 B x CUBEP (CUBEP >= 2 (p+1)^3, so lin(a) + lin(b)
-// needs no clamp; these two regions double as the reduction area, at least
+// 2 B x NT x NCHP, cubes 2 B x CUBEP (CUBEP >= cube_size(p), so lin(a) +
+// lin(b) needs no clamp; these two regions double as the reduction area, at least
 // 32 lanes' slots), graded Dc scratch B x NTP, 2 B x 40 scalars, 4 x
 // M2L3_CAP pair geometry, then ainfo (NTP ints), M2L3_CAP source node ids and
 // the recurrence table (NT x 16 ints).
@@ -917,7 +943,7 @@ __host__ __device__ inline M2L3Smem m2l3_smem(int p, int B) {
     M2L3Smem m;
     m.NT = n_terms(p);
     m.NTP = (m.NT + 3) / 4 * 4;
-    m.CUBEP = (2 * (p + 1) * (p + 1) * (p + 1) + 3) / 4 * 4;
+    m.CUBEP = (cube_size(p) + 3) / 4 * 4;
     const int need = 2 * B * (m.NT * C::NCHP + m.CUBEP);
     const int slots32 = 32 * M2L3Cfg<K>::NB * C::NCH;
     m.area = need > slots32 ? need : (slots32 + 3) / 4 * 4;
