@@ -1738,6 +1738,31 @@ int set_smem(KF kfn, size_t smem) {
     return TCT_OK;
 }
 
+// Per host thread and device: the high-priority stream that runs the
+// expansion stages next to P2P, and the fork / join events (created once,
+// kept for the process).
+struct SideStream {
+    int dev = -1;
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+inline SideStream* side_stream() {
+    static thread_local SideStream tab[16];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 16) return nullptr;
+    SideStream& e = tab[dev];
+    if (e.dev != dev) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+            cudaStreamCreateWithPriority(&e.s, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e.join, cudaEventDisableTiming) != cudaSuccess)
+            return nullptr;
+        e.dev = dev;
+    }
+    return &e;
+}
+
 template <typename R, int K, int NQ>
 int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double scale,
             const R* obs_pts, const int32_t* obs_tris, int64_t n_obs, const tct_fmm_tree& ot,
@@ -1771,18 +1796,17 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
     if (cudaMemsetAsync(W, 0, sizeof(R) * NA * (size_t)n_obs, st) != cudaSuccess ||
         cudaMemsetAsync(F, 0, sizeof(R) * C::NO * (size_t)NQ * n_obs, st) != cudaSuccess)
         return launch_status("fmm memset");
-    if (stt.n_leaves > 0) {
-        fmm_p2m<R, K, NQ><<<(unsigned)stt.n_leaves, 128, 0, st>>>(
-            c, p, stt.leaves, stt.start, stt.end, scent, srad, rec, mom);
-        if ((rc = launch_status("fmm p2m"))) return rc;
-    }
-    for (int h = 0; h < stt.n_levels; h++) {
-        const int64_t cnt = stt.level_offsets[h + 1] - stt.level_offsets[h];
-        if (cnt == 0) continue;
-        fmm_m2m<R, K><<<(unsigned)cnt, 128, 0, st>>>(p, stt.levels + stt.level_offsets[h],
-                                                     stt.children, scent, srad, mom);
-        if ((rc = launch_status("fmm m2m"))) return rc;
-    }
+    // The expansion stages (P2M .. L2P) run on a second, high-priority
+    // stream next to P2P: as P2P blocks retire the scheduler hands their SMs
+    // to M2L blocks first, so the FMA-bound P2P and the shared-memory-bound
+    // M2L share SMs instead of running back to back; joined before fmm_finish
+    SideStream* side = side_stream();
+    if (!side) return launch_status("fmm side stream");
+    const cudaStream_t sp = st;       // P2P
+    const cudaStream_t se = side->s;  // expansions
+    if (cudaEventRecord(side->fork, st) != cudaSuccess ||
+        cudaStreamWaitEvent(se, side->fork, 0) != cudaSuccess)
+        return launch_status("fmm fork");
     if (near.n_obs > 0) {
         if constexpr (p2p_packed<R, K, NQ>()) {
             const Rule2D<float>& rf = rule;
@@ -1792,19 +1816,19 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
                 (rc = set_smem(fmm_p2p_rh2<NQ, false>, smem)))
                 return rc;
             if (uniform) {
-                far_prep_rh2<NQ, true><<<pb, 128, 0, st>>>(c, rf, (const float*)src_pts,
+                far_prep_rh2<NQ, true><<<pb, 128, 0, sp>>>(c, rf, (const float*)src_pts,
                                                             src_tris, n_src, (const float*)in,
                                                             stt.orig, rec2);
                 if ((rc = launch_status("fmm prep (packed)"))) return rc;
-                fmm_p2p_rh2<NQ, true><<<(unsigned)near.n_obs, 128, smem, st>>>(
+                fmm_p2p_rh2<NQ, true><<<(unsigned)near.n_obs, 128, smem, sp>>>(
                     rf, (const float*)obs_pts, obs_tris, near.obs, near.start, near.src, ot.start,
                     ot.end, stt.start, stt.end, rec2, (float*)W);
             } else {
-                far_prep_rh2<NQ, false><<<pb, 128, 0, st>>>(c, rf, (const float*)src_pts,
+                far_prep_rh2<NQ, false><<<pb, 128, 0, sp>>>(c, rf, (const float*)src_pts,
                                                              src_tris, n_src, (const float*)in,
                                                              stt.orig, rec2);
                 if ((rc = launch_status("fmm prep (packed)"))) return rc;
-                fmm_p2p_rh2<NQ, false><<<(unsigned)near.n_obs, 128, smem, st>>>(
+                fmm_p2p_rh2<NQ, false><<<(unsigned)near.n_obs, 128, smem, sp>>>(
                     rf, (const float*)obs_pts, obs_tris, near.obs, near.start, near.src, ot.start,
                     ot.end, stt.start, stt.end, rec2, (float*)W);
             }
@@ -1812,26 +1836,38 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
         } else {
             const size_t smem = sizeof(R) * 128 * NA;
             if ((rc = set_smem(fmm_p2p<R, K, NQ>, smem))) return rc;
-            fmm_p2p<R, K, NQ><<<(unsigned)near.n_obs, 128, smem, st>>>(
+            fmm_p2p<R, K, NQ><<<(unsigned)near.n_obs, 128, smem, sp>>>(
                 c, rule, obs_pts, obs_tris, near.obs, near.start, near.src, ot.start, ot.end,
                 stt.start, stt.end, rec, W);
             if ((rc = launch_status("fmm p2p"))) return rc;
         }
     }
+    if (stt.n_leaves > 0) {
+        fmm_p2m<R, K, NQ><<<(unsigned)stt.n_leaves, 128, 0, se>>>(
+            c, p, stt.leaves, stt.start, stt.end, scent, srad, rec, mom);
+        if ((rc = launch_status("fmm p2m"))) return rc;
+    }
+    for (int h = 0; h < stt.n_levels; h++) {
+        const int64_t cnt = stt.level_offsets[h + 1] - stt.level_offsets[h];
+        if (cnt == 0) continue;
+        fmm_m2m<R, K><<<(unsigned)cnt, 128, 0, se>>>(p, stt.levels + stt.level_offsets[h],
+                                                     stt.children, scent, srad, mom);
+        if ((rc = launch_status("fmm m2m"))) return rc;
+    }
     if (mode == 0) {
         if (far.n_obs > 0) {
             const size_t smem = sizeof(R) * (size_t)C::NCHP * NT;
             if ((rc = set_smem(fmm_m2p<R, K>, smem))) return rc;
-            fmm_m2p<R, K><<<(unsigned)far.n_obs, 128, smem, st>>>(
+            fmm_m2p<R, K><<<(unsigned)far.n_obs, 128, smem, se>>>(
                 p, rule, NQ, far.obs, far.start, far.src, ot.start, ot.end, scent, srad, obs_pts,
                 obs_tris, mom, F);
             if ((rc = launch_status("fmm m2p"))) return rc;
         }
     } else {
-        if (cudaMemsetAsync(loc, 0, sz.loc, st) != cudaSuccess) return launch_status("fmm memset");
+        if (cudaMemsetAsync(loc, 0, sz.loc, se) != cudaSuccess) return launch_status("fmm memset");
         if (far.n_obs > 0) {
             const int64_t n_el = stt.n_nodes * (int64_t)NT * C::NCHP;
-            fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, st>>>(
+            fmm_moment_factorials<R><<<(unsigned)((n_el + 127) / 128), 128, 0, se>>>(
                 p, C::NCHP, stt.n_nodes, mom);
             if ((rc = launch_status("fmm moment factorials"))) return rc;
             bool lanes = false;  // the lane plan (fmm_m2l3) for FP32
@@ -1843,17 +1879,17 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
                 lanes = m2l3_make_plan(p, M2L3Cfg<K>::NB, &host_plan) == 0 && smem1 <= 227 * 1024;
                 if (lanes) {
                     M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
-                    fmm_m2l3_plan<<<1, 32, 0, st>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);
+                    fmm_m2l3_plan<<<1, 32, 0, se>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);
                     if ((rc = launch_status("fmm m2l plan"))) return rc;
                     // two pairs per stage while two CTAs still fit an SM
                     if (smem2 + 1024 <= 113 * 1024) {
                         if ((rc = set_smem(fmm_m2l3<K, 2>, (size_t)smem2))) return rc;
-                        fmm_m2l3<K, 2><<<(unsigned)far.n_obs, M2L3_THREADS, smem2, st>>>(
+                        fmm_m2l3<K, 2><<<(unsigned)far.n_obs, M2L3_THREADS, smem2, se>>>(
                             p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad,
                             mom, plan3, loc);
                     } else {
                         if ((rc = set_smem(fmm_m2l3<K, 1>, (size_t)smem1))) return rc;
-                        fmm_m2l3<K, 1><<<(unsigned)far.n_obs, M2L3_THREADS, smem1, st>>>(
+                        fmm_m2l3<K, 1><<<(unsigned)far.n_obs, M2L3_THREADS, smem1, se>>>(
                             p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad,
                             mom, plan3, loc);
                     }
@@ -1865,13 +1901,13 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
                     return TCT_ERR_ARG;
                 }
                 M2LPlan2* plan2 = reinterpret_cast<M2LPlan2*>(plan);
-                fmm_m2l2_plan<<<1, 32, 0, st>>>(p, plan2, plan_err);
+                fmm_m2l2_plan<<<1, 32, 0, se>>>(p, plan2, plan_err);
                 if ((rc = launch_status("fmm m2l plan"))) return rc;
                 const size_t smem_all = sizeof(R) * (2 * (size_t)NT * C::NCHP +
                                                      2 * (size_t)((NT + 3) / 4 * 4) + 80 +
                                                      (size_t)m2l2_items(p) * C::NCHP);
                 if ((rc = set_smem(fmm_m2l2<R, K>, smem_all))) return rc;
-                fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, st>>>(
+                fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, se>>>(
                     p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
                     plan2, loc);
             }
@@ -1883,18 +1919,21 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
         for (int d = 0; d < ot.n_levels; d++) {
             const int64_t cnt = ot.level_offsets[d + 1] - ot.level_offsets[d];
             if (cnt == 0) continue;
-            fmm_l2l<R, K><<<(unsigned)cnt, 128, smem_l2l, st>>>(
+            fmm_l2l<R, K><<<(unsigned)cnt, 128, smem_l2l, se>>>(
                 p, ot.levels + ot.level_offsets[d], ot.parent, ocent, orad, loc);
             if ((rc = launch_status("fmm l2l"))) return rc;
         }
         if (ot.n_leaves > 0) {
             const size_t smem = sizeof(R) * (size_t)C::NCHP * NT;
             if ((rc = set_smem(fmm_l2p<R, K>, smem))) return rc;
-            fmm_l2p<R, K><<<(unsigned)ot.n_leaves, 128, smem, st>>>(
+            fmm_l2p<R, K><<<(unsigned)ot.n_leaves, 128, smem, se>>>(
                 p, rule, NQ, ot.leaves, ot.start, ot.end, ocent, orad, obs_pts, obs_tris, loc, F);
             if ((rc = launch_status("fmm l2p"))) return rc;
         }
     }
+    if (cudaEventRecord(side->join, se) != cudaSuccess ||
+        cudaStreamWaitEvent(st, side->join, 0) != cudaSuccess)
+        return launch_status("fmm join");
     fmm_finish<R, K, NQ><<<(unsigned)((n_obs + 127) / 128), 128, 0, st>>>(
         rule, obs_pts, obs_tris, n_obs, ot.orig, W, F, (R)scale, out, accumulate);
     return launch_status("fmm finish");
