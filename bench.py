@@ -1410,6 +1410,77 @@ def run_c4solve_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def run_near_workload(args, rank, world, torch, dist):
+    """Near-pair search of the C4 mesh (1,016,894 triangles, threshold 2.5,
+    the operator build's first step): get_nearfield_device (host octrees and
+    traversal to leaf pairs, device ball tests, row fill and row sort) against
+    the host search; both give the reference's pair set in (obs, src) order."""
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.mesh import find_near_adj as fna
+    pts, tris = c4_mesh(args.grid or 707)
+    c, r = fna.get_tri_centroids_rs(pts, tris)
+    thr = 2.5
+    for _ in range(max(1, min(args.warmup, 2))):
+        out = fna.get_nearfield_device(c, r, c, r, thr)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    l0 = _lib.launch_count()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = fna.get_nearfield_device(c, r, c, r, thr)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    clocks = sampler.stop()
+    launches = (_lib.launch_count() - l0) // args.steps
+    n_pairs = int(out.shape[0])
+    t0 = time.perf_counter()
+    host_out = out.cpu().numpy()
+    d2h = time.perf_counter() - t0
+    # the device plan's host half alone (octrees + traversal)
+    t0 = time.perf_counter()
+    h = fna.near_plan(c, r, c, r, thr)
+    t_plan = time.perf_counter() - t0
+    n_leaf_pairs = int(_lib.lib.tct_near_plan_leaf_pairs(h))
+    _lib.lib.tct_near_plan_free(h)
+    if rank != 0:
+        return
+    line = {
+        "metric": "near-pair search pairs/s (get_nearfield, C4 mesh)",
+        "value": world * n_pairs / dt, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 tests, int64 pairs",
+        "data": "synthetic (seeded hills)",
+        "config": {"workload": ("near pairs of the C4 mesh (%d triangles), threshold %.1f: "
+                                "host octrees + traversal to leaf pairs, device tests, fill "
+                                "and per-row sort" % (tris.shape[0], thr)),
+                   "n_tris": int(tris.shape[0]), "pairs": n_pairs,
+                   "leaf_pairs": n_leaf_pairs, "host_plan_s": t_plan,
+                   "timing": "wall clock (host phases included)", "parallelism": "replicas",
+                   "l2": "inputs and pair arrays larger than L2"},
+        "roofline": {"kernel": "near_count / near_fill (ball tests)", "bound": "fp64",
+                     "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None,
+                     "traffic": None},
+        "e2e": {"value": world * n_pairs / (dt + d2h), "unit": "pairs/s",
+                "h2d_bytes_per_step": int(c.nbytes + r.nbytes),
+                "d2h_bytes_per_step": int(host_out.nbytes),
+                "api": "get_nearfield_device(numpy) -> torch, then .cpu()"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        ref = fna.get_nearfield(c, r, c, r, thr)
+        th = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": ref.shape[0] / th, "unit": "pairs/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": "the whole search once with the host restatement (tct_find_near_pairs, "
+                      "OpenMP on all host threads, bit-exact with the reference's finder): "
+                      "%.2f s; identical output: %s" % (th, bool(np.array_equal(ref, host_out)))}
+    print(json.dumps(line), flush=True)
+
+
 def run_interior_workload(args, rank, world, torch, dist):
     """Interior evaluation (InteriorOp.dot) on the reference's interior
     nearfield test configuration, scaled: a make_rect(n, n) fault in the
@@ -1725,7 +1796,7 @@ def main():
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
                     choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd",
-                             "interior", "c4solve"],
+                             "interior", "c4solve", "near"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -1763,11 +1834,12 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd", "interior",
-                         "c4solve"):
+                         "c4solve", "near"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
          "panel": run_panel_workload, "batch": run_batch_workload,
          "serve": run_serve_workload, "qd": run_qd_workload,
-         "interior": run_interior_workload, "c4solve": run_c4solve_workload}[args.workload](
+         "interior": run_interior_workload, "c4solve": run_c4solve_workload,
+         "near": run_near_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()

@@ -229,6 +229,24 @@ int64_t tct_pairs_count(const tct_pair_list* list);
 int tct_pairs_copy(const tct_pair_list* list, int64_t* dst);
 void tct_pairs_free(tct_pair_list* list);
 
+/* Device near-pair search: the same pair set and (obs, src) order as
+ * tct_find_near_pairs (mesh/fast_find_nearfield.cpp:22-74, 96-141,
+ * get_nearfield :255-285), with the ball tests, row fill and row sort on the
+ * GPU.  tct_near_plan_build (host) builds the reference's octrees and runs
+ * its dual traversal down to leaf pairs; tct_near_device_count uploads the
+ * plan, counts the pairs and synchronises `stream` to return the total;
+ * tct_near_device_fill writes the pairs (total x 2 int64, caller-owned
+ * device memory) in (obs, src) order.  The plan owns its device buffers;
+ * tct_near_plan_free releases them.  At most 2^31 - 1 pairs. */
+typedef struct tct_near_plan tct_near_plan;
+int tct_near_plan_build(const double* obs_centers, const double* obs_radii, int64_t n_obs,
+                        const double* src_centers, const double* src_radii, int64_t n_src,
+                        double threshold, int n_threads, tct_near_plan** out);
+int64_t tct_near_plan_leaf_pairs(const tct_near_plan* plan);
+int tct_near_device_count(tct_near_plan* plan, void* stream, int64_t* total);
+int tct_near_device_fill(tct_near_plan* plan, int64_t* pairs, void* stream);
+void tct_near_plan_free(tct_near_plan* plan);
+
 /* Split close pairs by the number of shared vertices
  * (mesh/fast_find_nearfield.cpp:143-182): 0 -> near (2 cols), 1 -> vertex
  * adjacent (4 cols: obs, src, obs corner, src corner), 2 -> edge adjacent

@@ -66,6 +66,12 @@ _SIGS = {
     "tct_pairs_count": ([c_p], c_i64),
     "tct_pairs_copy": ([c_p, c_i64p], c_i),
     "tct_pairs_free": ([c_p], None),
+    "tct_near_plan_build": ([c_dp, c_dp, c_i64, c_dp, c_dp, c_i64, ctypes.c_double, c_i,
+                             ctypes.POINTER(c_p)], c_i),
+    "tct_near_plan_leaf_pairs": ([c_p], c_i64),
+    "tct_near_device_count": ([c_p, c_p, ctypes.POINTER(c_i64)], c_i),
+    "tct_near_device_fill": ([c_p, c_p, c_p], c_i),
+    "tct_near_plan_free": ([c_p], None),
     "tct_split_adjacent_close": ([c_i64p, c_i64, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p, c_i64p,
                                   c_i64p, c_i64p], c_i),
     "tct_resolve_ea_rotation": ([c_i64p, c_i64p, c_i64, c_i64p], c_i),

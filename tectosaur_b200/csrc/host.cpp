@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "tct_b200.h"
+#include "near_plan.h"
 
 namespace tct {
 
@@ -230,6 +231,27 @@ void query(const Query& q, int64_t on, int64_t sn, std::vector<int64_t>& out) {
     }
 }
 
+// The same traversal, stopping at leaf pairs: (obs node, src node) pairs
+// whose balls the leaf test above would examine.
+void query_leaves(const Query& q, int64_t on, int64_t sn, std::vector<int64_t>& out) {
+    const Node& o = q.ot.nodes[on];
+    const Node& s = q.st.nodes[sn];
+    const double r1 = q.oer[on], r2 = q.ser[sn];
+    const double limit = std::pow((r1 + r2) * q.thr, 2);
+    if (dist2(o.c, s.c) > limit) return;
+    if (o.leaf && s.leaf) {
+        out.push_back(on);
+        out.push_back(sn);
+        return;
+    }
+    const bool split_src = ((r1 < r2) && !s.leaf) || o.leaf;
+    if (split_src) {
+        for (int k = 0; k < 8; k++) query_leaves(q, on, s.child[k], out);
+    } else {
+        for (int k = 0; k < 8; k++) query_leaves(q, o.child[k], sn, out);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -316,6 +338,89 @@ int tct_find_near_pairs(const double* obs_c, const double* obs_r, int64_t n_obs,
     }
     *out = list;
     return TCT_OK;
+}
+
+// Host half of the device near-pair search (tct_near_device_count/_fill,
+// csrc/near.cu): the same octrees and traversal as tct_find_near_pairs, down
+// to leaf pairs, grouped by obs leaf.
+int tct_near_plan_build(const double* obs_c, const double* obs_r, int64_t n_obs,
+                        const double* src_c, const double* src_r, int64_t n_src,
+                        double threshold, int n_threads, tct_near_plan** out) {
+    using namespace tct;
+    if (!out) {
+        set_error("tct_near_plan_build: null output handle");
+        return TCT_ERR_ARG;
+    }
+    *out = nullptr;
+    if (n_obs < 0 || n_src < 0 || !(threshold >= 0)) {
+        set_error("tct_near_plan_build: bad size or threshold");
+        return TCT_ERR_ARG;
+    }
+    auto* plan = new tct_near_plan();
+    plan->n_obs = n_obs;
+    plan->n_src = n_src;
+    plan->threshold = threshold;
+    plan->lp_start.push_back(0);
+    if (n_obs == 0 || n_src == 0) {
+        *out = plan;
+        return TCT_OK;
+    }
+    if (!obs_c || !obs_r || !src_c || !src_r) {
+        delete plan;
+        set_error("tct_near_plan_build: null pointer");
+        return TCT_ERR_ARG;
+    }
+    if (n_threads <= 0) n_threads = omp_get_max_threads();
+    const int64_t leaf = 50;
+    Octree ot = build_octree(obs_c, obs_r, n_obs, leaf);
+    Octree st = build_octree(src_c, src_r, n_src, leaf);
+    std::vector<double> oer = expanded_r(ot, obs_r);
+    std::vector<double> ser = expanded_r(st, src_r);
+    Query q{ot, st, oer, ser, obs_r, src_r, threshold};
+    std::vector<int64_t> starts;
+    for (size_t k = 0; k < ot.nodes.size(); k++) {
+        const Node& n = ot.nodes[k];
+        if (n.depth > 2) continue;
+        if (n.depth != 2 && !n.leaf) continue;
+        starts.push_back((int64_t)k);
+    }
+    std::vector<std::vector<int64_t>> parts(starts.size());
+#pragma omp parallel for num_threads(n_threads) schedule(dynamic, 1)
+    for (int64_t k = 0; k < (int64_t)starts.size(); k++) query_leaves(q, starts[k], 0, parts[k]);
+    // group the leaf pairs by obs leaf (counting sort on the node id, stable)
+    std::vector<int64_t> cnt(ot.nodes.size() + 1, 0);
+    for (auto& p : parts)
+        for (size_t m = 0; m < p.size(); m += 2) cnt[p[m] + 1]++;
+    for (size_t k = 0; k < ot.nodes.size(); k++) cnt[k + 1] += cnt[k];
+    const int64_t n_lp = cnt[ot.nodes.size()];
+    std::vector<int64_t> srcn(n_lp);
+    {
+        std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+        for (auto& p : parts)
+            for (size_t m = 0; m < p.size(); m += 2) srcn[fill[p[m]]++] = p[m + 1];
+    }
+    for (size_t k = 0; k < ot.nodes.size(); k++) {
+        if (cnt[k + 1] == cnt[k]) continue;
+        plan->leaf_start.push_back(ot.nodes[k].start);
+        plan->leaf_end.push_back(ot.nodes[k].end);
+        for (int64_t m = cnt[k]; m < cnt[k + 1]; m++) {
+            plan->lp_s.push_back(st.nodes[srcn[m]].start);
+            plan->lp_e.push_back(st.nodes[srcn[m]].end);
+        }
+        plan->lp_start.push_back((int64_t)plan->lp_s.size());
+    }
+    plan->oc = std::move(ot.centers);
+    plan->sc = std::move(st.centers);
+    plan->orq.assign(obs_r, obs_r + n_obs);
+    plan->srq.assign(src_r, src_r + n_src);
+    plan->oorig = std::move(ot.orig);
+    plan->sorig = std::move(st.orig);
+    *out = plan;
+    return TCT_OK;
+}
+
+int64_t tct_near_plan_leaf_pairs(const tct_near_plan* plan) {
+    return plan ? (int64_t)plan->lp_s.size() : -1;
 }
 
 // ---- treecode trees and interaction lists (fmm/tsfmm.py:22-28, 66-70) --------

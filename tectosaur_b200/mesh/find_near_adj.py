@@ -37,11 +37,57 @@ def get_nearfield(obs_centers, obs_radii, src_centers, src_radii, threshold, n_t
     return out
 
 
+def near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads=0):
+    """Host half of the device search: the reference's octrees and dual
+    traversal down to leaf pairs (an opaque handle; free with
+    `_lib.lib.tct_near_plan_free`)."""
+    oc = np.ascontiguousarray(obs_centers, dtype=np.float64).reshape(-1, 3)
+    orr = np.ascontiguousarray(obs_radii, dtype=np.float64).reshape(-1)
+    sc = np.ascontiguousarray(src_centers, dtype=np.float64).reshape(-1, 3)
+    sr = np.ascontiguousarray(src_radii, dtype=np.float64).reshape(-1)
+    handle = ctypes.c_void_p()
+    _lib.check(_lib.lib.tct_near_plan_build(
+        _lib.dptr(oc), _lib.dptr(orr), oc.shape[0], _lib.dptr(sc), _lib.dptr(sr), sc.shape[0],
+        float(threshold), int(n_threads), ctypes.byref(handle)), "tct_near_plan_build")
+    return handle
+
+
+def get_nearfield_device(obs_centers, obs_radii, src_centers, src_radii, threshold,
+                         n_threads=0, stream=None):
+    """get_nearfield with the ball tests, row fill and row sort on the GPU:
+    the same pairs in the same order, as an int64 (P, 2) CUDA tensor."""
+    from ..util import device
+    t = device.require_cuda()
+    handle = near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads)
+    try:
+        s = _lib.stream_ptr(stream)
+        total = ctypes.c_int64()
+        _lib.check(_lib.lib.tct_near_device_count(handle, s, ctypes.byref(total)),
+                   "tct_near_device_count")
+        out = t.empty((total.value, 2), dtype=t.int64, device="cuda")
+        _lib.check(_lib.lib.tct_near_device_fill(handle, ctypes.c_void_p(out.data_ptr()), s),
+                   "tct_near_device_fill")
+        # the plan's device buffers are released after the fill has run
+        t.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+    finally:
+        _lib.lib.tct_near_plan_free(handle)
+    return out
+
+
+# meshes from this many triangles search on the GPU when one is visible
+DEVICE_NEAR_MIN_TRIS = 100_000
+
+
 def find_close_or_touching(a_pts, a_tris, b_pts, b_tris, threshold):
     """Pairs (i in a, j in b) whose bounding balls, scaled by `threshold`,
-    touch (find_near_adj.py:29-35)."""
+    touch (find_near_adj.py:29-35).  Large meshes use the device search when
+    a GPU is visible; both give the same pairs in the same order."""
     ca, ra = get_tri_centroids_rs(a_pts, a_tris)
     cb, rb = get_tri_centroids_rs(b_pts, b_tris)
+    if max(ca.shape[0], cb.shape[0]) >= DEVICE_NEAR_MIN_TRIS:
+        from ..util import device
+        if device.cuda_available():
+            return get_nearfield_device(ca, ra, cb, rb, threshold).cpu().numpy()
     return get_nearfield(ca, ra, cb, rb, threshold)
 
 

@@ -8,6 +8,13 @@ def torch():
     return _torch
 
 
+def cuda_available():
+    try:
+        return torch().cuda.is_available()
+    except ImportError:
+        return False
+
+
 def require_cuda():
     t = torch()
     if not t.cuda.is_available():

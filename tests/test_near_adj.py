@@ -153,3 +153,22 @@ def test_bit_exact_vs_compiled_reference(n, thr):
     b = fna.split_adjacent_close(mine, tris, tris)
     for x, y in zip(a, b):
         assert np.array_equal(lexsorted(x), lexsorted(y))
+
+
+def test_device_plan_builds_on_host():
+    """The host half of the device search (octrees + traversal to leaf pairs)
+    needs no GPU: leaf pairs exist for a touching mesh, none for far meshes."""
+    from tectosaur_b200 import _lib
+    pts, tris = bumpy_mesh(40, seed=40)
+    c, r = fna.get_tri_centroids_rs(pts, tris)
+    h = fna.near_plan(c, r, c, r, 2.5)
+    try:
+        assert _lib.lib.tct_near_plan_leaf_pairs(h) > 0
+    finally:
+        _lib.lib.tct_near_plan_free(h)
+    h = fna.near_plan(c, r, c + 1e3, r, 2.5)
+    try:
+        assert _lib.lib.tct_near_plan_leaf_pairs(h) == 0
+    finally:
+        _lib.lib.tct_near_plan_free(h)
+
