@@ -37,6 +37,7 @@
 // P2P runs the direct farfield's triangle-level pair loop (far_common.cuh) on
 // the listed leaf pairs, from the same per-source records the P2M reads.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -792,7 +793,9 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 constexpr int M2L3_THREADS = 256;
 constexpr int M2L3_LANES = M2L3_THREADS - 32;
 constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
+constexpr int M2L3_PLAN_TAG = 0x4d324c33;  // "M2L3": the plan below is complete
 struct M2LPlan3 {
+    int tag;  // M2L3_PLAN_TAG once built (written last)
     int p, nb, L, n_lanes, n_k;
     int lane_k[M2L3_LANES];    // tuple of the lane (b = k NB + j), -1 for none
     int lane_a0[M2L3_LANES];   // first source term (graded) and chunk length
@@ -913,10 +916,20 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
     return 0;
 }
 
+// Builds the plan in the operator's workspace once: a plan tagged complete
+// for this (p, nb) -- it depends on nothing else -- is reused.
 __global__ void __launch_bounds__(32) fmm_m2l3_plan(int p, int nb, M2LPlan3* __restrict__ plan,
                                                     int* err) {
     if (threadIdx.x != 0) return;
-    if (m2l3_make_plan(p, nb, plan)) *err = 1;
+    volatile int* tag = &plan->tag;
+    if (*tag == M2L3_PLAN_TAG && plan->p == p && plan->nb == nb) return;
+    *tag = 0;
+    if (m2l3_make_plan(p, nb, plan)) {
+        *err = 1;
+        return;
+    }
+    __threadfence();
+    *tag = M2L3_PLAN_TAG;
 }
 
 // Terms b per lane (FP32): the accumulators (NB x NCH values) stay near 64
@@ -1678,6 +1691,19 @@ struct Sizes {
     size_t rec, mom, loc, plan, W, F, rec2;
 };
 
+// Whether the lane plan fits for (p, nb), decided on the host once.
+inline bool m2l3_plan_fits(int p, int nb) {
+    static std::atomic<int> fits[FMM_MAXP + 1][16];  // 0 unknown, 1 yes, 2 no
+    if (p < 0 || p > FMM_MAXP || nb < 1 || nb > 15) return false;
+    int v = fits[p][nb].load(std::memory_order_relaxed);
+    if (v == 0) {
+        std::vector<unsigned char> buf(sizeof(M2LPlan3));
+        v = m2l3_make_plan(p, nb, reinterpret_cast<M2LPlan3*>(buf.data())) == 0 ? 1 : 2;
+        fits[p][nb].store(v, std::memory_order_relaxed);
+    }
+    return v == 1;
+}
+
 inline size_t m2l_plan_bytes() {
     return sizeof(M2LPlan2) > sizeof(M2LPlan3) ? sizeof(M2LPlan2) : sizeof(M2LPlan3);
 }
@@ -1873,10 +1899,9 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             bool lanes = false;  // the lane plan (fmm_m2l3) for FP32
             int* plan_err = reinterpret_cast<int*>(plan + al256(m2l_plan_bytes()));
             if constexpr (sizeof(R) == 4) {
-                M2LPlan3 host_plan;
                 const int smem1 = m2l3_smem<K>(p, 1).total_bytes;
                 const int smem2 = m2l3_smem<K>(p, 2).total_bytes;
-                lanes = m2l3_make_plan(p, M2L3Cfg<K>::NB, &host_plan) == 0 && smem1 <= 227 * 1024;
+                lanes = m2l3_plan_fits(p, M2L3Cfg<K>::NB) && smem1 <= 227 * 1024;
                 if (lanes) {
                     M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
                     fmm_m2l3_plan<<<1, 32, 0, se>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);

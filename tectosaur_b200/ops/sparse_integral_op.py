@@ -51,8 +51,42 @@ class RegularizedSparseIntegralOp:
         return twin
 
     # -- device apply -------------------------------------------------------
+    # operators from this many rows run the nearfield next to an FMM farfield
+    OVERLAP_MIN_ROWS = 9 * 100_000
+
+    def _overlap_near(self):
+        from ..fmm.tsfmm import FMMFarfieldOpImpl
+        return (isinstance(self.farfield, FMMFarfieldOpImpl)
+                and hasattr(self.nearfield, "dot_device") and self.shape[0] >= self.OVERLAP_MIN_ROWS)
+
+    def _overlapped(self, x, y, stream, near_into, far):
+        """near_into(buf, side stream) next to far(main stream); y += buf."""
+        t = device.torch()
+        main = stream if stream is not None else t.cuda.current_stream()
+        if getattr(self, "_near_stream", None) is None:
+            self._near_stream = t.cuda.Stream(priority=t.cuda.Stream.priority_range()[1])
+        side = self._near_stream
+        buf = getattr(self, "_near_buf", None)
+        if buf is None or buf.dtype != y.dtype or buf.shape != y.shape:
+            buf = self._near_buf = t.empty_like(y)
+        side.wait_stream(main)
+        near_into(buf, side)
+        far(main)
+        main.wait_stream(side)
+        with t.cuda.stream(main):
+            y.add_(buf)
+        return y
+
     def dot_device(self, x, y, stream=None):
-        """y = (Far + Near) x on device tensors of float_type."""
+        """y = (Far + Near) x on device tensors of float_type.  With an FMM
+        farfield on a large mesh the nearfield BSR (HBM-bound) runs on a
+        high-priority second stream into its own buffer while the FMM
+        (compute-bound) runs, and is added at the end."""
+        if self._overlap_near():
+            return self._overlapped(
+                x, y, stream, lambda b, s: self.nearfield.dot_device(x, b, accumulate=False,
+                                                                      stream=s),
+                lambda s: self.farfield.dot_device(x, y, accumulate=False, stream=s))
         if hasattr(self.farfield, "dot_device"):
             self.farfield.dot_device(x, y, accumulate=False, stream=stream)
         else:
@@ -66,6 +100,13 @@ class RegularizedSparseIntegralOp:
         elasticRH3 FP32 farfield runs on the tensor cores, the nearfield BSR
         in one launch)."""
         far = self.farfield
+        if self._overlap_near() and not hasattr(far, "dot_panel_device"):
+            def far_all(s):
+                for r in range(X.shape[0]):
+                    far.dot_device(X[r], Y[r], accumulate=False, stream=s)
+            return self._overlapped(
+                X, Y, stream, lambda b, s: self.nearfield.dot_panel_device(X, b, accumulate=False,
+                                                                            stream=s), far_all)
         if hasattr(far, "dot_panel_device"):
             far.dot_panel_device(X, Y, accumulate=False, stream=stream)
         else:

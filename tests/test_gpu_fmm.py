@@ -110,3 +110,39 @@ def test_fmm_farfield_op_in_sparse_op(cuda, mode):
     a = direct.dot(v)
     b = fmm.dot(v)
     assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-5
+
+
+@pytest.mark.parametrize("float_type", [np.float32, np.float64])
+def test_nearfield_overlap_path(cuda, float_type, monkeypatch):
+    """Large FMM operators run the nearfield BSR on a second stream next to the
+    FMM and add it at the end; forced on a small operator, the single apply,
+    the panel apply and a captured graph equal the sequential apply."""
+    torch = cuda
+    n = 12
+    pts, tris = make_rect(n, n, CORNERS)
+    pts = pts.copy()
+    pts[:, 2] = 0.1 * np.sin(2 * pts[:, 0]) * np.cos(pts[:, 1])
+    pts[:, :2] += 2.0
+    args = (4, 4, 3, 2, 3, 2.5, "elasticRH3", "elasticRH3", [1.0, 0.25], pts, tris, float_type)
+    op = RegularizedSparseIntegralOp(*args, farfield_op_type=FMMFarfieldOp(2.5, 8, 8, "fmm"))
+    v = np.random.default_rng(6).random(tris.shape[0] * 9).astype(float_type)
+    x = torch.from_numpy(v).cuda()
+    seq = torch.empty(op.shape[0], dtype=x.dtype, device="cuda")
+    assert not op._overlap_near()
+    op.dot_device(x, seq)
+    monkeypatch.setattr(RegularizedSparseIntegralOp, "OVERLAP_MIN_ROWS", 0)
+    assert op._overlap_near()
+    ov = torch.empty_like(seq)
+    op.dot_device(x, ov)
+    torch.cuda.synchronize()
+    assert torch.equal(ov, seq)
+    X = torch.stack([x, 2 * x])
+    Y = torch.empty((2, op.shape[0]), dtype=x.dtype, device="cuda")
+    op.dot_panel_device(X, Y)
+    torch.cuda.synchronize()
+    assert torch.equal(Y[0], seq)
+    g, gx, gy = op.capture_graph()
+    gx.copy_(x)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(gy, seq)
