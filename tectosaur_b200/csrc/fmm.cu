@@ -777,12 +777,15 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 // sum_a f_|a| Dc_(a+b) (N_a with the Yl correction Y_dj - R0_d m_j), |a| + |b|
 // <= p (ts_kernels.cl's m2l restated as a contraction over the pair's Dc
 // tensor).  Organised for throughput:
-//  * warp 0 is the producer: for source node k + 1 it computes rho, f_n,
-//    (s_o/rho)^n / rho and Dc level by level, and scatters Dc into a dense
-//    (p+1)^3 cube, so that Dc_(a+b) = cube[lin(a) + lin(b)] is one indexed
-//    load; every thread copies its share of node k + 1's moments into the
-//    second row buffer with cp.async while node k is contracted;
-//  * each of the 224 contraction lanes owns a fixed tuple of NB consecutive
+//  * warps 0 and 1 are producers: for the next stage's source nodes (one
+//    each when a stage holds two pairs) they compute rho, f_n,
+//    (s_o/rho)^n / rho and Dc level by level, and scatter Dc into a dense
+//    cube, so that Dc_(a+b) = cube[lin(a) + lin(b)] is one indexed load;
+//    every thread copies its share of the next stage's moments into the
+//    second row buffers with cp.async while the current stage is
+//    contracted (the recurrence is latency-bound: one producer warp per
+//    pair keeps it off the critical path);
+//  * each of the 192 contraction lanes owns a fixed tuple of NB consecutive
 //    local terms b (all channels, accumulated in registers across the whole
 //    list) and a contiguous chunk of source terms a, the same chunk for the
 //    tuples that share it, so lanes of a warp mostly read the same source
@@ -791,7 +794,8 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 //    and each b sums its chunks in a fixed lane order and scales by 1 / b!.
 // The plan (tuples, chunk length, lane tables) depends only on p and NB.
 constexpr int M2L3_THREADS = 256;
-constexpr int M2L3_LANES = M2L3_THREADS - 32;
+constexpr int M2L3_NPROD = 2;  // producer warps (with one pair per stage, warp 1 idles)
+constexpr int M2L3_LANES = M2L3_THREADS - 32 * M2L3_NPROD;
 constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
 constexpr int M2L3_PLAN_TAG = 0x4d324c33;  // "M2L3": the plan below is complete
 struct M2LPlan3 {
@@ -1035,11 +1039,16 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     // coef(a, b) = f_|a| (s_o/rho)^|b| / rho Dc_(a+b) = S_|a| Dh_(a+b) with
     // Dh_c = Dc_c (s_o/rho)^|c| / rho (the cube) and S_n = (-s_s/s_o)^n; the
     // B pairs' recurrences run interleaved (independent chains)
-    auto produce = [&](int64_t k0, int st) {  // warp 0
+    // producer warp w handles the stage's pairs u0 .. u0 + PB - 1
+    constexpr int PB = (B % M2L3_NPROD == 0) ? B / M2L3_NPROD : B;
+    auto produce = [&](int64_t k0, int st) {  // warps 0 .. M2L3_NPROD - 1
+        const int u0 = (B % M2L3_NPROD == 0) ? warp * PB : 0;
+        if (B % M2L3_NPROD != 0 && warp > 0) return;
         float Rh[B][3], q[B], pwn[B];
         bool on[B];
 #pragma unroll
-        for (int u = 0; u < B; u++) {
+        for (int uu = 0; uu < PB; uu++) {
+            const int u = u0 + uu;
             const int64_t k = k0 + u;
             on[u] = k < npair;
             float cs[3] = {co[0] + 1.f, co[1], co[2]}, rs = 0.f;  // any distinct point if off
@@ -1081,7 +1090,8 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
                 const int4* rt = reinterpret_cast<const int4*>(rtab + 16 * (b0 + w));
                 const int4 i0 = rt[0], i1 = rt[1], f0 = rt[2], f1 = rt[3];
 #pragma unroll
-                for (int u = 0; u < B; u++) {
+                for (int uu = 0; uu < PB; uu++) {
+                    const int u = u0 + uu;
                     const float* D = Dg + u * sm.NTP;
                     v[u][h] = __int_as_float(f0.x) * Rh[u][0] * D[i0.x] +
                               __int_as_float(f0.y) * Rh[u][1] * D[i0.y] +
@@ -1093,7 +1103,8 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
                 cl[h] = i0.w;
             }
 #pragma unroll
-            for (int u = 0; u < B; u++) {
+            for (int uu = 0; uu < PB; uu++) {
+                const int u = u0 + uu;
                 pwn[u] *= q[u];
 #pragma unroll
                 for (int h = 0; h < 2; h++)
@@ -1107,14 +1118,14 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     };
 
     // this lane's tuple and source chunk
-    const int ct = tid - 32;
+    const int ct = tid - 32 * M2L3_NPROD;
     int kk = -1, a_first = 0, cnt = 0, wsteps = 0;
     int blin[NB], thr[NB];
-    if (warp > 0) {
+    if (warp >= M2L3_NPROD) {
         kk = plan->lane_k[ct];
         a_first = plan->lane_a0[ct];
         cnt = plan->lane_cnt[ct];
-        wsteps = plan->warp_steps[warp - 1];
+        wsteps = plan->warp_steps[warp - M2L3_NPROD];
     }
 #pragma unroll
     for (int j = 0; j < NB; j++) {
@@ -1138,7 +1149,7 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     const int64_t nst = (npair + B - 1) / B;  // pipeline stages of B pairs
     if (nst > 0) {
         issue_copy(0, 0);
-        if (warp == 0) produce(0, 0);
+        if (warp < M2L3_NPROD) produce(0, 0);
     }
     for (int64_t st = 0; st < nst; st++) {
         const int buf = (int)(st & 1);
@@ -1146,9 +1157,9 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
         __syncthreads();  // stage st's rows, cubes and scalars are complete; st - 1 is done
         if (st + 1 < nst) {
             issue_copy((st + 1) * B, buf ^ 1);
-            if (warp == 0) produce((st + 1) * B, buf ^ 1);
+            if (warp < M2L3_NPROD) produce((st + 1) * B, buf ^ 1);
         }
-        if (warp == 0) continue;
+        if (warp < M2L3_NPROD) continue;
 #pragma unroll 1
         for (int u = 0; u < B; u++) {
             if (st * B + u >= npair) break;
@@ -1200,7 +1211,7 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     float* Lg = loc + node * (int64_t)rowsz;
     for (int lo = 0; lo < M2L3_LANES; lo += lpr) {
         const int hi = lo + lpr < M2L3_LANES ? lo + lpr : M2L3_LANES;
-        if (warp > 0 && ct >= lo && ct < hi) {
+        if (warp >= M2L3_NPROD && ct >= lo && ct < hi) {
             float* sl = base + (ct - lo) * PER;
 #pragma unroll
             for (int j = 0; j < NB; j++)
