@@ -350,12 +350,14 @@ size_t tct_fmm_workspace_bytes(int kernel, int prec, int mode, int order, int n_
                                int64_t n_obs, int64_t n_src, int64_t n_obs_nodes,
                                int64_t n_src_nodes);
 
-/* Host-side check of the FMM M2L work plan (no GPU): for order p and nb
- * local terms per lane, out[0] = valid (a, b) pairs covered, out[1] = pairs
- * covered twice (or lanes over their warp's step count), out[2] = the chunk
- * length, out[3] = lanes used, out[4] = summed warp step counts.  Returns 0,
- * or 1 when the plan does not fit.  Test support for tct_fmm_matvec. */
-int tct_fmm_m2l_plan_stats(int order, int nb, int64_t* out);
+/* Host-side check of the FMM M2L work plan (no GPU): for order p, nb local
+ * terms per lane and `lanes` contraction lanes (a multiple of 32, at most
+ * 224; the FP32 M2L uses 192 with two source nodes per pipeline stage, 224
+ * with one), out[0] = valid (a, b) pairs covered, out[1] = pairs covered
+ * twice (or lanes over their warp's step count), out[2] = the chunk length,
+ * out[3] = lanes used, out[4] = summed warp step counts.  Returns 0, or 1
+ * when the plan does not fit.  Test support for tct_fmm_matvec. */
+int tct_fmm_m2l_plan_stats(int order, int nb, int lanes, int64_t* out);
 
 /* Treecode / FMM farfield matvec for elasticU3, elasticRT3, elasticRA3 and
  * elasticRH3; replaces TSFMM.dot (fmm/tsfmm.py:241-256, the p2m, m2m, p2p and

@@ -171,7 +171,7 @@ class FmmList(ctypes.Structure):
 
 _FMM_SIGS = {
     "tct_fmm_workspace_bytes": ([c_i, c_i, c_i, c_i, c_i, c_i64, c_i64, c_i64, c_i64], c_sz),
-    "tct_fmm_m2l_plan_stats": ([c_i, c_i, ctypes.POINTER(c_i64)], c_i),
+    "tct_fmm_m2l_plan_stats": ([c_i, c_i, c_i, ctypes.POINTER(c_i64)], c_i),
     "tct_fmm_matvec": ([c_i, c_i, c_i, c_i, c_i, c_dp, c_dp, c_dp, ctypes.c_double, c_p, c_p,
                         c_i64, ctypes.POINTER(FmmTree), c_p, c_p, c_i64,
                         ctypes.POINTER(FmmTree), ctypes.POINTER(FmmList),

@@ -777,15 +777,16 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 // sum_a f_|a| Dc_(a+b) (N_a with the Yl correction Y_dj - R0_d m_j), |a| + |b|
 // <= p (ts_kernels.cl's m2l restated as a contraction over the pair's Dc
 // tensor).  Organised for throughput:
-//  * warps 0 and 1 are producers: for the next stage's source nodes (one
-//    each when a stage holds two pairs) they compute rho, f_n,
+//  * warps 0 and 1 (warp 0 alone for one-pair stages) are producers: for
+//    the next stage's source nodes (one each) they compute rho, f_n,
 //    (s_o/rho)^n / rho and Dc level by level, and scatter Dc into a dense
 //    cube, so that Dc_(a+b) = cube[lin(a) + lin(b)] is one indexed load;
 //    every thread copies its share of the next stage's moments into the
 //    second row buffers with cp.async while the current stage is
 //    contracted (the recurrence is latency-bound: one producer warp per
 //    pair keeps it off the critical path);
-//  * each of the 192 contraction lanes owns a fixed tuple of NB consecutive
+//  * each contraction lane (192 with two-pair stages, 224 with one-pair
+//    stages) owns a fixed tuple of NB consecutive
 //    local terms b (all channels, accumulated in registers across the whole
 //    list) and a contiguous chunk of source terms a, the same chunk for the
 //    tuples that share it, so lanes of a warp mostly read the same source
@@ -794,13 +795,16 @@ __device__ __forceinline__ R mfact(int b0, int b1, int b2) {
 //    and each b sums its chunks in a fixed lane order and scales by 1 / b!.
 // The plan (tuples, chunk length, lane tables) depends only on p and NB.
 constexpr int M2L3_THREADS = 256;
-constexpr int M2L3_NPROD = 2;  // producer warps (with one pair per stage, warp 1 idles)
-constexpr int M2L3_LANES = M2L3_THREADS - 32 * M2L3_NPROD;
+// producer warps: one per pair of a two-pair stage, one for a one-pair stage
+// (at the large orders that need one-pair stages the contraction dominates)
+__host__ __device__ constexpr int m2l3_nprod(int B) { return B == 2 ? 2 : 1; }
+__host__ __device__ constexpr int m2l3_lanes(int B) { return M2L3_THREADS - 32 * m2l3_nprod(B); }
+constexpr int M2L3_LANES = M2L3_THREADS - 32;  // table capacity (the most lanes)
 constexpr int FMM_NTMAX = (FMM_MAXP + 1) * (FMM_MAXP + 2) * (FMM_MAXP + 3) / 6;
 constexpr int M2L3_PLAN_TAG = 0x4d324c33;  // "M2L3": the plan below is complete
 struct M2LPlan3 {
     int tag;  // M2L3_PLAN_TAG once built (written last)
-    int p, nb, L, n_lanes, n_k;
+    int p, nb, lanes, L, n_lanes, n_k;
     int lane_k[M2L3_LANES];    // tuple of the lane (b = k NB + j), -1 for none
     int lane_a0[M2L3_LANES];   // first source term (graded) and chunk length
     int lane_cnt[M2L3_LANES];
@@ -837,11 +841,13 @@ __host__ __device__ inline int cube_size(int p) {
 // into chunks of L terms, L the smallest length whose chunks fit the lanes;
 // lanes are dealt chunk-major (every tuple's first chunk, then every second
 // chunk, ...), so the lanes of one chunk index are adjacent.
-__host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
+__host__ __device__ inline int m2l3_make_plan(int p, int nb, int lanes, M2LPlan3* plan) {
     const int NT = n_terms(p);
     const int nk = (NT + nb - 1) / nb;
+    if (lanes < 32 || lanes > M2L3_LANES || lanes % 32) return 1;
     plan->p = p;
     plan->nb = nb;
+    plan->lanes = lanes;
     plan->n_k = nk;
     auto A = [&](int k) {
         int b0, b1, b2;
@@ -850,12 +856,12 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
     };
     int total = 0;
     for (int k = 0; k < nk; k++) total += A(k);
-    int L = (total + M2L3_LANES - 1) / M2L3_LANES;
+    int L = (total + lanes - 1) / lanes;
     if (L < 1) L = 1;
     for (;; L++) {
         int cnt = 0;
         for (int k = 0; k < nk; k++) cnt += (A(k) + L - 1) / L;
-        if (cnt <= M2L3_LANES) break;
+        if (cnt <= lanes) break;
         if (L > NT) return 1;
     }
     plan->L = L;
@@ -879,7 +885,7 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
         plan->lane_a0[l] = 0;
         plan->lane_cnt[l] = 0;
     }
-    for (int w = 0; w < M2L3_LANES / 32; w++) {
+    for (int w = 0; w < lanes / 32; w++) {
         int m = 0;
         for (int l = 32 * w; l < 32 * w + 32; l++) m = plan->lane_cnt[l] > m ? plan->lane_cnt[l] : m;
         plan->warp_steps[w] = m;
@@ -922,13 +928,13 @@ __host__ __device__ inline int m2l3_make_plan(int p, int nb, M2LPlan3* plan) {
 
 // Builds the plan in the operator's workspace once: a plan tagged complete
 // for this (p, nb) -- it depends on nothing else -- is reused.
-__global__ void __launch_bounds__(32) fmm_m2l3_plan(int p, int nb, M2LPlan3* __restrict__ plan,
-                                                    int* err) {
+__global__ void __launch_bounds__(32) fmm_m2l3_plan(int p, int nb, int lanes,
+                                                    M2LPlan3* __restrict__ plan, int* err) {
     if (threadIdx.x != 0) return;
     volatile int* tag = &plan->tag;
-    if (*tag == M2L3_PLAN_TAG && plan->p == p && plan->nb == nb) return;
+    if (*tag == M2L3_PLAN_TAG && plan->p == p && plan->nb == nb && plan->lanes == lanes) return;
     *tag = 0;
-    if (m2l3_make_plan(p, nb, plan)) {
+    if (m2l3_make_plan(p, nb, lanes, plan)) {
         *err = 1;
         return;
     }
@@ -985,6 +991,7 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     constexpr int NB = M2L3Cfg<K>::NB;
     constexpr int NCH = C::NCH;
     constexpr int NP = (NCH + 1) / 2;  // channel pairs (f32x2)
+    constexpr int NPROD = m2l3_nprod(B), LANES = m2l3_lanes(B);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const M2L3Smem sm = m2l3_smem<K>(p, B);
     const int NT = sm.NT;
@@ -1040,10 +1047,9 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     // Dh_c = Dc_c (s_o/rho)^|c| / rho (the cube) and S_n = (-s_s/s_o)^n; the
     // B pairs' recurrences run interleaved (independent chains)
     // producer warp w handles the stage's pairs u0 .. u0 + PB - 1
-    constexpr int PB = (B % M2L3_NPROD == 0) ? B / M2L3_NPROD : B;
-    auto produce = [&](int64_t k0, int st) {  // warps 0 .. M2L3_NPROD - 1
-        const int u0 = (B % M2L3_NPROD == 0) ? warp * PB : 0;
-        if (B % M2L3_NPROD != 0 && warp > 0) return;
+    constexpr int PB = B / NPROD;
+    auto produce = [&](int64_t k0, int st) {  // warps 0 .. NPROD - 1
+        const int u0 = warp * PB;
         float Rh[B][3], q[B], pwn[B];
         bool on[B];
 #pragma unroll
@@ -1118,14 +1124,14 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     };
 
     // this lane's tuple and source chunk
-    const int ct = tid - 32 * M2L3_NPROD;
+    const int ct = tid - 32 * NPROD;
     int kk = -1, a_first = 0, cnt = 0, wsteps = 0;
     int blin[NB], thr[NB];
-    if (warp >= M2L3_NPROD) {
+    if (warp >= NPROD) {
         kk = plan->lane_k[ct];
         a_first = plan->lane_a0[ct];
         cnt = plan->lane_cnt[ct];
-        wsteps = plan->warp_steps[warp - M2L3_NPROD];
+        wsteps = plan->warp_steps[warp - NPROD];
     }
 #pragma unroll
     for (int j = 0; j < NB; j++) {
@@ -1149,7 +1155,7 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     const int64_t nst = (npair + B - 1) / B;  // pipeline stages of B pairs
     if (nst > 0) {
         issue_copy(0, 0);
-        if (warp < M2L3_NPROD) produce(0, 0);
+        if (warp < NPROD) produce(0, 0);
     }
     for (int64_t st = 0; st < nst; st++) {
         const int buf = (int)(st & 1);
@@ -1157,9 +1163,9 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
         __syncthreads();  // stage st's rows, cubes and scalars are complete; st - 1 is done
         if (st + 1 < nst) {
             issue_copy((st + 1) * B, buf ^ 1);
-            if (warp < M2L3_NPROD) produce((st + 1) * B, buf ^ 1);
+            if (warp < NPROD) produce((st + 1) * B, buf ^ 1);
         }
-        if (warp < M2L3_NPROD) continue;
+        if (warp < NPROD) continue;
 #pragma unroll 1
         for (int u = 0; u < B; u++) {
             if (st * B + u >= npair) break;
@@ -1209,9 +1215,9 @@ fmm_m2l3(int p, const int64_t* __restrict__ obs_nodes, int64_t n_obs_nodes,
     constexpr int PER = NB * NCH;
     const int lpr = sm.area / PER;
     float* Lg = loc + node * (int64_t)rowsz;
-    for (int lo = 0; lo < M2L3_LANES; lo += lpr) {
-        const int hi = lo + lpr < M2L3_LANES ? lo + lpr : M2L3_LANES;
-        if (warp >= M2L3_NPROD && ct >= lo && ct < hi) {
+    for (int lo = 0; lo < LANES; lo += lpr) {
+        const int hi = lo + lpr < LANES ? lo + lpr : LANES;
+        if (warp >= NPROD && ct >= lo && ct < hi) {
             float* sl = base + (ct - lo) * PER;
 #pragma unroll
             for (int j = 0; j < NB; j++)
@@ -1702,15 +1708,18 @@ struct Sizes {
     size_t rec, mom, loc, plan, W, F, rec2;
 };
 
-// Whether the lane plan fits for (p, nb), decided on the host once.
-inline bool m2l3_plan_fits(int p, int nb) {
-    static std::atomic<int> fits[FMM_MAXP + 1][16];  // 0 unknown, 1 yes, 2 no
-    if (p < 0 || p > FMM_MAXP || nb < 1 || nb > 15) return false;
-    int v = fits[p][nb].load(std::memory_order_relaxed);
+// Whether the lane plan fits for (p, nb, lanes), decided on the host once.
+inline bool m2l3_plan_fits(int p, int nb, int lanes) {
+    static std::atomic<int> fits[FMM_MAXP + 1][16][8];  // 0 unknown, 1 yes, 2 no
+    if (p < 0 || p > FMM_MAXP || nb < 1 || nb > 15 || lanes < 32 || lanes > M2L3_LANES ||
+        lanes % 32)
+        return false;
+    std::atomic<int>& f = fits[p][nb][lanes / 32];
+    int v = f.load(std::memory_order_relaxed);
     if (v == 0) {
         std::vector<unsigned char> buf(sizeof(M2LPlan3));
-        v = m2l3_make_plan(p, nb, reinterpret_cast<M2LPlan3*>(buf.data())) == 0 ? 1 : 2;
-        fits[p][nb].store(v, std::memory_order_relaxed);
+        v = m2l3_make_plan(p, nb, lanes, reinterpret_cast<M2LPlan3*>(buf.data())) == 0 ? 1 : 2;
+        f.store(v, std::memory_order_relaxed);
     }
     return v == 1;
 }
@@ -1912,13 +1921,15 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
             if constexpr (sizeof(R) == 4) {
                 const int smem1 = m2l3_smem<K>(p, 1).total_bytes;
                 const int smem2 = m2l3_smem<K>(p, 2).total_bytes;
-                lanes = m2l3_plan_fits(p, M2L3Cfg<K>::NB) && smem1 <= 227 * 1024;
+                // two pairs per stage while two CTAs still fit an SM
+                const bool two = smem2 + 1024 <= 113 * 1024;
+                const int nl = two ? m2l3_lanes(2) : m2l3_lanes(1);
+                lanes = m2l3_plan_fits(p, M2L3Cfg<K>::NB, nl) && smem1 <= 227 * 1024;
                 if (lanes) {
                     M2LPlan3* plan3 = reinterpret_cast<M2LPlan3*>(plan);
-                    fmm_m2l3_plan<<<1, 32, 0, se>>>(p, M2L3Cfg<K>::NB, plan3, plan_err);
+                    fmm_m2l3_plan<<<1, 32, 0, se>>>(p, M2L3Cfg<K>::NB, nl, plan3, plan_err);
                     if ((rc = launch_status("fmm m2l plan"))) return rc;
-                    // two pairs per stage while two CTAs still fit an SM
-                    if (smem2 + 1024 <= 113 * 1024) {
+                    if (two) {
                         if ((rc = set_smem(fmm_m2l3<K, 2>, (size_t)smem2))) return rc;
                         fmm_m2l3<K, 2><<<(unsigned)far.n_obs, M2L3_THREADS, smem2, se>>>(
                             p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad,
@@ -2061,15 +2072,16 @@ extern "C" int tct_fmm_matvec(int kernel, int prec, int mode, int order, int n_q
     return TCT_ERR_ARG;
 }
 
-// Host-side check of the M2L work plan for order p and nb terms b per lane:
+// Host-side check of the M2L work plan for order p, nb terms b per lane and
+// `lanes` contraction lanes (192 with two-pair stages, 224 with one-pair ones):
 // out[0] = valid (a, b) pairs covered, out[1] = pairs covered more than once
 // or invalid and unmasked, out[2] = the chunk length L, out[3] = lanes used,
 // out[4] = the sum over warps of their step counts.  Returns 0, or 1 when the
 // plan does not fit.
-extern "C" int tct_fmm_m2l_plan_stats(int order, int nb, int64_t* out) {
+extern "C" int tct_fmm_m2l_plan_stats(int order, int nb, int lanes, int64_t* out) {
     if (order < 0 || order > FMM_MAXP || nb < 1 || !out) return TCT_ERR_ARG;
     M2LPlan3* plan = new M2LPlan3();
-    const int rc = m2l3_make_plan(order, nb, plan);
+    const int rc = m2l3_make_plan(order, nb, lanes, plan);
     if (rc) {
         delete plan;
         return 1;
@@ -2096,7 +2108,7 @@ extern "C" int tct_fmm_m2l_plan_stats(int order, int nb, int64_t* out) {
     }
     // a lane's steps may not exceed its warp's count
     int64_t steps = 0;
-    for (int w = 0; w < M2L3_LANES / 32; w++) {
+    for (int w = 0; w < lanes / 32; w++) {
         steps += plan->warp_steps[w];
         for (int l = 32 * w; l < 32 * w + 32; l++)
             if (plan->lane_cnt[l] > plan->warp_steps[w]) bad++;

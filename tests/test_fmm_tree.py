@@ -117,23 +117,33 @@ def test_fmm_abi_rejects_bad_arguments():
     assert ws(6, 1, 1, 8, 3, 10, 10, 5, 5) > ws(6, 1, 0, 8, 3, 10, 10, 5, 5)  # locals
 
 
+@pytest.mark.parametrize("lanes", [192, 224])
 @pytest.mark.parametrize("nb", [1, 2, 3, 4, 6, 9])
 @pytest.mark.parametrize("p", range(13))
-def test_m2l_plan_covers_every_pair(p, nb):
+def test_m2l_plan_covers_every_pair(p, nb, lanes):
     """The M2L work plan (csrc/fmm.cu m2l3_make_plan, built on the host here)
     covers every (a, b) with |a| + |b| <= p exactly once, within the lanes.
-    FP32 uses nb = 3 (elasticRH3), 4 (RA), 6 (RT) or 9 (U) terms per lane."""
+    FP32 uses nb = 3 (elasticRH3), 4 (RA), 6 (RT) or 9 (U) terms per lane, on
+    192 lanes (two source nodes per stage) or 224 (one)."""
     import ctypes
     from tectosaur_b200 import _lib
     out = (ctypes.c_int64 * 5)()
-    rc = _lib.lib.tct_fmm_m2l_plan_stats(p, nb, out)
+    rc = _lib.lib.tct_fmm_m2l_plan_stats(p, nb, lanes, out)
     nt = (p + 1) * (p + 2) * (p + 3) // 6
-    if nb < 3 and -(-nt // nb) > 192 - 10:
+    if nb < 3 and -(-nt // nb) > lanes - 10:
         return  # more tuples than lanes: the item form runs instead (rc may be 0 or 1)
     assert rc == 0  # every FP32 configuration (nb >= 3) fits
-    covered, bad, L, lanes, steps = list(out)
+    covered, bad, L, used, steps = list(out)
     total = (p + 1) * (p + 2) * (p + 3) * (p + 4) * (p + 5) * (p + 6) // 720
     assert covered == total and bad == 0
-    assert 1 <= lanes <= 192
+    assert 1 <= used <= lanes
     if p == 8 and nb == 3:
-        assert L == 7 and lanes == 181  # chunks of at most 7 source terms
+        assert (L, used) == ((7, 181) if lanes == 192 else (6, 209))
+
+
+def test_m2l_plan_rejects_bad_lane_counts():
+    import ctypes
+    from tectosaur_b200 import _lib
+    out = (ctypes.c_int64 * 5)()
+    for lanes in (0, 100, 256):
+        assert _lib.lib.tct_fmm_m2l_plan_stats(8, 3, lanes, out) != 0
