@@ -177,7 +177,8 @@ Octree build_octree(const double* centers, const double* radii, int64_t n, int64
 // Node radius enlarged to cover every member ball (fast_find_nearfield.cpp:77-94).
 std::vector<double> expanded_r(const Octree& t, const double* orig_radii) {
     std::vector<double> out(t.nodes.size());
-    for (size_t k = 0; k < t.nodes.size(); k++) {
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t k = 0; k < (int64_t)t.nodes.size(); k++) {
         const Node& n = t.nodes[k];
         double m = n.R;
         for (int64_t j = n.start; j < n.end; j++) {
@@ -187,6 +188,34 @@ std::vector<double> expanded_r(const Octree& t, const double* orig_radii) {
         out[k] = m;
     }
     return out;
+}
+
+// The two trees and expanded radii of a search.  A self search (the same
+// arrays on both sides) builds one tree; otherwise the two build side by side.
+struct TreePair {
+    Octree ot, st_own;
+    std::vector<double> oer, ser_own;
+    bool same = false;
+    const Octree& st() const { return same ? ot : st_own; }
+    const std::vector<double>& ser() const { return same ? oer : ser_own; }
+};
+
+void build_tree_pair(const double* obs_c, const double* obs_r, int64_t n_obs, const double* src_c,
+                     const double* src_r, int64_t n_src, int64_t leaf, TreePair& tp) {
+    tp.same = obs_c == src_c && obs_r == src_r && n_obs == n_src;
+    if (tp.same) {
+        tp.ot = build_octree(obs_c, obs_r, n_obs, leaf);
+    } else {
+#pragma omp parallel sections num_threads(2)
+        {
+#pragma omp section
+            tp.ot = build_octree(obs_c, obs_r, n_obs, leaf);
+#pragma omp section
+            tp.st_own = build_octree(src_c, src_r, n_src, leaf);
+        }
+    }
+    tp.oer = expanded_r(tp.ot, obs_r);
+    if (!tp.same) tp.ser_own = expanded_r(tp.st_own, src_r);
 }
 
 struct Query {
@@ -298,11 +327,11 @@ int tct_find_near_pairs(const double* obs_c, const double* obs_r, int64_t n_obs,
     }
     if (n_threads <= 0) n_threads = omp_get_max_threads();
     const int64_t leaf = 50;
-    Octree ot = build_octree(obs_c, obs_r, n_obs, leaf);
-    Octree st = build_octree(src_c, src_r, n_src, leaf);
-    std::vector<double> oer = expanded_r(ot, obs_r);
-    std::vector<double> ser = expanded_r(st, src_r);
-    Query q{ot, st, oer, ser, obs_r, src_r, threshold};
+    TreePair tp;
+    build_tree_pair(obs_c, obs_r, n_obs, src_c, src_r, n_src, leaf, tp);
+    const Octree& ot = tp.ot;
+    const Octree& st = tp.st();
+    Query q{ot, st, tp.oer, tp.ser(), obs_r, src_r, threshold};
     std::vector<int64_t> starts;
     for (size_t k = 0; k < ot.nodes.size(); k++) {
         const Node& n = ot.nodes[k];
@@ -372,11 +401,11 @@ int tct_near_plan_build(const double* obs_c, const double* obs_r, int64_t n_obs,
     }
     if (n_threads <= 0) n_threads = omp_get_max_threads();
     const int64_t leaf = 50;
-    Octree ot = build_octree(obs_c, obs_r, n_obs, leaf);
-    Octree st = build_octree(src_c, src_r, n_src, leaf);
-    std::vector<double> oer = expanded_r(ot, obs_r);
-    std::vector<double> ser = expanded_r(st, src_r);
-    Query q{ot, st, oer, ser, obs_r, src_r, threshold};
+    TreePair tp;
+    build_tree_pair(obs_c, obs_r, n_obs, src_c, src_r, n_src, leaf, tp);
+    const Octree& ot = tp.ot;
+    const Octree& st = tp.st();
+    Query q{ot, st, tp.oer, tp.ser(), obs_r, src_r, threshold};
     std::vector<int64_t> starts;
     for (size_t k = 0; k < ot.nodes.size(); k++) {
         const Node& n = ot.nodes[k];
@@ -409,12 +438,12 @@ int tct_near_plan_build(const double* obs_c, const double* obs_r, int64_t n_obs,
         }
         plan->lp_start.push_back((int64_t)plan->lp_s.size());
     }
-    plan->oc = std::move(ot.centers);
-    plan->sc = std::move(st.centers);
+    plan->oc = ot.centers;
+    plan->sc = st.centers;
     plan->orq.assign(obs_r, obs_r + n_obs);
     plan->srq.assign(src_r, src_r + n_src);
-    plan->oorig = std::move(ot.orig);
-    plan->sorig = std::move(st.orig);
+    plan->oorig = ot.orig;
+    plan->sorig = st.orig;
     *out = plan;
     return TCT_OK;
 }
