@@ -48,7 +48,11 @@ class TSFMM:
         self.params = np.ascontiguousarray(np.asarray(params, np.float64)[:2])
         self.obs_m, self.src_m = obs_m, src_m
         self.obs_tree = Tree(*tri_centers_radii(*obs_m), max_pts_per_cell)
-        self.src_tree = Tree(*tri_centers_radii(*src_m), max_pts_per_cell)
+        same = (obs_m[0] is src_m[0] or np.array_equal(obs_m[0], src_m[0])) and \
+            np.array_equal(obs_m[1], src_m[1])
+        # a self operator (the same triangles on both sides) shares one tree
+        self.src_tree = self.obs_tree if same else Tree(*tri_centers_radii(*src_m),
+                                                        max_pts_per_cell)
         if mode == "treecode":
             lists = interactions(self.obs_tree, self.src_tree, 1.0, mac, 0, True)
             far = lists["m2p"]
