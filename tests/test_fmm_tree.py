@@ -26,8 +26,10 @@ def _ref():
     pytest.skip("reference C++ not compiled (make -C oracle ref)")
 
 
-@pytest.mark.parametrize("n,leaf", [(12, 2), (25, 20), (40, 100)])
+@pytest.mark.parametrize("n,leaf", [(12, 2), (25, 20), (40, 100), (180, 50), (200, 128)])
 def test_tree_matches_reference(n, leaf):
+    # n = 180, 200: 64 k and 79 k balls, built with threads (subtrees spliced
+    # into the serial depth-first order)
     ref = _ref()
     pts, tris = bumpy_mesh(n, seed=n)
     c, r = tri_centers_radii(pts, tris)

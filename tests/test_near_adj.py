@@ -139,7 +139,7 @@ def _load_ref_finder():
     return None
 
 
-@pytest.mark.parametrize("n,thr", [(40, 2.5), (75, 1.25), (120, 2.5)])
+@pytest.mark.parametrize("n,thr", [(40, 2.5), (75, 1.25), (120, 2.5), (180, 2.5)])
 def test_bit_exact_vs_compiled_reference(n, thr):
     ref = _load_ref_finder()
     if ref is None:
