@@ -83,7 +83,10 @@ def find_close_or_touching(a_pts, a_tris, b_pts, b_tris, threshold):
     touch (find_near_adj.py:29-35).  Large meshes use the device search when
     a GPU is visible; both give the same pairs in the same order."""
     ca, ra = get_tri_centroids_rs(a_pts, a_tris)
-    cb, rb = get_tri_centroids_rs(b_pts, b_tris)
+    if (a_pts is b_pts or np.array_equal(a_pts, b_pts)) and np.array_equal(a_tris, b_tris):
+        cb, rb = ca, ra  # a self search: one set of balls (and one octree)
+    else:
+        cb, rb = get_tri_centroids_rs(b_pts, b_tris)
     if max(ca.shape[0], cb.shape[0]) >= DEVICE_NEAR_MIN_TRIS:
         from ..util import device
         if device.cuda_available():
