@@ -140,6 +140,9 @@ extern "C" int tct_near_device_count(tct_near_plan* plan, void* stream, int64_t*
     *total = 0;
     plan->total = 0;
     if (plan->n_obs == 0 || plan->n_src == 0) return TCT_OK;
+    // source indices are sorted as int32 keys; the scan and sort count in int
+    TCT_CHECK_ARG(plan->n_obs < 0x7fffffff && plan->n_src < 0x7fffffff,
+                  "tct_near_device_count: more than 2^31 - 2 balls on a side");
     if (plan->dev == nullptr) {
         plan->dev_bytes = device_bytes(plan);
         if (cudaMalloc(&plan->dev, plan->dev_bytes) != cudaSuccess) {
