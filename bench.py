@@ -177,98 +177,134 @@ def fp32_peak_tflops(torch, lib):
 
 
 # ---- CPU baseline: the reference's algorithm on the host cores ---------------
-def cpu_apply_sample(pts, tris, n_obs_sample, seed=3, n_threads=None):
-    """Time one apply restricted to `n_obs_sample` observation triangles
-    (farfield over all sources + their nearfield rows), FP32, with the
-    oracle restatement of the reference's kernels on all host threads.
-    Returns (seconds_far, seconds_near, n_blocks_sample)."""
-    from oracle import oracle as orc
-    from tectosaur_b200.nearfield import triangle_rules as trr
-    from tectosaur_b200.nearfield.nearfield_op import nearfield_pairs
-    from tectosaur_b200.util.quadrature import gauss2d_tri, gauss4d_tri
-    n = tris.shape[0]
+# These legs import nothing from tectosaur_b200 (no libtct_b200.so): meshes,
+# near pairs (the reference's own compiled finder), rules (the reference's own
+# arrays) and kernels (liboracle) all come from oracle/ref_pipeline.py.
+def c2_mesh_ref(n=174, seed=2):
+    """c2_mesh built without the product package (same arrays)."""
+    from oracle import ref_pipeline as rp
+    pts, tris = rp.make_rect(n, n, [[-10, -10, 0], [10, -10, 0], [10, 10, 0], [-10, 10, 0]])
     rng = np.random.default_rng(seed)
-    obs = np.sort(rng.choice(n, size=n_obs_sample, replace=False))
-    x = rng.standard_normal(n * 9)
-    # nearfield blocks of the sampled rows (assembly: setup, not timed)
-    cl = nearfield_pairs(pts, tris, obs, np.arange(n), NQ["thr"])
-    rules = {"co": (trr.coincident_quad(NQ["nq_co"]), False, True),
-             "ea": (trr.edge_adj_quad(NQ["nq_ea"]), True, True),
-             "va": (trr.vertex_adj_quad(NQ["nq_va"], NQ["nq_va"], NQ["nq_va"]), True, True),
-             "near": (gauss4d_tri(NQ["nq_near"], NQ["nq_near"]), False, False)}
-    far4 = gauss4d_tri(NQ["nq_far"], NQ["nq_far"])
-    rows, cols, blocks = [], [], []
-    for c, (rule, adj, check0) in rules.items():
-        recs, dofs = cl[c]
-        if dofs.shape[0] == 0:
-            continue
-        b = orc.pairs(K_NAME, np.float32, rule, pts, tris, recs[:, :5 if adj else 2], PARAMS,
-                      adj=adj, check0=check0, n_threads=n_threads)
-        b = b - orc.pairs(K_NAME, np.float32, far4, pts, tris, recs[:, :2], PARAMS,
-                          check0=(c == "co"), n_threads=n_threads)
-        rows.append(dofs[:, 0])
-        cols.append(dofs[:, 1])
-        blocks.append(b.reshape(-1, 9, 9))
-    rows = np.concatenate(rows)
-    cols = np.concatenate(cols)
-    blocks = np.concatenate(blocks).astype(np.float32).astype(np.float64)
+    pts = pts.copy()
+    pts[:, 2] = 0.5 * np.exp(-(pts[:, 0] ** 2 + pts[:, 1] ** 2) / 8.0) + \
+        0.02 * rng.standard_normal(pts.shape[0])
+    return pts, tris
+
+
+def c2_sample(pts, tris, classes, n_rows, seed, float_type, fast, n_threads=None):
+    """Seeded observation rows of the C2 operator (oracle/ref_pipeline), their
+    nearfield blocks integrated (setup)."""
+    from oracle import ref_pipeline as rp
+    n = tris.shape[0]
+    rows = np.sort(np.random.default_rng(seed).choice(n, size=min(n_rows, n), replace=False))
+    return rp.SampledRows(pts, tris, rows, NQ["nq_co"], NQ["nq_ea"], NQ["nq_va"], NQ["nq_far"],
+                          NQ["nq_near"], NQ["thr"], K_NAME, PARAMS, float_type,
+                          classes=classes, n_threads=n_threads, fast=fast)
+
+
+def c2_classes(pts, tris):
+    from oracle import ref_pipeline as rp
+    return rp.classify(tris, rp.near_pairs(pts, tris, NQ["thr"]))
+
+
+def cpu_step_rows(pts, tris, classes, target_s):
+    """Rows per timed CPU step so that one step takes about target_s (timed
+    build, all host threads)."""
+    n = tris.shape[0]
+    probe = c2_sample(pts, tris, classes, 32, 99, np.float32, True)
+    x = np.random.default_rng(98).standard_normal(9 * n)
+    probe.apply(x)
     t0 = time.perf_counter()
-    orc.farfield_tris(K_NAME, np.float32, gauss2d_tri(NQ["nq_far"]), pts, tris[obs], tris, x,
-                      PARAMS, n_threads=n_threads)
-    t1 = time.perf_counter()
-    orc.bcoo_matvec(np.float32, rows, cols, blocks, x, obs.shape[0] * 9, n_threads=n_threads)
-    t2 = time.perf_counter()
-    return t1 - t0, t2 - t1, rows.shape[0]
+    probe.apply(x)
+    per_row = max((time.perf_counter() - t0) / 32, 1e-6)
+    return int(min(max(32, target_s / per_row), n // 4))
 
 
-def cpu_baseline(pts, tris, nnzb_full, target_s=12.0):
+def cpu_baseline(pts, tris, classes=None, target_s=3.0, reps=3):
+    """The reference operator's apply on the host cores: FP32 (the reference's
+    default precision), the timed build of the oracle restatement (-O3
+    -march=native, OpenMP on every host thread) on a seeded sample of
+    observation rows -- farfield against all sources plus their nearfield
+    BCOO rows; value = the fraction of an apply per second."""
     n = tris.shape[0]
     threads = os.cpu_count() or 1
-    probe = 8
-    tf, tn, nb = cpu_apply_sample(pts, tris, probe)
-    per_obs = max(tf / probe, 1e-6)
-    n_s = int(min(max(probe, target_s / per_obs), n // 4))
-    tf, tn, nb = cpu_apply_sample(pts, tris, n_s)
-    t_full = tf * (n / n_s) + tn * (nnzb_full / max(nb, 1))
+    if classes is None:
+        classes = c2_classes(pts, tris)
+    n_s = cpu_step_rows(pts, tris, classes, target_s)
+    s = c2_sample(pts, tris, classes, n_s, 3, np.float32, True)
+    x = np.random.default_rng(3).standard_normal(9 * n)
+    s.apply(x)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        s.apply(x)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
     return {
-        "value": 1.0 / t_full, "unit": "matvecs/s", "cores": threads, "kind": "port",
-        "sample": ("oracle restatement of the reference kernels (FP32, OpenMP %d threads): "
-                   "farfield of %d of %d observation triangles against all sources (%.1f s) "
-                   "+ BCOO matvec of their %d nearfield blocks (%.3f s), extrapolated by "
-                   "triangle count and block count to one full apply (%.1f s)"
-                   % (threads, n_s, n, tf, nb, tn, t_full)),
+        "value": (n_s / n) / t, "unit": "matvecs/s", "cores": threads, "kind": "port",
+        "sample": ("oracle restatement of the reference kernels, FP32, -O3 -march=native, "
+                   "OpenMP %d threads: rows of %d seeded observation triangles of %d (farfield "
+                   "against all sources + their %d nearfield blocks), median of %d applies "
+                   "%.2f s; value = (%d / %d of an apply) / time"
+                   % (threads, n_s, n, s.n_blocks, reps, t, n_s, n)),
     }
 
 
+def c2_parity(pts, tris, y_dev, x, classes=None, n_rows=512, seed=17):
+    """Relative 2-norm error of the timed FP32 apply y_dev on n_rows seeded
+    observation rows against the FP64 oracle (checker build) of the same
+    rows: farfield against all sources + corrected nearfield rows."""
+    if classes is None:
+        classes = c2_classes(pts, tris)
+    s = c2_sample(pts, tris, classes, n_rows, seed, np.float64, False)
+    want = s.apply(np.asarray(x, dtype=np.float64))
+    got = np.asarray(y_dev, dtype=np.float64).reshape(-1, 9)[s.rows].reshape(-1)
+    err = float(np.linalg.norm(got - want) / np.linalg.norm(want))
+    far = s.farfield(np.asarray(x, dtype=np.float64))
+    return {"rel_err_fp64": err, "rows": int(s.rows.shape[0]), "seed": seed,
+            "oracle": "FP64 oracle restatement (no FMA contraction) of the reference operator "
+                      "on the sampled rows; near pairs from the reference's compiled finder, "
+                      "rules from the reference's arrays",
+            "far_share_of_norm": float(np.linalg.norm(far) / np.linalg.norm(want))}
+
+
 def run_reference(args, rank, world):
+    """The reference arm: the reference operator's apply on the host cores
+    (see cpu_baseline), one sampled partial apply per step."""
     if rank != 0:
         return
-    pts, tris = c2_mesh()
+    pts, tris = c2_mesh_ref()
     n = tris.shape[0]
-    from tectosaur_b200.nearfield.nearfield_op import nearfield_pairs
-    cl = nearfield_pairs(pts, tris, np.arange(n), np.arange(n), NQ["thr"])
-    nnzb = sum(v[1].shape[0] for v in cl.values())
+    classes = c2_classes(pts, tris)
+    nnzb = int(sum(v.shape[0] for v in classes.values()))
     threads = os.cpu_count() or 1
-    probe = 8
-    tf, tn, nb = cpu_apply_sample(pts, tris, probe)
-    n_s = int(min(max(probe, 6.0 / max(tf / probe, 1e-6)), n // 4))
+    n_s = cpu_step_rows(pts, tris, classes, 1.0)
+    s = c2_sample(pts, tris, classes, n_s, 3, np.float32, True)
+    x = np.random.default_rng(3).standard_normal(9 * n)
     times = []
     for i in range(args.warmup + args.steps):
-        tf, tn, nb = cpu_apply_sample(pts, tris, n_s, seed=3 + i)
+        t0 = time.perf_counter()
+        s.apply(x)
         if i >= args.warmup:
-            times.append(tf * (n / n_s) + tn * (nnzb / max(nb, 1)))
-    t = float(np.mean(times))
-    value = 1.0 / t
+            times.append(time.perf_counter() - t0)
+    t = float(np.sum(times))
+    frac = n_s / n
+    value = args.steps * frac / t
     line = {
         "metric": "BEM matvecs/s", "value": value, "unit": "matvecs/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": config_block(n, nnzb),
+        "config": dict(config_block(n, nnzb), step=(
+            "one partial apply: the %d seeded observation rows of %d (%.4f of an apply); "
+            "value = steps x %.4f / time" % (n_s, n, frac, frac))),
         "cpu_baseline": {"value": value, "unit": "matvecs/s", "cores": threads, "kind": "port",
                          "sample": "each step: farfield of %d of %d observation triangles "
-                                   "against all sources + their nearfield BCOO rows, "
-                                   "extrapolated to one full apply" % (n_s, n)},
+                                   "against all sources + their %d nearfield BCOO blocks, "
+                                   "oracle restatement FP32, -O3 -march=native, OpenMP %d "
+                                   "threads (the reference's PyOpenCL CPU path cannot run: "
+                                   "no pyopencl, no CPU OpenCL platform)"
+                                   % (n_s, n, s.n_blocks, threads)},
         "e2e": {"value": value, "unit": "matvecs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -1927,7 +1963,8 @@ def main():
             "data": "synthetic (seeded mesh and inputs)",
             "config": config_block(n, nnzb),
             "roofline": {
-                "kernel": "far_main<float, elasticRH3, 3> (tri-to-tri farfield)",
+                "kernel": "far_main_rh2<3, uniform> (packed f32x2 elasticRH3 tri-to-tri "
+                          "farfield)",
                 "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
                 "peak_source": "measured live: best of the FP32 FMA probes (scalar FFMA "
@@ -1945,8 +1982,10 @@ def main():
             "clocks": clocks,
             "setup_s": t_build,
         }
+        classes = c2_classes(pts, tris)
+        line["parity"] = c2_parity(pts, tris, y.cpu().numpy(), x.cpu().numpy(), classes)
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(pts, tris, nnzb)
+            line["cpu_baseline"] = cpu_baseline(pts, tris, classes)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

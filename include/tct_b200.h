@@ -200,8 +200,10 @@ int tct_fp64_fma_probe(void* out, int64_t n_blocks, int iters, void* stream);
  * workspace (tct_farfield_workspace_bytes) exceeds it are rejected with
  * TCT_ERR_ARG and a message; nothing is ever allocated.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) -- make
- * it before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (different streams or host threads) race. */
+ * it before any stream capture; the address belongs to the device's primary
+ * context, so do not call cudaDeviceReset between calls.  All calls share the
+ * one array: calls that overlap on the GPU (different streams or host
+ * threads) race. */
 #define TCT_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 size_t tct_farfield_noalloc_capacity(void);
 int tct_farfield_tris_matvec_noalloc(int kernel, int prec, void* out, const void* in,

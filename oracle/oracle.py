@@ -4,8 +4,14 @@ the reference's kernel math, oracle.cpp).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module, and only as the checker or the timed CPU baseline.  The product
 (tectosaur_b200) never imports it.
+
+Two builds of the same source: liboracle.so (no FMA contraction, portable
+x86-64-v2: the parity checker) and a timed build for the host that runs it
+(-O3 -march=native), selected by ``fast=True`` on the calls the CPU baseline
+times.
 """
 import ctypes
+import hashlib
 import os
 import subprocess
 
@@ -20,19 +26,57 @@ KERNEL_IDS = {
 }
 
 _lib = None
+_fast = None
 
 
 def build():
     subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
 
 
-def lib():
+def lib(fast=False):
     global _lib
+    if fast:
+        return fast_lib()
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
         _lib = ctypes.CDLL(LIB_PATH)
     return _lib
+
+
+def _host_key():
+    """Identifies the host CPU (model and feature flags) for -march=native."""
+    model, flags = "", ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if not model and line.startswith("model name"):
+                    model = line
+                elif not flags and line.startswith("flags"):
+                    flags = line
+                if model and flags:
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1((model + flags).encode()).hexdigest()[:12]
+
+
+def fast_lib_path():
+    return os.path.join(HERE, "_native", "liboracle_fast_%s.so" % _host_key())
+
+
+def fast_lib():
+    """The timed CPU build, compiled for this host on first use (a few
+    seconds; a library built for another CPU could use instructions this one
+    lacks)."""
+    global _fast
+    if _fast is None:
+        path = fast_lib_path()
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", HERE, "fast",
+                                   "FAST_OUT=" + os.path.relpath(path, HERE)])
+        _fast = ctypes.CDLL(path)
+    return _fast
 
 
 def _d(a):
@@ -64,7 +108,7 @@ def _threads(n):
 
 
 def pairs(kernel, float_type, quad, pts, tris, pair_list, params, adj=False,
-          check0=False, n_threads=None):
+          check0=False, n_threads=None, fast=False):
     """(n, 3, 3, 3, 3) pair integrals (assemble.cl single_pairs{Z,N}[_adj])."""
     pair_list = np.asarray(pair_list)
     n = pair_list.shape[0]
@@ -76,7 +120,7 @@ def pairs(kernel, float_type, quad, pts, tris, pair_list, params, adj=False,
     pl, plp = _i(pair_list.reshape(n, 5 if adj else 2))
     pr, prp = _d(params)
     _, op = _d(out)
-    rc = lib().orc_pairs(KERNEL_IDS[kernel], _prec(float_type), int(adj), int(check0),
+    rc = lib(fast).orc_pairs(KERNEL_IDS[kernel], _prec(float_type), int(adj), int(check0),
                          op, qp.shape[0], qpp, qwp, pp, tp, plp, n, prp,
                          _threads(n_threads))
     _check(rc, "pairs")
@@ -84,7 +128,7 @@ def pairs(kernel, float_type, quad, pts, tris, pair_list, params, adj=False,
 
 
 def farfield_tris(kernel, float_type, quad2d, pts, obs_tris, src_tris, v, params,
-                  n_threads=None):
+                  n_threads=None, fast=False):
     """Matrix-free tri-to-tri farfield matvec (matrix_free.cl farfield_tris_to_tris)."""
     obs_tris = np.asarray(obs_tris)
     src_tris = np.asarray(src_tris)
@@ -97,7 +141,7 @@ def farfield_tris(kernel, float_type, quad2d, pts, obs_tris, src_tris, v, params
     qw, qwp = _d(quad2d[1])
     pr, prp = _d(params)
     _, op = _d(out)
-    rc = lib().orc_farfield_tris(KERNEL_IDS[kernel], _prec(float_type), op, vp, pp,
+    rc = lib(fast).orc_farfield_tris(KERNEL_IDS[kernel], _prec(float_type), op, vp, pp,
                                  otp, ot.shape[0], stp, st.shape[0], qp.shape[0], qpp,
                                  qwp, prp, _threads(n_threads))
     _check(rc, "farfield_tris")
@@ -105,7 +149,7 @@ def farfield_tris(kernel, float_type, quad2d, pts, obs_tris, src_tris, v, params
 
 
 def farfield_pts(kernel, float_type, obs_pts, obs_ns, src_pts, src_ns, v, params,
-                 n_threads=None):
+                 n_threads=None, fast=False):
     """Point-to-point farfield (farfield_direct.cl farfield_pts{K})."""
     out = np.zeros(np.asarray(obs_pts).shape[0] * 3)
     a, ap = _d(obs_pts)
@@ -115,7 +159,7 @@ def farfield_pts(kernel, float_type, obs_pts, obs_ns, src_pts, src_ns, v, params
     vin, vp = _d(v)
     pr, prp = _d(params)
     _, op = _d(out)
-    rc = lib().orc_farfield_pts(KERNEL_IDS[kernel], _prec(float_type), op, ap, bp,
+    rc = lib(fast).orc_farfield_pts(KERNEL_IDS[kernel], _prec(float_type), op, ap, bp,
                                 a.shape[0], cp, dp, c.shape[0], vp, prp,
                                 _threads(n_threads))
     _check(rc, "farfield_pts")
@@ -239,7 +283,7 @@ def bsr_matvec(float_type, indptr, indices, data, x):
     return y
 
 
-def bcoo_matvec(float_type, rows, cols, data, x, n_rows, n_threads=1):
+def bcoo_matvec(float_type, rows, cols, data, x, n_rows, n_threads=1, fast=False):
     data = np.ascontiguousarray(data, dtype=np.float64)
     bs = data.shape[1]
     y = np.zeros(n_rows)
@@ -248,7 +292,7 @@ def bcoo_matvec(float_type, rows, cols, data, x, n_rows, n_threads=1):
     _, dp = _d(data)
     xx, xp = _d(x)
     _, yp = _d(y)
-    rc = lib().orc_bcoo_matvec(_prec(float_type), ctypes.c_long(data.shape[0]), bs, ap,
+    rc = lib(fast).orc_bcoo_matvec(_prec(float_type), ctypes.c_long(data.shape[0]), bs, ap,
                                bp, dp, xp, yp, _threads(n_threads))
     _check(rc, "bcoo_matvec")
     return y

@@ -19,7 +19,9 @@
 // contents: nothing in it has to start at zero (every byte a call reads was
 // written earlier in the same call), but two calls that run at the same time
 // on the GPU -- on different streams, or from different host threads --
-// overwrite each other's scratch and race.
+// overwrite each other's scratch and race.  The cached address belongs to the
+// device's primary context: do not call cudaDeviceReset between calls (the
+// context it creates afterwards holds the array at a new address).
 #include <mutex>
 
 #include "common.cuh"
@@ -72,8 +74,17 @@ extern "C" int tct_farfield_tris_matvec_noalloc(int kernel, int prec, void* out,
                                                 const double* quad_wts, const double* params,
                                                 int accumulate, void* stream) {
     using namespace tct;
+    // Same order of argument checks as tct_farfield_tris_matvec: sizes first,
+    // then the cases with nothing to integrate (no scratch needed), then the
+    // scratch capacity.
+    TCT_CHECK_ARG(n_obs >= 0 && n_src >= 0, "tct_farfield_tris_matvec_noalloc: negative size");
+    if (n_obs == 0) return TCT_OK;
+    if (n_src == 0)
+        return tct_farfield_tris_matvec(kernel, prec, out, in, pts, obs_tris, n_obs, src_tris,
+                                        n_src, n_q, quad_pts, quad_wts, params, accumulate,
+                                        nullptr, 0, stream);
     const size_t need = tct_farfield_workspace_bytes(kernel, prec, n_obs, n_src, n_q);
-    if (need == 0 && n_src > 0) {
+    if (need == 0) {
         set_error("tct_farfield_tris_matvec_noalloc: unsupported kernel %d, precision %d or "
                   "%d-point rule", kernel, prec, n_q);
         return TCT_ERR_ARG;

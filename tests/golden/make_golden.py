@@ -1,8 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference.
 
-Run once on a machine that has the reference checkout (default
-/root/reference, override with TCT_REFERENCE) and the reference's C++ modules
-built by ``make -C oracle ref``:
+Run once on a machine that has the reference checkout (TCT_REFERENCE, else a
+directory named "reference" beside this repository) and the reference's C++
+modules built by ``make -C oracle ref REF=<checkout>``:
 
     python tests/golden/make_golden.py
 
@@ -93,6 +93,31 @@ def quad_rules():
         digests.append("gauss4d_tri %d,%d %d %s %s" % (a, b, p.shape[0], sha(p), sha(w)))
     out["digests"] = np.array(digests)
     np.savez_compressed(os.path.join(HERE, "quad_rules.npz"), **out)
+
+
+def op_rules():
+    """The reference's own rules for the operator configurations the CPU
+    baseline and the sampled-row parity check run without the product package
+    (oracle/ref_pipeline.py): (nq_co, nq_ea, nq_va, nq_far, nq_near) =
+    (6, 6, 6, 2, 5) for the 722-triangle fault, (6, 6, 6, 1, 5) for the 60k
+    surface, (3, 3, 3, 2, 3) for small test operators."""
+    import tectosaur.util.quadrature as rq
+    import tectosaur.nearfield.triangle_rules as rtr
+    out = {}
+    for n in (3, 6):
+        for name, f in [("coincident", rtr.coincident_quad), ("edge_adj", rtr.edge_adj_quad),
+                        ("vertex_adj", lambda k: rtr.vertex_adj_quad(k, k, k))]:
+            p, w = f(n)
+            out["%s_%d_p" % (name, n)] = p
+            out["%s_%d_w" % (name, n)] = w
+    for n in (1, 2, 3, 5):
+        p, w = rq.gauss4d_tri(n, n)
+        out["gauss4d_%d_p" % n] = p
+        out["gauss4d_%d_w" % n] = w
+        p, w = rq.gauss2d_tri(n)
+        out["gauss2d_tri_%d_p" % n] = p
+        out["gauss2d_tri_%d_w" % n] = w
+    np.savez_compressed(os.path.join(HERE, "op_rules.npz"), **out)
 
 
 def kernel_values():
@@ -200,12 +225,12 @@ def qd():
 
 
 if __name__ == "__main__":
-    qd()
-    ref_goldens()
-    quad_rules()
-    kernel_values()
-    near_split()
-    mass_op()
+    # no arguments: every fixture; otherwise only the named generators
+    gens = [qd, ref_goldens, quad_rules, op_rules, kernel_values, near_split, mass_op]
+    names = sys.argv[1:]
+    for g in gens:
+        if not names or g.__name__ in names:
+            g()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

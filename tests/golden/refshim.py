@@ -20,8 +20,12 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("TCT_REFERENCE", "/root/reference")
 REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+# the reference checkout: TCT_REFERENCE, else a directory named "reference"
+# beside this repository
+REF = os.environ.get("TCT_REFERENCE") or os.path.join(os.path.dirname(REPO), "reference")
+if not os.path.isdir(os.path.join(REF, "tectosaur")):
+    raise ImportError("refshim: no reference checkout at %r (set TCT_REFERENCE)" % REF)
 REF_BUILD = os.path.join(REPO, "oracle", "_ref")
 
 

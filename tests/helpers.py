@@ -19,6 +19,18 @@ def c1_mesh():
     return make_rect(20, 20, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
 
 
+def c2_mesh(n=174, seed=2):
+    """The 60k-triangle direct-farfield surface: an n x n vertex grid over
+    [-10, 10]^2 with z = 0.5 exp(-(x^2 + y^2)/8) + 0.02 N(0, 1) (seed 2);
+    59,858 triangles at n = 174."""
+    pts, tris = make_rect(n, n, [[-10, -10, 0], [10, -10, 0], [10, 10, 0], [-10, 10, 0]])
+    rng = np.random.default_rng(seed)
+    pts = pts.copy()
+    pts[:, 2] = 0.5 * np.exp(-(pts[:, 0] ** 2 + pts[:, 1] ** 2) / 8.0) + \
+        0.02 * rng.standard_normal(pts.shape[0])
+    return pts, tris
+
+
 def bumpy_mesh(n, seed=0, amp=0.05, size=1.0):
     pts, tris = make_rect(n, n, [[-size, -size, 0], [size, -size, 0], [size, size, 0],
                                  [-size, size, 0]])

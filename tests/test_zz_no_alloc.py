@@ -5,13 +5,16 @@ device memory when they apply the operator (inside a stream capture that
 must not add memory nodes, under an application's own memory pool, or where
 cudaMalloc's implicit synchronisation is unacceptable).  It takes only inputs
 and outputs and runs on a fixed scratch array inside the library.  This file
-checks, twice in a row (the scratch keeps the previous call's contents), that
-it returns what the workspace-taking entry point returns for the same inputs,
-and that a problem larger than the built-in scratch is refused with a
-message.  It runs last so that a failure here leaves every other test already
-run; it passes alone in a fresh process as well.
+checks, twice in a row (the scratch keeps the previous call's contents; the
+second call is a smaller problem, so it lands on a scratch layout the first
+call left different), that it returns what the workspace-taking entry point
+returns for the same inputs, and that a problem larger than the built-in
+scratch is refused with a message before any CUDA call (a CPU test: the
+device pointers are NULL, so a refusal that stopped working would end at the
+null-pointer check, never in a launch).  It runs last so that a failure here
+leaves every other test already run; it passes alone in a fresh process as
+well.
 """
-import ctypes
 
 import numpy as np
 import pytest
@@ -22,13 +25,11 @@ from tectosaur_b200.util.quadrature import gauss2d_tri
 
 from helpers import PARAMS, bumpy_mesh, rel
 
-pytestmark = pytest.mark.gpu
-
 TOL = {np.float32: 2e-5, np.float64: 1e-10}
 
 
-def _inputs(ft, nq, seed):
-    pts, tris = bumpy_mesh(30, seed=seed)
+def _inputs(ft, nq, seed, grid):
+    pts, tris = bumpy_mesh(grid, seed=seed)
     obs = tris[::2]
     src = tris
     rng = np.random.default_rng(seed)
@@ -55,6 +56,7 @@ def _no_alloc(kid, prec, out, x, pts, obs, n_obs, src, n_src, qx, qw, params):
         _lib.stream_ptr()), "tct_farfield_tris_matvec_noalloc")
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("K,ft,nq", [("elasticRH3", np.float32, 1), ("elasticRH3", np.float32, 2),
                                      ("elasticU3", np.float64, 2), ("elasticH3", np.float32, 1)])
 def test_no_alloc_matches_workspace_entry_point(cuda, K, ft, nq):
@@ -62,8 +64,10 @@ def test_no_alloc_matches_workspace_entry_point(cuda, K, ft, nq):
     kid = _lib.kernel_id(K)
     prec = _lib.prec_of(ft)
     params = np.ascontiguousarray(PARAMS, np.float64)
-    for call in range(2):
-        pts, obs, src, x, n_obs, n_src, qx, qw = _inputs(ft, nq, seed=10 + call)
+    # a larger problem, then a smaller one: the second call's records and
+    # partial sums sit on scratch bytes the first call wrote differently
+    for call, grid in enumerate((40, 17)):
+        pts, obs, src, x, n_obs, n_src, qx, qw = _inputs(ft, nq, seed=10 + call, grid=grid)
         want = device.zeros(n_obs * 9, ft)
         got = device.zeros(n_obs * 9, ft)
         _with_workspace(kid, prec, want, x, pts, obs, n_obs, src, n_src, qx, qw, params)
@@ -75,7 +79,7 @@ def test_no_alloc_matches_workspace_entry_point(cuda, K, ft, nq):
         assert rel(g, w) <= TOL[ft], (K, call, rel(g, w))
 
 
-def test_no_alloc_rejects_oversized_problem(cuda):
+def test_no_alloc_rejects_oversized_problem():
     cap = _lib.lib.tct_farfield_noalloc_capacity()
     assert cap == 32 * 1024 * 1024
     n = 400_000  # needs more scratch than the built-in array holds
@@ -86,8 +90,18 @@ def test_no_alloc_rejects_oversized_problem(cuda):
     need = _lib.lib.tct_farfield_workspace_bytes(6, 0, n, n, 3)
     assert need > cap
     rc = _lib.lib.tct_farfield_tris_matvec_noalloc(
-        6, 0, ctypes.c_void_p(16), ctypes.c_void_p(16), ctypes.c_void_p(16),
-        ctypes.c_void_p(16), n, ctypes.c_void_p(16), n, 3, _lib.dptr(qx), _lib.dptr(qw),
-        _lib.dptr(params), 0, _lib.stream_ptr())
+        6, 0, None, None, None, None, n, None, n, 3, _lib.dptr(qx), _lib.dptr(qw),
+        _lib.dptr(params), 0, None)
     assert rc == _lib.TCT_ERR_ARG
     assert "scratch" in _lib.last_error()
+    # negative sizes are refused as such, before the scratch size is asked
+    rc = _lib.lib.tct_farfield_tris_matvec_noalloc(
+        6, 0, None, None, None, None, -1, None, n, 3, _lib.dptr(qx), _lib.dptr(qw),
+        _lib.dptr(params), 0, None)
+    assert rc == _lib.TCT_ERR_ARG
+    assert "negative size" in _lib.last_error()
+    # no observation triangles: nothing to do, whatever the source count
+    rc = _lib.lib.tct_farfield_tris_matvec_noalloc(
+        6, 0, None, None, None, None, 0, None, n, 3, _lib.dptr(qx), _lib.dptr(qw),
+        _lib.dptr(params), 0, None)
+    assert rc == _lib.TCT_OK
