@@ -77,9 +77,29 @@ def resolve_ea_rotation(tris, ea):
     return out
 
 
-def nearfield_pairs(pts, tris, obs_subset, src_subset, near_threshold):
+def restrict_rows(classes, row_range):
+    """Keep the pairs whose dof row lies in [r0, r1) and renumber the rows
+    from 0: the block rows r0..r1-1 of the operator the classes describe."""
+    r0, r1 = row_range
+    out = {}
+    for c, (recs, dofs) in classes.items():
+        m = (dofs[:, 0] >= r0) & (dofs[:, 0] < r1)
+        d = dofs[m].copy()
+        d[:, 0] -= r0
+        out[c] = (recs[m], d)
+    return out
+
+
+def nearfield_pairs(pts, tris, obs_subset, src_subset, near_threshold, row_range=None):
     """Host-side pair classes: dict of tri-space records and dof-space
-    (row, col) for 'co', 'ea', 'va', 'near' (nearfield_op.py:95-114)."""
+    (row, col) for 'co', 'ea', 'va', 'near' (nearfield_op.py:95-114).
+
+    row_range=(r0, r1) (an addition, for row shards): the search still runs
+    over the whole obs_subset, so the pair set is the full operator's, and
+    only the pairs of dof rows r0..r1-1 are kept (rows renumbered from 0).
+    Searching the shard's triangles alone would build different octrees, and
+    the reference's leaf test reads radii by tree position, so pairs at the
+    threshold could change."""
     obs_subset = np.asarray(obs_subset)
     src_subset = np.asarray(src_subset)
     co_tris = np.intersect1d(obs_subset, src_subset)
@@ -93,12 +113,13 @@ def nearfield_pairs(pts, tris, obs_subset, src_subset, near_threshold):
     va = to_tri_space(va_dofs, obs_subset, src_subset)
     va = np.hstack((va, np.zeros((va.shape[0], 1), dtype=np.int64)))
     ea = resolve_ea_rotation(tris, to_tri_space(ea_dofs, obs_subset, src_subset))
-    return {
+    out = {
         "co": (co, co_dofs),
         "ea": (ea, ea_dofs[:, :2]),
         "va": (va, va_dofs[:, :2]),
         "near": (near, near_dofs),
     }
+    return out if row_range is None else restrict_rows(out, row_range)
 
 
 CLASSES = ("co", "ea", "va", "near")
@@ -108,25 +129,31 @@ class RegularizedNearfieldIntegralOp:
     def __init__(self, pts, tris, obs_subset, src_subset,
                  nq_coincident, nq_edge_adj, nq_vert_adjacent,
                  nq_far, nq_near, near_threshold,
-                 K_near_name, K_far_name, params, float_type, keep_uncorrected=True):
+                 K_near_name, K_far_name, params, float_type, keep_uncorrected=True,
+                 row_range=None):
         device.require_cuda()
         pts = np.asarray(pts, dtype=np.float64)
         tris = np.asarray(tris, dtype=np.int64)
         obs_subset = np.asarray(obs_subset)
         src_subset = np.asarray(src_subset)
         self.float_type = np.dtype(float_type)
-        self.shape = (obs_subset.shape[0] * 9, src_subset.shape[0] * 9)
+        # row_range (an addition): this operator is block rows r0..r1-1 of the
+        # one over obs_subset -- the same pairs and blocks (see nearfield_pairs)
+        self.row_range = row_range
+        n_rows = obs_subset.shape[0] if row_range is None else row_range[1] - row_range[0]
+        self.shape = (n_rows * 9, src_subset.shape[0] * 9)
 
         pairs_int = PairsIntegrator(K_near_name, params, float_type, nq_far, nq_near, pts, tris)
         corr_int = PairsIntegrator(K_far_name, params, float_type, nq_far, nq_near, pts, tris)
-        self.classes = nearfield_pairs(pts, tris, obs_subset, src_subset, near_threshold)
+        self.classes = nearfield_pairs(pts, tris, obs_subset, src_subset, near_threshold,
+                                       row_range=row_range)
 
         rows = np.concatenate([self.classes[c][1][:, 0] for c in CLASSES]).astype(np.int64)
         cols = np.concatenate([self.classes[c][1][:, 1] for c in CLASSES]).astype(np.int64)
         order = np.lexsort((cols, rows))  # stable: duplicates keep class order
         slot = np.empty_like(order)
         slot[order] = np.arange(order.shape[0])
-        n_row_blocks = obs_subset.shape[0]
+        n_row_blocks = n_rows
         indptr = np.zeros(n_row_blocks + 1, dtype=np.int64)
         np.add.at(indptr, rows + 1, 1)
         indptr = np.cumsum(indptr)

@@ -16,21 +16,36 @@ class RegularizedSparseIntegralOp:
     def __init__(self, nq_coincident, nq_edge_adj, nq_vert_adjacent,
                  nq_far, nq_near, near_threshold,
                  K_near_name, K_far_name, params, pts, tris, float_type, farfield_op_type,
-                 obs_subset=None, src_subset=None, keep_uncorrected=True):
+                 obs_subset=None, src_subset=None, keep_uncorrected=True, row_range=None):
+        """row_range=(r0, r1) (an addition, for row shards): the operator is
+        block rows r0..r1-1 of the one over obs_subset x src_subset -- the
+        same near pairs and blocks (the search runs over the whole
+        obs_subset) and the farfield of those observation triangles -- so
+        stacking the applies of a partition of the rows gives the full
+        operator's apply."""
         tris = np.asarray(tris)
         if obs_subset is None:
             obs_subset = np.arange(tris.shape[0])
         if src_subset is None:
             src_subset = np.arange(tris.shape[0])
+        obs_subset = np.asarray(obs_subset)
         self.float_type = np.dtype(float_type)
+        self.row_range = row_range
         self.nearfield = RegularizedNearfieldIntegralOp(
             pts, tris, obs_subset, src_subset,
             nq_coincident, nq_edge_adj, nq_vert_adjacent, nq_far, nq_near,
             near_threshold, K_near_name, K_far_name, params, float_type,
-            keep_uncorrected=keep_uncorrected)
+            keep_uncorrected=keep_uncorrected, row_range=row_range)
+        far_obs = obs_subset if row_range is None else obs_subset[row_range[0]:row_range[1]]
         self.farfield = farfield_op_type(
-            nq_far, K_far_name, params, pts, tris, float_type, obs_subset, src_subset)
-        self._far_args = (farfield_op_type, nq_far, K_far_name, params, pts, tris, obs_subset,
+            nq_far, K_far_name, params, pts, tris, float_type, far_obs, src_subset)
+        if row_range is not None:
+            from ..fmm.tsfmm import FMMFarfieldOpImpl
+            if isinstance(self.farfield, FMMFarfieldOpImpl):
+                raise ValueError("row_range: the FMM farfield builds its trees and lists per "
+                                 "observation set, so its rows cannot be split off exactly; "
+                                 "use the direct farfield for row shards")
+        self._far_args = (farfield_op_type, nq_far, K_far_name, params, pts, tris, far_obs,
                           src_subset)
         self.shape = self.nearfield.shape
         self._graph = None
@@ -77,41 +92,44 @@ class RegularizedSparseIntegralOp:
             y.add_(buf)
         return y
 
-    def dot_device(self, x, y, stream=None):
-        """y = (Far + Near) x on device tensors of float_type.  With an FMM
-        farfield on a large mesh the nearfield BSR (HBM-bound) runs on a
+    def dot_device(self, x, y, stream=None, accumulate=False):
+        """y (+)= (Far + Near) x on device tensors of float_type.  With an
+        FMM farfield on a large mesh the nearfield BSR (HBM-bound) runs on a
         high-priority second stream into its own buffer while the FMM
         (compute-bound) runs, and is added at the end."""
+        acc = bool(accumulate)
         if self._overlap_near():
             return self._overlapped(
                 x, y, stream, lambda b, s: self.nearfield.dot_device(x, b, accumulate=False,
                                                                       stream=s),
-                lambda s: self.farfield.dot_device(x, y, accumulate=False, stream=s))
+                lambda s: self.farfield.dot_device(x, y, accumulate=acc, stream=s))
         if hasattr(self.farfield, "dot_device"):
-            self.farfield.dot_device(x, y, accumulate=False, stream=stream)
+            self.farfield.dot_device(x, y, accumulate=acc, stream=stream)
         else:
-            y.copy_(device.torch().as_tensor(self.farfield.dot(x.cpu().numpy()), device="cuda"))
+            far = device.torch().as_tensor(self.farfield.dot(x.cpu().numpy()), device="cuda")
+            y.add_(far) if acc else y.copy_(far)
         self.nearfield.dot_device(x, y, accumulate=True, stream=stream)
         return y
 
-    def dot_panel_device(self, X, Y, stream=None):
-        """Y[r] = (Far + Near) X[r] for device tensors X (R, 9 n_src),
+    def dot_panel_device(self, X, Y, stream=None, accumulate=False):
+        """Y[r] (+)= (Far + Near) X[r] for device tensors X (R, 9 n_src),
         Y (R, 9 n_obs) of float_type (an addition: R vectors per apply; the
         elasticRH3 FP32 farfield runs on the tensor cores, the nearfield BSR
         in one launch)."""
         far = self.farfield
+        acc = bool(accumulate)
         if self._overlap_near() and not hasattr(far, "dot_panel_device"):
             def far_all(s):
                 for r in range(X.shape[0]):
-                    far.dot_device(X[r], Y[r], accumulate=False, stream=s)
+                    far.dot_device(X[r], Y[r], accumulate=acc, stream=s)
             return self._overlapped(
                 X, Y, stream, lambda b, s: self.nearfield.dot_panel_device(X, b, accumulate=False,
                                                                             stream=s), far_all)
         if hasattr(far, "dot_panel_device"):
-            far.dot_panel_device(X, Y, accumulate=False, stream=stream)
+            far.dot_panel_device(X, Y, accumulate=acc, stream=stream)
         else:
             for r in range(X.shape[0]):
-                far.dot_device(X[r], Y[r], accumulate=False, stream=stream)
+                far.dot_device(X[r], Y[r], accumulate=acc, stream=stream)
         self.nearfield.dot_panel_device(X, Y, accumulate=True, stream=stream)
         return Y
 

@@ -7,7 +7,17 @@ an all-gather of the ranks' slices of x (NCCL over NVLink between GPUs; any
 torch.distributed backend works, gloo on CPU in the tests), no reduction
 (the outputs are disjoint).  The reference is single-device; this is the
 natural multi-GPU layout of its `RegularizedSparseIntegralOp.dot`
-(ops/sparse_integral_op.py:35-55), built on obs_subset.
+(ops/sparse_integral_op.py:35-55).
+
+A shard is the full operator's rows, not an operator over the shard's
+triangles: ``RegularizedSparseIntegralOp(..., row_range=(r0, r1))`` runs the
+near-pair search over all observation triangles and keeps the pairs of its
+rows, so every rank holds exactly the blocks of the one global operator (the
+reference's leaf test reads radii by octree position, so a search over the
+shard's triangles alone could move pairs at the threshold across the
+near/far line).  The FMM farfield is not sharded: its trees and interaction
+lists are built per observation set, so a shard of an FMM operator is not the
+rows of the global one.
 """
 import numpy as np
 
@@ -21,9 +31,9 @@ def row_ranges(n_rows, world):
 class RowShardedOp:
     """This rank's rows of y = A x.
 
-    op_factory(obs_subset) builds the operator restricted to the given
-    observation triangles (all sources), e.g.
-    ``lambda obs: RegularizedSparseIntegralOp(..., obs_subset=obs)``; its
+    op_factory(row_range) builds block rows [r0, r1) of the global operator
+    (all sources), e.g.
+    ``lambda rr: RegularizedSparseIntegralOp(..., row_range=rr)``; its
     ``dot`` takes the full x (9 n_tris values).  ``dot(x_local)`` takes this
     rank's slice of x and returns this rank's slice of y."""
 
@@ -34,7 +44,7 @@ class RowShardedOp:
         self.r0, self.r1 = self.ranges[rank]
         self.n_tris = n_tris
         self.max_rows = max(e - s for s, e in self.ranges)
-        self.op = op_factory(np.arange(self.r0, self.r1))
+        self.op = op_factory((self.r0, self.r1))
 
     def gather_x(self, x_local):
         """All-gather the ranks' slices into the full x (padded equal-size

@@ -63,3 +63,18 @@ def is_device_tensor(v):
     except ImportError:
         return False
     return isinstance(v, t.Tensor) and v.is_cuda
+
+
+def host_or_device_apply(op, v, float_type):
+    """op.dot_device on v: a CUDA tensor stays on the device (in its own
+    precision when float_type is not fixed by op), a host array is copied in
+    as float_type and the result copied back."""
+    t = torch()
+    ft = np.dtype(float_type)
+    if is_device_tensor(v):
+        x = v.to(torch_dtype(ft)).contiguous()
+        return op.dot_device(x, t.empty(op.shape[0], dtype=x.dtype, device=x.device))
+    x = to_dev(np.asarray(v).reshape(-1), ft)
+    y = t.empty(op.shape[0], dtype=x.dtype, device=x.device)
+    op.dot_device(x, y)
+    return y.cpu().numpy()

@@ -151,6 +151,44 @@ def test_combinators(cuda):
     assert rel(comp.dot(xx), H.dot(x) + M.dot(x)) < 1e-14
 
 
+@pytest.mark.parametrize("td", [3, 1])
+def test_mass_op_device_apply_matches_reference_matrix(cuda, golden, td):
+    # ops/mass_op.py:9-42 + _mass_op.cpp:11-40: the reference's matrix (golden)
+    # applied by the device block-diagonal BSR (tensor_dim 3) or CSR (1)
+    g = golden("mass_op.npz")
+    M = tct.MassOp(3, g["pts"], g["tris"], tensor_dim=td)
+    A = g["mat_3_%d" % td]
+    x = np.random.default_rng(1).standard_normal(A.shape[1])
+    y = M.dot(x)
+    assert y.dtype == np.float64
+    assert rel(y, A @ x) < 1e-14
+    xd = cuda.from_numpy(x.astype(np.float32)).cuda()
+    yd = M.dot(xd)
+    assert yd.is_cuda and yd.dtype == cuda.float32
+    assert rel(yd.cpu().numpy(), A @ x) < 1e-6
+
+
+def test_sum_with_mass_stays_on_device(cuda):
+    # SumOp([H, MultOp(M, 0.5)]) (examples/okada.py:354-358) applied to a
+    # device tensor: one device apply, no host round trip, in H's precision
+    pts, tris = bumpy_mesh(6, seed=3)
+    H = tct.RegularizedSparseIntegralOp(3, 3, 3, 2, 3, 2.0, "elasticRH3", "elasticRH3", PARAMS,
+                                        pts, tris, np.float32, TriToTriDirectFarfieldOp)
+    M = tct.MassOp(3, pts, tris)
+    op = tct.SumOp([H, tct.MultOp(M, 0.5)])
+    assert op.on_device()
+    x = np.random.default_rng(0).standard_normal(H.shape[1]).astype(np.float32)
+    yd = op.dot(cuda.from_numpy(x).cuda())
+    assert yd.is_cuda and yd.dtype == cuda.float32
+    want = H.dot(x).astype(np.float64) + 0.5 * (M.mat @ x.astype(np.float64))
+    assert rel(yd.cpu().numpy(), want) < 1e-6
+    y2 = cuda.ones_like(yd)
+    op.dot_device(cuda.from_numpy(x).cuda(), y2, accumulate=True)
+    assert rel(y2.cpu().numpy(), want + 1.0) < 1e-6
+    neg = tct.NegOp(op)
+    assert rel(neg.dot(x), -want) < 1e-6
+
+
 def test_empty_nearfield_classes(cuda, orc):
     # two far-apart surfaces: no near, edge or vertex pairs across, only
     # coincident + in-surface classes; obs/src disjoint -> no coincident

@@ -13,12 +13,12 @@ from tectosaur_b200.sharded import RowShardedOp, row_ranges
 
 
 class DenseRows:
-    """Stand-in operator: rows [obs] of a dense matrix (the GPU operator's
-    obs_subset restriction), applied on CPU tensors."""
+    """Stand-in operator: block rows [r0, r1) of a dense matrix (the GPU
+    operator's row_range restriction), applied on CPU tensors."""
 
-    def __init__(self, A, obs, k=9):
-        rows = (np.asarray(obs)[:, None] * k + np.arange(k)).reshape(-1)
-        self.A = torch.from_numpy(A[rows])
+    def __init__(self, A, row_range, k=9):
+        r0, r1 = row_range
+        self.A = torch.from_numpy(A[r0 * k:r1 * k])
 
     def dot(self, x):
         return self.A @ x
@@ -40,7 +40,7 @@ def _worker(rank, world, port, n_tris, out_q):
         rng = np.random.default_rng(0)
         A = rng.standard_normal((9 * n_tris, 9 * n_tris))
         x = rng.standard_normal(9 * n_tris)
-        op = RowShardedOp(lambda obs: DenseRows(A, obs), n_tris, rank, world)
+        op = RowShardedOp(lambda rr: DenseRows(A, rr), n_tris, rank, world)
         x_local = torch.from_numpy(x[op.r0 * 9:op.r1 * 9].copy())
         y_local = op.dot(x_local)
         ys = [None] * world
@@ -72,3 +72,46 @@ def test_row_ranges():
     assert r[0][0] == 0 and r[-1][1] == 59858
     sizes = [e - s for s, e in r]
     assert max(sizes) - min(sizes) <= 1
+
+
+def _pairs_worker(rank, world, port, out_q):
+    """Each rank finds its row shard's near pairs the way the row_range
+    operator does (search over all observation triangles, keep its rows);
+    rank 0 checks that the shards stack up to the full operator's pairs."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from helpers import bumpy_mesh
+        from tectosaur_b200.nearfield.nearfield_op import nearfield_pairs
+        pts, tris = bumpy_mesh(13, seed=4)
+        n = tris.shape[0]
+        r0, r1 = row_ranges(n, world)[rank]
+        idx = np.arange(n)
+        mine = nearfield_pairs(pts, tris, idx, idx, 2.5, row_range=(r0, r1))
+        got = [None] * world
+        dist.all_gather_object(got, (r0, mine))
+        if rank == 0:
+            full = nearfield_pairs(pts, tris, idx, idx, 2.5)
+            ok = True
+            for c in full:
+                recs = np.concatenate([m[c][0] for _, m in sorted(got, key=lambda t: t[0])])
+                dofs = np.concatenate([m[c][1] + [r, 0] for r, m in sorted(got, key=lambda t: t[0])])
+                ok = ok and np.array_equal(recs, full[c][0]) and np.array_equal(dofs, full[c][1])
+            out_q.put(bool(ok))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_row_shards_hold_the_full_operators_pairs(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_pairs_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    assert all(p.exitcode == 0 for p in procs)
+    assert q.get(timeout=5) is True
