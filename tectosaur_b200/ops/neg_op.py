@@ -4,6 +4,8 @@ With a device apply underneath, ``dot_device`` scales on the device: the
 wrapped operator writes into y (or a scratch buffer when accumulating) and
 one elementwise pass applies the factor.
 """
+import numpy as np
+
 from ..util import device
 
 
@@ -18,8 +20,8 @@ class MultOp:
 
     @property
     def float_type(self):
-        from .sum_op import device_float_type
-        return device_float_type([self.op])
+        from .sum_op import fixed_float_type
+        return fixed_float_type([self.op])
 
     def _scaled(self, apply, y, stream, accumulate):
         t = device.torch()
@@ -53,7 +55,7 @@ class MultOp:
 
     def dot(self, v):
         if self.on_device() and (device.is_device_tensor(v) or device.cuda_available()):
-            return device.host_or_device_apply(self, v, self.float_type)
+            return device.host_or_device_apply(self, v, self.float_type or np.float64)
         return self.factor * self.op.dot(v)
 
     def farfield_dot(self, v):

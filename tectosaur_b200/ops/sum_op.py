@@ -11,10 +11,11 @@ import numpy as np
 from ..util import device
 
 
-def device_float_type(ops):
-    """The widest float_type among ops that fix one (others follow x)."""
-    fts = [np.dtype(op.float_type) for op in ops if hasattr(op, "float_type")]
-    return max(fts, key=lambda f: f.itemsize) if fts else np.dtype(np.float64)
+def fixed_float_type(ops):
+    """The widest float_type among ops that fix one, or None when none does
+    (MassOp applies in the precision of its input)."""
+    fts = [np.dtype(op.float_type) for op in ops if getattr(op, "float_type", None) is not None]
+    return max(fts, key=lambda f: f.itemsize) if fts else None
 
 
 class SumOp:
@@ -27,7 +28,7 @@ class SumOp:
 
     @property
     def float_type(self):
-        return device_float_type(self.ops)
+        return fixed_float_type(self.ops)
 
     def dot_device(self, x, y, stream=None, accumulate=False):
         """y (+)= sum_k op_k x on device tensors."""
@@ -48,7 +49,7 @@ class SumOp:
 
     def dot(self, v):
         if self.on_device() and (device.is_device_tensor(v) or device.cuda_available()):
-            return device.host_or_device_apply(self, v, self.float_type)
+            return device.host_or_device_apply(self, v, self.float_type or np.float64)
         return sum([op.dot(v) for op in self.ops])
 
     def farfield_dot(self, v):
