@@ -1613,197 +1613,260 @@ def run_interior_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
-def serve_meshes(n_meshes=6, seed=6, lo=2000, hi=20000):
-    """The served stream's meshes: triangle counts log-uniform in [lo, hi]
-    (seeded), cycling through a vertical strike-slip fault, a 30-degree
-    dipping fault and a topographic surface patch with a Gaussian hill."""
-    from tectosaur_b200.mesh.mesh_gen import make_rect
+# ---- C5: the served quasidynamic stream ----------------------------------------
+C5_LO, C5_HI = 2_000, 200_000
+C5_TOL = 1e-8             # FP64 residual of every solve request
+C5_FMM_MIN = 60_000       # meshes from this size use the FMM farfield
+C5_FMM = dict(mac=3.0, pts_per_cell=128, order=10, mode="fmm")
+C5_SOLVES = (8, 6, 4, 3, 2, 2)   # solve requests per mesh, smallest mesh first
+C5_QD_MESHES = 2                  # the smallest meshes (faults) also take qd requests
+C5_QD_PER_MESH = 4
+
+
+def c5_meshes(n_meshes=6, seed=6, lo=C5_LO, hi=C5_HI):
+    """The served stream's meshes: one seeded log-uniform triangle count per
+    equal log-width stratum of [lo, hi] (so the draw spans the range),
+    kinds cycling through a vertical strike-slip fault, a 30-degree dipping
+    fault and a topographic surface (Gaussian hill) with a dipping fault
+    below it; 2 x 2 (nondimensional) patches."""
+    from tectosaur_b200.mesh.mesh_gen import concat_no_dedupe, make_rect
     rng = np.random.default_rng(seed)
-    out = []
+    edges = np.exp(np.linspace(np.log(lo), np.log(hi), n_meshes + 1))
     dip = np.radians(30.0)
+    out = []
     for i in range(n_meshes):
-        n_tris = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
-        g = int(round(np.sqrt(n_tris / 2.0))) + 1
+        n_tris = float(np.exp(rng.uniform(np.log(edges[i]), np.log(edges[i + 1]))))
         kind = ("planar", "dipping", "topo")[i % 3]
         if kind == "planar":
+            g = int(round(np.sqrt(n_tris / 2.0))) + 1
             pts, tris = make_rect(g, g, [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]])
         elif kind == "dipping":
-            pts, tris = make_rect(g, g, [[-1, 0, 0], [1, 0, 0], [1, 2 * np.cos(dip), -2 * np.sin(dip)],
+            g = int(round(np.sqrt(n_tris / 2.0))) + 1
+            pts, tris = make_rect(g, g, [[-1, 0, 0], [1, 0, 0],
+                                         [1, 2 * np.cos(dip), -2 * np.sin(dip)],
                                          [-1, 2 * np.cos(dip), -2 * np.sin(dip)]])
         else:
-            pts, tris = make_rect(g, g, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
-            pts = pts.copy()
+            gs = int(round(np.sqrt(0.75 * n_tris / 2.0))) + 1
+            gf = int(round(np.sqrt(0.25 * n_tris / 2.0))) + 1
+            sp, st = make_rect(gs, gs, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
+            sp = sp.copy()
             amp, w = rng.uniform(0.1, 0.3), rng.uniform(0.3, 0.6)
-            pts[:, 2] = amp * np.exp(-(pts[:, 0] ** 2 + pts[:, 1] ** 2) / (2 * w * w))
-        out.append(("%s-%d" % (kind, tris.shape[0]), np.asarray(pts), np.asarray(tris)))
+            sp[:, 2] = amp * np.exp(-(sp[:, 0] ** 2 + sp[:, 1] ** 2) / (2 * w * w))
+            z0, y1 = -0.1, np.cos(dip)
+            fp, ft = make_rect(gf, gf, [[-0.5, -0.5, z0], [0.5, -0.5, z0],
+                                        [0.5, -0.5 + y1, z0 - np.sin(dip)],
+                                        [-0.5, -0.5 + y1, z0 - np.sin(dip)]])
+            pts, tris = concat_no_dedupe((sp, st), (fp, ft))
+        out.append(("%s-%d" % (kind, tris.shape[0]), np.asarray(pts), np.asarray(tris), kind))
     return out
 
 
-def run_serve_workload(args, rank, world, torch, dist):
-    """The served stream (C5): solve requests on several resident meshes and
-    quasidynamic requests (qd_steps RK23 steps of the reference's example
-    fault from seeded states), served with continuous batching
-    (tectosaur_b200.serve), against the plain one-request-at-a-time GPU
-    paths (FP64 GMRES solve; single-state qd Integrator)."""
+def c5_stream(torch, quiet=True, seed=7):
+    """Serve the C5 stream (module-level C5_* settings) and time it against
+    the plain paths.  Returns a dict of results (no JSON printing).
+
+    Requests: C5_SOLVES[i] traction solves (seeded N(0, 1) right-hand sides,
+    FP64 residual C5_TOL, continuity + free-edge constraints) on mesh i, and
+    C5_QD_PER_MESH quasidynamic requests (200 RK23 steps of rate-and-state
+    friction, a 0.010, b 0.015, Dc 1e-4, V0 1e-6, eta = mu / (2 c_s), seeded
+    state perturbation) on each of the C5_QD_MESHES smallest meshes, in a
+    seeded order.  Served: serve.SolveServer (continuous batching, 16 slots
+    per mesh, FP32 operator in FP64 refinement; FMM farfield from C5_FMM_MIN
+    triangles).  Plain: one request at a time in arrival order -- the FP64
+    GMRES solve (simple_solver.iterative_solve) and the single-state
+    Integrator.  Saturation (all requests at t = 0) gives the throughput;
+    Poisson arrivals at 0.7 of the served saturation rate give the served
+    latencies, and the plain path's FIFO queue replayed against the same
+    arrivals (its measured service times) the plain latencies."""
     import tectosaur_b200 as tct
     from tectosaur_b200 import _lib, qd, serve
+    from tectosaur_b200.fmm.tsfmm import FMMFarfieldOp
     from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
     from tectosaur_b200.simple_solver import (free_edge_vertices, iterative_solve,
                                               shared_vertex_matrix)
-    tol = 1e-8
-    n_req = args.requests
-    n_qd = args.qd_requests
-    qd_steps = args.qd_steps
-    meshes = serve_meshes()
+
+    def log(*a):
+        if not quiet:
+            print("[c5]", *a, flush=True)
+
+    meshes = c5_meshes()
     t_build = time.perf_counter()
     srv = serve.SolveServer(slots=16, restart=64)
-    specs = {}
-    for key, pts, tris in meshes:
+    specs, fmm_err = {}, {}
+    for key, pts, tris, kind in meshes:
+        n = tris.shape[0]
         cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+        far = (FMMFarfieldOp(C5_FMM["mac"], C5_FMM["pts_per_cell"], C5_FMM["order"],
+                             C5_FMM["mode"]) if n >= C5_FMM_MIN else TriToTriDirectFarfieldOp)
         op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
-                                               np.float64, TriToTriDirectFarfieldOp,
-                                               keep_uncorrected=False)
-        srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64)
-        specs[key] = (op64, cm, tris.shape[0])
-    qpts, qtris = qd_mesh()
-    nq_tris = qtris.shape[0]
-    qcfg = qd_config(nq_tris)
-    qmodel = qd.FullspaceModel((qpts, qtris), qcfg) if n_qd else None
-    if n_qd:
-        srv.add_qd_mesh("qd-fault", qpts, qtris, qcfg, model=qmodel)
+                                               np.float64, far, keep_uncorrected=False)
+        srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64,
+                     farfield_op_type=far)
+        specs[key] = (op64, cm, n)
+        if n >= C5_FMM_MIN:
+            # the FMM farfield's error against the direct FP64 farfield on
+            # sampled observation rows (the order's truncation error)
+            idx = np.arange(n)
+            rows = np.sort(np.random.default_rng(31).choice(n, 256, replace=False))
+            xr = np.random.default_rng(32).standard_normal(9 * n)
+            direct = TriToTriDirectFarfieldOp(C1_NQ[3], K_NAME, PARAMS, pts, tris, np.float64,
+                                              rows, idx).dot(xr)
+            fm = op64.farfield.dot(xr).reshape(-1, 9)[rows].reshape(-1)
+            fmm_err[key] = float(np.linalg.norm(fm - direct) / np.linalg.norm(direct))
+        log("built", key, "%.1f s" % (time.perf_counter() - t_build))
+    qd_keys = []
+    for key, pts, tris, kind in sorted(meshes, key=lambda m: m[2].shape[0])[:C5_QD_MESHES]:
+        cfg = c5_qd_config(tris.shape[0])
+        model = qd.FullspaceModel((pts, tris), cfg)
+        srv.add_qd_mesh(key + "/qd", pts, tris, cfg, model=model)
+        specs[key + "/qd"] = (model, None, tris.shape[0])
+        qd_keys.append(key + "/qd")
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
-    rng = np.random.default_rng(7 + rank)
-    keys = [m[0] for m in meshes]
+    rng = np.random.default_rng(seed)
     stream = []
-    for i in range(n_req):
-        k = keys[int(rng.integers(len(keys)))]
-        stream.append(("solve", k, rng.standard_normal(9 * specs[k][2])))
-    for i in range(n_qd):
-        stream.insert(int(rng.integers(len(stream) + 1)),
-                      ("qd", "qd-fault", qd_initial(nq_tris, seed=100 + i)))
+    for (key, pts, tris, kind), k_req in zip(sorted(meshes, key=lambda m: m[2].shape[0]),
+                                              C5_SOLVES):
+        for _ in range(k_req):
+            stream.append(("solve", key, rng.standard_normal(9 * tris.shape[0])))
+    for i, key in enumerate(qd_keys):
+        for j in range(C5_QD_PER_MESH):
+            stream.append(("qd", key, c5_qd_initial(specs[key][2], seed=100 + 10 * i + j)))
+    stream = [stream[i] for i in rng.permutation(len(stream))]
+    kinds = [k for k, _, _ in stream]
     n_all = len(stream)
 
-    def replay(offsets):
+    def arrivals(offsets, qd_steps=C5_QD_STEPS, sub=None):
         arr = []
-        for off, (kind, k, payload) in zip(offsets, stream):
+        for i, (off, (kind, k, payload)) in enumerate(zip(offsets, stream)):
+            if sub is not None and i not in sub:
+                continue
             arr.append((off, "qd", k, payload, qd_steps) if kind == "qd" else
-                       (off, k, payload, tol))
-        return srv.replay(arr)
+                       (off, k, payload, C5_TOL))
+        return arr
 
-    zeros = [0.0] * n_all
-    for _ in range(args.warmup):
-        replay(zeros)
+    # warm-up: one request of every mesh (short qd runs) -- builds the
+    # resident operators and engines
+    first = {}
+    for i, (kind, k, _) in enumerate(stream):
+        first.setdefault(k, i)
+    srv.replay(arrivals([0.0] * n_all, qd_steps=3, sub=set(first.values())))
     torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
+    log("warm-up done")
     l0 = _lib.launch_count()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    sat = srv.replay(arrivals([0.0] * n_all))
     torch.cuda.synchronize()
-    a.record()
-    for _ in range(args.steps):
-        sat = replay(zeros)
-    b.record()
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
+    t_served = time.perf_counter() - t0
     launches = _lib.launch_count() - l0
-    total_ms = a.elapsed_time(b)
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    served_rate = n_all * args.steps / (total_ms * 1e-3)
-    kinds = [k for k, _, _ in stream]
-    sat_lat = {kd: np.array([r.latency for r, k in zip(sat, kinds) if k == kd])
-               for kd in ("solve", "qd") if kd in kinds}
     assert all(r.error is None for r in sat), [r.error for r in sat if r.error]
+    served_rate = n_all / t_served
+    log("served saturation %.2f s" % t_served)
     # the plain paths, one request at a time in arrival order
-    iterative_solve(specs[keys[0]][0], specs[keys[0]][1], stream[0][2] if kinds[0] == "solve"
-                    else np.ones(9 * specs[keys[0]][2]), cfg=dict(solver_tol=tol))
-    torch.cuda.synchronize()
     service, err_solve, err_qd = [], [], []
     for (kind, k, payload), r in zip(stream, sat):
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         if kind == "solve":
-            x = iterative_solve(specs[k][0], specs[k][1], payload, cfg=dict(solver_tol=tol))
+            x = iterative_solve(specs[k][0], specs[k][1], payload, cfg=dict(solver_tol=C5_TOL))
             err_solve.append(float(np.linalg.norm(r.x - x) / np.linalg.norm(x)))
         else:
-            integ = qd.Integrator(qmodel, (0.0, payload))
-            integ.integrate(qd_steps)
+            integ = qd.Integrator(specs[k][0], (0.0, payload))
+            integ.integrate(C5_QD_STEPS)
             y = integ.h_y[-1].cpu().numpy()
             err_qd.append(float(np.linalg.norm(r.y - y) / np.linalg.norm(y)))
         torch.cuda.synchronize()
         service.append(time.perf_counter() - t0)
     plain_rate = n_all / sum(service)
-    sweep = []
-    for frac in (0.5, 0.9):
-        lam = frac * served_rate / world
-        gaps = np.random.default_rng(11).exponential(1.0 / lam, n_all)
-        offs = np.cumsum(gaps) - gaps[0]
-        reqs = replay(list(offs))
-        fin, plat = 0.0, []
-        for off, sv in zip(offs, service):
-            fin = max(fin, off) + sv
-            plat.append(fin - off)
-        entry = {"arrival_rate_per_s": lam, "fraction_of_served_saturation": frac}
-        for kd in sat_lat:
-            lat = np.array([r.latency for r, k in zip(reqs, kinds) if k == kd])
-            pl = np.array([v for v, k in zip(plat, kinds) if k == kd])
-            entry.update({"served_%s_p50_ms" % kd: 1e3 * float(np.percentile(lat, 50)),
-                          "served_%s_p99_ms" % kd: 1e3 * float(np.percentile(lat, 99)),
-                          "plain_%s_p50_ms" % kd: 1e3 * float(np.percentile(pl, 50)),
-                          "plain_%s_p99_ms" % kd: 1e3 * float(np.percentile(pl, 99))})
-        sweep.append(entry)
+    log("plain %.2f s" % sum(service))
+    lam = 0.7 * served_rate
+    gaps = np.random.default_rng(11).exponential(1.0 / lam, n_all)
+    offs = np.cumsum(gaps) - gaps[0]
+    reqs = srv.replay(arrivals(list(offs)))
+    fin, plat = 0.0, []
+    for off, sv in zip(offs, service):
+        fin = max(fin, off) + sv
+        plat.append(fin - off)
+
+    def pct(v):
+        v = np.asarray(v, dtype=np.float64)
+        return {"p50_ms": 1e3 * float(np.percentile(v, 50)),
+                "p99_ms": 1e3 * float(np.percentile(v, 99))} if v.size else None
+    lat = {}
+    for kd in ("solve", "qd"):
+        lat[kd] = {"served": pct([r.latency for r, k in zip(reqs, kinds) if k == kd]),
+                   "plain": pct([v for v, k in zip(plat, kinds) if k == kd]),
+                   "served_saturation": pct([r.latency for r, k in zip(sat, kinds) if k == kd])}
+    by_kind = {kd: {"requests": int(sum(1 for k in kinds if k == kd)),
+                    "plain_s": float(sum(sv for sv, k in zip(service, kinds) if k == kd))}
+               for kd in ("solve", "qd")}
+    return {
+        "metric": "served vs plain requests/s (solves/s and qd integrations/s)",
+        "served_requests_per_s": served_rate, "plain_requests_per_s": plain_rate,
+        "speedup_vs_plain": served_rate / plain_rate,
+        "served_s": t_served, "plain_s": float(sum(service)),
+        "requests": by_kind,
+        "meshes": {key: {"n_tris": int(tris.shape[0]), "kind": kind,
+                         "farfield": ("fmm p=%d mac %.1f, %d per leaf"
+                                      % (C5_FMM["order"], C5_FMM["mac"], C5_FMM["pts_per_cell"])
+                                      if tris.shape[0] >= C5_FMM_MIN else "direct")}
+                   for key, pts, tris, kind in meshes},
+        "qd_meshes": qd_keys, "qd_steps": C5_QD_STEPS, "solve_tol": C5_TOL,
+        "max_rel_diff_solve_vs_plain_fp64": max(err_solve) if err_solve else None,
+        "max_rel_diff_qd_vs_plain_integrator": max(err_qd) if err_qd else None,
+        "fmm_rel_err_vs_direct_fp64": fmm_err,
+        "latency_poisson": {"arrival_rate_per_s": lam, "fraction_of_served_saturation": 0.7,
+                            **lat},
+        "gpu_launches": int(launches),
+        "build_s": t_build, "resident_bytes": int(srv.resident_bytes),
+        "h2d_bytes": int(sum(p.nbytes for _, _, p in stream)),
+        "d2h_bytes": int(sum((r.x if k == "solve" else r.y).nbytes for r, k in zip(sat, kinds))),
+    }
+
+
+C5_QD_STEPS = 200
+
+
+def c5_qd_config(n_tris, float_type=np.float32):
+    """The C5 quasidynamic configuration: the reference example run's
+    constants (shear modulus 3e10, density 2670 -> eta = mu / (2 c_s), f0
+    0.6, V0 1e-6, plate rate 1e-9, 50 MPa normal stress, step tolerance
+    1e-4) with a 0.010, b 0.015, Dc 1e-4 and the plain method's rules."""
+    cfg = qd_config(n_tris, float_type)
+    cfg["Dc"] = 1e-4
+    return cfg
+
+
+def c5_qd_initial(n_tris, seed):
+    """Zero slip and state 0.7 with a seeded perturbation (it perturbs the
+    initial slip rate)."""
+    return qd_initial(n_tris, seed)
+
+
+def run_serve_workload(args, rank, world, torch, dist):
+    """The C5 served stream as its own line (see c5_stream)."""
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    res = c5_stream(torch, quiet=(rank != 0))
+    clocks = sampler.stop()
     if rank != 0:
         return
-    ms = total_ms / args.steps
-    plain_by = {kd: sum(sv for sv, k in zip(service, kinds) if k == kd) for kd in sat_lat}
     line = {
         "metric": "BEM requests/s: served (continuous batching, mixed precision) vs plain",
-        "value": served_rate, "unit": "requests/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32 operator (tensor-core farfield panel) + f64 residual refinement / f64 "
-                 "qd state",
+        "value": res["served_requests_per_s"], "unit": "requests/s", "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * res["served_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 operator (tensor-core farfield panel / FMM) + f64 residual refinement; "
+                 "f64 qd state",
         "data": "synthetic (seeded meshes, arrivals, right-hand sides and qd states)",
-        "config": {"workload": ("%d solve requests (seeded N(0, 1) tractions, FP64 residual "
-                                "1e-8) on %d resident meshes of %s triangles (log-uniform "
-                                "2k-20k: vertical, 30-degree dipping faults, topographic "
-                                "patch; elasticRH3 RegularizedSparseIntegralOp(6,6,6,2,5,2.5), "
-                                "continuity + free-edge constraints) and %d quasidynamic "
-                                "requests (%d RK23 steps of the reference's example fault, "
-                                "%d triangles, from seeded states), all arriving at once "
-                                "(saturation); one step = the whole stream"
-                                % (n_req, len(meshes), [m[2].shape[0] for m in meshes], n_qd,
-                                   qd_steps, nq_tris)),
-                   "meshes": [m[0] for m in meshes] + (["qd-fault"] if n_qd else []),
-                   "requests": {"solve": n_req, "qd": n_qd}, "qd_steps": qd_steps,
-                   "slots_per_mesh": srv.slots, "restart": srv.restart,
-                   "plain_requests_per_s": plain_rate,
-                   "speedup_vs_plain": served_rate / plain_rate,
-                   "plain_seconds_by_kind": plain_by,
-                   "max_rel_diff_solve_vs_plain_fp64": max(err_solve) if err_solve else None,
-                   "max_rel_diff_qd_vs_plain_integrator": max(err_qd) if err_qd else None,
-                   "saturation_latency_ms": {kd: {"p50": 1e3 * float(np.percentile(v, 50)),
-                                                  "p99": 1e3 * float(np.percentile(v, 99))}
-                                             for kd, v in sat_lat.items()},
-                   "latency_sweep": sweep,
-                   "mesh_build_s": t_build, "resident_bytes": srv.resident_bytes,
-                   "l2": "operators and Krylov bases of the resident meshes (GBs, beyond L2)",
-                   "parallelism": "replicas"},
-        "roofline": {"kernel": "whole served stream (see the batch, panel and qd workloads)",
-                     "bound": "tensor", "achieved": None, "peak": None, "unit": "TFLOP/s",
-                     "frac": None, "traffic": None},
-        "e2e": {"value": served_rate, "unit": "requests/s",
-                "h2d_bytes_per_step": int(sum(p.nbytes for _, _, p in stream)),
-                "d2h_bytes_per_step": int(sum((r.x if k == "solve" else r.y).nbytes
-                                              for r, k in zip(sat, kinds))),
+        "config": {"workload": "C5 served stream (bench.c5_stream)", **{
+            k: res[k] for k in ("meshes", "requests", "qd_meshes", "qd_steps", "solve_tol")},
+            "parallelism": "replicas"},
+        "served": res,
+        "e2e": {"value": res["served_requests_per_s"], "unit": "requests/s",
+                "h2d_bytes_per_step": res["h2d_bytes"], "d2h_bytes_per_step": res["d2h_bytes"],
                 "api": "serve.SolveServer.replay(stream of solve and qd requests) -> numpy"},
-        "gpu_launches": int(launches),
-        "clocks": clocks,
+        "gpu_launches": res["gpu_launches"], "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 
@@ -1827,6 +1890,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the C5 served-vs-plain stream on the default line")
     ap.add_argument("--grid", type=int, default=None,
                     help="vertices per side of the surface grid (174 = the 59,858-triangle "
                          "workload; smaller for profiling; the fmm workload uses 707)")
@@ -1842,10 +1907,6 @@ def main():
     ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--qd-steps", type=int, default=200,
                     help="RK23 steps per quasidynamic integration (qd workload)")
-    ap.add_argument("--qd-requests", type=int, default=8,
-                    help="quasidynamic requests in the served stream (serve workload)")
-    ap.add_argument("--requests", type=int, default=48,
-                    help="solve requests in the served stream (serve workload)")
     ap.add_argument("--fmm-order", type=int, default=None)
     ap.add_argument("--fmm-ppc", type=int, default=None)
     ap.add_argument("--fmm-mode", default=None, choices=["fmm", "treecode"])
@@ -1984,6 +2045,14 @@ def main():
         }
         classes = c2_classes(pts, tris)
         line["parity"] = c2_parity(pts, tris, y.cpu().numpy(), x.cpu().numpy(), classes)
+        if world == 1 and not args.no_served:
+            # the north-star comparison: the C5 stream served vs plain
+            del op, far, near
+            torch.cuda.empty_cache()
+            try:
+                line["served"] = c5_stream(torch)
+            except Exception as e:  # keep the matvec line if the stream fails
+                line["served"] = {"error": "%s: %s" % (type(e).__name__, e)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pts, tris, classes)
         print(json.dumps(line), flush=True)

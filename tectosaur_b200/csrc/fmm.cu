@@ -1953,6 +1953,13 @@ int run_fmm(int mode, int p, const Rule2D<R>& rule, const double* params, double
                 const size_t smem_all = sizeof(R) * (2 * (size_t)NT * C::NCHP +
                                                      2 * (size_t)((NT + 3) / 4 * 4) + 80 +
                                                      (size_t)m2l2_items(p) * C::NCHP);
+                if (smem_all > 227 * 1024) {
+                    // FP64 at p = 12 needs 286 KB (p = 10: 190 KB)
+                    set_error("tct_fmm_matvec: the item-form M2L at order %d needs %zu bytes of "
+                              "shared memory (the limit is 227 KB; FP64 runs orders up to 10)",
+                              p, smem_all);
+                    return TCT_ERR_ARG;
+                }
                 if ((rc = set_smem(fmm_m2l2<R, K>, smem_all))) return rc;
                 fmm_m2l2<R, K><<<(unsigned)far.n_obs, M2L2_THREADS, smem_all, se>>>(
                     p, far.obs, far.n_obs, far.start, far.src, ocent, orad, scent, srad, mom,
