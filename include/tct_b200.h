@@ -105,6 +105,24 @@ int tct_pairs_integrate_batched(int kernel, int prec, void* out, int64_t n_pairs
                                 int accumulate, void* workspace,
                                 size_t workspace_bytes, void* stream);
 
+/* Slot form of tct_pairs_integrate_batched, used by the nearfield operator
+ * build (RegularizedNearfieldIntegralOp, nearfield/nearfield_op.py:76-150:
+ * its four pair classes and their far-rule corrections, each class
+ * integrated there by its own single_pairs launch): element e of pair p's
+ * block goes to out[e * slot_stride + slot[p]] (the BSR's structure-of-arrays
+ * blocks), times `sign`, added to the destination when `add`.  Pairs cut
+ * into several warp items are added atomically, so their slots must start
+ * at zero (or `add`); a plan without split items is deterministic. */
+int tct_pairs_integrate_batched_slots(int kernel, int prec, void* out, const int32_t* slot,
+                                      int64_t slot_stride, double sign, int add, int64_t n_pairs,
+                                      const void* pts, const int32_t* tris,
+                                      const int32_t* pairs, const int64_t* rule_off,
+                                      const int32_t* rule_flags, const void* rule_pts,
+                                      const void* rule_wts, const int32_t* items,
+                                      int64_t n_warp_items, int64_t n_thread_items,
+                                      const double* params, int n_param_sets, void* workspace,
+                                      size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Direct tri-to-tri farfield matvec.                                        */
 /* Replaces farfield_tris_to_tris{K} (tectosaur/matrix_free.cl:19-107) behind
@@ -505,6 +523,60 @@ int tct_cg_csr_batch(int64_t n, int n_sys, const int64_t* indptr, const int64_t*
                      const double* data, const double* b, int64_t b_stride, double* x,
                      int64_t x_stride, double* work, double rtol, double atol, int maxiter,
                      int* iters, void* stream);
+
+/* ---- tuned launch shapes (the autotuner) ---------------------------------- */
+/* The reference compiles a kernel per template argument set and caches the
+ * module (tectosaur/util/gpu.py:63-77); its launch shapes are fixed.  Here a
+ * launch's shape -- how the work is cut into CTAs -- is looked up in an
+ * in-library cache keyed by (op, kernel, prec, nq, rhs, bucket(n0),
+ * bucket(n1)), bucket(n) = round(log2 n) + 1 (0 for n <= 0); launches
+ * without an entry use the built-in heuristics.  Values per op:
+ *   TCT_TUNE_FARFIELD  n0 = n_obs, n1 = n_src, rhs = 1: v0 = source chunks
+ *                      (grid.y of the direct farfield; clamped to the sources
+ *                      and to the partial sums the workspace holds), v1 = 1;
+ *   TCT_TUNE_BSR9      kernel = -1, nq = 0, rhs = 1, n0 = block rows,
+ *                      n1 = blocks per row (data_stride / n_row_blocks):
+ *                      v0 = lanes per block row (32, 16, 8 or 4; below 32 a
+ *                      warp serves several short rows), v1 = CTAs per SM;
+ *   TCT_TUNE_FAR_PANEL reserved.
+ * A shape changes the floating-point summation order, not the quantity
+ * computed.  Host functions; the cache is shared by all threads. */
+#define TCT_TUNE_FARFIELD 1
+#define TCT_TUNE_BSR9 2
+#define TCT_TUNE_FAR_PANEL 3
+int tct_tune_set(int op, int kernel, int prec, int nq, int rhs, int64_t n0, int64_t n1, int v0,
+                 int v1);
+/* 1 and the values when the key has an entry, else 0. */
+int tct_tune_get(int op, int kernel, int prec, int nq, int rhs, int64_t n0, int64_t n1, int* v0,
+                 int* v1);
+int tct_tune_bucket(int64_t n);
+/* Enumeration and restore of the cache for persistence: key7 = {op, kernel,
+ * prec, nq, rhs, bucket0, bucket1}. */
+int64_t tct_tune_size(void);
+int tct_tune_entry(int64_t i, int* key7, int* v0, int* v1);
+int tct_tune_put_entry(const int* key7, int v0, int v1);
+void tct_tune_clear(void);
+
+/* Autotune the direct farfield's source chunking for one problem: times the
+ * candidate chunk counts with CUDA events (on `stream`, which is
+ * synchronised) on the caller's buffers -- the same arguments as
+ * tct_farfield_tris_matvec, out is overwritten -- stores the fastest in the
+ * cache and returns it in *chunks (host). */
+int tct_farfield_autotune(int kernel, int prec, void* out, const void* in, const void* pts,
+                          const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris,
+                          int64_t n_src, int n_q, const double* quad_pts,
+                          const double* quad_wts, const double* params, void* workspace,
+                          size_t workspace_bytes, void* stream, int* chunks);
+/* Autotune tct_bsr9_matvec's shape (lanes per block row x CTAs per SM) for
+ * one matrix, as above (y is overwritten); results in *lanes, *ctas_per_sm. */
+int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* indptr,
+                      const int32_t* indices, const void* data, int64_t data_stride,
+                      const void* x, void* y, void* stream, int* lanes, int* ctas_per_sm);
+/* Workspace of tct_farfield_tris_matvec that holds the partial sums of up to
+ * max_chunks source chunks (>= tct_farfield_workspace_bytes), for operators
+ * that let the autotuner raise the chunk count. */
+size_t tct_farfield_workspace_bytes_chunks(int kernel, int prec, int64_t n_obs, int64_t n_src,
+                                           int n_q, int max_chunks);
 
 /* ---- constrained solve -------------------------------------------------- */
 

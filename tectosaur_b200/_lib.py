@@ -223,6 +223,30 @@ for _name, (_args, _res) in _SOLVE_SIGS.items():
     _f.restype = _res
 EXPORTED = sorted(set(EXPORTED) | set(_SOLVE_SIGS))
 
+c_ip = ctypes.POINTER(c_i)
+_TUNE_SIGS = {
+    "tct_tune_set": ([c_i, c_i, c_i, c_i, c_i, c_i64, c_i64, c_i, c_i], c_i),
+    "tct_tune_get": ([c_i, c_i, c_i, c_i, c_i, c_i64, c_i64, c_ip, c_ip], c_i),
+    "tct_tune_bucket": ([c_i64], c_i),
+    "tct_tune_size": ([], c_i64),
+    "tct_tune_entry": ([c_i64, c_ip, c_ip, c_ip], c_i),
+    "tct_tune_put_entry": ([c_ip, c_i, c_i], c_i),
+    "tct_tune_clear": ([], None),
+    "tct_farfield_autotune": ([c_i, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_dp, c_dp,
+                               c_dp, c_p, c_sz, c_p, c_ip], c_i),
+    "tct_bsr9_autotune": ([c_i, c_i64, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_ip, c_ip], c_i),
+    "tct_farfield_workspace_bytes_chunks": ([c_i, c_i, c_i64, c_i64, c_i, c_i], c_sz),
+    "tct_pairs_integrate_batched_slots": ([c_i, c_i, c_p, c_p, c_i64, ctypes.c_double, c_i,
+                                           c_i64, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_i64,
+                                           c_i64, c_dp, c_i, c_p, c_sz, c_p], c_i),
+}
+for _name, (_args, _res) in _TUNE_SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+EXPORTED = sorted(set(EXPORTED) | set(_TUNE_SIGS))
+TCT_TUNE_FARFIELD, TCT_TUNE_BSR9, TCT_TUNE_FAR_PANEL = 1, 2, 3
+
 
 def launch_count():
     """Kernels launched by libtct_b200.so so far in this process."""

@@ -21,21 +21,34 @@ namespace {
 // unconstrained the compiler hoists all 81 block loads into registers (222
 // registers, 1 block per SM) and the per-row shuffle reduction then leaves
 // the SM with no loads in flight.
-template <typename R, bool TWO>
+//
+// LPR lanes serve one block row (LPR = 32: a warp per row, the shape for
+// the operator's ~90 blocks per row; 16, 8 or 4: a warp serves 32 / LPR rows
+// at once, the shape for rows of a few blocks).  The row loop is
+// warp-uniform -- every lane runs the same number of iterations, lanes past
+// the last row carry zeros -- so the shuffles always have the full warp.
+template <typename R, bool TWO, int LPR>
 __global__ void __launch_bounds__(256, 4)
 bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             const int32_t* __restrict__ indices, const R* __restrict__ data,
             const R* __restrict__ data2, int64_t stride, const R* __restrict__ x,
             R* __restrict__ y, int accumulate) {
+    constexpr int G = 32 / LPR;  // rows per warp
     const int lane = threadIdx.x & 31;
+    const int sub = lane % LPR;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = warp; row < n_rows; row += n_warps) {
-        const int32_t start = __ldg(indptr + row), end = __ldg(indptr + row + 1);
+    for (int64_t base = warp * G; base < n_rows; base += n_warps * G) {
+        const int64_t row = base + lane / LPR;
+        int32_t start = 0, end = 0;
+        if (row < n_rows) {
+            start = __ldg(indptr + row);
+            end = __ldg(indptr + row + 1);
+        }
         R acc[9];
 #pragma unroll
         for (int i = 0; i < 9; i++) acc[i] = 0;
-        for (int32_t s = start + lane; s < end; s += 32) {
+        for (int32_t s = start + sub; s < end; s += LPR) {
             const int64_t col = __ldg(indices + s);
             R xv[9];
 #pragma unroll
@@ -55,17 +68,46 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
 #pragma unroll
         for (int i = 0; i < 9; i++) {
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
+            for (int off = LPR / 2; off > 0; off >>= 1)
+                acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], off);
         }
-        if (lane < 9) {
-            R v = acc[0];
+        if (row < n_rows) {
 #pragma unroll
-            for (int i = 1; i < 9; i++)
-                if (lane == i) v = acc[i];
-            R* yp = y + row * 9 + lane;
-            *yp = accumulate ? *yp + v : v;
+            for (int i = 0; i < 9; i++) {
+                if (i % LPR == sub) {
+                    R* yp = y + row * 9 + i;
+                    *yp = accumulate ? *yp + acc[i] : acc[i];
+                }
+            }
         }
     }
+}
+
+// Launch shape of tct_bsr9_matvec: lanes per row and CTAs per SM, from the
+// shape cache (key: block rows, blocks per row) or the defaults (32, 8).
+void bsr_shape(int prec, int64_t n_rows, int64_t stride, int* lpr, int* cps) {
+    *lpr = 32;
+    *cps = 8;
+    int v0 = 0, v1 = 0;
+    const int64_t per_row = n_rows > 0 ? std::max<int64_t>(1, stride / n_rows) : 1;
+    if (tune_lookup(kTuneBsr9, -1, prec, 0, 1, n_rows, per_row, &v0, &v1)) {
+        if (v0 == 32 || v0 == 16 || v0 == 8 || v0 == 4) *lpr = v0;
+        if (v1 >= 1 && v1 <= 64) *cps = v1;
+    }
+}
+
+template <typename R, int LPR>
+void launch_bsr(int64_t blocks, int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+                const void* data, const void* data2, int64_t stride, const void* x, void* y,
+                int accumulate, cudaStream_t st) {
+    if (data2)
+        bsr9_kernel<R, true, LPR><<<(unsigned)blocks, 256, 0, st>>>(
+            n_rows, indptr, indices, (const R*)data, (const R*)data2, stride, (const R*)x, (R*)y,
+            accumulate);
+    else
+        bsr9_kernel<R, false, LPR><<<(unsigned)blocks, 256, 0, st>>>(
+            n_rows, indptr, indices, (const R*)data, nullptr, stride, (const R*)x, (R*)y,
+            accumulate);
 }
 
 template <typename R>
@@ -73,19 +115,23 @@ int run_bsr(int64_t n_rows, const int32_t* indptr, const int32_t* indices, const
             const void* data2, int64_t stride, const void* x, void* y, int accumulate,
             cudaStream_t st) {
     const int threads = 256;
-    const int64_t warps_needed = n_rows;
-    const int64_t max_blocks = (int64_t)sm_count() * 8;
+    int lpr = 32, cps = 8;
+    bsr_shape(sizeof(R) == 8 ? TCT_F64 : TCT_F32, n_rows, stride, &lpr, &cps);
+    const int64_t warps_needed = (n_rows + (32 / lpr) - 1) / (32 / lpr);
+    const int64_t max_blocks = (int64_t)sm_count() * cps;
     int64_t blocks = (warps_needed * 32 + threads - 1) / threads;
     if (blocks > max_blocks) blocks = max_blocks;
     if (blocks < 1) blocks = 1;
-    if (data2)
-        bsr9_kernel<R, true><<<(unsigned)blocks, threads, 0, st>>>(
-            n_rows, indptr, indices, (const R*)data, (const R*)data2, stride, (const R*)x, (R*)y,
-            accumulate);
-    else
-        bsr9_kernel<R, false><<<(unsigned)blocks, threads, 0, st>>>(
-            n_rows, indptr, indices, (const R*)data, nullptr, stride, (const R*)x, (R*)y,
-            accumulate);
+    switch (lpr) {
+        case 16: launch_bsr<R, 16>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                   accumulate, st); break;
+        case 8: launch_bsr<R, 8>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                 accumulate, st); break;
+        case 4: launch_bsr<R, 4>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                 accumulate, st); break;
+        default: launch_bsr<R, 32>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                   accumulate, st);
+    }
     return launch_status("tct_bsr9_matvec");
 }
 
@@ -192,6 +238,64 @@ extern "C" int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* in
                                accumulate, as_stream(stream));
     set_error("tct_bsr9_matvec: unsupported precision %d", prec);
     return TCT_ERR_PREC;
+}
+
+// Candidate shapes (lanes per row x CTAs per SM), each timed as one untimed
+// launch then the mean of three under CUDA events; the fastest stays in the
+// shape cache.
+extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* indptr,
+                                 const int32_t* indices, const void* data, int64_t data_stride,
+                                 const void* x, void* y, void* stream, int* lanes,
+                                 int* ctas_per_sm) {
+    using namespace tct;
+    TCT_CHECK_ARG(lanes && ctas_per_sm, "tct_bsr9_autotune: null result pointer");
+    TCT_CHECK_ARG(n_row_blocks > 0, "tct_bsr9_autotune: empty matrix");
+    const int64_t per_row = std::max<int64_t>(1, data_stride / n_row_blocks);
+    static const int kLanes[] = {32, 16, 8, 4};
+    static const int kCtas[] = {4, 8, 16};
+    cudaStream_t st = as_stream(stream);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return launch_status("tct_bsr9_autotune events");
+    int had0 = 0, had1 = 0;
+    const bool had = tune_lookup(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, &had0, &had1);
+    int rc = TCT_OK, bl = 0, bc = 0;
+    float best_ms = 0.f;
+    for (int l : kLanes) {
+        for (int c : kCtas) {
+            tune_store(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, l, c);
+            for (int rep = 0; rep < 4 && rc == TCT_OK; rep++) {
+                if (rep == 1) cudaEventRecord(e0, st);
+                rc = tct_bsr9_matvec(prec, n_row_blocks, indptr, indices, data, nullptr,
+                                     data_stride, x, y, 0, stream);
+            }
+            if (rc != TCT_OK) break;
+            float ms = 0.f;
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = launch_status("tct_bsr9_autotune timing");
+                break;
+            }
+            if (bl == 0 || ms < best_ms) {
+                bl = l;
+                bc = c;
+                best_ms = ms;
+            }
+        }
+        if (rc != TCT_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != TCT_OK || bl == 0) {
+        if (had) tune_store(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, had0, had1);
+        else tune_erase(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row);
+        return rc != TCT_OK ? rc : TCT_ERR_ARG;
+    }
+    tune_store(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, bl, bc);
+    *lanes = bl;
+    *ctas_per_sm = bc;
+    return TCT_OK;
 }
 
 extern "C" int tct_bsr9_matvec_panel(int prec, int64_t n_row_blocks, const int32_t* indptr,

@@ -46,6 +46,19 @@ inline bool aligned(const void* p, size_t a) {
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// ---- tuned launch shapes (tune.cu) -------------------------------------------
+// Operations whose launch shape is looked up: the direct farfield (value:
+// source chunk count), the BSR matvec (values: lanes per block row, CTAs per
+// SM), the multi-RHS farfield panel (reserved).
+enum TuneOp { kTuneFar = TCT_TUNE_FARFIELD, kTuneBsr9 = TCT_TUNE_BSR9,
+              kTuneFarPanel = TCT_TUNE_FAR_PANEL };
+int tune_bucket(int64_t n);
+bool tune_lookup(int op, int kernel, int prec, int nq, int rhs, int64_t n0, int64_t n1, int* v0,
+                 int* v1);
+void tune_store(int op, int kernel, int prec, int nq, int rhs, int64_t n0, int64_t n1, int v0,
+                int v1);
+void tune_erase(int op, int kernel, int prec, int nq, int rhs, int64_t n0, int64_t n1);
+
 // ---- kernel catalogue (ids match tct_kernel_id) -----------------------------
 enum KernelId { kU = 0, kT = 1, kA = 2, kH = 3, kRT = 4, kRA = 5, kRH = 6 };
 

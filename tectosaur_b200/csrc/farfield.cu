@@ -271,10 +271,29 @@ int64_t n_chunks_for(int64_t n_obs, int64_t n_src, int /*ts*/) {
 
 inline int tile_for(int nq) { return nq <= 4 ? 128 : 32; }
 
+// Largest source-chunk count a launch may use (tuned or not).
+constexpr int64_t MAX_CHUNKS = 64;
+
+// Source chunks of a direct-farfield launch: the tuned value of this
+// problem's key when the shape cache has one (tune.cu), else the heuristic;
+// at most one chunk per CHUNK_GRAIN sources, at most MAX_CHUNKS, and no more
+// than the workspace's partial-sum space (after rec_bytes of records) holds.
+int64_t choose_chunks(int kernel, int prec, int nq, int64_t n_obs, int64_t n_src,
+                      int64_t heuristic, size_t rec_bytes, size_t real_bytes, size_t ws_bytes) {
+    int64_t chunks = heuristic;
+    int v0 = 0, v1 = 0;
+    if (tune_lookup(kTuneFar, kernel, prec, nq, 1, n_obs, n_src, &v0, &v1)) chunks = v0;
+    chunks = std::min<int64_t>(chunks, std::max<int64_t>(1, n_src / CHUNK_GRAIN));
+    chunks = std::min<int64_t>(chunks, MAX_CHUNKS);
+    while (chunks > 1 && rec_bytes + align256(real_bytes * 9 * (size_t)n_obs * chunks) > ws_bytes)
+        chunks--;
+    return std::max<int64_t>(1, chunks);
+}
+
 template <typename R, int K, int NQ>
 int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, const R* pts,
             const int32_t* obs_tris, int64_t n_obs, const int32_t* src_tris, int64_t n_src,
-            int accumulate, unsigned char* ws, cudaStream_t st) {
+            int accumulate, unsigned char* ws, size_t ws_bytes, cudaStream_t st) {
     using L = Rec<K, NQ>;
     constexpr int TS = NQ <= 4 ? 128 : 32;
     R* rec = reinterpret_cast<R*>(ws);
@@ -283,7 +302,9 @@ int run_far(const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in, cons
                                                                       n_src, in, nullptr, rec);
     int rc = launch_status("farfield prep");
     if (rc) return rc;
-    const int64_t chunks = n_chunks_for(n_obs, n_src, TS);
+    const int64_t chunks =
+        choose_chunks(K, sizeof(R) == 8 ? TCT_F64 : TCT_F32, NQ, n_obs, n_src,
+                      n_chunks_for(n_obs, n_src, TS), rec_bytes, sizeof(R), ws_bytes);
     const int64_t per_chunk =
         ((n_src + chunks - 1) / chunks + CHUNK_GRAIN - 1) / CHUNK_GRAIN * CHUNK_GRAIN;
     const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
@@ -330,7 +351,7 @@ template <int NQ, bool UNIFORM>
 int run_far_rh2(const Consts<float>& c, const Rule2D<float>& rule, float* out, const float* in,
                 const float* pts, const int32_t* obs_tris, int64_t n_obs,
                 const int32_t* src_tris, int64_t n_src, int accumulate, unsigned char* ws,
-                cudaStream_t st) {
+                size_t ws_bytes, cudaStream_t st) {
     using L = RecRH2<NQ>;
     float* rec = reinterpret_cast<float*>(ws);
     const size_t rec_bytes = align256(sizeof(float) * L::LEN * (size_t)n_src);
@@ -338,7 +359,8 @@ int run_far_rh2(const Consts<float>& c, const Rule2D<float>& rule, float* out, c
         c, rule, pts, src_tris, n_src, in, nullptr, rec);
     int rc = launch_status("farfield prep (RH, packed)");
     if (rc) return rc;
-    const int64_t chunks = n_chunks_rh2(n_obs, n_src);
+    const int64_t chunks = choose_chunks(kRH, TCT_F32, NQ, n_obs, n_src,
+                                         n_chunks_rh2(n_obs, n_src), rec_bytes, 4, ws_bytes);
     const int64_t per_chunk =
         ((n_src + chunks - 1) / chunks + CHUNK_GRAIN - 1) / CHUNK_GRAIN * CHUNK_GRAIN;
     const int64_t real_chunks = (n_src + per_chunk - 1) / per_chunk;
@@ -367,12 +389,12 @@ int run_far_rh2(const Consts<float>& c, const Rule2D<float>& rule, float* out, c
 int run_far_rh2_nq(int nq, bool uniform, const Consts<float>& c, const Rule2D<float>& rule,
                    float* out, const float* in, const float* pts, const int32_t* ot,
                    int64_t n_obs, const int32_t* stris, int64_t n_src, int acc,
-                   unsigned char* ws, cudaStream_t st) {
+                   unsigned char* ws, size_t ws_bytes, cudaStream_t st) {
 #define TCT_RH2(NQV)                                                                          \
     return uniform ? run_far_rh2<NQV, true>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, \
-                                            ws, st)                                           \
+                                            ws, ws_bytes, st)                                 \
                    : run_far_rh2<NQV, false>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, \
-                                             ws, st);
+                                             ws, ws_bytes, st);
     switch (nq) {
         case 3: TCT_RH2(3)
         case 4: TCT_RH2(4)
@@ -393,12 +415,12 @@ inline bool use_rh2(int kernel, int prec, int nq) {
 template <typename R, int K>
 int run_far_nq(int nq, const Consts<R>& c, const Rule2D<R>& rule, R* out, const R* in,
                const R* pts, const int32_t* ot, int64_t n_obs, const int32_t* stris,
-               int64_t n_src, int acc, unsigned char* ws, cudaStream_t st) {
+               int64_t n_src, int acc, unsigned char* ws, size_t wsb, cudaStream_t st) {
     switch (nq) {
-        case 3: return run_far<R, K, 3>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
-        case 4: return run_far<R, K, 4>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
-        case 7: return run_far<R, K, 7>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
-        case 13: return run_far<R, K, 13>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, st);
+        case 3: return run_far<R, K, 3>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, wsb, st);
+        case 4: return run_far<R, K, 4>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, wsb, st);
+        case 7: return run_far<R, K, 7>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, wsb, st);
+        case 13: return run_far<R, K, 13>(c, rule, out, in, pts, ot, n_obs, stris, n_src, acc, ws, wsb, st);
         default:
             set_error("tct_farfield_tris_matvec: %d-point triangle rules are not supported "
                       "(supported: 3, 4, 7, 13 = gauss2d_tri(1..4))", nq);
@@ -409,7 +431,8 @@ int run_far_nq(int nq, const Consts<R>& c, const Rule2D<R>& rule, R* out, const 
 template <typename R>
 int far_dispatch(int kernel, int nq, const double* qp, const double* qw, const double* params,
                  void* out, const void* in, const void* pts, const int32_t* ot, int64_t n_obs,
-                 const int32_t* stris, int64_t n_src, int acc, void* ws, cudaStream_t st) {
+                 const int32_t* stris, int64_t n_src, int acc, void* ws, size_t wsb,
+                 cudaStream_t st) {
     Consts<R> c = make_consts<R>(params);
     Rule2D<R> rule;
     for (int q = 0; q < MAXQ; q++) {
@@ -423,13 +446,13 @@ int far_dispatch(int kernel, int nq, const double* qp, const double* qw, const d
             bool uniform = true;
             for (int q = 1; q < nq; q++) uniform = uniform && (qw[q] == qw[0]);
             return run_far_rh2_nq(nq, uniform, c, rule, (float*)out, (const float*)in,
-                                  (const float*)pts, ot, n_obs, stris, n_src, acc, w, st);
+                                  (const float*)pts, ot, n_obs, stris, n_src, acc, w, wsb, st);
         }
     }
 #define TCT_FAR_CASE(KID)                                                                 \
     case KID:                                                                               \
         return run_far_nq<R, KID>(nq, c, rule, (R*)out, (const R*)in, (const R*)pts, ot,   \
-                                  n_obs, stris, n_src, acc, w, st);
+                                  n_obs, stris, n_src, acc, w, wsb, st);
     switch (kernel) {
         TCT_FAR_CASE(kU)
         TCT_FAR_CASE(kT)
@@ -617,11 +640,15 @@ int dense_dispatch(int kernel, const double* params, void* out, int n_q, const v
 
 }  // namespace
 
-size_t farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_src, int n_q) {
+// Workspace of a direct-farfield launch: the source records plus the
+// partial sums of `max_chunks` source chunks (<= 0: the heuristic count).
+size_t farfield_workspace_bytes_chunks(int kernel, int prec, int64_t n_obs, int64_t n_src,
+                                       int n_q, int64_t max_chunks) {
     if (n_src < 0 || n_obs < 0) return 0;
     if (use_rh2(kernel, prec, n_q)) {
         const size_t rec_bytes = align256(4 * (size_t)rec_len_rh2(n_q) * (size_t)n_src);
-        const int64_t chunks = n_chunks_rh2(n_obs, n_src);
+        const int64_t chunks = max_chunks > 0 ? std::min(max_chunks, MAX_CHUNKS)
+                                              : n_chunks_rh2(n_obs, n_src);
         const size_t part = chunks > 1 ? align256(4 * 9 * (size_t)n_obs * chunks) : 0;
         return rec_bytes + part;
     }
@@ -629,9 +656,14 @@ size_t farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_s
     if (len < 0 || n_src < 0 || n_obs < 0) return 0;
     const size_t rs = prec == TCT_F64 ? 8 : 4;
     const size_t rec_bytes = align256(rs * len * (size_t)n_src);
-    const int64_t chunks = n_chunks_for(n_obs, n_src, tile_for(n_q));
+    const int64_t chunks = max_chunks > 0 ? std::min(max_chunks, MAX_CHUNKS)
+                                          : n_chunks_for(n_obs, n_src, tile_for(n_q));
     const size_t part = chunks > 1 ? align256(rs * 9 * (size_t)n_obs * chunks) : 0;
     return rec_bytes + part;
+}
+
+size_t farfield_workspace_bytes(int kernel, int prec, int64_t n_obs, int64_t n_src, int n_q) {
+    return farfield_workspace_bytes_chunks(kernel, prec, n_obs, n_src, n_q, 0);
 }
 
 }  // namespace tct
@@ -675,10 +707,12 @@ extern "C" int tct_farfield_tris_matvec(int kernel, int prec, void* out, const v
     }
     if (prec == TCT_F32)
         return far_dispatch<float>(kernel, n_q, quad_pts, quad_wts, params, out, in, pts, obs_tris,
-                                   n_obs, src_tris, n_src, accumulate, workspace, as_stream(stream));
+                                   n_obs, src_tris, n_src, accumulate, workspace, workspace_bytes,
+                                   as_stream(stream));
     if (prec == TCT_F64)
         return far_dispatch<double>(kernel, n_q, quad_pts, quad_wts, params, out, in, pts, obs_tris,
-                                    n_obs, src_tris, n_src, accumulate, workspace, as_stream(stream));
+                                    n_obs, src_tris, n_src, accumulate, workspace, workspace_bytes,
+                                    as_stream(stream));
     set_error("tct_farfield_tris_matvec: unsupported precision %d", prec);
     return TCT_ERR_PREC;
 }
@@ -801,4 +835,68 @@ extern "C" int tct_farfield_tris_dense(int kernel, int prec, void* out, int n_qu
                                       obs_tris, n_obs, src_tris, n_src, as_stream(stream));
     set_error("tct_farfield_tris_dense: unsupported precision %d", prec);
     return TCT_ERR_PREC;
+}
+
+extern "C" size_t tct_farfield_workspace_bytes_chunks(int kernel, int prec, int64_t n_obs,
+                                                      int64_t n_src, int n_q, int max_chunks) {
+    return tct::farfield_workspace_bytes_chunks(kernel, prec, n_obs, n_src, n_q, max_chunks);
+}
+
+// Candidate source-chunk counts: each is timed (one untimed launch, then the
+// mean of three under CUDA events) with the chunk count forced through the
+// shape cache; the fastest stays in the cache.
+extern "C" int tct_farfield_autotune(int kernel, int prec, void* out, const void* in,
+                                     const void* pts, const int32_t* obs_tris, int64_t n_obs,
+                                     const int32_t* src_tris, int64_t n_src, int n_q,
+                                     const double* quad_pts, const double* quad_wts,
+                                     const double* params, void* workspace,
+                                     size_t workspace_bytes, void* stream, int* chunks) {
+    using namespace tct;
+    TCT_CHECK_ARG(chunks, "tct_farfield_autotune: null result pointer");
+    TCT_CHECK_ARG(n_obs > 0 && n_src > 0, "tct_farfield_autotune: empty problem");
+    static const int kCand[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 48, 64};
+    cudaStream_t st = as_stream(stream);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return launch_status("tct_farfield_autotune events");
+    int rc = TCT_OK, best = 0;
+    float best_ms = 0.f;
+    int had0 = 0, had1 = 0;
+    const bool had = tune_lookup(kTuneFar, kernel, prec, n_q, 1, n_obs, n_src, &had0, &had1);
+    for (int c : kCand) {
+        if (c > 1 && c > n_src / CHUNK_GRAIN) break;
+        if (c > 1 && farfield_workspace_bytes_chunks(kernel, prec, n_obs, n_src, n_q, c) >
+                         workspace_bytes)
+            break;  // the workspace holds no more chunk partials
+        tune_store(kTuneFar, kernel, prec, n_q, 1, n_obs, n_src, c, 1);
+        float ms = 0.f;
+        for (int rep = 0; rep < 4 && rc == TCT_OK; rep++) {
+            if (rep == 1) cudaEventRecord(e0, st);
+            rc = tct_farfield_tris_matvec(kernel, prec, out, in, pts, obs_tris, n_obs, src_tris,
+                                          n_src, n_q, quad_pts, quad_wts, params, 0, workspace,
+                                          workspace_bytes, stream);
+        }
+        if (rc != TCT_OK) break;
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = launch_status("tct_farfield_autotune timing");
+            break;
+        }
+        if (best == 0 || ms < best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != TCT_OK || best == 0) {
+        // leave the cache as it was
+        if (had) tune_store(kTuneFar, kernel, prec, n_q, 1, n_obs, n_src, had0, had1);
+        else tune_erase(kTuneFar, kernel, prec, n_q, 1, n_obs, n_src);
+        return rc != TCT_OK ? rc : TCT_ERR_ARG;
+    }
+    tune_store(kTuneFar, kernel, prec, n_q, 1, n_obs, n_src, best, 1);
+    *chunks = best;
+    return TCT_OK;
 }

@@ -34,6 +34,13 @@ struct BatchArgs {
     int64_t n_warp_items;
     int64_t n_thread_items;
     int* counters;            // 2 ints, zero at launch
+    // destination: slot == nullptr -> block of pair p at out + 81 p; else
+    // element e of pair p at out[e * slot_stride + slot[p]] (the nearfield
+    // BSR's structure-of-arrays blocks)
+    const int32_t* slot;
+    int64_t slot_stride;
+    int add;                  // whole-pair stores add to the destination
+    double sign;              // factor on every stored value
 };
 
 template <typename R, int K>
@@ -65,9 +72,12 @@ __device__ __forceinline__ void load_pair(const BatchArgs& a, const R* pts, cons
 // Write (or atomically add) the de-rotated, Jacobian-scaled block; when
 // `lane_mask` >= 0 only the outputs idx with idx % 32 == lane_mask are written.
 template <typename R>
-__device__ __forceinline__ void store_block(R* out, int32_t pair, const R res[81], R scale,
-                                            const int od[3], const int sd[3], bool atomic,
-                                            int lane_mask) {
+__device__ __forceinline__ void store_block(const BatchArgs& a, R* out, int32_t pair,
+                                            const R res[81], R scale, const int od[3],
+                                            const int sd[3], bool atomic, int lane_mask) {
+    const int64_t base = a.slot ? (int64_t)__ldg(a.slot + pair) : (int64_t)pair * 81;
+    const int64_t step = a.slot ? a.slot_stride : 1;
+    scale *= (R)a.sign;
 #pragma unroll
     for (int b1 = 0; b1 < 3; b1++)
 #pragma unroll
@@ -84,9 +94,9 @@ __device__ __forceinline__ void store_block(R* out, int32_t pair, const R res[81
 #pragma unroll
                         for (int y = 0; y < 3; y++)
                             if (od[b1] == x && sd[b2] == y) val = res[x * 27 + d1 * 9 + y * 3 + d2];
-                    R* dst = out + (int64_t)pair * 81 + out_idx;
+                    R* dst = out + base + (int64_t)out_idx * step;
                     if (atomic) atomicAdd(dst, scale * val);
-                    else *dst = scale * val;
+                    else *dst = a.add ? *dst + scale * val : scale * val;
                 }
 }
 
@@ -124,7 +134,7 @@ pairs_batched_kernel(const Consts<R>* __restrict__ cs, BatchArgs a, R* __restric
         acc.warp_reduce();
         R res[81];
         acc.finish(c, o, s, res);
-        store_block(out, pair, res, o.J * s.J, od, sd, split, lane);
+        store_block(a, out, pair, res, o.J * s.J, od, sd, split, lane);
     }
     // ---- thread items: one whole pair per lane ----
     for (;;) {
@@ -152,7 +162,7 @@ pairs_batched_kernel(const Consts<R>* __restrict__ cs, BatchArgs a, R* __restric
             }
             R res[81];
             acc.finish(c, o, s, res);
-            store_block(out, pair, res, o.J * s.J, od, sd, false, -1);
+            store_block(a, out, pair, res, o.J * s.J, od, sd, false, -1);
         }
         __syncwarp();
     }
@@ -174,7 +184,7 @@ int launch_batched(int kernel, const double* params, int n_psets, void* out, int
             return TCT_ERR_CUDA;
         }
     }
-    if (!accumulate) {
+    if (!accumulate && !a.slot) {
         cudaError_t e = cudaMemsetAsync(out, 0, sizeof(R) * 81 * (size_t)n_pairs, st);
         if (e != cudaSuccess) {
             set_error("tct_pairs_integrate_batched: memset: %s", cudaGetErrorString(e));
@@ -235,7 +245,7 @@ extern "C" int tct_pairs_integrate_batched(int kernel, int prec, void* out, int6
                   "tct_pairs_integrate_batched: workspace of >= 2048 bytes, 256-byte aligned, "
                   "required");
     BatchArgs a{pairs, rule_off, rule_flags, items, n_warp_items, n_thread_items,
-                reinterpret_cast<int*>(workspace)};
+                reinterpret_cast<int*>(workspace), nullptr, 0, 0, 1.0};
     if (prec == TCT_F32)
         return launch_batched<float>(kernel, params, n_param_sets, out, n_pairs, pts, tris, a,
                                      rule_pts, rule_wts, accumulate, as_stream(stream));
@@ -243,5 +253,46 @@ extern "C" int tct_pairs_integrate_batched(int kernel, int prec, void* out, int6
         return launch_batched<double>(kernel, params, n_param_sets, out, n_pairs, pts, tris, a,
                                       rule_pts, rule_wts, accumulate, as_stream(stream));
     set_error("tct_pairs_integrate_batched: unsupported precision %d", prec);
+    return TCT_ERR_PREC;
+}
+
+// Slot form (an addition, for the operator build): the same work queues,
+// blocks written into a structure-of-arrays block array through a slot map:
+// element e of pair p at out[e * slot_stride + slot[p]], times `sign`, added
+// to what is there when `add`.  Pairs cut into several warp items (split
+// flag) are added atomically, so a plan with split items needs its
+// destination slots zeroed (or `add`); a plan without split items is
+// deterministic.
+extern "C" int tct_pairs_integrate_batched_slots(
+    int kernel, int prec, void* out, const int32_t* slot, int64_t slot_stride, double sign,
+    int add, int64_t n_pairs, const void* pts, const int32_t* tris, const int32_t* pairs,
+    const int64_t* rule_off, const int32_t* rule_flags, const void* rule_pts,
+    const void* rule_wts, const int32_t* items, int64_t n_warp_items, int64_t n_thread_items,
+    const double* params, int n_param_sets, void* workspace, size_t workspace_bytes,
+    void* stream) {
+    using namespace tct;
+    TCT_CHECK_ARG(n_pairs >= 0 && n_warp_items >= 0 && n_thread_items >= 0 && slot_stride >= 0,
+                  "tct_pairs_integrate_batched_slots: negative size");
+    if (n_pairs == 0) return TCT_OK;
+    TCT_CHECK_ARG(n_pairs < (int64_t(1) << 31) && slot_stride < (int64_t(1) << 31),
+                  "tct_pairs_integrate_batched_slots: too many pairs");
+    TCT_CHECK_ARG(out && slot && pts && tris && pairs && rule_off && rule_flags && rule_pts &&
+                      rule_wts && params && (items || n_warp_items + n_thread_items == 0),
+                  "tct_pairs_integrate_batched_slots: null pointer");
+    TCT_CHECK_ARG(slot_stride > 0, "tct_pairs_integrate_batched_slots: bad slot stride");
+    TCT_CHECK_ARG(n_param_sets >= 1 && n_param_sets <= MAX_PSETS,
+                  "tct_pairs_integrate_batched_slots: 1 to %d parameter sets", MAX_PSETS);
+    TCT_CHECK_ARG(workspace && workspace_bytes >= 2048 && aligned(workspace, 256),
+                  "tct_pairs_integrate_batched_slots: workspace of >= 2048 bytes, 256-byte "
+                  "aligned, required");
+    BatchArgs a{pairs, rule_off, rule_flags, items, n_warp_items, n_thread_items,
+                reinterpret_cast<int*>(workspace), slot, slot_stride, add ? 1 : 0, sign};
+    if (prec == TCT_F32)
+        return launch_batched<float>(kernel, params, n_param_sets, out, n_pairs, pts, tris, a,
+                                     rule_pts, rule_wts, 1, as_stream(stream));
+    if (prec == TCT_F64)
+        return launch_batched<double>(kernel, params, n_param_sets, out, n_pairs, pts, tris, a,
+                                      rule_pts, rule_wts, 1, as_stream(stream));
+    set_error("tct_pairs_integrate_batched_slots: unsupported precision %d", prec);
     return TCT_ERR_PREC;
 }

@@ -14,6 +14,11 @@ Construction follows the reference step for step:
 B200 layout: all four classes share one device BSR matrix whose blocks the
 pair kernels write in place (accurate rule, then the correction subtracted
 into the same slots), so the nearfield apply is a single tct_bsr9_matvec.
+The build integrates every class in one persistent launch of the batched
+pair kernel (work queues of uneven rules: the reference launches one
+single_pairs kernel per class and rule, nearfield/pairs_integrator.py:43-68)
+and all the corrections in a second; ``batched=False`` keeps the per-class
+launches.
 The uncorrected blocks (``nearfield_no_correction_dot``) are kept as the
 correction array C beside the corrected array D (no-correction = D + C);
 ``keep_uncorrected=False`` drops C to halve the footprint.
@@ -130,7 +135,7 @@ class RegularizedNearfieldIntegralOp:
                  nq_coincident, nq_edge_adj, nq_vert_adjacent,
                  nq_far, nq_near, near_threshold,
                  K_near_name, K_far_name, params, float_type, keep_uncorrected=True,
-                 row_range=None):
+                 row_range=None, batched=True):
         device.require_cuda()
         pts = np.asarray(pts, dtype=np.float64)
         tris = np.asarray(tris, dtype=np.int64)
@@ -168,6 +173,12 @@ class RegularizedNearfieldIntegralOp:
             if keep_uncorrected else None
 
         stride = max(self.bsr.nnzb, 1)
+        self.n_pairs = {c: self.classes[c][1].shape[0] for c in CLASSES}
+        if batched:
+            self._integrate_batched(pairs_int, corr_int, nq_coincident, nq_edge_adj,
+                                    nq_vert_adjacent, nq_far, nq_near, stride)
+            self._mats = None
+            return
         rules = {
             "co": (pairs_int.coincident_rule(nq_coincident), False, True),
             "ea": (pairs_int.edge_adj_rule(nq_edge_adj), True, True),
@@ -175,11 +186,9 @@ class RegularizedNearfieldIntegralOp:
             "near": (pairs_int.near_rule(), False, False),
         }
         far_rule = corr_int.far_rule()
-        self.n_pairs = {}
         for c in CLASSES:
             recs, dofs = self.classes[c]
             n = dofs.shape[0]
-            self.n_pairs[c] = n
             if n == 0:
                 continue
             rule, adj, check0 = rules[c]
@@ -196,6 +205,48 @@ class RegularizedNearfieldIntegralOp:
                 corr_int.integrate_into(self.correction, far_rule, base_dev, n, False,
                                         corr_check0, slot=slot_dev, slot_stride=stride)
         self._mats = None
+
+    def _integrate_batched(self, pairs_int, corr_int, nq_co, nq_ea, nq_va, nq_far, nq_near,
+                           stride):
+        """All four classes in one persistent launch of the batched pair
+        kernel (tct_pairs_integrate_batched_slots: the coincident, edge- and
+        vertex-adjacent rules as warp items, the near rule as thread items),
+        written into the BSR slots; then the far-rule corrections of every
+        pair in one launch, subtracted in place (and written to the
+        uncorrected-form array C when kept).  No pair is split, so the
+        blocks do not depend on the launch's scheduling."""
+        from ..util.quadrature import gauss4d_tri
+        from . import triangle_rules
+        host_rules = {
+            "co": (triangle_rules.coincident_quad(nq_co), False, True),
+            "ea": (triangle_rules.edge_adj_quad(nq_ea), True, True),
+            "va": (triangle_rules.vertex_adj_quad(nq_va, nq_va, nq_va), True, True),
+            "near": (gauss4d_tri(nq_near, nq_near), False, False),
+        }
+        far_q = gauss4d_tri(nq_far, nq_far)
+        groups, corr_groups, slots = [], [], []
+        for c in CLASSES:
+            recs, dofs = self.classes[c]
+            n = dofs.shape[0]
+            if n == 0:
+                continue
+            (qp, qw), adj, check0 = host_rules[c]
+            base = np.zeros((n, 5), dtype=np.int64)
+            base[:, :2] = recs[:, :2]
+            r5 = recs[:, :5] if adj else base
+            groups.append((r5, (qp, qw, adj, check0)))
+            corr_groups.append((base, (far_q[0], far_q[1], False, c == "co")))
+            slots.append(self.class_slots[c])
+        if not groups:
+            return
+        slot_dev = device.to_dev(np.concatenate(slots).astype(np.int32))
+        plan = pairs_int.class_plan(groups)
+        pairs_int.batched_run_slots(plan, self.bsr.data, slot_dev, stride, 1.0, add=False)
+        del plan
+        cplan = corr_int.class_plan(corr_groups)
+        corr_int.batched_run_slots(cplan, self.bsr.data, slot_dev, stride, -1.0, add=True)
+        if self.correction is not None:
+            corr_int.batched_run_slots(cplan, self.correction, slot_dev, stride, 1.0, add=False)
 
     # -- apply ------------------------------------------------------------
     def dot_device(self, x, y, accumulate=False, stream=None):

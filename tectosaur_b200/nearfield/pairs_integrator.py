@@ -122,10 +122,13 @@ class PairsIntegrator:
         wi_p0 = first
         wi_p1 = np.minimum(first + chunk, psize[wi_pair])
         wi_split = np.repeat((nchunk > 1).astype(np.int64), nchunk)
-        order = np.argsort(-(wi_p1 - wi_p0), kind="stable")
+        # largest items first (load balance); among equal sizes, grouped by
+        # rule and rule segment, so that the warps running at the same time
+        # read the same rule points (from L2, not HBM)
+        order = np.lexsort((wi_p0, rule_ids[wi_pair], -(wi_p1 - wi_p0)))
         witems = np.stack([wi_pair, wi_p0, wi_p1, wi_split], axis=1)[order]
         tp = np.nonzero(~big)[0]
-        tp = tp[np.argsort(-psize[tp], kind="stable")]
+        tp = tp[np.lexsort((rule_ids[tp], -psize[tp]))]
         titems = np.stack([tp, np.zeros_like(tp), psize[tp], np.zeros_like(tp)], axis=1)
         items = np.ascontiguousarray(np.concatenate([witems, titems]).astype(np.int32))
         ft = self.float_type
@@ -137,6 +140,65 @@ class PairsIntegrator:
                          device.to_dev(wts_all, ft),
                          device.to_dev(items if items.size else np.zeros((1, 4), np.int32))])
         return plan
+
+    def class_plan(self, classes, small=768):
+        """Work plan for groups of pairs that share a rule (the nearfield
+        operator's classes), no pair split: classes = [(records (n, 5), rule
+        (pts, wts, adjacent, check0))].  Pairs of rules above `small` points
+        are warp items (the 32 lanes stride over the rule), the others thread
+        items; both queues run the larger rules first and keep each class
+        contiguous, so no sort of the (possibly 10^8) pairs is needed.
+        Deterministic: every block is summed in a fixed order by one warp or
+        one thread.  Pair p of the plan is the p-th record in class order."""
+        groups = [(np.asarray(r).reshape(-1, 5), q) for r, q in classes]
+        rules = [q for _, q in groups]
+        sizes = np.array([q[0].shape[0] for q in rules], dtype=np.int64)
+        rule_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        rule_flags = np.array([(1 if q[2] else 0) | (2 if q[3] else 0) for q in rules], np.int32)
+        pts_all = np.concatenate([np.asarray(q[0], np.float64).reshape(-1, 4) for q in rules])
+        wts_all = np.concatenate([np.asarray(q[1], np.float64).reshape(-1) for q in rules])
+        n = int(sum(r.shape[0] for r, _ in groups))
+        rec7 = np.empty((n, 7), dtype=np.int32)
+        starts = np.concatenate([[0], np.cumsum([r.shape[0] for r, _ in groups])]).astype(np.int64)
+        for g, (r, _) in enumerate(groups):
+            rec7[starts[g]:starts[g + 1], :5] = r
+            rec7[starts[g]:starts[g + 1], 5] = g
+        rec7[:, 6] = 0
+        witems, titems = [], []
+        for g in np.argsort(-sizes, kind="stable"):
+            k = np.arange(starts[g], starts[g + 1], dtype=np.int64)
+            it = np.stack([k, np.zeros_like(k), np.full_like(k, sizes[g]), np.zeros_like(k)],
+                          axis=1)
+            (witems if sizes[g] > small else titems).append(it)
+        witems = np.concatenate(witems) if witems else np.zeros((0, 4), np.int64)
+        titems = np.concatenate(titems) if titems else np.zeros((0, 4), np.int64)
+        items = np.ascontiguousarray(np.concatenate([witems, titems]).astype(np.int32))
+        ft = self.float_type
+        return dict(n=n, n_warp=witems.shape[0], n_thread=titems.shape[0],
+                    param_sets=self.params.reshape(1, 2), n_points=int(sizes[rec7[:, 5]].sum()),
+                    ws=device.workspace(2048),
+                    dev=[device.to_dev(rec7), device.to_dev(rule_off),
+                         device.to_dev(rule_flags), device.to_dev(pts_all, ft),
+                         device.to_dev(wts_all, ft),
+                         device.to_dev(items if items.size else np.zeros((1, 4), np.int32))])
+
+    def batched_run_slots(self, plan, out, slot_dev, slot_stride, sign=1.0, add=False,
+                          stream=None):
+        """Launch a plan writing pair p's block into the structure-of-arrays
+        array `out` at slot slot_dev[p] (element e at e * slot_stride + slot),
+        times sign, added to the destination when `add`."""
+        if plan["n"] == 0:
+            return out
+        d = plan["dev"]
+        _lib.check(_lib.lib.tct_pairs_integrate_batched_slots(
+            self.kid, self.prec, _lib.tptr(out), _lib.tptr(slot_dev), int(slot_stride),
+            float(sign), int(bool(add)), plan["n"], _lib.tptr(self.gpu_pts),
+            _lib.tptr(self.gpu_tris), _lib.tptr(d[0]), _lib.tptr(d[1]), _lib.tptr(d[2]),
+            _lib.tptr(d[3]), _lib.tptr(d[4]), _lib.tptr(d[5]), plan["n_warp"],
+            plan["n_thread"], _lib.dptr(plan["param_sets"]), plan["param_sets"].shape[0],
+            _lib.tptr(plan["ws"]), 2048, _lib.stream_ptr(stream)),
+            "tct_pairs_integrate_batched_slots")
+        return out
 
     def batched_run(self, plan, out=None, stream=None):
         """Launch a batched plan: out (n * 81 device array, allocated when

@@ -45,6 +45,12 @@ class TriToTriDirectFarfieldOp:
         self.workspace = device.workspace(self.ws_bytes)
         self._panel_ws = {}
 
+    def autotune(self, x=None):
+        """Tune the source chunking of this operator's launch (cached in the
+        library, tectosaur_b200.autotune); returns the chosen chunk count."""
+        from .. import autotune
+        return autotune.tune_farfield(self, x)
+
     def dot_device(self, x, y, accumulate=False, stream=None):
         """y (+)= Far x on device tensors of float_type."""
         _lib.check(_lib.lib.tct_farfield_tris_matvec(

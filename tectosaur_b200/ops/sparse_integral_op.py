@@ -16,7 +16,8 @@ class RegularizedSparseIntegralOp:
     def __init__(self, nq_coincident, nq_edge_adj, nq_vert_adjacent,
                  nq_far, nq_near, near_threshold,
                  K_near_name, K_far_name, params, pts, tris, float_type, farfield_op_type,
-                 obs_subset=None, src_subset=None, keep_uncorrected=True, row_range=None):
+                 obs_subset=None, src_subset=None, keep_uncorrected=True, row_range=None,
+                 batched=True):
         """row_range=(r0, r1) (an addition, for row shards): the operator is
         block rows r0..r1-1 of the one over obs_subset x src_subset -- the
         same near pairs and blocks (the search runs over the whole
@@ -35,7 +36,7 @@ class RegularizedSparseIntegralOp:
             pts, tris, obs_subset, src_subset,
             nq_coincident, nq_edge_adj, nq_vert_adjacent, nq_far, nq_near,
             near_threshold, K_near_name, K_far_name, params, float_type,
-            keep_uncorrected=keep_uncorrected, row_range=row_range)
+            keep_uncorrected=keep_uncorrected, row_range=row_range, batched=batched)
         far_obs = obs_subset if row_range is None else obs_subset[row_range[0]:row_range[1]]
         self.farfield = farfield_op_type(
             nq_far, K_far_name, params, pts, tris, float_type, far_obs, src_subset)
@@ -49,6 +50,13 @@ class RegularizedSparseIntegralOp:
                           src_subset)
         self.shape = self.nearfield.shape
         self._graph = None
+
+    def autotune(self):
+        """Tune this operator's launch shapes (direct-farfield source
+        chunking, nearfield BSR shape) on its own data and keep them in the
+        library's shape cache (tectosaur_b200.autotune); returns them."""
+        from .. import autotune
+        return autotune.tune_operator(self)
 
     def astype(self, float_type, keep_uncorrected=True):
         """The same operator in another precision (an addition, for mixed-
