@@ -1890,6 +1890,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch shapes (skip the autotuner in setup)")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the C5 served-vs-plain stream on the default line")
     ap.add_argument("--grid", type=int, default=None,
@@ -1949,6 +1951,10 @@ def main():
     op = build_op(pts, tris)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t_build
+    # launch shapes picked by the autotuner on this operator (setup, untimed)
+    t_tune = time.perf_counter()
+    shapes = op.autotune() if not args.no_autotune else {}
+    t_tune = time.perf_counter() - t_tune
     n = tris.shape[0]
     nnzb = op.nearfield.bsr.nnzb
     x = torch.from_numpy(np.random.default_rng(3 + rank).standard_normal(9 * n)
@@ -2042,6 +2048,7 @@ def main():
             "gpu_launches": args.steps * (2 + (1 if chunks > 1 else 0) + (1 if nnzb else 0)),
             "clocks": clocks,
             "setup_s": t_build,
+            "autotune": dict(shapes, seconds=t_tune),
         }
         classes = c2_classes(pts, tris)
         line["parity"] = c2_parity(pts, tris, y.cpu().numpy(), x.cpu().numpy(), classes)
