@@ -1661,7 +1661,7 @@ def c5_meshes(n_meshes=6, seed=6, lo=C5_LO, hi=C5_HI):
     return out
 
 
-def c5_stream(torch, quiet=True, seed=7):
+def c5_stream(torch, quiet=True, seed=7, inner="direct"):
     """Serve the C5 stream (module-level C5_* settings) and time it against
     the plain paths.  Returns a dict of results (no JSON printing).
 
@@ -1672,7 +1672,10 @@ def c5_stream(torch, quiet=True, seed=7):
     state perturbation) on each of the C5_QD_MESHES smallest meshes, in a
     seeded order.  Served: serve.SolveServer (continuous batching, 16 slots
     per mesh, FP32 operator in FP64 refinement; FMM farfield from C5_FMM_MIN
-    triangles).  Plain: one request at a time in arrival order -- the FP64
+    triangles; inner="direct": the FP32 correction operator of an FMM mesh
+    uses the direct farfield, whose panel runs on the tensor cores, while the
+    FP64 residual keeps the FMM farfield -- "fmm": both FMM).  Plain: one
+    request at a time in arrival order -- the FP64
     GMRES solve (simple_solver.iterative_solve) and the single-state
     Integrator.  Saturation (all requests at t = 0) gives the throughput;
     Poisson arrivals at 0.7 of the served saturation rate give the served
@@ -1701,7 +1704,9 @@ def c5_stream(torch, quiet=True, seed=7):
         op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
                                                np.float64, far, keep_uncorrected=False)
         srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64,
-                     farfield_op_type=far)
+                     farfield_op_type=far,
+                     inner_farfield_op_type=(TriToTriDirectFarfieldOp
+                                             if inner == "direct" and n >= C5_FMM_MIN else None))
         specs[key] = (op64, cm, n)
         if n >= C5_FMM_MIN:
             # the FMM farfield's error against the direct FP64 farfield on
@@ -1809,7 +1814,10 @@ def c5_stream(torch, quiet=True, seed=7):
         "meshes": {key: {"n_tris": int(tris.shape[0]), "kind": kind,
                          "farfield": ("fmm p=%d mac %.1f, %d per leaf"
                                       % (C5_FMM["order"], C5_FMM["mac"], C5_FMM["pts_per_cell"])
-                                      if tris.shape[0] >= C5_FMM_MIN else "direct")}
+                                      if tris.shape[0] >= C5_FMM_MIN else "direct"),
+                         "served_inner_farfield": ("direct (tensor-core panel)"
+                                                   if tris.shape[0] < C5_FMM_MIN or
+                                                   inner == "direct" else "fmm")}
                    for key, pts, tris, kind in meshes},
         "qd_meshes": qd_keys, "qd_steps": C5_QD_STEPS, "solve_tol": C5_TOL,
         "max_rel_diff_solve_vs_plain_fp64": max(err_solve) if err_solve else None,
@@ -1847,7 +1855,7 @@ def run_serve_workload(args, rank, world, torch, dist):
     """The C5 served stream as its own line (see c5_stream)."""
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    res = c5_stream(torch, quiet=(rank != 0))
+    res = c5_stream(torch, quiet=(rank != 0), inner=args.c5_inner)
     clocks = sampler.stop()
     if rank != 0:
         return
@@ -1892,6 +1900,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch shapes (skip the autotuner in setup)")
+    ap.add_argument("--c5-inner", default="direct", choices=["direct", "fmm"],
+                    help="farfield of the served FP32 correction operator on FMM meshes")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the C5 served-vs-plain stream on the default line")
     ap.add_argument("--grid", type=int, default=None,
@@ -2057,7 +2067,7 @@ def main():
             del op, far, near
             torch.cuda.empty_cache()
             try:
-                line["served"] = c5_stream(torch)
+                line["served"] = c5_stream(torch, inner=args.c5_inner)
             except Exception as e:  # keep the matvec line if the stream fails
                 line["served"] = {"error": "%s: %s" % (type(e).__name__, e)}
         if not args.no_cpu_baseline:

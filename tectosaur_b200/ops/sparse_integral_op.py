@@ -58,16 +58,22 @@ class RegularizedSparseIntegralOp:
         from .. import autotune
         return autotune.tune_operator(self)
 
-    def astype(self, float_type, keep_uncorrected=True):
+    def astype(self, float_type, keep_uncorrected=True, farfield_op_type=None):
         """The same operator in another precision (an addition, for mixed-
         precision solves): the nearfield blocks are cast from this operator's
         (structure shared, no re-integration), the farfield is set up anew in
-        float_type."""
+        float_type -- with this operator's farfield type, or with
+        `farfield_op_type` (e.g. the direct farfield, whose multi-RHS form runs
+        on the tensor cores, as the inner operator of a solve whose FP64
+        residual uses an FMM farfield)."""
         import copy
         twin = copy.copy(self)
         twin.float_type = np.dtype(float_type)
         twin.nearfield = self.nearfield.astype(float_type, keep_uncorrected)
         factory, nq_far, K_far, params, pts, tris, obs_subset, src_subset = self._far_args
+        if farfield_op_type is not None:
+            factory = farfield_op_type
+            twin._far_args = (factory,) + self._far_args[1:]
         twin.farfield = factory(nq_far, K_far, params, pts, tris, float_type, obs_subset,
                                 src_subset)
         twin._graph = None

@@ -509,8 +509,12 @@ class MeshSpec:
     RegularizedSparseIntegralOp arguments."""
 
     def __init__(self, key, pts, tris, cm=None, nq=(6, 6, 6, 2, 5, 2.5), kernel="elasticRH3",
-                 params=(1.0, 0.25), farfield_op_type=None, op64=None):
+                 params=(1.0, 0.25), farfield_op_type=None, op64=None,
+                 inner_farfield_op_type=None):
         self.key = key
+        # farfield of the FP32 correction operator when it differs from the
+        # FP64 residual operator's (None: the same type)
+        self.inner_farfield_op_type = inner_farfield_op_type
         self.op64 = op64  # an FP64 operator built by the caller (kept while registered)
         self.pts = np.asarray(pts, np.float64)
         self.tris = np.asarray(tris, np.int64)
@@ -635,7 +639,8 @@ class SolveServer:
             op64 = RegularizedSparseIntegralOp(*spec.nq, spec.kernel, spec.kernel, spec.params,
                                                spec.pts, spec.tris, np.float64,
                                                spec.farfield_op_type, keep_uncorrected=False)
-        op32 = op64.astype(np.float32, keep_uncorrected=False)
+        op32 = op64.astype(np.float32, keep_uncorrected=False,
+                           farfield_op_type=getattr(spec, "inner_farfield_op_type", None))
         cm = spec.cm
         S = self.slots
         if cm is None:
