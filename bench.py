@@ -1349,6 +1349,8 @@ def run_c4solve_workload(args, rank, world, torch, dist):
     n = tris.shape[0]
     n_surf = (grid - 1) ** 2 * 2
     cfg = dict(FMM_CFG)
+    if args.fmm_order:
+        cfg["order"] = args.fmm_order
     t0 = time.perf_counter()
     op64 = tct.RegularizedSparseIntegralOp(*[NQ[k] for k in ("nq_co", "nq_ea", "nq_va",
                                                                "nq_far", "nq_near", "thr")],
@@ -1392,6 +1394,25 @@ def run_c4solve_workload(args, rank, world, torch, dist):
     t_plain = time.perf_counter() - t1
     plain_steps = iterative_solve.last["n_iter"]
     diff = float(np.linalg.norm(u - u64) / np.linalg.norm(u64))
+    # error of the FMM operator against the direct FP64 farfield (the
+    # reference's CPU-runnable algorithm, parity-pinned to the oracle) on
+    # 1,024 seeded observation rows: on a random vector, and on the solution
+    # itself (the extra residual the solution has under the direct operator)
+    from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
+    rows = np.sort(np.random.default_rng(41).choice(n, 1024, replace=False))
+    direct = TriToTriDirectFarfieldOp(NQ["nq_far"], K_NAME, PARAMS, pts, tris, np.float64, rows,
+                                      np.arange(n))
+    xr = np.random.default_rng(42).standard_normal(9 * n)
+
+    def rows_of(v):
+        return np.asarray(v).reshape(-1, 9)[rows].reshape(-1)
+    dref = direct.dot(xr)
+    fmm_err = float(np.linalg.norm(rows_of(op64.farfield.dot(xr)) - dref) / np.linalg.norm(dref))
+    fmm32_err = float(np.linalg.norm(rows_of(op32.farfield.dot(xr.astype(np.float32))) - dref) /
+                      np.linalg.norm(dref))
+    du = direct.dot(u)
+    sol_err = float(np.linalg.norm(rows_of(op64.farfield.dot(u)) - du) /
+                    np.linalg.norm(rows_of(op64.dot(u))))
     # matvec timings (device)
     x32 = torch.randn(9 * n, device="cuda")
     y32 = torch.empty_like(x32)
@@ -1415,8 +1436,9 @@ def run_c4solve_workload(args, rank, world, torch, dist):
                                 "surface DOFs unknown (continuity, zero on the outer edges), "
                                 "unit thrust slip prescribed on the fault; elasticRH3 "
                                 "RegularizedSparseIntegralOp(6,6,6,1,5,2.5) with the FMM "
-                                "farfield (order 8, mac 3, 128 per leaf); FP32 GMRES inside "
-                                "FP64-residual refinement to 1e-6" % (grid, grid, n)),
+                                "farfield (order %d, mac 3, 128 per leaf); FP32 GMRES inside "
+                                "FP64-residual refinement to 1e-6" % (grid, grid, n,
+                                                                      cfg["order"])),
                    "n_tris": n, "n_free": int(cm.shape[1]),
                    "nearfield_blocks": int(op64.nearfield.bsr.nnzb),
                    "gmres_steps": hist["gmres_steps"], "residuals": hist["residuals"],
@@ -1424,6 +1446,11 @@ def run_c4solve_workload(args, rank, world, torch, dist):
                    "plain_fp64_gmres_steps": int(plain_steps),
                    "speedup_vs_plain": value / (1.0 / t_plain),
                    "rel_diff_vs_plain_fp64": diff, "fp32_matvec_s": t_mv32,
+                   "fmm_order": cfg["order"],
+                   "fmm_fp64_rel_err_vs_direct_fp64": fmm_err,
+                   "fmm_fp32_rel_err_vs_direct_fp64": fmm32_err,
+                   "solution_apply_rel_err_fmm_vs_direct_fp64": sol_err,
+                   "error_rows": "1,024 seeded observation rows, direct FP64 farfield",
                    "build_s": t_build, "hbm_gb": mem_gb,
                    "l2": "operator of %.0f GB (FP64 + FP32 nearfield blocks), beyond L2"
                          % mem_gb,
