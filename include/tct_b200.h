@@ -266,6 +266,17 @@ int64_t tct_near_plan_leaf_pairs(const tct_near_plan* plan);
 int tct_near_device_count(tct_near_plan* plan, void* stream, int64_t* total);
 int tct_near_device_fill(tct_near_plan* plan, int64_t* pairs, void* stream);
 void tct_near_plan_free(tct_near_plan* plan);
+/* The same plan built entirely on the GPU (the reference builds its octrees
+ * and runs the traversal on the host, fmm/octree.cpp:27-76,
+ * mesh/fast_find_nearfield.cpp:96-141): the octrees level by level (equal
+ * to tct_tree_build's node for node), the expanded node radii, the dual
+ * traversal breadth first to leaf pairs, grouped by obs leaf; inputs are host
+ * arrays (copied in); synchronises `stream`.  Use with tct_near_device_count
+ * / _fill / tct_near_plan_free as a host-built plan; the pairs are the same
+ * in the same order.  Fewer than 2^31 - 1 balls per side. */
+int tct_near_plan_build_device(const double* obs_centers, const double* obs_radii, int64_t n_obs,
+                               const double* src_centers, const double* src_radii, int64_t n_src,
+                               double threshold, void* stream, tct_near_plan** out);
 
 /* Split close pairs by the number of shared vertices
  * (mesh/fast_find_nearfield.cpp:143-182): 0 -> near (2 cols), 1 -> vertex
@@ -312,6 +323,11 @@ typedef struct tct_lists tct_lists;
  * children match the reference exactly.  Host. */
 int tct_tree_build(const double* centers, const double* radii, int64_t n, int64_t leaf_size,
                    tct_tree** out);
+/* The same tree built on the GPU (level by level, centres of mass summed in
+ * the host builder's order and rounding), exported depth first: node for
+ * node equal to tct_tree_build's.  Host inputs; synchronises `stream`. */
+int tct_tree_build_device(const double* centers, const double* radii, int64_t n,
+                          int64_t leaf_size, void* stream, tct_tree** out);
 int64_t tct_tree_n_nodes(const tct_tree* tree);
 int tct_tree_max_height(const tct_tree* tree);
 /* Per-node arrays (any may be NULL): orig_idx (n balls: tree position ->

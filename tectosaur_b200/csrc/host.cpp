@@ -15,6 +15,7 @@
 
 #include "tct_b200.h"
 #include "near_plan.h"
+#include "octree.h"
 
 namespace tct {
 
@@ -66,21 +67,8 @@ inline double dist2(const double* a, const double* b) {
 // node centre (x bit 2, y bit 1, z bit 0, "greater than" = 1), stably; an
 // empty child gets (parent centre, parent R / 50), a single-ball child the
 // ball itself.  Nodes are stored in depth-first preorder.
-struct Node {
-    int64_t start, end;
-    double c[3];
-    double R;
-    bool leaf;
-    int depth;
-    int64_t child[8];
-};
-
-struct Octree {
-    std::vector<double> centers;   // tree order, 3 per ball
-    std::vector<double> radii;     // tree order
-    std::vector<int64_t> orig;     // tree position -> original index
-    std::vector<Node> nodes;
-};
+using Node = tct::OctNode;
+using tct::Octree;
 
 inline double dist(const double* a, const double* b) { return std::sqrt(dist2(a, b)); }
 
@@ -455,11 +443,6 @@ int64_t tct_near_plan_leaf_pairs(const tct_near_plan* plan) {
 // ---- treecode trees and interaction lists (fmm/tsfmm.py:22-28, 66-70) --------
 }  // extern "C"
 
-struct tct_tree {
-    Octree t;
-    int max_height = 0;
-    std::vector<int> height;
-};
 
 struct tct_lists {
     // compressed lists (fmm/traversal.cpp:20-53): obs nodes with a non-empty

@@ -91,10 +91,17 @@ T* carve(unsigned char*& p, size_t count) {
     return out;
 }
 
+size_t n_leaves(const tct_near_plan* pl) {
+    return pl->dev_built ? (size_t)pl->nl_dev : pl->leaf_start.size();
+}
+size_t n_leaf_pairs(const tct_near_plan* pl) {
+    return pl->dev_built ? (size_t)pl->nlp_dev : pl->lp_s.size();
+}
+
 NearDev device_view(tct_near_plan* pl) {
     unsigned char* p = static_cast<unsigned char*>(pl->dev);
     NearDev d;
-    const size_t nl = pl->leaf_start.size(), nlp = pl->lp_s.size();
+    const size_t nl = n_leaves(pl), nlp = n_leaf_pairs(pl);
     d.oc = carve<double>(p, 3 * pl->n_obs);
     d.orq = carve<double>(p, pl->n_obs);
     d.sc = carve<double>(p, 3 * pl->n_src);
@@ -111,7 +118,7 @@ NearDev device_view(tct_near_plan* pl) {
 }
 
 size_t device_bytes(const tct_near_plan* pl) {
-    const size_t nl = pl->leaf_start.size(), nlp = pl->lp_s.size();
+    const size_t nl = n_leaves(pl), nlp = n_leaf_pairs(pl);
     return al256(8 * 3 * pl->n_obs) + al256(8 * pl->n_obs) + al256(8 * 3 * pl->n_src) +
            al256(8 * pl->n_src) + al256(8 * pl->n_obs) + al256(8 * pl->n_src) + 2 * al256(8 * nl) +
            al256(8 * (nl + 1)) + 2 * al256(8 * nlp) + al256(8 * (pl->n_obs + 1));
@@ -127,6 +134,29 @@ int upload(const T* dst, const std::vector<T>& src, cudaStream_t st) {
 }
 
 }  // namespace
+
+int near_plan_alloc_device(tct_near_plan* plan) {
+    if (plan->dev) return TCT_OK;
+    plan->dev_bytes = device_bytes(plan);
+    if (cudaMalloc(&plan->dev, plan->dev_bytes) != cudaSuccess) {
+        plan->dev = nullptr;
+        cudaGetLastError();
+        set_error("near plan: out of device memory (%zu bytes)", plan->dev_bytes);
+        return TCT_ERR_OOM;
+    }
+    return TCT_OK;
+}
+
+NearDevPtrs near_plan_device_ptrs(tct_near_plan* plan) {
+    NearDev d = device_view(plan);
+    return NearDevPtrs{const_cast<double*>(d.oc), const_cast<double*>(d.orq),
+                       const_cast<double*>(d.sc), const_cast<double*>(d.srq),
+                       const_cast<int64_t*>(d.oorig), const_cast<int64_t*>(d.sorig),
+                       const_cast<int64_t*>(d.leaf_start), const_cast<int64_t*>(d.leaf_end),
+                       const_cast<int64_t*>(d.lp_start), const_cast<int64_t*>(d.lp_s),
+                       const_cast<int64_t*>(d.lp_e)};
+}
+
 }  // namespace tct
 
 using namespace tct;
@@ -143,29 +173,22 @@ extern "C" int tct_near_device_count(tct_near_plan* plan, void* stream, int64_t*
     // source indices are sorted as int32 keys; the scan and sort count in int
     TCT_CHECK_ARG(plan->n_obs < 0x7fffffff && plan->n_src < 0x7fffffff,
                   "tct_near_device_count: more than 2^31 - 2 balls on a side");
-    if (plan->dev == nullptr) {
-        plan->dev_bytes = device_bytes(plan);
-        if (cudaMalloc(&plan->dev, plan->dev_bytes) != cudaSuccess) {
-            plan->dev = nullptr;
-            cudaGetLastError();
-            set_error("tct_near_device_count: out of device memory (%zu bytes)", plan->dev_bytes);
-            return TCT_ERR_OOM;
-        }
-    }
-    NearDev d = device_view(plan);
     int rc;
-    if ((rc = upload(d.oc, plan->oc, st)) || (rc = upload(d.orq, plan->orq, st)) ||
+    if ((rc = near_plan_alloc_device(plan))) return rc;
+    NearDev d = device_view(plan);
+    if (!plan->dev_built &&
+        ((rc = upload(d.oc, plan->oc, st)) || (rc = upload(d.orq, plan->orq, st)) ||
         (rc = upload(d.sc, plan->sc, st)) || (rc = upload(d.srq, plan->srq, st)) ||
         (rc = upload(d.oorig, plan->oorig, st)) || (rc = upload(d.sorig, plan->sorig, st)) ||
         (rc = upload(d.leaf_start, plan->leaf_start, st)) ||
         (rc = upload(d.leaf_end, plan->leaf_end, st)) ||
         (rc = upload(d.lp_start, plan->lp_start, st)) || (rc = upload(d.lp_s, plan->lp_s, st)) ||
-        (rc = upload(d.lp_e, plan->lp_e, st)))
+        (rc = upload(d.lp_e, plan->lp_e, st))))
         return rc;
     int64_t* counts = plan->d_counts;
     if (cudaMemsetAsync(counts, 0, sizeof(int64_t) * (plan->n_obs + 1), st) != cudaSuccess)
         return launch_status("near memset");
-    const int64_t nl = (int64_t)plan->leaf_start.size();
+    const int64_t nl = (int64_t)n_leaves(plan);
     if (nl > 0) {
         near_count<<<(unsigned)nl, 64, 0, st>>>(d, plan->threshold, counts);
         if ((rc = launch_status("near_count"))) return rc;
@@ -221,7 +244,7 @@ extern "C" int tct_near_device_fill(tct_near_plan* plan, int64_t* pairs, void* s
         return TCT_ERR_OOM;
     }
     int rc = TCT_OK;
-    const int64_t nl = (int64_t)plan->leaf_start.size();
+    const int64_t nl = (int64_t)n_leaves(plan);
     near_fill<<<(unsigned)nl, 64, 0, st>>>(d, plan->threshold, offs, keys);
     rc = launch_status("near_fill");
     if (!rc) {

@@ -23,4 +23,19 @@ struct tct_near_plan {
     size_t dev_bytes = 0;
     int64_t* d_counts = nullptr;  // n_obs + 1 (row offsets after the scan)
     int64_t total = -1;
+    // a plan built on the device (tct_near_plan_build_device) has its arrays
+    // in `dev` already and its leaf counts here; the host vectors stay empty
+    bool dev_built = false;
+    int64_t nl_dev = 0, nlp_dev = 0;
 };
+
+namespace tct {
+// The plan's device arrays (carved from plan->dev in this order).
+struct NearDevPtrs {
+    double *oc, *orq, *sc, *srq;
+    int64_t *oorig, *sorig, *leaf_start, *leaf_end, *lp_start, *lp_s, *lp_e;
+};
+// Allocate plan->dev for the plan's sizes (near.cu).
+int near_plan_alloc_device(tct_near_plan* plan);
+NearDevPtrs near_plan_device_ptrs(tct_near_plan* plan);
+}  // namespace tct

@@ -16,17 +16,33 @@ def tri_centers_radii(pts, tris):
     return centers, Rs
 
 
+# trees from this many balls are built on the GPU when one is visible (the
+# same tree, node for node)
+DEVICE_TREE_MIN = 100_000
+
+
 class Tree:
     """Ball octree: node arrays in depth-first preorder and the permutation
-    from tree positions to original indices."""
+    from tree positions to original indices.  device: build on the GPU
+    (tct_tree_build_device) -- None picks the GPU from DEVICE_TREE_MIN balls
+    when one is visible."""
 
-    def __init__(self, centers, radii, max_pts_per_cell):
+    def __init__(self, centers, radii, max_pts_per_cell, device=None):
         c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
         r = np.ascontiguousarray(radii, dtype=np.float64).reshape(-1)
+        if device is None:
+            from ..util import device as dev
+            device = c.shape[0] >= DEVICE_TREE_MIN and dev.cuda_available()
         h = ctypes.c_void_p()
-        _lib.check(_lib.lib.tct_tree_build(_lib.dptr(c), _lib.dptr(r), c.shape[0],
-                                           int(max_pts_per_cell), ctypes.byref(h)),
-                   "tct_tree_build")
+        if device:
+            _lib.check(_lib.lib.tct_tree_build_device(
+                _lib.dptr(c), _lib.dptr(r), c.shape[0], int(max_pts_per_cell),
+                _lib.stream_ptr(), ctypes.byref(h)), "tct_tree_build_device")
+        else:
+            _lib.check(_lib.lib.tct_tree_build(_lib.dptr(c), _lib.dptr(r), c.shape[0],
+                                               int(max_pts_per_cell), ctypes.byref(h)),
+                       "tct_tree_build")
+        self.on_device = bool(device)
         self._h = h
         n = _lib.lib.tct_tree_n_nodes(h)
         self.n_nodes = n

@@ -37,15 +37,25 @@ def get_nearfield(obs_centers, obs_radii, src_centers, src_radii, threshold, n_t
     return out
 
 
-def near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads=0):
-    """Host half of the device search: the reference's octrees and dual
-    traversal down to leaf pairs (an opaque handle; free with
-    `_lib.lib.tct_near_plan_free`)."""
+def near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads=0,
+              device_tree=False, stream=None):
+    """The octrees and dual traversal of the device search, down to leaf
+    pairs (an opaque handle; free with `_lib.lib.tct_near_plan_free`): built
+    on the host, or with device_tree on the GPU (the same leaf pairs)."""
     oc = np.ascontiguousarray(obs_centers, dtype=np.float64).reshape(-1, 3)
     orr = np.ascontiguousarray(obs_radii, dtype=np.float64).reshape(-1)
-    sc = np.ascontiguousarray(src_centers, dtype=np.float64).reshape(-1, 3)
-    sr = np.ascontiguousarray(src_radii, dtype=np.float64).reshape(-1)
+    if src_centers is obs_centers and src_radii is obs_radii:
+        sc, sr = oc, orr  # a self search: one tree
+    else:
+        sc = np.ascontiguousarray(src_centers, dtype=np.float64).reshape(-1, 3)
+        sr = np.ascontiguousarray(src_radii, dtype=np.float64).reshape(-1)
     handle = ctypes.c_void_p()
+    if device_tree:
+        _lib.check(_lib.lib.tct_near_plan_build_device(
+            _lib.dptr(oc), _lib.dptr(orr), oc.shape[0], _lib.dptr(sc), _lib.dptr(sr),
+            sc.shape[0], float(threshold), _lib.stream_ptr(stream), ctypes.byref(handle)),
+            "tct_near_plan_build_device")
+        return handle
     _lib.check(_lib.lib.tct_near_plan_build(
         _lib.dptr(oc), _lib.dptr(orr), oc.shape[0], _lib.dptr(sc), _lib.dptr(sr), sc.shape[0],
         float(threshold), int(n_threads), ctypes.byref(handle)), "tct_near_plan_build")
@@ -53,12 +63,14 @@ def near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threa
 
 
 def get_nearfield_device(obs_centers, obs_radii, src_centers, src_radii, threshold,
-                         n_threads=0, stream=None):
-    """get_nearfield with the ball tests, row fill and row sort on the GPU:
-    the same pairs in the same order, as an int64 (P, 2) CUDA tensor."""
+                         n_threads=0, stream=None, device_tree=True):
+    """get_nearfield on the GPU -- octrees, dual traversal (device_tree;
+    else on the host), ball tests, row fill and row sort: the same pairs in
+    the same order, as an int64 (P, 2) CUDA tensor."""
     from ..util import device
     t = device.require_cuda()
-    handle = near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads)
+    handle = near_plan(obs_centers, obs_radii, src_centers, src_radii, threshold, n_threads,
+                       device_tree=device_tree, stream=stream)
     try:
         s = _lib.stream_ptr(stream)
         total = ctypes.c_int64()
