@@ -1645,6 +1645,11 @@ C5_LO, C5_HI = 2_000, 200_000
 C5_TOL = 1e-8             # FP64 residual of every solve request
 C5_FMM_MIN = 60_000       # meshes from this size use the FMM farfield
 C5_FMM = dict(mac=3.0, pts_per_cell=128, order=10, mode="fmm")
+# the served FP32 correction operator of an FMM mesh: a lower order (its
+# FP32 rounding floor, 1e-5 - 3e-5, is above the truncation error of order
+# 6 anyway) and a correction tolerance above that floor
+C5_INNER_ORDER = 6
+C5_INNER_TOL_FMM = 1e-4
 C5_SOLVES = (8, 6, 4, 3, 2, 2)   # solve requests per mesh, smallest mesh first
 C5_QD_MESHES = 2                  # the smallest meshes (faults) also take qd requests
 C5_QD_PER_MESH = 4
@@ -1688,7 +1693,7 @@ def c5_meshes(n_meshes=6, seed=6, lo=C5_LO, hi=C5_HI):
     return out
 
 
-def c5_stream(torch, quiet=True, seed=7, inner="direct"):
+def c5_stream(torch, quiet=True, seed=7, inner="fmm-low"):
     """Serve the C5 stream (module-level C5_* settings) and time it against
     the plain paths.  Returns a dict of results (no JSON printing).
 
@@ -1699,9 +1704,12 @@ def c5_stream(torch, quiet=True, seed=7, inner="direct"):
     state perturbation) on each of the C5_QD_MESHES smallest meshes, in a
     seeded order.  Served: serve.SolveServer (continuous batching, 16 slots
     per mesh, FP32 operator in FP64 refinement; FMM farfield from C5_FMM_MIN
-    triangles; inner="direct": the FP32 correction operator of an FMM mesh
-    uses the direct farfield, whose panel runs on the tensor cores, while the
-    FP64 residual keeps the FMM farfield -- "fmm": both FMM).  Plain: one
+    triangles; the FP32 correction operator of an FMM mesh is, with
+    inner="fmm-low", the FMM at order C5_INNER_ORDER solved to
+    C5_INNER_TOL_FMM, with "fmm" the FMM at the residual's order, with
+    "direct" the direct farfield (tensor-core panel) -- the FP64 residual
+    always uses the order-C5_FMM FMM, so the converged solution is that
+    operator's).  Plain: one
     request at a time in arrival order -- the FP64
     GMRES solve (simple_solver.iterative_solve) and the single-state
     Integrator.  Saturation (all requests at t = 0) gives the throughput;
@@ -1730,10 +1738,18 @@ def c5_stream(torch, quiet=True, seed=7, inner="direct"):
                              C5_FMM["mode"]) if n >= C5_FMM_MIN else TriToTriDirectFarfieldOp)
         op64 = tct.RegularizedSparseIntegralOp(*C1_NQ, K_NAME, K_NAME, PARAMS, pts, tris,
                                                np.float64, far, keep_uncorrected=False)
+        inner_far, inner_tol = None, None
+        if n >= C5_FMM_MIN:
+            if inner == "direct":
+                inner_far = TriToTriDirectFarfieldOp
+            elif inner == "fmm-low":
+                inner_far = FMMFarfieldOp(C5_FMM["mac"], C5_FMM["pts_per_cell"], C5_INNER_ORDER,
+                                          C5_FMM["mode"])
+                inner_tol = C5_INNER_TOL_FMM
+            else:
+                inner_tol = C5_INNER_TOL_FMM
         srv.add_mesh(key, pts, tris, cm, nq=C1_NQ, params=PARAMS, op64=op64,
-                     farfield_op_type=far,
-                     inner_farfield_op_type=(TriToTriDirectFarfieldOp
-                                             if inner == "direct" and n >= C5_FMM_MIN else None))
+                     farfield_op_type=far, inner_farfield_op_type=inner_far, inner_tol=inner_tol)
         specs[key] = (op64, cm, n)
         if n >= C5_FMM_MIN:
             # the FMM farfield's error against the direct FP64 farfield on
@@ -1794,6 +1810,9 @@ def c5_stream(torch, quiet=True, seed=7, inner="direct"):
     assert all(r.error is None for r in sat), [r.error for r in sat if r.error]
     served_rate = n_all / t_served
     log("served saturation %.2f s" % t_served)
+    for r, (kind, k, _) in zip(sat, stream):
+        log("  %s %s latency %.2f s steps %s refinements %s" % (
+            kind, k, r.latency, getattr(r, "gmres_steps", "-"), getattr(r, "refinements", "-")))
     # the plain paths, one request at a time in arrival order
     service, err_solve, err_qd = [], [], []
     for (kind, k, payload), r in zip(stream, sat):
@@ -1809,6 +1828,7 @@ def c5_stream(torch, quiet=True, seed=7, inner="direct"):
             err_qd.append(float(np.linalg.norm(r.y - y) / np.linalg.norm(y)))
         torch.cuda.synchronize()
         service.append(time.perf_counter() - t0)
+        log("  plain %s %s %.2f s" % (kind, k, service[-1]))
     plain_rate = n_all / sum(service)
     log("plain %.2f s" % sum(service))
     lam = 0.7 * served_rate
@@ -1842,9 +1862,21 @@ def c5_stream(torch, quiet=True, seed=7, inner="direct"):
                          "farfield": ("fmm p=%d mac %.1f, %d per leaf"
                                       % (C5_FMM["order"], C5_FMM["mac"], C5_FMM["pts_per_cell"])
                                       if tris.shape[0] >= C5_FMM_MIN else "direct"),
-                         "served_inner_farfield": ("direct (tensor-core panel)"
-                                                   if tris.shape[0] < C5_FMM_MIN or
-                                                   inner == "direct" else "fmm")}
+                         "served_inner_farfield": (
+                             "direct (tensor-core panel)"
+                             if tris.shape[0] < C5_FMM_MIN or inner == "direct" else
+                             ("fmm p=%d, correction tol %g" % (C5_INNER_ORDER, C5_INNER_TOL_FMM)
+                              if inner == "fmm-low" else
+                              "fmm p=%d, correction tol %g" % (C5_FMM["order"],
+                                                                C5_INNER_TOL_FMM))),
+                         "served_gmres_steps_mean": float(np.mean(
+                             [r.gmres_steps for r, (k_, m_, _) in zip(sat, stream)
+                              if k_ == "solve" and m_ == key] or [0])),
+                         "served_refinements_mean": float(np.mean(
+                             [r.refinements for r, (k_, m_, _) in zip(sat, stream)
+                              if k_ == "solve" and m_ == key] or [0])),
+                         "plain_s": float(sum(sv for sv, (k_, m_, _) in zip(service, stream)
+                                              if m_ in (key, key + "/qd")))}
                    for key, pts, tris, kind in meshes},
         "qd_meshes": qd_keys, "qd_steps": C5_QD_STEPS, "solve_tol": C5_TOL,
         "max_rel_diff_solve_vs_plain_fp64": max(err_solve) if err_solve else None,
@@ -1927,7 +1959,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch shapes (skip the autotuner in setup)")
-    ap.add_argument("--c5-inner", default="direct", choices=["direct", "fmm"],
+    ap.add_argument("--c5-inner", default="fmm-low", choices=["fmm-low", "fmm", "direct"],
                     help="farfield of the served FP32 correction operator on FMM meshes")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the C5 served-vs-plain stream on the default line")

@@ -224,9 +224,11 @@ class SolveEngine:
                 jt = cd[4 * S:]
                 act = t.zeros(S, dtype=t.bool, device=self.dev)
                 act[ii] = True
-                ar = t.arange(S, device=self.dev)
-                Vc = self.V[ar, jt] * act[:, None]
-                W = self.A32(Vc)
+                # the operator is applied to the active slots' columns only
+                # (an FMM farfield costs one pass per column; columns are
+                # independent, so a slot's result does not depend on the others)
+                W = t.zeros((S, self.n), dtype=t.float64, device=self.dev)
+                W[ii] = self.A32(self.V[ii, jt[ii]])
                 self.n_panel_applies += 1
                 self.n_vector_applies += inner.size
                 mask = ((t.arange(J, device=self.dev)[None, :] <= jt[:, None]) & act[:, None])
@@ -510,8 +512,12 @@ class MeshSpec:
 
     def __init__(self, key, pts, tris, cm=None, nq=(6, 6, 6, 2, 5, 2.5), kernel="elasticRH3",
                  params=(1.0, 0.25), farfield_op_type=None, op64=None,
-                 inner_farfield_op_type=None):
+                 inner_farfield_op_type=None, inner_tol=None):
         self.key = key
+        # relative tolerance floor of the FP32 correction solves (None: the
+        # server's); an FP32 operator whose rounding floor is above the
+        # server's floor (the FP32 FMM) needs a looser one
+        self.inner_tol = inner_tol
         # farfield of the FP32 correction operator when it differs from the
         # FP64 residual operator's (None: the same type)
         self.inner_farfield_op_type = inner_farfield_op_type
@@ -659,7 +665,8 @@ class SolveServer:
             out = t.empty(cm.shape[0], dtype=t.float64, device="cuda")
             return cmd.dot_device(x.contiguous(), out)
 
-        engine = SolveEngine(A32, A64, to_free, to_full, n, S, self.restart, self.inner_tol,
+        inner_tol = spec.inner_tol if spec.inner_tol is not None else self.inner_tol
+        engine = SolveEngine(A32, A64, to_free, to_full, n, S, self.restart, inner_tol,
                              self.max_refine, "cuda", t.cuda.Stream())
         t.cuda.synchronize()
         nbytes = t.cuda.memory_allocated() - before
