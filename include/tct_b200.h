@@ -443,6 +443,25 @@ int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
 int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
                                 int n_q, void* stream, int* host_flag);
 
+/* Point farfield on R = 16 weight vectors at once (FP32 elasticU3/T3/A3/H3;
+ * the reference applies farfield_pts{K}, tectosaur/farfield_direct.cl:15-113,
+ * one vector per call): out[r][i][d] (+)= sum_j sum_k M_dk(x_i, y_j, n_i, n_j)
+ * w[r][j][k] with M the kernel's 3x3 point-pair matrix (r^2 == 0 pairs
+ * skipped), generated on the CUDA cores and contracted with the weight panel
+ * on the tensor cores (tcgen05.mma kind::tf32, split TF32 hi/lo,
+ * compensated folds of the TMEM accumulator, bounded mbarrier waits).
+ * in: (R, n_src, 3) float; out: (R, n_obs, 3); points and normals float
+ * (n, 3).  Workspace from tct_farfield_pts_panel_workspace_bytes (0 = R
+ * unsupported).  tct_farfield_pts_panel_error copies the workspace's timeout
+ * flag to host (0 = none; synchronises `stream`). */
+size_t tct_farfield_pts_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R);
+int tct_farfield_pts_panel(int kernel, void* out, const void* in, const void* obs_pts,
+                           const void* obs_ns, int64_t n_obs, const void* src_pts,
+                           const void* src_ns, int64_t n_src, int R, const double* params,
+                           int accumulate, void* workspace, size_t workspace_bytes, void* stream);
+int tct_farfield_pts_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
+                                 void* stream, int* host_flag);
+
 /* ---- interior evaluation (tectosaur/interior.py InteriorOp) --------------- */
 
 /* Triangle sources to observation points (matrix_free.cl:109-194,

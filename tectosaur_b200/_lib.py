@@ -236,6 +236,10 @@ _TUNE_SIGS = {
                                c_dp, c_p, c_sz, c_p, c_ip], c_i),
     "tct_bsr9_autotune": ([c_i, c_i64, c_p, c_p, c_p, c_i64, c_p, c_p, c_p, c_ip, c_ip], c_i),
     "tct_farfield_workspace_bytes_chunks": ([c_i, c_i, c_i64, c_i64, c_i, c_i], c_sz),
+    "tct_farfield_pts_panel_workspace_bytes": ([c_i64, c_i64, c_i], c_sz),
+    "tct_farfield_pts_panel": ([c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_p, c_i64, c_i, c_dp, c_i,
+                                c_p, c_sz, c_p], c_i),
+    "tct_farfield_pts_panel_error": ([c_p, c_i64, c_i64, c_i, c_p, ctypes.POINTER(c_i)], c_i),
     "tct_tree_build_device": ([c_dp, c_dp, c_i64, c_i64, c_p, ctypes.POINTER(c_p)], c_i),
     "tct_near_plan_build_device": ([c_dp, c_dp, c_i64, c_dp, c_dp, c_i64, ctypes.c_double, c_p,
                                     ctypes.POINTER(c_p)], c_i),
