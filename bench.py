@@ -1082,6 +1082,113 @@ def run_panel_workload(args, rank, world, torch, dist):
     print(json.dumps(line), flush=True)
 
 
+def c2_point_form(n=174):
+    """The 60k-triangle surface's 3-point-rule quadrature points (179,574)
+    with their triangle normals: the point form of the C2 configuration."""
+    from tectosaur_b200.util.quadrature import gauss2d_tri
+    pts, tris = c2_mesh(n)
+    q, _ = gauss2d_tri(NQ["nq_far"])
+    tp = pts[tris]
+    b = np.stack([1 - q[:, 0] - q[:, 1], q[:, 0], q[:, 1]], axis=1)   # (nq, 3)
+    P = np.einsum("qb,tbd->tqd", b, tp).reshape(-1, 3)
+    nrm = np.cross(tp[:, 2] - tp[:, 0], tp[:, 2] - tp[:, 1])
+    nrm /= np.linalg.norm(nrm, axis=1)[:, None]
+    Nn = np.repeat(nrm, q.shape[0], axis=0)
+    return P, Nn
+
+
+def run_ptspanel_workload(args, rank, world, torch, dist):
+    """The C2 point form (179,574 quadrature points of the 60k-triangle
+    surface, elasticT3 and elasticH3) on a panel of R weight vectors on the
+    tensor cores, against the single-vector point kernel and the FP64
+    oracle on sampled rows."""
+    from tectosaur_b200 import _lib
+    from tectosaur_b200.farfield import farfield_pts_panel_device
+    R = args.rhs
+    P, Nn = c2_point_form(args.grid or 174)
+    n = P.shape[0]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    op, on = dev(P), dev(Nn)
+    W = dev(np.random.default_rng(3 + rank).standard_normal((R, 3 * n)))
+    Y = torch.empty((R, 3 * n), dtype=torch.float32, device="cuda")
+    res = {}
+    for K in ("elasticH3", "elasticT3"):
+        for _ in range(args.warmup):
+            farfield_pts_panel_device(K, op, on, op, on, W, PARAMS, out=Y)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            farfield_pts_panel_device(K, op, on, op, on, W, PARAMS, out=Y)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        # the single-vector kernel
+        y1 = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+        params = np.ascontiguousarray(PARAMS, np.float64)
+        kid = _lib.kernel_id(K)
+
+        def single(r):
+            _lib.check(_lib.lib.tct_farfield_pts(
+                kid, _lib.TCT_F32, _lib.tptr(y1), _lib.tptr(op), _lib.tptr(on), n,
+                _lib.tptr(op), _lib.tptr(on), n, _lib.tptr(W[r]), _lib.dptr(params),
+                _lib.stream_ptr()), "tct_farfield_pts")
+        single(0)
+        torch.cuda.synchronize()
+        c = torch.cuda.Event(enable_timing=True)
+        d = torch.cuda.Event(enable_timing=True)
+        c.record()
+        for _ in range(3):
+            single(0)
+        d.record()
+        torch.cuda.synchronize()
+        single_ms = c.elapsed_time(d) / 3
+        # FP64 oracle on 256 seeded observation points, columns 0 and R - 1
+        from oracle import oracle as orc
+        rows = np.sort(np.random.default_rng(19).choice(n, 256, replace=False))
+        Wh = W.cpu().numpy().astype(np.float64)
+        Yh = Y.cpu().numpy()
+        errs = []
+        for r in (0, R - 1):
+            want = orc.farfield_pts(K, np.float64, P[rows], Nn[rows], P, Nn, Wh[r], PARAMS)
+            got = Yh[r].reshape(-1, 3)[rows].reshape(-1)
+            errs.append(float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+        n_pad_o = (n + 127) // 128 * 128
+        n_pad_s = (n + 7) // 8 * 8
+        panels = (R + 15) // 16
+        mma_flops = panels * 3 * 2.0 * n_pad_o * 9 * n_pad_s * 48
+        res[K] = {"ms_per_panel_apply": ms, "vector_applies_per_s": R / (ms * 1e-3),
+                  "single_vector_ms": single_ms, "speedup_vs_single_vector": single_ms * R / ms,
+                  "rel_err_fp64_oracle_256_rows": errs,
+                  "tensor_tflops_executed": mma_flops / (ms * 1e-3) / 1e12}
+    if rank != 0:
+        return
+    mp = measured_peaks()
+    bf16 = mp.get("bf16_tflops") if mp else 1590.0
+    tf32_peak = bf16 / 2.0
+    hv = res["elasticH3"]
+    line = {
+        "metric": "point farfield vector applies/s (multi-RHS panel, tensor cores)",
+        "value": world * hv["vector_applies_per_s"], "unit": "vector applies/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": hv["ms_per_panel_apply"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded mesh and weights)",
+        "config": {"workload": ("point form of the 60k-triangle surface: %d quadrature points "
+                                "(3-point rule) with their triangle normals, all-pairs "
+                                "elasticH3 / elasticT3 on a panel of %d N(0, 1) weight vectors "
+                                "(tct_farfield_pts_panel)" % (n, R)),
+                   "n_points": int(n), "rhs": R, "kernels": res, "parallelism": "replicas"},
+        "roofline": {"kernel": "pts_panel_main<elasticH3> (tcgen05.mma kind::tf32)",
+                     "bound": "tensor", "achieved": hv["tensor_tflops_executed"],
+                     "peak": tf32_peak, "unit": "TFLOP/s",
+                     "frac": hv["tensor_tflops_executed"] / tf32_peak, "traffic": None,
+                     "peak_source": "TF32 dense = half of the measured BF16 GEMM rate"},
+        "gpu_launches": args.steps * ((R + 15) // 16) * 4,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_batch_workload(args, rank, world, torch, dist):
     """Batched mixed-precision solves against the plain FP64 one-at-a-time
     solve on the 722-triangle configuration."""
@@ -1968,7 +2075,7 @@ def main():
                          "workload; smaller for profiling; the fmm workload uses 707)")
     ap.add_argument("--workload", default="c2",
                     choices=["c2", "fmm", "solve", "pairs", "panel", "batch", "serve", "qd",
-                             "interior", "c4solve", "near"],
+                             "interior", "c4solve", "near", "ptspanel"],
                     help="c2: the operator apply line (default); fmm: the 1M-triangle FMM "
                          "farfield; solve: the 722-triangle FP64 GMRES solve; pairs: the "
                          "400k-pair batched singular quadrature + BSR matvec; panel: the "
@@ -2002,12 +2109,12 @@ def main():
                                 device_id=torch.device("cuda", local_rank))
 
     if args.workload in ("fmm", "solve", "pairs", "panel", "batch", "serve", "qd", "interior",
-                         "c4solve", "near"):
+                         "c4solve", "near", "ptspanel"):
         {"fmm": run_fmm_workload, "solve": run_solve_workload, "pairs": run_pairs_workload,
          "panel": run_panel_workload, "batch": run_batch_workload,
          "serve": run_serve_workload, "qd": run_qd_workload,
          "interior": run_interior_workload, "c4solve": run_c4solve_workload,
-         "near": run_near_workload}[args.workload](
+         "near": run_near_workload, "ptspanel": run_ptspanel_workload}[args.workload](
             args, rank, world, torch, dist)
         if dist is not None:
             dist.barrier()
