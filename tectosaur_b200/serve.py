@@ -27,9 +27,10 @@ the new Hessenberg columns, and the Givens updates on the host
 so a request's result does not depend on what else is in the batch beyond
 the summation order of library reductions.
 
-Engines of different meshes run on their own CUDA streams.  A scheduling
-tick first enqueues every engine's device work and then completes them, so
-the work of different meshes overlaps on the device.
+Engines of different meshes run on their own CUDA streams.  The scheduling
+loop completes an engine's tick as soon as the device has finished it (an
+event query, no wait) and enqueues its next one, so the work of different
+meshes overlaps on the device and a slow engine holds back no other.
 
 HBM admission.  A mesh's operators (FP64 nearfield blocks, their FP32 cast,
 farfield workspaces) and its engine state are built when its first request
@@ -161,6 +162,15 @@ class SolveEngine:
     @property
     def busy(self):
         return bool((self.state != FREE).any())
+
+    @property
+    def pending(self):
+        """A tick enqueued and not yet completed."""
+        return getattr(self, "_pending", None) is not None
+
+    def ready(self):
+        """The enqueued tick has finished on the device (no wait)."""
+        return self._event is None or self._event.query()
 
     def admit(self, req):
         """Put a request into a free slot (False if none)."""
@@ -392,6 +402,13 @@ class QdEngine:
     @property
     def busy(self):
         return any(r is not None for r in self.req)
+
+    @property
+    def pending(self):
+        return self._pending is not None
+
+    def ready(self):
+        return self._event.query()
 
     def admit(self, req):
         free = [s for s in range(self.S) if self.req[s] is None]
@@ -627,7 +644,8 @@ class SolveServer:
         for key in list(self.resident):
             if self.resident_bytes + need <= self.hbm_budget:
                 break
-            if not self.resident[key].engine.busy:
+            e = self.resident[key].engine
+            if not (e.busy or e.pending):
                 self._release(key)
         return self.resident_bytes + need <= self.hbm_budget
 
@@ -741,18 +759,29 @@ class SolveServer:
 
     @property
     def idle(self):
-        return not self.queue and not any(r.engine.busy for r in self.resident.values())
+        return not self.queue and not any(r.engine.busy or r.engine.pending
+                                          for r in self.resident.values())
 
     def step(self):
-        """One scheduling tick: admit, enqueue every engine's work, complete.
-        Returns the requests finished in this tick."""
+        """One pass of the scheduling loop: admit, then for every resident
+        engine complete its tick if the device has finished it (an event
+        query, no wait) and enqueue its next tick.  Engines of different
+        meshes and kinds advance at their own pace: a slow engine (a batch
+        of quasidynamic RK23 attempts) does not hold back the Arnoldi steps
+        of the others.  Returns the requests finished in this pass."""
         self._admit()
-        engines = [r.engine for r in self.resident.values() if r.engine.busy]
-        for e in engines:
-            e.launch()
         done = []
-        for e in engines:
-            done.extend(e.complete())
+        waiting = True
+        for r in list(self.resident.values()):
+            e = r.engine
+            if e.pending and e.ready():
+                done.extend(e.complete())
+                waiting = False
+            if not e.pending and e.busy:
+                e.launch()
+                waiting = False
+        if waiting and done == []:
+            time.sleep(20e-6)  # every engine is waiting for the device
         self.completed.extend(done)
         return done
 
