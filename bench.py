@@ -1154,6 +1154,12 @@ def run_ptspanel_workload(args, rank, world, torch, dist):
             want = orc.farfield_pts(K, np.float64, P[rows], Nn[rows], P, Nn, Wh[r], PARAMS)
             got = Yh[r].reshape(-1, 3)[rows].reshape(-1)
             errs.append(float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+            if r == 0:
+                # the single-vector FP32 kernel on the same rows, for scale
+                single(0)
+                s1 = y1.cpu().numpy().reshape(-1, 3)[rows].reshape(-1)
+                err_single = float(np.linalg.norm(s1 - want) / np.linalg.norm(want))
+                err_vs_single = float(np.linalg.norm(got - s1) / np.linalg.norm(s1))
         n_pad_o = (n + 127) // 128 * 128
         n_pad_s = (n + 7) // 8 * 8
         panels = (R + 15) // 16
@@ -1161,6 +1167,8 @@ def run_ptspanel_workload(args, rank, world, torch, dist):
         res[K] = {"ms_per_panel_apply": ms, "vector_applies_per_s": R / (ms * 1e-3),
                   "single_vector_ms": single_ms, "speedup_vs_single_vector": single_ms * R / ms,
                   "rel_err_fp64_oracle_256_rows": errs,
+                  "single_vector_fp32_rel_err_fp64_oracle": err_single,
+                  "rel_diff_vs_single_vector_fp32": err_vs_single,
                   "tensor_tflops_executed": mma_flops / (ms * 1e-3) / 1e12}
     if rank != 0:
         return

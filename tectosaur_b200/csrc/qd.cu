@@ -18,7 +18,10 @@
 //   cg_csr_block     one CTA: conjugate gradients on a CSR matrix with x0 = 0,
 //                    stopping when ||r|| < max(atol, rtol ||b||), the
 //                    iteration of scipy.sparse.linalg.cg, with the vector
-//                    updates rounded as scipy's (no fused multiply-add).
+//                    updates rounded as scipy's (no fused multiply-add); a
+//                    non-finite right-hand side or residual returns the NaN
+//                    solution at once (iterations -1), where scipy's
+//                    iteration runs out its maxiter first.
 #include "common.cuh"
 
 namespace tct {
@@ -169,6 +172,14 @@ cg_csr_block(int64_t n, const int64_t* __restrict__ indptr, const int64_t* __res
         if (tid == 0) *iters = 0;
         return;
     }
+    if (!isfinite(bnrm2)) {
+        // a non-finite right-hand side (a state the stepper will reject):
+        // scipy's cg never meets its stopping test then and returns a NaN
+        // solution after maxiter iterations; return that solution at once
+        for (int64_t i = tid; i < n; i += blockDim.x) x[i] = nan("");
+        if (tid == 0) *iters = -1;
+        return;
+    }
     const double atol = fmax(atol_in, rtol * bnrm2);
     for (int64_t i = tid; i < n; i += blockDim.x) {
         x[i] = 0.0;
@@ -182,6 +193,11 @@ cg_csr_block(int64_t n, const int64_t* __restrict__ indptr, const int64_t* __res
         for (int64_t i = tid; i < n; i += blockDim.x) rr += r[i] * r[i];
         const double rho = block_sum(rr, red);  // r . z with z = r
         if (sqrt(rho) < atol) break;
+        if (!isfinite(rho)) {  // the iteration broke down: the NaN solution, at once
+            for (int64_t i = tid; i < n; i += blockDim.x) x[i] = nan("");
+            it = -1;
+            break;
+        }
         const double beta = it > 0 ? rho / rho_prev : 0.0;
         for (int64_t i = tid; i < n; i += blockDim.x)
             p[i] = it > 0 ? __dadd_rn(__dmul_rn(p[i], beta), r[i]) : r[i];

@@ -113,6 +113,28 @@ def test_cg_kernel(cuda):
     np.testing.assert_allclose(x.cpu().numpy(), x_want, rtol=1e-10, atol=1e-12 * np.abs(x_want).max())
 
 
+def test_cg_kernel_non_finite_rhs(cuda):
+    # a non-finite right-hand side (an oversized trial step): the NaN
+    # solution at once (scipy's cg returns NaN only after maxiter iterations)
+    pts, tris = make_rect(9, 7, [[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]])
+    cm = shared_vertex_matrix(tris, fixed_vertices=free_edge_vertices(tris))
+    M = (cm.T @ MassOp(4, pts, tris).mat @ cm).tocsr()
+    M.sort_indices()
+    n = M.shape[0]
+    for bad in (np.nan, np.inf):
+        b = np.random.default_rng(2).standard_normal(n)
+        b[n // 2] = bad
+        d = [dev(M.indptr, torch.int64), dev(M.indices, torch.int64), dev(M.data), dev(b)]
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        work = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        it = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _lib.check(_lib.lib.tct_cg_csr(n, *[_lib.tptr(v) for v in d], _lib.tptr(x),
+                                       _lib.tptr(work), 1e-5, 1e-12, 10 * n, _lib.tptr(it), None),
+                   "cg")
+        assert int(it.item()) == -1
+        assert np.all(np.isnan(x.cpu().numpy()))
+
+
 def _pair(n=7, seed=0):
     pts, tris = make_rect(n, n, [[-1, 0, 1], [-1, 0, -1], [1, 0, -1], [1, 0, 1]])
     cfg = qd_cfg(tris.shape[0])
