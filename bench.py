@@ -907,17 +907,25 @@ def run_pairs_workload(args, rank, world, torch, dist):
     bsr.data.view(81, -1)[:, :blocks.shape[0]] = blocks.index_select(0, order).t()
     xb = torch.from_numpy(np.random.default_rng(5).standard_normal(9 * n_tri)).cuda()
     yb = torch.empty_like(xb)
-    for _ in range(3):
-        bsr.matvec(xb, yb)
-    torch.cuda.synchronize()
-    c = torch.cuda.Event(enable_timing=True)
-    d = torch.cuda.Event(enable_timing=True)
-    c.record()
-    for _ in range(20):
-        bsr.matvec(xb, yb)
-    d.record()
-    torch.cuda.synchronize()
-    bsr_ms = c.elapsed_time(d) / 20
+
+    def time_bsr():
+        for _ in range(3):
+            bsr.matvec(xb, yb)
+        torch.cuda.synchronize()
+        c = torch.cuda.Event(enable_timing=True)
+        d = torch.cuda.Event(enable_timing=True)
+        c.record()
+        for _ in range(20):
+            bsr.matvec(xb, yb)
+        d.record()
+        torch.cuda.synchronize()
+        return c.elapsed_time(d) / 20
+    # the default shape (a warp per block row), then the autotuned one (rows
+    # of one or two blocks: several rows per warp)
+    from tectosaur_b200 import autotune
+    bsr_ms_default = time_bsr()
+    bsr_shape = autotune.tune_bsr(bsr, xb)
+    bsr_ms = time_bsr()
     nnzb = bsr.nnzb
     bsr_bytes = nnzb * (81 * 8 + 4) + (n_tri + 1) * 4 + 2 * 9 * n_tri * 8
     # e2e: the public per-call API (plan + upload + launch + copy out)
@@ -948,6 +956,9 @@ def run_pairs_workload(args, rank, world, torch, dist):
                                 "(one per kernel)" % (n_pairs, len(runs))),
                    "quadrature_points": points, "setup_s": t_setup,
                    "bsr": {"blocks": int(nnzb), "ms": bsr_ms, "bytes": int(bsr_bytes),
+                           "ms_default_shape": bsr_ms_default,
+                           "tuned_shape": {"lanes_per_row": bsr_shape[0],
+                                           "ctas_per_sm": bsr_shape[1]},
                            "achieved_gbs": bsr_bytes / (bsr_ms * 1e-3) / 1e9,
                            "blocks_per_s": nnzb / (bsr_ms * 1e-3), "hbm_peak_gbs": hbm},
                    "l2": "inputs larger than L2 (blocks %.0f MB per step)" % (n_pairs * 648 / 1e6),
