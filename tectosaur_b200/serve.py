@@ -701,7 +701,11 @@ class SolveServer:
         t.cuda.synchronize()
         before = t.cuda.memory_allocated()
         model = spec.model or FullspaceModel((spec.pts, spec.tris), spec.qd_cfg)
-        engine = QdEngine(model, self.slots, t.cuda.Stream())
+        # a high-priority stream: an RK23 tick is a chain of small,
+        # latency-bound kernels and a host sync, which would otherwise queue
+        # behind the solve engines' panel and FMM kernels
+        engine = QdEngine(model, self.slots,
+                          t.cuda.Stream(priority=t.cuda.Stream.priority_range()[1]))
         t.cuda.synchronize()
         spec.measured_bytes = max(t.cuda.memory_allocated() - before, 1)
         self.n_builds += 1
