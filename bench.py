@@ -1601,9 +1601,11 @@ def run_c4solve_workload(args, rank, world, torch, dist):
 
 def run_near_workload(args, rank, world, torch, dist):
     """Near-pair search of the C4 mesh (1,016,894 triangles, threshold 2.5,
-    the operator build's first step): get_nearfield_device (host octrees and
-    traversal to leaf pairs, device ball tests, row fill and row sort) against
-    the host search; both give the reference's pair set in (obs, src) order."""
+    the operator build's first step): get_nearfield_device (octrees, dual
+    traversal to leaf pairs, ball tests, row fill and row sort, all on the
+    device) against the host search; both give the reference's pair set in
+    (obs, src) order.  The host-built plan (host octrees and traversal) is
+    timed beside it."""
     from tectosaur_b200 import _lib
     from tectosaur_b200.mesh import find_near_adj as fna
     pts, tris = c4_mesh(args.grid or 707)
@@ -1626,12 +1628,26 @@ def run_near_workload(args, rank, world, torch, dist):
     t0 = time.perf_counter()
     host_out = out.cpu().numpy()
     d2h = time.perf_counter() - t0
-    # the device plan's host half alone (octrees + traversal)
+    # the plans alone: octrees + traversal to leaf pairs on the host, and on
+    # the device
     t0 = time.perf_counter()
     h = fna.near_plan(c, r, c, r, thr)
     t_plan = time.perf_counter() - t0
     n_leaf_pairs = int(_lib.lib.tct_near_plan_leaf_pairs(h))
     _lib.lib.tct_near_plan_free(h)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h = fna.near_plan(c, r, c, r, thr, device_tree=True)
+    torch.cuda.synchronize()
+    t_plan_dev = time.perf_counter() - t0
+    _lib.lib.tct_near_plan_free(h)
+    # the whole search with the host-built plan
+    t0 = time.perf_counter()
+    out_h = fna.get_nearfield_device(c, r, c, r, thr, device_tree=False)
+    torch.cuda.synchronize()
+    t_hostplan = time.perf_counter() - t0
+    same_plans = bool(torch.equal(out_h, out))
+    del out_h
     if rank != 0:
         return
     line = {
@@ -1641,10 +1657,13 @@ def run_near_workload(args, rank, world, torch, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 tests, int64 pairs",
         "data": "synthetic (seeded hills)",
         "config": {"workload": ("near pairs of the C4 mesh (%d triangles), threshold %.1f: "
-                                "host octrees + traversal to leaf pairs, device tests, fill "
-                                "and per-row sort" % (tris.shape[0], thr)),
+                                "octrees, traversal to leaf pairs, tests, fill and per-row "
+                                "sort on the device" % (tris.shape[0], thr)),
                    "n_tris": int(tris.shape[0]), "pairs": n_pairs,
                    "leaf_pairs": n_leaf_pairs, "host_plan_s": t_plan,
+                   "device_plan_s": t_plan_dev,
+                   "search_with_host_plan_s": t_hostplan,
+                   "device_plan_equals_host_plan_output": same_plans,
                    "timing": "wall clock (host phases included)", "parallelism": "replicas",
                    "l2": "inputs and pair arrays larger than L2"},
         "roofline": {"kernel": "near_count / near_fill (ball tests)", "bound": "fp64",
