@@ -38,7 +38,16 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
     const int sub = lane % LPR;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = warp * G; base < n_rows; base += n_warps * G) {
+    // each warp takes a contiguous range of row groups, in order: the
+    // 128-byte line that the end of one row's segment of an element plane
+    // shares with the start of the next row's is then read twice by the same
+    // warp, a few microseconds apart (an L2 hit), not by two warps at once
+    // (two DRAM fetches: 1.35x the algorithmic bytes at ~90 blocks per row)
+    const int64_t n_groups = (n_rows + G - 1) / G;
+    const int64_t per_warp = (n_groups + n_warps - 1) / n_warps;
+    const int64_t g_end = min(n_groups, (warp + 1) * per_warp);
+    for (int64_t gi = warp * per_warp; gi < g_end; gi++) {
+        const int64_t base = gi * G;
         const int64_t row = base + lane / LPR;
         int32_t start = 0, end = 0;
         if (row < n_rows) {
