@@ -40,6 +40,10 @@ K_NAME = "elasticRH3"
 # kernel (FMA = 2): D 3, r^2 5, rsqrt 1, weights 4, S0 1, g*D 3, T 12 = 29,
 # plus the per-triangle-pair W update 63 flops / 9 point pairs = 7.
 FLOPS_PER_POINT_PAIR_RH = 36.0
+# DRAM bytes of one far_main_rh2 launch on the 59,858-triangle surface (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum, one full-size capture): the
+# kernel reads its source records through L2 and is compute-bound
+FAR_TRAFFIC_BYTES = 14.586e6
 
 
 def c2_mesh(n=174, seed=2):
@@ -2247,7 +2251,9 @@ def main():
                 "kernel": "far_main_rh2<3, uniform> (packed f32x2 elasticRH3 tri-to-tri "
                           "farfield)",
                 "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak, "traffic": FAR_TRAFFIC_BYTES,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "full-size launch (profiles/far_main_rh2_c2_full.md)",
                 "peak_source": "measured live: best of the FP32 FMA probes (scalar FFMA "
                                "%.1f, packed fma.rn.f32x2 %.1f TFLOP/s); MEASURED_PEAKS.json "
                                "has no FP32 figure" % (peak_ffma, peak_ffma2),
