@@ -10,6 +10,12 @@
 // (FP32) or 256-byte (FP64) transaction; x is gathered through L1/L2 (it is
 // 9 Reals per triangle and stays cache resident).  Each lane keeps 9 row
 // partial sums, reduced across the warp with shuffles at the end of the row.
+//
+// Slots with a negative column index are padding: the operator's matrix
+// starts every block row on a sector boundary of the element planes, so a
+// row's loads never share a 32-byte sector with another row or with another
+// step of the same row.  Unpadded, each such shared sector is fetched from
+// DRAM once per reader (1.35x the algorithmic bytes at ~90 blocks per row).
 #include <algorithm>
 
 #include "common.cuh"
@@ -38,11 +44,7 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
     const int sub = lane % LPR;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // each warp takes a contiguous range of row groups, in order: the
-    // 128-byte line that the end of one row's segment of an element plane
-    // shares with the start of the next row's is then read twice by the same
-    // warp, a few microseconds apart (an L2 hit), not by two warps at once
-    // (two DRAM fetches: 1.35x the algorithmic bytes at ~90 blocks per row)
+    // each warp takes a contiguous range of row groups, in order
     const int64_t n_groups = (n_rows + G - 1) / G;
     const int64_t per_warp = (n_groups + n_warps - 1) / n_warps;
     const int64_t g_end = min(n_groups, (warp + 1) * per_warp);
@@ -59,6 +61,7 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
         for (int i = 0; i < 9; i++) acc[i] = 0;
         for (int32_t s = start + sub; s < end; s += LPR) {
             const int64_t col = __ldg(indices + s);
+            if (col < 0) continue;  // padding slot
             R xv[9];
 #pragma unroll
             for (int j = 0; j < 9; j++) xv[j] = __ldg(x + col * 9 + j);
@@ -177,6 +180,7 @@ bsr9_panel_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             for (int i = 0; i < 9; i++) acc[v][i] = 0;
         for (int32_t s = start + lane; s < end; s += 32) {
             const int64_t col9 = (int64_t)__ldg(indices + s) * 9;
+            if (col9 < 0) continue;  // padding slot
 #pragma unroll 1
             for (int j = 0; j < 9; j++) {
                 R a[9];

@@ -162,17 +162,17 @@ class RegularizedNearfieldIntegralOp:
         indptr = np.zeros(n_row_blocks + 1, dtype=np.int64)
         np.add.at(indptr, rows + 1, 1)
         indptr = np.cumsum(indptr)
-        self.bsr = DeviceBSR9(self.shape, indptr, cols[order], float_type)
-        self.class_slots = {}
+        self.bsr = DeviceBSR9(self.shape, indptr, cols[order], float_type, row_align="auto")
+        self.class_slots = {}  # CSR positions of each class's blocks
         start = 0
         for c in CLASSES:
             n = self.classes[c][1].shape[0]
             self.class_slots[c] = slot[start:start + n]
             start += n
-        self.correction = device.zeros(max(81 * self.bsr.nnzb, 1), float_type) \
+        self.correction = device.zeros(81 * self.bsr.stride, float_type) \
             if keep_uncorrected else None
 
-        stride = max(self.bsr.nnzb, 1)
+        stride = self.bsr.stride
         self.n_pairs = {c: self.classes[c][1].shape[0] for c in CLASSES}
         if batched:
             self._integrate_batched(pairs_int, corr_int, nq_coincident, nq_edge_adj,
@@ -193,7 +193,7 @@ class RegularizedNearfieldIntegralOp:
                 continue
             rule, adj, check0 = rules[c]
             rec_dev = device.to_dev(np.ascontiguousarray(recs[:, :5 if adj else 2]), np.int32)
-            slot_dev = device.to_dev(self.class_slots[c], np.int32)
+            slot_dev = device.to_dev(self.bsr.slots(self.class_slots[c]), np.int32)
             pairs_int.integrate_into(self.bsr.data, rule, rec_dev, n, adj, check0,
                                      slot=slot_dev, slot_stride=stride)
             base_dev = rec_dev if not adj else device.to_dev(
@@ -236,7 +236,7 @@ class RegularizedNearfieldIntegralOp:
             r5 = recs[:, :5] if adj else base
             groups.append((r5, (qp, qw, adj, check0)))
             corr_groups.append((base, (far_q[0], far_q[1], False, c == "co")))
-            slots.append(self.class_slots[c])
+            slots.append(self.bsr.slots(self.class_slots[c]))
         if not groups:
             return
         slot_dev = device.to_dev(np.concatenate(slots).astype(np.int32))

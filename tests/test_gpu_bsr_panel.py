@@ -7,14 +7,14 @@ import torch
 
 import tectosaur_b200 as tct
 from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
-from tectosaur_b200.util.sparse import DeviceBSR9, make_bsr_index
+from tectosaur_b200.util.sparse import DeviceBSR9, auto_row_align, make_bsr_index
 
 from helpers import PARAMS, bumpy_mesh, rel
 
 pytestmark = pytest.mark.gpu
 
 
-def _random_bsr(n_rows, n_cols, nnz, ft, seed):
+def _random_bsr(n_rows, n_cols, nnz, ft, seed, row_align=1):
     rng = np.random.default_rng(seed)
     rows = rng.integers(0, n_rows, nnz)
     cols = rng.integers(0, n_cols, nnz)
@@ -22,10 +22,40 @@ def _random_bsr(n_rows, n_cols, nnz, ft, seed):
     rows[rows == 1] = 0
     rows[:70] = 2
     indptr, indices, slot = make_bsr_index(n_rows, rows, cols)
-    m = DeviceBSR9((9 * n_rows, 9 * n_cols), indptr, indices, ft)
+    m = DeviceBSR9((9 * n_rows, 9 * n_cols), indptr, indices, ft, row_align=row_align)
     blocks = rng.standard_normal((nnz, 81))
-    m.data.copy_(torch.from_numpy(np.ascontiguousarray(blocks.T).ravel()).to(m.data.dtype))
+    planes = torch.from_numpy(np.ascontiguousarray(blocks.T)).to(m.data.dtype).cuda()
+    if m.pos is None:
+        m.data.copy_(planes.reshape(-1))
+    else:
+        m.data.view(81, m.stride)[:, torch.from_numpy(m.pos).cuda()] = planes
     return m
+
+
+@pytest.mark.parametrize("ft", [np.float32, np.float64])
+@pytest.mark.parametrize("align", [8, 32])
+def test_padded_rows_match_unpadded(cuda, ft, align):
+    """Rows padded to `align` slots: the same lane takes the same block of a
+    row as unpadded, so single and panel applies agree bit for bit, and the
+    padding (index -1) is never read."""
+    a = _random_bsr(300, 250, 6000, ft, seed=3)
+    b = _random_bsr(300, 250, 6000, ft, seed=3, row_align=align)
+    assert b.stride % align == 0 and b.stride > b.nnzb
+    assert torch.all(b.indices.view(-1)[torch.from_numpy(b.pos).cuda()] >= 0)
+    assert int((b.indices < 0).sum()) == b.stride - b.nnzb
+    # poison the padding: a padded slot that were read would show
+    pad = torch.ones(b.stride, dtype=torch.bool, device="cuda")
+    pad[torch.from_numpy(b.pos).cuda()] = False
+    b.data.view(81, b.stride)[:, pad] = float("nan")
+    tdt = torch.float32 if ft == np.float32 else torch.float64
+    x = torch.randn(9 * 250, dtype=tdt, device="cuda")
+    assert torch.equal(a.matvec(x, torch.empty(9 * 300, dtype=tdt, device="cuda")),
+                       b.matvec(x, torch.empty(9 * 300, dtype=tdt, device="cuda")))
+    X = torch.randn((5, 9 * 250), dtype=tdt, device="cuda")
+    Ya = a.matvec_panel(X, torch.empty((5, 9 * 300), dtype=tdt, device="cuda"))
+    Yb = b.matvec_panel(X, torch.empty((5, 9 * 300), dtype=tdt, device="cuda"))
+    assert torch.equal(Ya, Yb)
+    assert np.array_equal(a.blocks_host(), b.blocks_host())
 
 
 @pytest.mark.parametrize("ft", [np.float32, np.float64])
@@ -70,3 +100,20 @@ def test_operator_panel_matches_dot(cuda, ft):
     want = np.stack([op.dot(X[r]) for r in range(5)])
     tol = 1e-5 if ft == np.float32 else 1e-13
     assert rel(got, want) < tol
+
+
+def test_operator_nearfield_rows_padded(cuda):
+    """The operator's nearfield matrix pads its rows (their average length is
+    above the threshold) and gives the unpadded matrix's apply bit for bit."""
+    pts, tris = bumpy_mesh(10, seed=4)
+    op = tct.RegularizedSparseIntegralOp(3, 3, 3, 1, 3, 2.5, "elasticRH3", "elasticRH3", PARAMS,
+                                         pts, tris, np.float32, TriToTriDirectFarfieldOp)
+    bsr = op.nearfield.bsr
+    assert bsr.row_align == auto_row_align(bsr.n_row_blocks, bsr.nnzb) > 1
+    assert bsr.stride % bsr.row_align == 0 and bsr.stride >= bsr.nnzb
+    flat = DeviceBSR9(bsr.shape, bsr.indptr_host, bsr.indices_host, np.float32)
+    flat.data.copy_(torch.from_numpy(
+        np.ascontiguousarray(bsr.blocks_host().reshape(-1, 81).T).ravel()).cuda())
+    x = torch.randn(op.shape[1], device="cuda")
+    assert torch.equal(bsr.matvec(x, torch.empty(op.shape[0], device="cuda")),
+                       flat.matvec(x, torch.empty(op.shape[0], device="cuda")))
