@@ -44,6 +44,10 @@ FLOPS_PER_POINT_PAIR_RH = 36.0
 # dram__bytes_read.sum + dram__bytes_write.sum, one full-size capture): the
 # kernel reads its source records through L2 and is compute-bound
 FAR_TRAFFIC_BYTES = 14.586e6
+# DRAM bytes of one bsr9_kernel launch on the same surface's nearfield matrix
+# (5,477,848 blocks, rows aligned to 32 slots; one full-size capture):
+# 1.06x the algorithmic 1.801e9 bytes
+NEAR_TRAFFIC_BYTES = 1.9132e9
 
 
 def c2_mesh(n=174, seed=2):
@@ -109,6 +113,14 @@ class ClockSampler:
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (NVML initialisation) stalls the driver for
+        # up to a second: a timed region that overlapped it measured a C4
+        # near search at 0.93 s instead of 0.22 s; timing starts after the
+        # first sample
+        t0 = time.perf_counter()
+        while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 10.0:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -335,7 +347,7 @@ def fmm_algorithmic_flops(fmm, n_q):
     return p2p_pairs * FLOPS_PER_POINT_PAIR_RH + m2l, p2p_pairs, m2l
 
 
-def cpu_direct_far_baseline(pts, tris, target_s=10.0):
+def cpu_direct_far_baseline(pts, tris, target_s=10.0, K=None):
     """The direct farfield on the host cores (oracle restatement, FP32, all
     threads) for a sample of observation triangles against all sources,
     extrapolated to one full apply (the reference's FMM has no CPU path)."""
@@ -348,7 +360,7 @@ def cpu_direct_far_baseline(pts, tris, target_s=10.0):
     def t_sample(m):
         obs = np.sort(rng.choice(n, size=m, replace=False))
         t0 = time.perf_counter()
-        orc.farfield_tris(K_NAME, np.float32, q, pts, tris[obs], tris, x, PARAMS)
+        orc.farfield_tris(K or K_NAME, np.float32, q, pts, tris[obs], tris, x, PARAMS)
         return time.perf_counter() - t0
     probe = 16
     per = max(t_sample(probe) / probe, 1e-6)
@@ -987,13 +999,15 @@ def run_pairs_workload(args, rank, world, torch, dist):
 
 
 def run_panel_workload(args, rank, world, torch, dist):
-    """C2 farfield applied to a panel of R right-hand sides on the tensor cores."""
+    """C2 farfield (elasticRH3, or elasticRT3 with --panel-kernel) applied to
+    a panel of R right-hand sides on the tensor cores."""
     from tectosaur_b200.ops.sparse_farfield_op import TriToTriDirectFarfieldOp
     R = args.rhs
+    K = args.panel_kernel
     pts, tris = c2_mesh(args.grid or 174)
     n = tris.shape[0]
     idx = np.arange(n)
-    op = TriToTriDirectFarfieldOp(NQ["nq_far"], K_NAME, PARAMS, pts, tris, np.float32, idx, idx)
+    op = TriToTriDirectFarfieldOp(NQ["nq_far"], K, PARAMS, pts, tris, np.float32, idx, idx)
     X = torch.from_numpy(np.random.default_rng(3 + rank).standard_normal((R, 9 * n))
                          .astype(np.float32)).cuda()
     Y = torch.empty((R, 9 * n), dtype=torch.float32, device="cuda")
@@ -1048,14 +1062,24 @@ def run_panel_workload(args, rank, world, torch, dist):
     if rank != 0:
         return
     # executed tensor work: per panel of width w, 3 split-TF32 products of
-    # (n_obs padded to 128) x (7 n_src padded to 56) x 9w
+    # RH: (n_obs padded to 128) x (7 n_src padded to 56) x 9w;
+    # RT: (3 n_obs points padded to 128) x (10 n_src padded to 40) x 3w
     widths, r0 = [], 0
     while r0 < R:
         widths.append(16)
         r0 += 16
-    n_obs_p = (n + 127) // 128 * 128
-    n_src_p = (n + 7) // 8 * 8
-    mma_flops = sum(3 * 2.0 * n_obs_p * 7 * n_src_p * 9 * w for w in widths)
+    if K == "elasticRT3":
+        n_obs_p = (3 * n + 127) // 128 * 128
+        n_src_p = (n + 3) // 4 * 4
+        mma_flops = sum(3 * 2.0 * n_obs_p * 10 * n_src_p * 3 * w for w in widths)
+        kname, b_mb = "rt_main (tcgen05.mma kind::tf32, A in tensor memory, split TF32)", \
+            n_src_p * 10 * 3 * 16 * 8 / 1e6
+    else:
+        n_obs_p = (n + 127) // 128 * 128
+        n_src_p = (n + 7) // 8 * 8
+        mma_flops = sum(3 * 2.0 * n_obs_p * 7 * n_src_p * 9 * w for w in widths)
+        kname, b_mb = "mrhs_main<R> (tcgen05.mma kind::tf32, split TF32)", \
+            n_src_p * 7 * 9 * 16 * 8 / 1e6
     mp = measured_peaks()
     bf16 = mp.get("bf16_tflops") if mp else 1590.0
     tf32_peak = bf16 / 2.0
@@ -1067,17 +1091,17 @@ def run_panel_workload(args, rank, world, torch, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded mesh and inputs)",
         "config": {"workload": ("direct farfield of the 60k-triangle topographic surface "
-                                "(elasticRH3, 3-point rule) applied to a panel of %d N(0, 1) "
+                                "(%s, 3-point rule) applied to a panel of %d N(0, 1) "
                                 "vectors: kernel scalars on the CUDA cores, contraction with "
                                 "the panel by split-TF32 tcgen05.mma (panels of %s)"
-                                % (R, "+".join(str(w) for w in widths))),
+                                % (K, R, "+".join(str(w) for w in widths))),
+                   "kernel": K,
                    "n_tris": int(n), "rhs": R, "single_vector_ms": single_ms,
                    "speedup_vs_single_vector": single_ms * R / ms,
                    "rel_err_vs_single_vector_fp32": rel, "error_words": errs,
-                   "l2": "inputs larger than L2 (panel B operand %.0f MB)" % (
-                       n_src_p * 7 * 9 * max(widths) * 8 / 1e6),
+                   "l2": "inputs larger than L2 (panel B operand %.0f MB)" % b_mb,
                    "parallelism": "replicas"},
-        "roofline": {"kernel": "mrhs_main<R> (tcgen05.mma kind::tf32, split TF32)",
+        "roofline": {"kernel": kname,
                      "bound": "tensor", "achieved": achieved, "peak": tf32_peak,
                      "unit": "TFLOP/s", "frac": achieved / tf32_peak, "traffic": None,
                      "peak_source": "TF32 dense = half of the measured BF16 GEMM rate "
@@ -1091,7 +1115,7 @@ def run_panel_workload(args, rank, world, torch, dist):
         "clocks": clocks,
     }
     if not args.no_cpu_baseline:
-        cb = cpu_direct_far_baseline(pts, tris)
+        cb = cpu_direct_far_baseline(pts, tris, K=K)
         cb["unit"] = "vector applies/s"
         line["cpu_baseline"] = cb
     print(json.dumps(line), flush=True)
@@ -2124,6 +2148,8 @@ def main():
                          "C2 farfield on a panel of --rhs vectors (tensor cores); batch: "
                          "batched mixed-precision solves vs the plain FP64 solve")
     ap.add_argument("--rhs", type=int, default=64)
+    ap.add_argument("--panel-kernel", default="elasticRH3", choices=["elasticRH3", "elasticRT3"],
+                    help="kernel of the panel workload")
     ap.add_argument("--pairs", type=int, default=400_000)
     ap.add_argument("--qd-steps", type=int, default=200,
                     help="RK23 steps per quasidynamic integration (qd workload)")
@@ -2263,7 +2289,12 @@ def main():
             },
             "nearfield": {"ms": near_ms, "bytes": near_bytes,
                           "achieved_gbs": near_bytes / (near_ms * 1e-3) / 1e9 if near_ms > 0 else None,
-                          "hbm_peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json" if mp else "fallback"},
+                          "hbm_peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json" if mp else "fallback",
+                          "row_align": int(near.bsr.row_align), "slots": int(near.bsr.stride),
+                          "traffic": NEAR_TRAFFIC_BYTES if near.bsr.row_align == 32 else None,
+                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                            "of one full-size launch "
+                                            "(profiles/bsr9_fp32_c2.md)"},
             "e2e": e2e,
             "gpu_launches": args.steps * (2 + (1 if chunks > 1 else 0) + (1 if nnzb else 0)),
             "clocks": clocks,

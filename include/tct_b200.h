@@ -174,6 +174,9 @@ int tct_farfield_tris_dense(int kernel, int prec, void* out, int n_quad,
  * structure-of-arrays order, element e (= i*9 + j) of block s at
  * data[e * data_stride + s], data_stride >= nnzb.
  * y[9*r + i] (+)= sum_{s in row r} sum_j A_s[i][j] x[9*indices[s] + j].
+ * A slot whose index is negative is padding and is skipped (its data is
+ * not read): rows may start on 32-byte sector boundaries of the element
+ * planes, so that no sector holds the blocks of two rows.
  * With data2 != NULL the blocks are data + data2 (no-correction form). */
 int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
                     const int32_t* indices, const void* data, const void* data2,
@@ -441,6 +444,25 @@ int tct_farfield_rh_panel_matvec(void* out, const void* in, const void* pts,
 /* Reads (synchronising the stream) the error word of the last panel apply
  * with this workspace: 0 = ok, 1 = a bounded wait on the tensor cores gave up. */
 int tct_farfield_rh_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
+                                int n_q, void* stream, int* host_flag);
+
+/* The same for elasticRT3 (FP32, n_q = 3; R = 16): the RT kernel's sums
+ * over the source points of one source triangle are linear in the source
+ * triangle's curl of the input and the input at its points, with
+ * coefficients (per observation point: sum 1/r, sum D D^T / r^3 and
+ * (n_s . D) / r^3 per source point) generated on the CUDA cores straight
+ * into tensor memory and contracted with the input panel by tcgen05.mma
+ * (A from tensor memory, split TF32, Kahan-folded accumulation).  Replaces
+ * R calls of farfield_tris_to_tris{elasticRT3} (matrix_free.cl:19-107).
+ * Same arguments, workspace and error word as the RH form. */
+size_t tct_farfield_rt_panel_workspace_bytes(int64_t n_obs, int64_t n_src, int R, int n_q);
+int tct_farfield_rt_panel_matvec(void* out, const void* in, const void* pts,
+                                 const int32_t* obs_tris, int64_t n_obs,
+                                 const int32_t* src_tris, int64_t n_src, int R, int n_q,
+                                 const double* quad_pts, const double* quad_wts,
+                                 const double* params, int accumulate, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+int tct_farfield_rt_panel_error(const void* workspace, int64_t n_obs, int64_t n_src, int R,
                                 int n_q, void* stream, int* host_flag);
 
 /* Point farfield on R = 16 weight vectors at once (FP32 elasticU3/T3/A3/H3;

@@ -216,6 +216,10 @@ _SOLVE_SIGS = {
     "tct_farfield_rh_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_dp, c_dp,
                                       c_dp, c_i, c_p, c_sz, c_p], c_i),
     "tct_farfield_rh_panel_error": ([c_p, c_i64, c_i64, c_i, c_i, c_p, ctypes.POINTER(c_i)], c_i),
+    "tct_farfield_rt_panel_workspace_bytes": ([c_i64, c_i64, c_i, c_i], c_sz),
+    "tct_farfield_rt_panel_matvec": ([c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_i, c_i, c_dp, c_dp,
+                                      c_dp, c_i, c_p, c_sz, c_p], c_i),
+    "tct_farfield_rt_panel_error": ([c_p, c_i64, c_i64, c_i, c_i, c_p, ctypes.POINTER(c_i)], c_i),
 }
 for _name, (_args, _res) in _SOLVE_SIGS.items():
     _f = getattr(lib, _name)

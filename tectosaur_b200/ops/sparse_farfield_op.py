@@ -73,21 +73,31 @@ class TriToTriDirectFarfieldOp:
 
     # -- many right-hand sides ------------------------------------------------
     def panel_supported(self):
-        """The tensor-core panel path: elasticRH3, FP32, a 3-, 4- or 7-point rule."""
-        return (self.K_name == "elasticRH3" and self.prec == _lib.TCT_F32
-                and self.n_q in (3, 4, 7))
+        """The tensor-core panel path: FP32 elasticRH3 (a 3-, 4- or 7-point
+        rule) or elasticRT3 (a 3-point rule)."""
+        if self.prec != _lib.TCT_F32:
+            return False
+        return ((self.K_name == "elasticRH3" and self.n_q in (3, 4, 7))
+                or (self.K_name == "elasticRT3" and self.n_q == 3))
+
+    def _panel_fns(self):
+        pre = "tct_farfield_rh_panel" if self.K_name == "elasticRH3" else "tct_farfield_rt_panel"
+        return (getattr(_lib.lib, pre + "_workspace_bytes"), getattr(_lib.lib, pre + "_matvec"),
+                getattr(_lib.lib, pre + "_error"), pre)
 
     def dot_panel_device(self, X, Y, accumulate=False, stream=None):
         """Y[r] (+)= Far X[r] for device tensors X (R, 9 n_src), Y (R, 9 n_obs).
-        elasticRH3 / FP32 (3-, 4- or 7-point rule) runs on the tensor cores in panels
-        of 16 vectors (split TF32, compensated FP32 accumulation); other
-        kernels apply dot_device vector by vector."""
+        FP32 elasticRH3 (3-, 4- or 7-point rule) and elasticRT3 (3-point
+        rule) run on the tensor cores in panels of 16 vectors (split TF32,
+        compensated FP32 accumulation); other kernels apply dot_device
+        vector by vector."""
         t = device.torch()
         R = X.shape[0]
         if not self.panel_supported():
             for r in range(R):
                 self.dot_device(X[r].contiguous(), Y[r], accumulate=accumulate, stream=stream)
             return Y
+        ws_fn, mv_fn, _, name = self._panel_fns()
         r0 = 0
         while r0 < R:
             width = 16
@@ -101,18 +111,17 @@ class TriToTriDirectFarfieldOp:
                 (width, Y.shape[1]), dtype=Y.dtype, device=Y.device)
             if take != width and accumulate:
                 out[:take] = Y[r0:r0 + take]
-            nbytes = _lib.lib.tct_farfield_rh_panel_workspace_bytes(self.n_obs, self.n_src, width,
-                                                                    self.n_q)
+            nbytes = ws_fn(self.n_obs, self.n_src, width, self.n_q)
             ws = self._panel_ws.get(width)
             if ws is None or ws.numel() < nbytes:
                 ws = device.workspace(nbytes)
                 self._panel_ws[width] = ws
-            _lib.check(_lib.lib.tct_farfield_rh_panel_matvec(
+            _lib.check(mv_fn(
                 _lib.tptr(out), _lib.tptr(xin), _lib.tptr(self.gpu_pts),
                 _lib.tptr(self.gpu_obs_tris), self.n_obs, _lib.tptr(self.gpu_src_tris), self.n_src,
                 width, self.n_q, _lib.dptr(self.qx), _lib.dptr(self.qw), _lib.dptr(self.params),
                 int(bool(accumulate)), _lib.tptr(ws), nbytes,
-                _lib.stream_ptr(stream)), "tct_farfield_rh_panel_matvec")
+                _lib.stream_ptr(stream)), name + "_matvec")
             if take != width:
                 Y[r0:r0 + take] = out[:take]
             r0 += take
@@ -125,9 +134,10 @@ class TriToTriDirectFarfieldOp:
         ws = self._panel_ws.get(width)
         if ws is None:
             return 0
-        _lib.check(_lib.lib.tct_farfield_rh_panel_error(
+        _, _, err_fn, name = self._panel_fns()
+        _lib.check(err_fn(
             _lib.tptr(ws), self.n_obs, self.n_src, width, self.n_q, _lib.stream_ptr(stream),
-            ctypes.byref(flag)), "tct_farfield_rh_panel_error")
+            ctypes.byref(flag)), name + "_error")
         return flag.value
 
     def dot_panel(self, X):

@@ -128,8 +128,8 @@ class RegularizedSparseIntegralOp:
     def dot_panel_device(self, X, Y, stream=None, accumulate=False):
         """Y[r] (+)= (Far + Near) X[r] for device tensors X (R, 9 n_src),
         Y (R, 9 n_obs) of float_type (an addition: R vectors per apply; the
-        elasticRH3 FP32 farfield runs on the tensor cores, the nearfield BSR
-        in one launch)."""
+        FP32 elasticRH3 / elasticRT3 farfield runs on the tensor cores, the
+        nearfield BSR in one launch)."""
         far = self.farfield
         acc = bool(accumulate)
         if self._overlap_near() and not hasattr(far, "dot_panel_device"):

@@ -57,6 +57,29 @@ def test_make_bsr_index_matches_oracle(orc):
     assert np.array_equal(out, d2)
 
 
+def test_padded_rows_layout():
+    """Padded BSR rows: every row starts on a multiple of the alignment, the
+    blocks keep their CSR order inside the row, and the padding fills only
+    the gap up to the next row."""
+    from tectosaur_b200.util.sparse import auto_row_align, padded_rows
+    counts = np.array([0, 1, 7, 8, 9, 0, 33, 2])
+    indptr = np.concatenate([[0], np.cumsum(counts)])
+    pstart, pos = padded_rows(indptr, 8)
+    assert pstart.tolist() == [0, 0, 8, 16, 24, 40, 40, 80, 88]
+    for r in range(len(counts)):
+        k = np.arange(indptr[r], indptr[r + 1])
+        assert np.array_equal(pos[k], pstart[r] + np.arange(counts[r]))
+    assert np.unique(pos).shape[0] == pos.shape[0] == indptr[-1]
+    p1, q1 = padded_rows(indptr, 1)
+    assert np.array_equal(p1, indptr) and np.array_equal(q1, np.arange(indptr[-1]))
+    # mean padding (align - 1) / 2 at most a fifth of the mean row length
+    assert auto_row_align(100, 9150) == 32 and auto_row_align(100, 7750) == 32
+    assert auto_row_align(100, 7749) == 16 and auto_row_align(100, 3750) == 16
+    assert auto_row_align(100, 3749) == 8 and auto_row_align(100, 1750) == 8
+    assert auto_row_align(100, 1749) == 1 and auto_row_align(100, 150) == 1
+    assert auto_row_align(0, 0) == 1
+
+
 def test_mass_op_matches_reference(golden):
     from tectosaur_b200.ops.mass_op import MassOp
     g = golden("mass_op.npz")
@@ -71,3 +94,15 @@ def test_make_rect_matches_reference_order():
     pts, tris = make_rect(3, 3, [[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]])
     assert tris.shape == (8, 3)
     assert np.array_equal(tris[:4], [[0, 3, 1], [3, 4, 1], [3, 6, 4], [6, 7, 4]])
+
+
+def test_panel_workspace_sizes():
+    """The tensor-core panels report 0 bytes (unsupported) outside R = 16 and
+    their rules: RH 3/4/7 points, RT 3 points, point form any R = 16."""
+    from tectosaur_b200 import _lib
+    L = _lib.lib
+    assert L.tct_farfield_rt_panel_workspace_bytes(100, 100, 8, 3) == 0
+    assert L.tct_farfield_rt_panel_workspace_bytes(100, 100, 16, 4) == 0
+    assert L.tct_farfield_rt_panel_workspace_bytes(100, 100, 16, 3) > 0
+    assert L.tct_farfield_rh_panel_workspace_bytes(100, 100, 16, 5) == 0
+    assert L.tct_farfield_rh_panel_workspace_bytes(100, 100, 16, 7) > 0
