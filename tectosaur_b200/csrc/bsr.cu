@@ -12,10 +12,11 @@
 // partial sums, reduced across the warp with shuffles at the end of the row.
 //
 // Slots with a negative column index are padding: the operator's matrix
-// starts every block row on a sector boundary of the element planes, so a
-// row's loads never share a 32-byte sector with another row or with another
-// step of the same row.  Unpadded, each such shared sector is fetched from
-// DRAM once per reader (1.35x the algorithmic bytes at ~90 blocks per row).
+// starts every block row on a 128-byte line of the element planes, so a
+// row's loads never share a line with another row or with another step of
+// the same row.  Unpadded, each such shared line is fetched from DRAM once
+// per reader (1.35x the algorithmic bytes at ~90 blocks per row, 1.06x
+// padded).
 #include <algorithm>
 
 #include "common.cuh"
@@ -29,8 +30,8 @@ namespace {
 // the SM with no loads in flight.
 //
 // LPR lanes serve one block row (LPR = 32: a warp per row, the shape for
-// the operator's ~90 blocks per row; 16, 8 or 4: a warp serves 32 / LPR rows
-// at once, the shape for rows of a few blocks).  The row loop is
+// the operator's ~90 blocks per row; 16 down to 1: a warp serves 32 / LPR
+// rows at once, the shapes for rows of a few blocks).  The row loop is
 // warp-uniform -- every lane runs the same number of iterations, lanes past
 // the last row carry zeros -- so the shuffles always have the full warp.
 template <typename R, bool TWO, int LPR>
@@ -69,9 +70,9 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             for (int i = 0; i < 9; i++)
 #pragma unroll
                 for (int j = 0; j < 9; j++) {
-                    // default (L2-retaining) loads: a row's segment of each
-                    // element plane shares its first and last 128-byte lines
-                    // with the neighbouring rows, read by nearby warps
+                    // default (L2-retaining) loads: in an unpadded matrix a
+                    // row's segment of an element plane shares its first and
+                    // last lines with the neighbouring rows
                     R a = __ldg(data + (int64_t)(i * 9 + j) * stride + s);
                     if (TWO) a += __ldg(data2 + (int64_t)(i * 9 + j) * stride + s);
                     acc[i] += a * xv[j];
@@ -103,7 +104,7 @@ void bsr_shape(int prec, int64_t n_rows, int64_t stride, int* lpr, int* cps) {
     int v0 = 0, v1 = 0;
     const int64_t per_row = n_rows > 0 ? std::max<int64_t>(1, stride / n_rows) : 1;
     if (tune_lookup(kTuneBsr9, -1, prec, 0, 1, n_rows, per_row, &v0, &v1)) {
-        if (v0 == 32 || v0 == 16 || v0 == 8 || v0 == 4) *lpr = v0;
+        if (v0 == 32 || v0 == 16 || v0 == 8 || v0 == 4 || v0 == 2 || v0 == 1) *lpr = v0;
         if (v1 >= 1 && v1 <= 64) *cps = v1;
     }
 }
@@ -140,6 +141,10 @@ int run_bsr(int64_t n_rows, const int32_t* indptr, const int32_t* indices, const
         case 8: launch_bsr<R, 8>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
                                  accumulate, st); break;
         case 4: launch_bsr<R, 4>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                 accumulate, st); break;
+        case 2: launch_bsr<R, 2>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
+                                 accumulate, st); break;
+        case 1: launch_bsr<R, 1>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
                                  accumulate, st); break;
         default: launch_bsr<R, 32>(blocks, n_rows, indptr, indices, data, data2, stride, x, y,
                                    accumulate, st);
@@ -264,7 +269,7 @@ extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* 
     TCT_CHECK_ARG(lanes && ctas_per_sm, "tct_bsr9_autotune: null result pointer");
     TCT_CHECK_ARG(n_row_blocks > 0, "tct_bsr9_autotune: empty matrix");
     const int64_t per_row = std::max<int64_t>(1, data_stride / n_row_blocks);
-    static const int kLanes[] = {32, 16, 8, 4};
+    static const int kLanes[] = {32, 16, 8, 4, 2, 1};
     static const int kCtas[] = {4, 8, 16};
     cudaStream_t st = as_stream(stream);
     cudaEvent_t e0, e1;

@@ -49,7 +49,7 @@ constexpr int RT_C = 7 + RT_NQ;       // 10 A columns per source triangle
 constexpr int RT_S = 8;               // source triangles per tile
 constexpr int RT_K = RT_C * RT_S;     // 80: GEMM K per tile
 constexpr int RT_KSTEPS = RT_K / 8;   // tf32 MMA K = 8
-constexpr int RT_G = 4;               // A-generating warp groups (2 sources each)
+constexpr int RT_G = 2;               // A-generating warp groups (2 packed pairs each)
 constexpr int RT_FLUSH = 8;           // tiles per tensor-memory accumulation
 constexpr float RT_EPS = 1e-24f;
 constexpr int RT_COPIES = 4;          // bulk copies per B tile
@@ -192,27 +192,32 @@ rt_prep(Consts<float> c, Rule2D<float> rule, float wbar, const float* __restrict
 
 // ---- main: generate A into tensor memory, copy B, tcgen05.mma --------------
 // grid (point blocks of 128, source chunks); RT_G x 128 threads generate A
-// (thread (row, group): observation point `row`, the group's 2 of the tile's
-// 8 source triangles as one packed pair, whose records are loaded while the
-// previous tile is stored and issued), one more warp issues the B copies and the MMAs and polls their
-// barriers.  Per tile t: A(t) is generated in registers and stored to A
-// buffer t & 1 while the MMAs of t - 1 run (they read the other buffer;
-// those of t - 2 have completed); then, once the MMAs of t - 1 have
-// completed, the accumulator is folded when a group of RT_FLUSH tiles ends,
-// the B tile of t + 1 is issued into the buffer they read, and the MMAs of
-// t are issued.
+// (thread (row, group): observation point `row`, the group's 4 of the tile's
+// 8 source triangles as two packed pairs, their records loaded while the
+// previous tile is stored), one more warp issues the B copies and the MMAs.
+// Per tile t: A(t) is generated in registers while the MMAs of t - 1 run;
+// each thread waits (itself, on the mbarrier) for the MMAs of t - 2, which
+// read A buffer t & 1, and stores A(t) there; the B tile of t + 1 goes into
+// the B buffer those MMAs read (three B buffers); after one CTA barrier the
+// MMAs of t are issued behind those of t - 1.  At the end of each group of
+// RT_FLUSH tiles all MMAs complete and D is folded into the Kahan pair.
+// Measured on the 60k-triangle surface (16 vectors, 152 ms): timing copies
+// without the MMAs take 98 ms, without the A arithmetic 126 ms -- the
+// per-tile B traffic from L2 (every CTA of 128 points re-reads the 230 MB B
+// operand) and the per-tile barrier, not the arithmetic, set the pace.
 template <bool UNIFORM>
 __global__ void __launch_bounds__(128 * RT_G + 32, 1)
 rt_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __restrict__ obs_tris,
         int64_t n_pts, const float* __restrict__ srcy, int64_t n_tiles, int64_t tiles_per_chunk,
         const float* __restrict__ Bg, float* __restrict__ partial, int* __restrict__ err) {
-    constexpr int SG = RT_S / RT_G;  // source triangles per thread group (one packed pair)
-    constexpr int KG = RT_C * SG;    // 20 A values per thread and tile
-    static_assert(SG == 2, "one packed source pair per thread");
+    constexpr int SG = RT_S / RT_G;  // source triangles per thread group
+    constexpr int NP = SG / 2;       // packed source pairs per thread
+    constexpr int KG = RT_C * SG;    // A values per thread and tile
+    static_assert(SG % 2 == 0 && KG % 4 == 0, "whole packed pairs, 4-column stores");
     extern __shared__ __align__(128) unsigned char smem[];
-    unsigned char* Bs0 = smem;  // two B buffers, each hi then lo
-    __shared__ __align__(8) uint64_t bar_mma;
-    __shared__ __align__(8) uint64_t bar_b[2];
+    unsigned char* Bs0 = smem;  // three B buffers, each hi then lo
+    __shared__ __align__(8) uint64_t bar_m[2];
+    __shared__ __align__(8) uint64_t bar_b[3];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
 
@@ -237,22 +242,28 @@ rt_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __rest
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_mma)), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b[0])), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b[1])), "r"(1));
+        for (int i = 0; i < 2; i++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_m[i])),
+                         "r"(1));
+        for (int i = 0; i < 3; i++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_b[i])),
+                         "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_slot;
-    const uint32_t barm = smem_u32(&bar_mma);
-    const uint32_t barb0 = smem_u32(&bar_b[0]), barb1 = smem_u32(&bar_b[1]);
+    const uint32_t barm0 = smem_u32(&bar_m[0]), barm1 = smem_u32(&bar_m[1]);
+    const uint32_t barb0 = smem_u32(&bar_b[0]), barb1 = smem_u32(&bar_b[1]),
+                   barb2 = smem_u32(&bar_b[2]);
 
-    // this thread's observation point (packed, negated: D = y_pair + negx)
+    // this thread's observation point (packed, negated: D = y_pair + negx);
+    // a row past the last point sits 1e18 away, where every A entry
+    // underflows to 0 (r^-3 < 1e-54; or D = 0 against a padding source)
     f2_t negx[3];
     {
-        float x[3] = {0.f, 0.f, 0.f};
+        float x[3] = {1e18f, 1e18f, 1e18f};
         if (valid) {
             TriGeom<float> ot;
             load_tri(ot, pts, obs_tris, p / RT_NQ, 0, false, false);
@@ -271,17 +282,32 @@ rt_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __rest
     }
     const f2_t eps2 = pk(RT_EPS, RT_EPS);
 
-    uint32_t phase_m = 0, phase_b0 = 0, phase_b1 = 0;
-    bool pend0 = false, pend1 = false;  // CTA-uniform: B copies issued, not waited for
-    bool ok = true;                     // CTA-uniform
-    bool mma_pending = false;           // CTA-uniform: a commit not yet waited for
+    // Pipeline state, the same in every thread (each thread runs every wait
+    // itself): MMAs of tile t commit to bar_m[t & 1]; B tiles rotate through
+    // three buffers, so the copy of tile t + 1 needs only the MMAs of t - 2
+    // to have completed, and the MMAs of t queue behind those of t - 1.
+    uint32_t ph_m0 = 0, ph_m1 = 0, ph_b0 = 0, ph_b1 = 0, ph_b2 = 0;
+    bool pm0 = false, pm1 = false;              // MMA commit not yet observed
+    bool pb0 = false, pb1 = false, pb2 = false;  // B copy not yet observed
+    bool ok = true;                             // CTA-uniform after each barrier
     const uint32_t idesc = mr_instr_desc(RT_N);
     const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
     const uint32_t lane_base = tmem + lane_off;
     // this warp's accumulator columns in the fold and the epilogue
     const int col0 = (grp * (RT_N / 8) / RT_G) * 8, col1 = ((grp + 1) * (RT_N / 8) / RT_G) * 8;
+    auto wait_m = [&](int i, bool& good) {
+        if (i == 0 && pm0) {
+            good = mbar_wait(barm0, ph_m0) && good;
+            ph_m0 ^= 1;
+            pm0 = false;
+        } else if (i == 1 && pm1) {
+            good = mbar_wait(barm1, ph_m1) && good;
+            ph_m1 ^= 1;
+            pm1 = false;
+        }
+    };
     auto issue_b = [&](int64_t tile, int buf) {
-        const uint32_t bar = buf ? barb1 : barb0;
+        const uint32_t bar = buf == 0 ? barb0 : (buf == 1 ? barb1 : barb2);
         if (mma_lead) {
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                          "r"(RT_B_BYTES)
@@ -294,122 +320,142 @@ rt_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __rest
                 bulk_g2s(dst + cpy * (RT_B_BYTES / RT_COPIES),
                          src + cpy * (RT_B_BYTES / RT_COPIES), RT_B_BYTES / RT_COPIES, bar);
         }
-        if (buf) pend1 = true;
-        else pend0 = true;
+        if (buf == 0) pb0 = true;
+        else if (buf == 1) pb1 = true;
+        else pb2 = true;
     };
     // this thread's source pair record of tile t
-    const f2_t* recs = reinterpret_cast<const f2_t*>(srcy) + grp * RT_REC;
+    const f2_t* recs = reinterpret_cast<const f2_t*>(srcy) + grp * NP * RT_REC;
     constexpr int64_t REC_STRIDE = (RT_S / 2) * RT_REC;  // f2 values per tile
-    f2_t yc[RT_REC];
+    f2_t yc[NP][RT_REC];
     if (!mma_warp && t0 < t1) {
 #pragma unroll
-        for (int k = 0; k < RT_REC; k++) yc[k] = __ldg(recs + t0 * REC_STRIDE + k);
+        for (int sp = 0; sp < NP; sp++)
+#pragma unroll
+            for (int k = 0; k < RT_REC; k++)
+                yc[sp][k] = __ldg(recs + t0 * REC_STRIDE + sp * RT_REC + k);
     }
     if (t0 < t1) issue_b(t0, 0);
     for (int64_t t = t0; t < t1; t++) {
-        const int buf = (int)((t - t0) & 1);
+        const int64_t k = t - t0;
+        const int abuf = (int)(k & 1), bbuf = (int)(k % 3);
+        bool good = true;
+        if (k > 0 && k % RT_FLUSH == 0) {
+            // an accumulation group ends: its MMAs (up to those of t - 1)
+            // complete, then D is folded into the Kahan pair before the
+            // MMAs of t restart it
+            wait_m(0, good);
+            wait_m(1, good);
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (!mma_warp) tmem_fold<RT_N>(lane_base, col0, col1, k == RT_FLUSH);
+        }
+        float av[KG];
         if (!mma_warp) {
-            // A of the group's source pair for this point: 10 values per source
-            const f2_t n0 = yc[3 * RT_NQ], n1 = yc[3 * RT_NQ + 1], n2 = yc[3 * RT_NQ + 2];
-            f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
-            f2_t V[RT_NQ];
 #pragma unroll
-            for (int q2 = 0; q2 < RT_NQ; q2++) {
-                const f2_t D0 = add2(yc[3 * q2], negx[0]);
-                const f2_t D1 = add2(yc[3 * q2 + 1], negx[1]);
-                const f2_t D2 = add2(yc[3 * q2 + 2], negx[2]);
-                f2_t r2 = fma2(D0, D0, eps2);
-                r2 = fma2(D1, D1, r2);
-                r2 = fma2(D2, D2, r2);
-                float ra, rb;
-                upk(r2, ra, rb);
-                const f2_t ir = pk(rsqrtf(ra), rsqrtf(rb));
-                f2_t gg = mul2(mul2(ir, ir), ir);
-                if constexpr (!UNIFORM) gg = mul2(gg, wq2[q2]);
-                const f2_t g0 = mul2(gg, D0), g1 = mul2(gg, D1), g2 = mul2(gg, D2);
-                T00 = fma2(g0, D0, T00);
-                T01 = fma2(g0, D1, T01);
-                T02 = fma2(g0, D2, T02);
-                T11 = fma2(g1, D1, T11);
-                T12 = fma2(g1, D2, T12);
-                T22 = fma2(g2, D2, T22);
-                V[q2] = fma2(g2, n2, fma2(g1, n1, mul2(g0, n0)));
-            }
-            const f2_t S0 = add2(add2(T00, T11), T22);
-            const f2_t Tc[RT_C] = {S0, T00, T01, T02, T11, T12, T22, V[0], V[1], V[2]};
-            float av[KG];
+            for (int sp = 0; sp < NP; sp++) {
+                // A of one packed source pair for this point: 10 values per source
+                const f2_t* yr = yc[sp];
+                const f2_t n0 = yr[3 * RT_NQ], n1 = yr[3 * RT_NQ + 1], n2 = yr[3 * RT_NQ + 2];
+                f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
+                f2_t V[RT_NQ];
 #pragma unroll
-            for (int cc = 0; cc < RT_C; cc++) {
-                float va, vb;
-                upk(Tc[cc], va, vb);
-                av[cc] = valid ? va : 0.f;
-                av[RT_C + cc] = valid ? vb : 0.f;
+                for (int q2 = 0; q2 < RT_NQ; q2++) {
+                    const f2_t D0 = add2(yr[3 * q2], negx[0]);
+                    const f2_t D1 = add2(yr[3 * q2 + 1], negx[1]);
+                    const f2_t D2 = add2(yr[3 * q2 + 2], negx[2]);
+                    f2_t r2 = fma2(D0, D0, eps2);
+                    r2 = fma2(D1, D1, r2);
+                    r2 = fma2(D2, D2, r2);
+                    float ra, rb;
+                    upk(r2, ra, rb);
+                    const f2_t ir = pk(rsqrtf(ra), rsqrtf(rb));
+                    f2_t gg = mul2(mul2(ir, ir), ir);
+                    if constexpr (!UNIFORM) gg = mul2(gg, wq2[q2]);
+                    const f2_t g0 = mul2(gg, D0), g1 = mul2(gg, D1), g2 = mul2(gg, D2);
+                    T00 = fma2(g0, D0, T00);
+                    T01 = fma2(g0, D1, T01);
+                    T02 = fma2(g0, D2, T02);
+                    T11 = fma2(g1, D1, T11);
+                    T12 = fma2(g1, D2, T12);
+                    T22 = fma2(g2, D2, T22);
+                    V[q2] = fma2(g2, n2, fma2(g1, n1, mul2(g0, n0)));
+                }
+                const f2_t S0 = add2(add2(T00, T11), T22);
+                const f2_t Tc[RT_C] = {S0, T00, T01, T02, T11, T12, T22, V[0], V[1], V[2]};
+#pragma unroll
+                for (int cc = 0; cc < RT_C; cc++) {
+                    float va, vb;
+                    upk(Tc[cc], va, vb);
+                    av[2 * RT_C * sp + cc] = va;
+                    av[2 * RT_C * sp + RT_C + cc] = vb;
+                }
             }
             // the next tile's records: in flight while A is stored and the
-            // CTA waits for the MMAs and the B tile
+            // CTA waits for the B tile
             if (t + 1 < t1) {
 #pragma unroll
-                for (int k = 0; k < RT_REC; k++) yc[k] = __ldg(recs + (t + 1) * REC_STRIDE + k);
+                for (int sp = 0; sp < NP; sp++)
+#pragma unroll
+                    for (int q = 0; q < RT_REC; q++)
+                        yc[sp][q] = __ldg(recs + (t + 1) * REC_STRIDE + sp * RT_REC + q);
             }
-            // hi / lo parts into A buffer `buf`, columns [KG grp, KG (grp + 1));
-            // the MMAs that read this buffer (tile t - 2) completed before the
-            // last CTA barrier
+        }
+        // the MMAs of t - 2 read A buffer abuf and B buffer (k + 1) % 3
+        wait_m(abuf, good);
+        if (!mma_warp) {
+            // hi / lo parts into A buffer abuf, columns [KG grp, KG (grp + 1));
+            // lo is left in FP32: the MMA reads the top 19 bits of a TF32
+            // operand, so it is truncated there (|lo| <= 2^-11 |v|, its
+            // truncation <= 2^-21 |v|)
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t ahi = lane_base + RT_COL_A + 2 * RT_K * buf + KG * grp;
+            const uint32_t ahi = lane_base + RT_COL_A + 2 * RT_K * abuf + KG * grp;
 #pragma unroll
             for (int ch = 0; ch < KG / 4; ch++) {
                 float h[4], l[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     h[u] = tf32_round(av[4 * ch + u]);
-                    l[u] = tf32_round(av[4 * ch + u] - h[u]);
+                    l[u] = av[4 * ch + u] - h[u];
                 }
                 tmem_st4(ahi + 4 * ch, h[0], h[1], h[2], h[3]);
                 tmem_st4(ahi + RT_K + 4 * ch, l[0], l[1], l[2], l[3]);
             }
             asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         }
-        // the MMAs of tile t - 1 have read B buffer buf ^ 1 and A buffer buf ^ 1
-        if (mma_pending) {
-            const bool w = mma_warp ? mbar_wait(barm, phase_m) : true;
-            if (!__syncthreads_and(w)) {
-                ok = false;  // the MMAs of the previous tile did not complete in time
-                break;
-            }
-            phase_m ^= 1;
-            mma_pending = false;
-            if ((t - t0) % RT_FLUSH == 0) {
-                asm volatile("tcgen05.fence::after_thread_sync;");
-                if (!mma_warp) tmem_fold<RT_N>(lane_base, col0, col1, t - t0 == RT_FLUSH);
-            }
-        }
-        if (t + 1 < t1) issue_b(t + 1, buf ^ 1);
+        if (good && t + 1 < t1) issue_b(t + 1, (int)((k + 1) % 3));
         asm volatile("tcgen05.fence::before_thread_sync;");
         {
-            const bool wb = mma_warp ? mbar_wait(buf ? barb1 : barb0, buf ? phase_b1 : phase_b0)
-                                     : true;
-            if (!__syncthreads_and(wb)) {
-                ok = false;
-                break;
+            bool wb = true;
+            if (mma_warp) {
+                const uint32_t bar = bbuf == 0 ? barb0 : (bbuf == 1 ? barb1 : barb2);
+                const uint32_t ph = bbuf == 0 ? ph_b0 : (bbuf == 1 ? ph_b1 : ph_b2);
+                wb = mbar_wait(bar, ph);
             }
-            if (buf) {
-                phase_b1 ^= 1;
-                pend1 = false;
+            if (bbuf == 0) {
+                ph_b0 ^= 1;
+                pb0 = false;
+            } else if (bbuf == 1) {
+                ph_b1 ^= 1;
+                pb1 = false;
             } else {
-                phase_b0 ^= 1;
-                pend0 = false;
+                ph_b2 ^= 1;
+                pb2 = false;
+            }
+            if (!__syncthreads_and(good && wb)) {
+                ok = false;  // a bounded wait gave up
+                break;
             }
         }
         if (mma_lead) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t lboB = RT_N / 8 * 128;
-            const uint32_t bH = smem_u32(Bs0) + (uint32_t)buf * RT_B_BYTES,
+            const uint32_t bH = smem_u32(Bs0) + (uint32_t)bbuf * RT_B_BYTES,
                            bL = bH + RT_N * RT_K * 4;
-            const uint32_t aH = tmem + RT_COL_A + 2 * RT_K * buf, aL = aH + RT_K;
+            const uint32_t aH = tmem + RT_COL_A + 2 * RT_K * abuf, aL = aH + RT_K;
 #pragma unroll
             for (int ks = 0; ks < RT_KSTEPS; ks++) {
                 // D restarts at the first tile of every RT_FLUSH group
-                const uint32_t first = ((t - t0) % RT_FLUSH == 0 && ks == 0) ? 0u : 1u;
+                const uint32_t first = (k % RT_FLUSH == 0 && ks == 0) ? 0u : 1u;
                 const uint64_t dBh = mr_smem_desc(bH + 2 * ks * lboB, lboB, 128);
                 const uint64_t dBl = mr_smem_desc(bL + 2 * ks * lboB, lboB, 128);
                 mma_tf32_ts(tmem, aH + 8 * ks, dBh, idesc, first);
@@ -418,22 +464,26 @@ rt_main(Rule2D<float> rule, const float* __restrict__ pts, const int32_t* __rest
             }
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    barm)
+                    abuf ? barm1 : barm0)
                 : "memory");
         }
-        mma_pending = true;
+        if (abuf) pm1 = true;
+        else pm0 = true;
     }
-    if (ok && mma_pending) {
-        const bool w = mma_warp ? mbar_wait(barm, phase_m) : true;
-        if (!__syncthreads_and(w)) ok = false;
-        else mma_pending = false;
+    if (ok) {
+        bool good = true;
+        wait_m(0, good);
+        wait_m(1, good);
+        if (!__syncthreads_and(good)) ok = false;
     }
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
         // one more bounded wait for whatever is still in flight
-        if (mma_pending) mbar_wait(barm, phase_m);
-        if (pend0) mbar_wait(barb0, phase_b0);
-        if (pend1) mbar_wait(barb1, phase_b1);
+        if (pm0) mbar_wait(barm0, ph_m0);
+        if (pm1) mbar_wait(barm1, ph_m1);
+        if (pb0) mbar_wait(barb0, ph_b0);
+        if (pb1) mbar_wait(barb1, ph_b1);
+        if (pb2) mbar_wait(barb2, ph_b2);
     }
     asm volatile("tcgen05.fence::after_thread_sync;");
 
@@ -561,7 +611,7 @@ int run_rt(const Consts<float>& c, const Rule2D<float>& rule, float* out, const 
     const int64_t chunks = rt_chunks(n_pts, n_tiles);
     const int64_t per = (n_tiles + chunks - 1) / chunks;
     const int64_t real = (n_tiles + per - 1) / per;
-    const size_t smem = (size_t)2 * RT_B_BYTES;
+    const size_t smem = (size_t)3 * RT_B_BYTES;
     auto kfn = rt_main<UNIFORM>;
     if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
