@@ -566,6 +566,41 @@ int tct_qd_velocity_state_batch(int64_t n_dofs, int n_sys, const int32_t* vert_s
                                 double f0, double* velocity, int64_t velocity_stride,
                                 double* dstatedt, int64_t dstate_stride, void* stream);
 
+/* Fused element-wise steps of the batched derivative and RK23 step (no
+ * reference counterpart as kernels: qd/full_model.py:178-200 evaluates them
+ * with numpy; scipy's RK23 forms the stages).  Each rounds every value in
+ * the order of the element-wise expression it replaces (no fused
+ * multiply-add), so the results are bit-identical to it, except the error
+ * norm's sum of squares (a block reduction).  Device arrays; strides in
+ * elements.
+ * Slip deficit, cast to out_prec (TCT_F32 / TCT_F64):
+ *   out[r][i] = interior[i] * ((ts[r] * plate_rate) * inslipdir[i] - Y[r][i]),
+ *   i < n9 (the slip part of state row r). */
+int tct_qd_deficit_batch(int64_t n9, int n_sys, const double* ts, double plate_rate,
+                         const double* inslipdir, const double* interior, const double* Y,
+                         int64_t y_stride, int out_prec, void* out, int64_t out_stride,
+                         void* stream);
+/* Derivative rows: out[r] = (V[r], dstate[r]), or Y[r] * inf when Y[r] has a
+ * non-finite entry, a state entry (Y[r][n9 ..]) below 0 or above state_max,
+ * or V[r] a non-finite entry (full_model.py's rejection of such states). */
+int tct_qd_finish_batch(int64_t n9, int64_t n_state, int n_sys, const double* Y, int64_t y_stride,
+                        const double* V, int64_t v_stride, const double* dstate,
+                        int64_t ds_stride, double state_max, double* out, int64_t out_stride,
+                        void* stream);
+/* Stage combination: out[r][i] = y[r][i] + (((k0 c0 + k1 c1) + k2 c2) + k3 c3)[r][i] * h[r]
+ * for the first n_terms (1..4) terms; y may be NULL (no y term).  k,
+ * k_strides, coeffs: host arrays of n_terms (device row pointers). */
+int tct_qd_combine_batch(int64_t n, int n_sys, int n_terms, const double* const* k,
+                         const int64_t* k_strides, const double* coeffs, const double* h,
+                         const double* y, int64_t y_stride, double* out, int64_t out_stride,
+                         void* stream);
+/* Error norm of an RK23 attempt: norms[r] = || e / (tol + max(|y|, |y_new|) tol) ||_2
+ * with e = (combination of the terms) * h[r]. */
+int tct_qd_error_norm_batch(int64_t n, int n_sys, int n_terms, const double* const* k,
+                            const int64_t* k_strides, const double* coeffs, const double* h,
+                            const double* y, int64_t y_stride, const double* y_new,
+                            int64_t yn_stride, double tol, double* norms, void* stream);
+
 /* Conjugate gradients on a CSR matrix (int64 indices, double values) in one
  * CTA, x0 = 0, stopping when ||r|| < max(atol, rtol ||b||) or after maxiter
  * iterations: the scipy.sparse.linalg.cg solve of the constrained mass

@@ -208,6 +208,14 @@ _SOLVE_SIGS = {
                                      ctypes.c_double, c_i, c_p, c_i64, c_p, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_double, c_p, c_i64, c_p, c_i64,
                                      c_p], c_i),
+    "tct_qd_deficit_batch": ([c_i64, c_i, c_p, ctypes.c_double, c_p, c_p, c_p, c_i64, c_i, c_p,
+                              c_i64, c_p], c_i),
+    "tct_qd_finish_batch": ([c_i64, c_i64, c_i, c_p, c_i64, c_p, c_i64, c_p, c_i64,
+                             ctypes.c_double, c_p, c_i64, c_p], c_i),
+    "tct_qd_combine_batch": ([c_i64, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_p],
+                             c_i),
+    "tct_qd_error_norm_batch": ([c_i64, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64,
+                                 ctypes.c_double, c_p, c_p], c_i),
     "tct_cg_csr_batch": ([c_i64, c_i, c_p, c_p, c_p, c_p, c_i64, c_p, c_i64, c_p,
                           ctypes.c_double, ctypes.c_double, c_i, c_p, c_p], c_i),
     "tct_cg_csr": ([c_i64, c_p, c_p, c_p, c_p, c_p, c_p, ctypes.c_double, ctypes.c_double, c_i,

@@ -39,7 +39,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off",
 
 CU_SOURCES = ["pairs.cu", "pairs_batched.cu", "farfield.cu", "bsr.cu", "probe.cu", "noalloc.cu",
               "fmm.cu", "csr.cu", "far_mrhs.cu", "qd.cu", "interior.cu", "near.cu", "tune.cu", "tree_dev.cu", "pts_mrhs.cu",
-              "rt_mrhs.cu"]
+              "rt_mrhs.cu", "qd_batch.cu"]
 CXX_SOURCES = ["host.cpp"]
 HEADERS = ["common.cuh", "pair_math.cuh", "far_common.cuh", "near_plan.h", "octree.h", "tc_common.cuh"]
 

@@ -16,6 +16,8 @@ gives inf * y (the reference's signal to its time stepper to shrink the
 step); it is selected on the device.  Newton solves that stop at maxiter
 are counted on the device (newton_failures()).
 """
+import ctypes
+
 import numpy as np
 
 from .. import _lib
@@ -221,13 +223,16 @@ class FullspaceModel:
 
     def slip_to_traction_batch(self, D):
         """slip_to_traction for the rows of D (R, 9 n): one panel apply of H,
-        one CG launch with a CTA per row."""
+        one CG launch with a CTA per row.  The constrained mass solve runs on
+        H D instead of -H D and the sign goes into the final scale: every
+        step of the CSR products and of CG commutes exactly with negation,
+        so the result is bit-identical and two element-wise passes fewer."""
         t = device.torch()
         R = D.shape[0]
         X = D.to(self.H_dtype).contiguous()
         Yh = t.empty_like(X)
         self._panel(X, Yh)
-        rhs = (-Yh).to(t.float64)
+        rhs = Yh if Yh.dtype == t.float64 else Yh.to(t.float64)
         rc = t.empty((R, self.n_free), dtype=t.float64, device="cuda")
         self._csr_panel(self.cmT, rhs, rc)
         soln = t.empty_like(rc)
@@ -240,7 +245,7 @@ class FullspaceModel:
             10 * self.n_free, _lib.tptr(iters), _lib.stream_ptr()), "tct_cg_csr_batch")
         out = t.empty((R, 9 * self.n_tris), dtype=t.float64, device="cuda")
         self._csr_panel(self.cm, soln, out)
-        out *= self.cfg["sm"]
+        out *= -self.cfg["sm"]
         if self.cfg.get("only_x", False):
             out.view(R, -1, 3)[:, :, 1:] = 0.0
         return out
@@ -273,19 +278,35 @@ class FullspaceModel:
         return V, dstate
 
     def derivs_batch(self, ts, Y):
-        """derivs for R states at once: ts (R,) device float64, Y (R, n_y)."""
+        """derivs for R states at once: ts (R,) device float64, Y (R, n_y).
+        The slip deficit (cast to H's precision) and the derivative's
+        assembly with the rejection of non-finite or out-of-range states
+        are one fused launch each (tct_qd_deficit_batch,
+        tct_qd_finish_batch), bit-identical to the element-wise forms
+        plate = (ts rate) dir, deficit = interior (plate - slip);
+        where(bad, Y inf, (V, dstate))."""
         t = device.torch()
-        self.n_evals += Y.shape[0]
+        R = Y.shape[0]
+        self.n_evals += R
         n9 = 9 * self.n_tris
-        slip, state = Y[:, :n9], Y[:, n9:]
-        plate = (ts[:, None] * self.cfg["plate_rate"]) * self.d_inslipdir[None, :]
-        deficit = self.d_interior[None, :] * (plate - slip)
-        traction = self.slip_to_traction_batch(deficit)
+        if Y.stride(1) != 1:
+            Y = Y.contiguous()
+        ts = ts.contiguous()
+        state = Y[:, n9:]
+        D = t.empty((R, n9), dtype=self.H_dtype, device="cuda")
+        _lib.check(_lib.lib.tct_qd_deficit_batch(
+            n9, R, _lib.tptr(ts), float(self.cfg["plate_rate"]), _lib.tptr(self.d_inslipdir),
+            _lib.tptr(self.d_interior), _lib.tptr(Y), Y.stride(0),
+            _lib.prec_of(np.float32 if self.H_dtype == t.float32 else np.float64),
+            _lib.tptr(D), D.stride(0), _lib.stream_ptr()), "tct_qd_deficit_batch")
+        traction = self.slip_to_traction_batch(D)
         V, dstate = self.rate_state_solve_batch(traction, state)
-        bad = (~t.isfinite(Y).all(dim=1)) | (state < 0).any(dim=1) | (state > 1.2).any(dim=1) | \
-            (~t.isfinite(V).all(dim=1))
-        out = t.cat((V, dstate), dim=1)
-        return t.where(bad[:, None], Y * float("inf"), out)
+        out = t.empty((R, Y.shape[1]), dtype=t.float64, device="cuda")
+        _lib.check(_lib.lib.tct_qd_finish_batch(
+            n9, Y.shape[1] - n9, R, _lib.tptr(Y), Y.stride(0), _lib.tptr(V), V.stride(0),
+            _lib.tptr(dstate), dstate.stride(0), 1.2, _lib.tptr(out), out.stride(0),
+            _lib.stream_ptr()), "tct_qd_finish_batch")
+        return out
 
     def newton_failures(self, reset=True):
         """DOFs whose Newton iteration stopped at maxiter since the last call
@@ -301,3 +322,38 @@ class FullspaceModel:
     @property
     def last_cg_iterations(self):
         return int(self._cg_iters.item())
+
+
+def _terms(Ks, coeffs):
+    n = len(Ks)
+    for k in Ks:
+        if k.dtype != device.torch().float64 or k.stride(1) != 1:
+            raise ValueError("RK terms: float64 rows with unit stride")
+    return (n, (ctypes.c_void_p * n)(*[k.data_ptr() for k in Ks]),
+            (ctypes.c_int64 * n)(*[k.stride(0) for k in Ks]),
+            (ctypes.c_double * n)(*[float(c) for c in coeffs]))
+
+
+def combine_batch(Ks, coeffs, h, y, out):
+    """out = y + (((K0 c0 + K1 c1) + K2 c2) + K3 c3) * h[:, None] for 1-4
+    (R, n) float64 terms (y None: no y term), rounded as that element-wise
+    expression; one launch (tct_qd_combine_batch)."""
+    n, kp, ks, cs = _terms(Ks, coeffs)
+    R, m = out.shape
+    _lib.check(_lib.lib.tct_qd_combine_batch(
+        m, R, n, kp, ks, cs, _lib.tptr(h.contiguous()), _lib.tptr(y) if y is not None else None,
+        y.stride(0) if y is not None else 0, _lib.tptr(out), out.stride(0), _lib.stream_ptr()),
+        "tct_qd_combine_batch")
+    return out
+
+
+def error_norm_batch(Ks, coeffs, h, y, y_new, tol, out):
+    """out[r] = || (combination of the terms) h[r] / (tol + max(|y|, |y_new|) tol) ||_2
+    per row (tct_qd_error_norm_batch)."""
+    n, kp, ks, cs = _terms(Ks, coeffs)
+    R, m = y.shape
+    _lib.check(_lib.lib.tct_qd_error_norm_batch(
+        m, R, n, kp, ks, cs, _lib.tptr(h.contiguous()), _lib.tptr(y), y.stride(0),
+        _lib.tptr(y_new), y_new.stride(0), float(tol), _lib.tptr(out), _lib.stream_ptr()),
+        "tct_qd_error_norm_batch")
+    return out

@@ -367,8 +367,9 @@ class QdEngine:
 
     def __init__(self, model, slots=16, stream=None):
         t = device.torch()
+        from .qd import model as qd_model
         from .qd import rk23 as rk
-        self.t, self.rk = t, rk
+        self.t, self.rk, self.qm = t, rk, qd_model
         self.model = model
         self.derivs = model.derivs_batch
         self.S = int(slots)
@@ -382,6 +383,7 @@ class QdEngine:
         self.rejected_now = np.zeros(self.S, bool)
         self.req = [None] * self.S
         self._norms = t.zeros(self.S, dtype=t.float64, pin_memory=True)
+        self._ndev = t.zeros(self.S, dtype=t.float64, device="cuda")
         self._tpin = t.zeros((4, self.S), dtype=t.float64, pin_memory=True)
         self._tdev = t.zeros((4, self.S), dtype=t.float64, device="cuda")
         self._ipin = t.zeros(self.S, dtype=t.int64, pin_memory=True)
@@ -462,15 +464,22 @@ class QdEngine:
             self._tdev.copy_(self._tpin, non_blocking=True)
             self._idev.copy_(self._ipin, non_blocking=True)
             idx = self._idev[:k]
-            hd = self._tdev[0, :k][:, None]
+            h = self._tdev[0, :k]
             y, K0 = self.Y[idx], self.F[idx]
-            K1 = self.derivs(self._tdev[1, :k], y + (K0 * rk.A[1][0]) * hd)
-            K2 = self.derivs(self._tdev[2, :k], y + (K0 * rk.A[2][0] + K1 * rk.A[2][1]) * hd)
-            y_new = y + hd * (K0 * rk.B[0] + K1 * rk.B[1] + K2 * rk.B[2])
+            # stage inputs, the new state and the error norm: one fused
+            # launch each, rounded as y + (K0 a10) h, y + (K0 a20 + K1 a21) h,
+            # y + h (K0 b0 + K1 b1 + K2 b2), ||(sum_j K_j e_j) h / scale||
+            ys = t.empty_like(y)
+            self.qm.combine_batch([K0], [rk.A[1][0]], h, y, ys)
+            K1 = self.derivs(self._tdev[1, :k], ys)
+            self.qm.combine_batch([K0, K1], [rk.A[2][0], rk.A[2][1]], h, y, ys)
+            K2 = self.derivs(self._tdev[2, :k], ys)
+            y_new = t.empty_like(y)
+            self.qm.combine_batch([K0, K1, K2], rk.B[:3], h, y, y_new)
             f_new = self.derivs(self._tdev[3, :k], y_new)
-            err = (K0 * rk.E[0] + K1 * rk.E[1] + K2 * rk.E[2] + f_new * rk.E[3]) * hd
-            scale = self.tol + t.maximum(y.abs(), y_new.abs()) * self.tol
-            self._norms[:k].copy_(t.linalg.norm(err / scale, dim=1), non_blocking=True)
+            self.qm.error_norm_batch([K0, K1, K2, f_new], rk.E[:4], h, y, y_new, self.tol,
+                                     self._ndev[:k])
+            self._norms[:k].copy_(self._ndev[:k], non_blocking=True)
             self._event.record()
         self._pending = (act, h, y_new, f_new)
 

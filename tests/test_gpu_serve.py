@@ -129,3 +129,90 @@ def test_qd_same_alone_and_in_mix(cuda):
     assert r1.steps == r0.steps == 12
     np.testing.assert_allclose(r1.ts, r0.ts, rtol=1e-9)
     assert np.linalg.norm(r1.y - r0.y) / np.linalg.norm(r0.y) < 1e-9
+
+
+def _elementwise_derivs(model, ts, Y):
+    """The batched derivative as element-wise tensor operations (deficit,
+    -H D through the constrained mass solve, rate-state, rejection)."""
+    import torch as t
+    n9 = 9 * model.n_tris
+    slip, state = Y[:, :n9], Y[:, n9:]
+    plate = (ts[:, None] * model.cfg["plate_rate"]) * model.d_inslipdir[None, :]
+    deficit = model.d_interior[None, :] * (plate - slip)
+    X = deficit.to(model.H_dtype).contiguous()
+    Yh = t.empty_like(X)
+    model._panel(X, Yh)
+    rhs = (-Yh).to(t.float64)
+    R = Y.shape[0]
+    rc = t.empty((R, model.n_free), dtype=t.float64, device="cuda")
+    model._csr_panel(model.cmT, rhs, rc)
+    soln = t.empty_like(rc)
+    work = t.empty(3 * max(model.n_free, 1) * R, dtype=t.float64, device="cuda")
+    iters = t.empty(R, dtype=t.int32, device="cuda")
+    ip, ix, dv = model.mass_c
+    _lib.check(_lib.lib.tct_cg_csr_batch(
+        model.n_free, R, _lib.tptr(ip), _lib.tptr(ix), _lib.tptr(dv), _lib.tptr(rc),
+        rc.stride(0), _lib.tptr(soln), soln.stride(0), _lib.tptr(work), 1e-5, 1e-12,
+        10 * model.n_free, _lib.tptr(iters), _lib.stream_ptr()), "cg")
+    traction = t.empty((R, n9), dtype=t.float64, device="cuda")
+    model._csr_panel(model.cm, soln, traction)
+    traction *= model.cfg["sm"]
+    V, dstate = model.rate_state_solve_batch(traction, state)
+    bad = (~t.isfinite(Y).all(dim=1)) | (state < 0).any(dim=1) | (state > 1.2).any(dim=1) | \
+        (~t.isfinite(V).all(dim=1))
+    return t.where(bad[:, None], Y * float("inf"), t.cat((V, dstate), dim=1))
+
+
+@pytest.mark.parametrize("ft", [np.float64, np.float32])
+def test_fused_derivs_batch_bit_identical(cuda, ft):
+    """derivs_batch's fused deficit / rejection kernels and the sign folded
+    into the traction scale give the element-wise computation bit for bit,
+    rejected rows (a NaN, a state above 1.2, a negative state) included."""
+    import torch as t
+    pts, tris, cfg, model, y0s = _qd_setup(ft)
+    nt = tris.shape[0]
+    rng = np.random.default_rng(5)
+    Y = np.stack([np.concatenate([1e-3 * rng.standard_normal(9 * nt),
+                                  0.7 + 0.05 * rng.standard_normal(3 * nt)]) for _ in range(5)])
+    Y[1, 3] = np.nan
+    Y[2, 9 * nt + 4] = 1.3
+    Y[3, 9 * nt] = -0.1
+    Yd = t.from_numpy(Y).cuda()
+    ts = t.from_numpy(rng.uniform(0, 1e7, 5)).cuda()
+    got = model.derivs_batch(ts, Yd)
+    want = _elementwise_derivs(model, ts, Yd)
+    t.testing.assert_close(got, want, rtol=0, atol=0, equal_nan=True)
+    assert t.isinf(got[2]).any() and t.isinf(got[3]).any() and not t.isfinite(got[1]).all()
+    assert t.isfinite(got[0]).all() and t.isfinite(got[4]).all()
+
+
+def test_fused_rk_combinations(cuda):
+    """The RK23 stage combinations bit for bit against their element-wise
+    expressions; the error norm to rounding."""
+    import torch as t
+    from tectosaur_b200.qd import model as qm, rk23 as rk
+    rng = np.random.default_rng(6)
+    R, n = 7, 3001
+    y, K0, K1, K2, f = [t.from_numpy(rng.standard_normal((R, n))).cuda() for _ in range(5)]
+    K1[2, 7] = float("inf")
+    h = t.from_numpy(rng.uniform(1e-3, 1e3, R)).cuda()
+    hd = h[:, None]
+    out = t.empty_like(y)
+    cases = [([K0], [rk.A[1][0]], y + (K0 * rk.A[1][0]) * hd),
+             ([K0, K1], [rk.A[2][0], rk.A[2][1]], y + (K0 * rk.A[2][0] + K1 * rk.A[2][1]) * hd),
+             ([K0, K1, K2], rk.B[:3], y + hd * (K0 * rk.B[0] + K1 * rk.B[1] + K2 * rk.B[2]))]
+    for Ks, cs, want in cases:
+        qm.combine_batch(Ks, cs, h, y, out)
+        t.testing.assert_close(out, want, rtol=0, atol=0, equal_nan=True)
+    qm.combine_batch([K0, K2], [0.3, -0.7], h, None, out)
+    t.testing.assert_close(out, (K0 * 0.3 + K2 * -0.7) * hd, rtol=0, atol=0)
+    y_new = y + 0.01 * K2
+    tol = 1e-4
+    err = (K0 * rk.E[0] + K1 * rk.E[1] + K2 * rk.E[2] + f * rk.E[3]) * hd
+    scale = tol + t.maximum(y.abs(), y_new.abs()) * tol
+    want = t.linalg.norm(err / scale, dim=1)
+    norms = t.empty(R, dtype=t.float64, device="cuda")
+    qm.error_norm_batch([K0, K1, K2, f], rk.E[:4], h, y, y_new, tol, norms)
+    assert not t.isfinite(norms[2]) and not t.isfinite(want[2])
+    ok = t.arange(R, device="cuda") != 2
+    t.testing.assert_close(norms[ok], want[ok], rtol=1e-13, atol=0)
