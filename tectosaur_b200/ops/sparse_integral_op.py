@@ -21,9 +21,10 @@ class RegularizedSparseIntegralOp:
         """row_range=(r0, r1) (an addition, for row shards): the operator is
         block rows r0..r1-1 of the one over obs_subset x src_subset -- the
         same near pairs and blocks (the search runs over the whole
-        obs_subset) and the farfield of those observation triangles -- so
-        stacking the applies of a partition of the rows gives the full
-        operator's apply."""
+        obs_subset) and the farfield of those observation triangles (an FMM
+        farfield: the whole set's trees and lists, evaluated on the leaves
+        that hold the rows) -- so stacking the applies of a partition of the
+        rows gives the full operator's apply."""
         tris = np.asarray(tris)
         if obs_subset is None:
             obs_subset = np.arange(tris.shape[0])
@@ -37,19 +38,26 @@ class RegularizedSparseIntegralOp:
             nq_coincident, nq_edge_adj, nq_vert_adjacent, nq_far, nq_near,
             near_threshold, K_near_name, K_far_name, params, float_type,
             keep_uncorrected=keep_uncorrected, row_range=row_range, batched=batched)
-        far_obs = obs_subset if row_range is None else obs_subset[row_range[0]:row_range[1]]
-        self.farfield = farfield_op_type(
-            nq_far, K_far_name, params, pts, tris, float_type, far_obs, src_subset)
-        if row_range is not None:
-            from ..fmm.tsfmm import FMMFarfieldOpImpl
-            if isinstance(self.farfield, FMMFarfieldOpImpl):
-                raise ValueError("row_range: the FMM farfield builds its trees and lists per "
-                                 "observation set, so its rows cannot be split off exactly; "
-                                 "use the direct farfield for row shards")
-        self._far_args = (farfield_op_type, nq_far, K_far_name, params, pts, tris, far_obs,
+        self._far_args = (farfield_op_type, nq_far, K_far_name, params, pts, tris, obs_subset,
                           src_subset)
+        self.farfield = self._make_far(farfield_op_type, float_type)
         self.shape = self.nearfield.shape
         self._graph = None
+
+    def _make_far(self, factory, float_type):
+        """The farfield of this operator's rows: the direct farfield over
+        the row range's observation triangles; an FMM farfield keeps the
+        whole observation set's trees and lists and evaluates the rows'
+        leaves (FMMFarfieldOpImpl(row_range=)), so its rows are exactly the
+        unsharded FMM's."""
+        from ..fmm.tsfmm import FMMFarfieldOp
+        _, nq_far, K_far, params, pts, tris, obs_subset, src_subset = self._far_args
+        rr = self.row_range
+        if rr is not None and isinstance(factory, FMMFarfieldOp):
+            return factory(nq_far, K_far, params, pts, tris, float_type, obs_subset, src_subset,
+                           row_range=rr)
+        far_obs = obs_subset if rr is None else obs_subset[rr[0]:rr[1]]
+        return factory(nq_far, K_far, params, pts, tris, float_type, far_obs, src_subset)
 
     def autotune(self):
         """Tune this operator's launch shapes (direct-farfield source
@@ -70,12 +78,11 @@ class RegularizedSparseIntegralOp:
         twin = copy.copy(self)
         twin.float_type = np.dtype(float_type)
         twin.nearfield = self.nearfield.astype(float_type, keep_uncorrected)
-        factory, nq_far, K_far, params, pts, tris, obs_subset, src_subset = self._far_args
+        factory = self._far_args[0]
         if farfield_op_type is not None:
             factory = farfield_op_type
             twin._far_args = (factory,) + self._far_args[1:]
-        twin.farfield = factory(nq_far, K_far, params, pts, tris, float_type, obs_subset,
-                                src_subset)
+        twin.farfield = twin._make_far(factory, float_type)
         twin._graph = None
         return twin
 

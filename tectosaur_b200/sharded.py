@@ -15,9 +15,12 @@ near-pair search over all observation triangles and keeps the pairs of its
 rows, so every rank holds exactly the blocks of the one global operator (the
 reference's leaf test reads radii by octree position, so a search over the
 shard's triangles alone could move pairs at the threshold across the
-near/far line).  The FMM farfield is not sharded: its trees and interaction
-lists are built per observation set, so a shard of an FMM operator is not the
-rows of the global one.
+near/far line).  An FMM farfield shard likewise keeps the whole observation
+set's trees and interaction lists and evaluates only the observation nodes
+that hold its rows (their P2P and M2L/M2P entries, L2L chain and L2P); every
+rank computes all source moments (P2M, M2M: a few per cent of an apply), so
+the only exchange stays the all-gather of x, and the shard's rows are the
+unsharded FMM's bit for bit.
 """
 import numpy as np
 

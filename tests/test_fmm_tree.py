@@ -149,3 +149,47 @@ def test_m2l_plan_rejects_bad_lane_counts():
     out = (ctypes.c_int64 * 5)()
     for lanes in (0, 100, 256):
         assert _lib.lib.tct_fmm_m2l_plan_stats(8, 3, lanes, out) != 0
+
+
+@pytest.mark.parametrize("world", [2, 3, 5])
+def test_row_shard_restriction(world):
+    """A row shard's FMM observation side: a node is kept iff it holds a
+    triangle of the range, every ancestor of a kept node is kept, the kept
+    leaves hold every row of the range, and each kept list entry keeps its
+    whole source list; over a partition of the rows every list entry is
+    kept by some shard (but those of empty octree children)."""
+    from tectosaur_b200.fmm.tsfmm import restrict_list, touching_nodes
+    from tectosaur_b200.sharded import row_ranges
+    pts, tris = bumpy_mesh(20, seed=1, amp=0.3)
+    c, r = tri_centers_radii(pts, tris)
+    tree = Tree(c, r, 25, device=False)
+    lists = interactions(tree, tree, 3.0, 3.0, 0, False)
+    n = tris.shape[0]
+    pos_of = np.empty(n, np.int64)
+    pos_of[tree.orig_idxs] = np.arange(n)
+    seen = {k: np.zeros(v.obs_n_idxs.shape[0], bool) for k, v in lists.items()}
+    for r0, r1 in row_ranges(n, world):
+        touch = touching_nodes(tree, r0, r1)
+        for k in range(tree.n_nodes):
+            rows = tree.orig_idxs[tree.start[k]:tree.end[k]]
+            assert touch[k] == bool(((rows >= r0) & (rows < r1)).any())
+        kept = np.nonzero(touch)[0]
+        par = tree.parent[kept]
+        assert touch[par[par >= 0]].all()
+        leaves = tree.leaves()[touch[tree.leaves()]]
+        covered = np.zeros(n, bool)
+        for lf in leaves:
+            covered[tree.orig_idxs[tree.start[lf]:tree.end[lf]]] = True
+        assert covered[r0:r1].all()
+        for name, lst in lists.items():
+            sub = restrict_list(lst, touch)
+            assert np.all(touch[sub.obs_n_idxs])
+            for j, o in enumerate(sub.obs_n_idxs):
+                i = int(np.nonzero(lst.obs_n_idxs == o)[0][0])
+                full_src = lst.src_n_idxs[lst.obs_src_starts[i]:lst.obs_src_starts[i + 1]]
+                assert np.array_equal(
+                    sub.src_n_idxs[sub.obs_src_starts[j]:sub.obs_src_starts[j + 1]], full_src)
+            seen[name] |= touch[lst.obs_n_idxs]
+    nonempty = tree.end > tree.start  # empty octree children hold no rows and do no work
+    for name, lst in lists.items():
+        assert seen[name][nonempty[lst.obs_n_idxs]].all()
