@@ -194,14 +194,55 @@ class FullspaceModel:
             (~t.isfinite(V).all())
         return slip, slip_deficit, state, traction, V, dstate, bad
 
-    def make_derivs(self):
+    def make_derivs(self, graph=True):
+        """The derivative function (t, y) -> dy/dt of one state (full_model.py
+        make_derivs).  With graph (the default) the evaluation -- the
+        operator apply, the constrained mass solve, Newton, averaging and
+        the rejection, ~30 launches -- is captured once as a CUDA graph on
+        private buffers and replayed: the time and state are copied in, the
+        derivative is copied out.  The graph holds the same kernels with the
+        same arguments, so its values are the eager evaluation's bit for
+        bit (the time enters as a device scalar: t * plate_rate is the same
+        one rounding); the eager form is used where capture fails."""
         t = device.torch()
 
-        def derivs(t_, y):
-            self.n_evals += 1
+        def eager(t_, y):
             *_, V, dstate, bad = self.solve_for_full_state(t_, y)
             out = t.cat((V, dstate))
             return t.where(bad, y * float("inf"), out)
+
+        st = {}
+
+        def capture(t_, y):
+            ts = t.zeros((), dtype=t.float64, device="cuda")
+            yin = t.empty_like(y)
+            ts.fill_(float(t_))
+            yin.copy_(y)
+            side = t.cuda.Stream()
+            side.wait_stream(t.cuda.current_stream())
+            with t.cuda.stream(side):
+                eager(ts, yin)  # warm-up outside the capture
+            t.cuda.current_stream().wait_stream(side)
+            g = t.cuda.CUDAGraph()
+            with t.cuda.graph(g):
+                out = eager(ts, yin)
+            st.update(g=g, ts=ts, yin=yin, out=out)
+
+        def derivs(t_, y):
+            self.n_evals += 1
+            if not graph or st.get("off"):
+                return eager(t_, y)
+            if "g" not in st:
+                try:
+                    capture(t_, y)
+                except RuntimeError:
+                    st.clear()
+                    st["off"] = True
+                    return eager(t_, y)
+            st["ts"].fill_(float(t_))
+            st["yin"].copy_(y)
+            st["g"].replay()
+            return st["out"].clone()
 
         return derivs
 

@@ -193,3 +193,33 @@ def test_integrate_matches_oracle(cuda, orc):
         t_got, y_got = integ.h_t[i], integ.h_y[i].cpu().numpy()
         assert abs(t_got - ref.t) <= 1e-8 * abs(ref.t), (i, t_got, ref.t)
         assert np.linalg.norm(y_got - ref.y) <= 1e-8 * np.linalg.norm(ref.y), i
+
+
+@pytest.mark.parametrize("ft", [np.float64, np.float32])
+def test_graph_derivs_bit_identical(cuda, ft):
+    """The single-state derivative replayed as a CUDA graph equals the eager
+    evaluation bit for bit, over several times and states (a rejected one
+    included), and the Integrator's trajectory with it is the eager one's."""
+    pts, tris = make_rect(7, 7, [[-1, 0, 1], [-1, 0, -1], [1, 0, -1], [1, 0, 1]])
+    cfg = qd_cfg(tris.shape[0], ft)
+    model = qd.FullspaceModel((pts, tris), cfg)
+    n = tris.shape[0]
+    rng = np.random.default_rng(8)
+    fg, fe = model.make_derivs(graph=True), model.make_derivs(graph=False)
+    for k, t in enumerate((0.0, 3.3e3, 1e7, 2.5)):
+        y = np.concatenate([rng.standard_normal(9 * n) * 1e-6, rng.uniform(0.6, 0.8, 3 * n)])
+        if k == 3:
+            y[-2] = 1.5  # rejected: inf * y
+        yd = torch.from_numpy(y).cuda()
+        a, b = fg(t, yd), fe(t, yd)
+        torch.testing.assert_close(a, b, rtol=0, atol=0, equal_nan=True)
+    y0 = np.concatenate([np.zeros(9 * n), 0.7 + 0.01 * rng.standard_normal(3 * n)])
+    runs = []
+    for graph in (True, False):
+        integ = qd.Integrator(model, (0.0, y0))
+        integ.derivs = model.make_derivs(graph=graph)
+        integ.rk23.fun = integ.derivs
+        integ.integrate(8)
+        runs.append((list(integ.h_t), integ.h_y[-1].cpu().numpy()))
+    assert runs[0][0] == runs[1][0]
+    assert np.array_equal(runs[0][1], runs[1][1])
