@@ -121,7 +121,12 @@ class SolveEngine:
         self.Rv = t.zeros((S, self.n), dtype=f64, device=self.dev)
         pin = self.dev.type == "cuda"
         self._pin = pin
-        self._cols = t.zeros((S, m + 2), dtype=f64, pin_memory=pin)
+        # the new Hessenberg columns of a tick, (S, J + 1) row-major in the
+        # first S (J + 1) entries: a contiguous destination, so the copy from
+        # the device is one asynchronous memcpy (a copy into a strided slice
+        # of pinned memory falls back to a synchronous one, which held the
+        # host on every engine's tick until the tick had run on the device)
+        self._cols = t.zeros(S * (m + 2), dtype=f64, pin_memory=pin)
         self._norms = t.zeros(S, dtype=f64, pin_memory=pin)
         # host -> device control block of a tick (slot lists and step counts)
         # and back-substitution results, staged in pinned memory so that no
@@ -232,8 +237,10 @@ class SolveEngine:
                 J = int(self.j[inner].max()) + 1
                 ii = cd[3 * S: 3 * S + inner.size]
                 jt = cd[4 * S:]
-                act = t.zeros(S, dtype=t.bool, device=self.dev)
-                act[ii] = True
+                # index_fill_ passes the value as a kernel argument; an
+                # assignment `act[ii] = True` would make it a host tensor and
+                # copy it synchronously, holding the host on every tick
+                act = t.zeros(S, dtype=t.bool, device=self.dev).index_fill_(0, ii, True)
                 # the operator is applied to the active slots' columns only
                 # (an FMM farfield costs one pass per column; columns are
                 # independent, so a slot's result does not depend on the others)
@@ -252,8 +259,8 @@ class SolveEngine:
                 hn = t.linalg.norm(W, dim=1)
                 hs = t.where(hn > 0, hn, t.ones_like(hn))
                 self.V[ii, jt[ii] + 1] = W[ii] / hs[ii, None]
-                self._cols[:, :J].copy_(h, non_blocking=True)
-                self._cols[:, J].copy_(hn, non_blocking=True)
+                hc = t.cat((h, hn[:, None]), dim=1)
+                self._cols[: S * (J + 1)].copy_(hc.reshape(-1), non_blocking=True)
             if self._event is not None:
                 self._event.record()
         self._pending = (resid, inner, J)
@@ -269,7 +276,8 @@ class SolveEngine:
         t = self.t
         finished = []
         norms = self._norms.numpy()[: resid.size].copy()
-        cols = self._cols.numpy()[:, : J + 1].copy() if inner.size else None
+        cols = (self._cols.numpy()[: self.S * (J + 1)].reshape(self.S, J + 1).copy()
+                if inner.size else None)
         now = time.perf_counter()
         self.last_used = now
         # residual phase: finish, or start a GMRES cycle on the residual
@@ -464,20 +472,20 @@ class QdEngine:
             self._tdev.copy_(self._tpin, non_blocking=True)
             self._idev.copy_(self._ipin, non_blocking=True)
             idx = self._idev[:k]
-            h = self._tdev[0, :k]
+            hdev = self._tdev[0, :k]  # the step sizes on the device (h stays on the host)
             y, K0 = self.Y[idx], self.F[idx]
             # stage inputs, the new state and the error norm: one fused
             # launch each, rounded as y + (K0 a10) h, y + (K0 a20 + K1 a21) h,
             # y + h (K0 b0 + K1 b1 + K2 b2), ||(sum_j K_j e_j) h / scale||
             ys = t.empty_like(y)
-            self.qm.combine_batch([K0], [rk.A[1][0]], h, y, ys)
+            self.qm.combine_batch([K0], [rk.A[1][0]], hdev, y, ys)
             K1 = self.derivs(self._tdev[1, :k], ys)
-            self.qm.combine_batch([K0, K1], [rk.A[2][0], rk.A[2][1]], h, y, ys)
+            self.qm.combine_batch([K0, K1], [rk.A[2][0], rk.A[2][1]], hdev, y, ys)
             K2 = self.derivs(self._tdev[2, :k], ys)
             y_new = t.empty_like(y)
-            self.qm.combine_batch([K0, K1, K2], rk.B[:3], h, y, y_new)
+            self.qm.combine_batch([K0, K1, K2], rk.B[:3], hdev, y, y_new)
             f_new = self.derivs(self._tdev[3, :k], y_new)
-            self.qm.error_norm_batch([K0, K1, K2, f_new], rk.E[:4], h, y, y_new, self.tol,
+            self.qm.error_norm_batch([K0, K1, K2, f_new], rk.E[:4], hdev, y, y_new, self.tol,
                                      self._ndev[:k])
             self._norms[:k].copy_(self._ndev[:k], non_blocking=True)
             self._event.record()
@@ -785,14 +793,28 @@ class SolveServer:
         self._admit()
         done = []
         waiting = True
-        for r in list(self.resident.values()):
-            e = r.engine
+
+        def service(e):
+            nonlocal waiting
             if e.pending and e.ready():
                 done.extend(e.complete())
                 waiting = False
             if not e.pending and e.busy:
                 e.launch()
                 waiting = False
+
+        engines = [r.engine for r in self.resident.values()]
+        # quasidynamic engines are chains of short RK23 attempts, each waiting
+        # for the host to accept or reject the previous one: they are
+        # serviced again after every other engine, so a finished attempt is
+        # followed at once rather than after a whole pass over the solve
+        # engines (whose host work is a millisecond or more each)
+        quick = [e for e in engines if isinstance(e, QdEngine)]
+        for e in engines:
+            service(e)
+            if not isinstance(e, QdEngine):
+                for q in quick:
+                    service(q)
         if waiting and done == []:
             time.sleep(20e-6)  # every engine is waiting for the device
         self.completed.extend(done)

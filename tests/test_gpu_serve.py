@@ -128,6 +128,15 @@ def test_qd_same_alone_and_in_mix(cuda):
     assert r0.converged and r1.converged and all(o.converged for o in others)
     assert r1.steps == r0.steps == 12
     np.testing.assert_allclose(r1.ts, r0.ts, rtol=1e-9)
+    # a pending tick's step sizes stay on the host: its completion reads
+    # them per slot, and a device scalar there would be a blocking copy
+    srv = serve.SolveServer(slots=4)
+    srv.add_qd_mesh("fault", pts, tris, cfg, model=model)
+    srv.submit_qd("fault", y0s[0], 3)
+    srv.step()
+    eng = srv.resident["fault"].engine
+    assert eng.pending and isinstance(eng._pending[1], np.ndarray)
+    srv.run_until_idle(max_ticks=10_000)
     assert np.linalg.norm(r1.y - r0.y) / np.linalg.norm(r0.y) < 1e-9
 
 
