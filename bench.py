@@ -1419,7 +1419,7 @@ def run_qd_workload(args, rank, world, torch, dist):
         dist.barrier()
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    l0 = _lib.launch_count()
+    l0 = _lib.launch_count() + model.graph_kernel_launches
     e0 = model.n_evals
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
@@ -1430,7 +1430,9 @@ def run_qd_workload(args, rank, world, torch, dist):
     b.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    launches = _lib.launch_count() - l0
+    # the derivative runs as a replayed CUDA graph: its library kernels are
+    # counted per replay (FullspaceModel.graph_kernel_launches)
+    launches = _lib.launch_count() + model.graph_kernel_launches - l0
     evals = (model.n_evals - e0) / args.steps
     total_ms = a.elapsed_time(b)
     if dist is not None:

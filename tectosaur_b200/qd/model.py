@@ -138,6 +138,7 @@ class FullspaceModel:
         self._vn = t.zeros(n9, dtype=f64, device="cuda")
         self.n_failed = t.zeros(1, dtype=t.int32, device="cuda")
         self.n_evals = 0
+        self.graph_kernel_launches = 0  # library kernels run by derivative graph replays
 
     # -- pieces ---------------------------------------------------------------
     def slip_to_traction(self, slip):
@@ -224,9 +225,12 @@ class FullspaceModel:
                 eager(ts, yin)  # warm-up outside the capture
             t.cuda.current_stream().wait_stream(side)
             g = t.cuda.CUDAGraph()
+            n0 = _lib.launch_count()
             with t.cuda.graph(g):
                 out = eager(ts, yin)
-            st.update(g=g, ts=ts, yin=yin, out=out)
+            # library kernels recorded in the graph: a replay runs them
+            # without passing the launch counter
+            st.update(g=g, ts=ts, yin=yin, out=out, kernels=_lib.launch_count() - n0)
 
         def derivs(t_, y):
             self.n_evals += 1
@@ -242,6 +246,7 @@ class FullspaceModel:
             st["ts"].fill_(float(t_))
             st["yin"].copy_(y)
             st["g"].replay()
+            self.graph_kernel_launches += st["kernels"]
             return st["out"].clone()
 
         return derivs
