@@ -425,16 +425,41 @@ far_prep_rh2(Consts<float> c, Rule2D<float> rule, const float* __restrict__ pts,
 // One packed source record r against this thread's two observation
 // triangles (negated target points negx, pair weights wq for unequal-weight
 // rules): W[3 d + j] += S0 P[d][j] + sum_k T[d][k] M[k][j], both halves.
-template <int NQ, bool UNIFORM>
+template <int NQ, bool UNIFORM, bool VEC = false>
 __device__ __forceinline__ void rh2_pair(const f2_t* __restrict__ r, const f2_t (&negx)[NQ][3],
                                          const f2_t (&wq)[UNIFORM ? 1 : NQ * NQ], f2_t eps,
                                          f2_t (&W)[9]) {
     using L = RecRH2<NQ>;
+    // VEC: the record (16-byte aligned: LEN is a multiple of 4 floats) is read
+    // with 16-byte loads, two packed values each -- the points before the
+    // pair loop, P and M after it: half the shared-memory load instructions,
+    // for ~30 more registers (the direct farfield kernel with the 3-point
+    // rule, which has them: 5.6 % faster at 60k triangles; the FMM P2P keeps
+    // its 128-register cap)
+    constexpr int NYV = (3 * NQ + 1) / 2;
+    f2_t yv[VEC ? 2 * NYV : 1];
+    if constexpr (VEC) {
+        const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(r);
+#pragma unroll
+        for (int k = 0; k < NYV; k++) {
+            const ulonglong2 u = r2[k];
+            yv[2 * k] = u.x;
+            yv[2 * k + 1] = u.y;
+        }
+    }
     f2_t T00 = 0ull, T01 = 0ull, T02 = 0ull, T11 = 0ull, T12 = 0ull, T22 = 0ull;
 #pragma unroll
     for (int q2 = 0; q2 < NQ; q2++) {
-        const f2_t y0 = r[L::Y + 3 * q2 + 0], y1 = r[L::Y + 3 * q2 + 1],
-                   y2 = r[L::Y + 3 * q2 + 2];
+        f2_t y0, y1, y2;
+        if constexpr (VEC) {
+            y0 = yv[L::Y + 3 * q2 + 0];
+            y1 = yv[L::Y + 3 * q2 + 1];
+            y2 = yv[L::Y + 3 * q2 + 2];
+        } else {
+            y0 = r[L::Y + 3 * q2 + 0];
+            y1 = r[L::Y + 3 * q2 + 1];
+            y2 = r[L::Y + 3 * q2 + 2];
+        }
 #pragma unroll
         for (int q1 = 0; q1 < NQ; q1++) {
             const f2_t D0 = add2(y0, negx[q1][0]);
@@ -459,14 +484,38 @@ __device__ __forceinline__ void rh2_pair(const f2_t* __restrict__ r, const f2_t 
     }
     const f2_t S0 = add2(add2(T00, T11), T22);
     const f2_t T[3][3] = {{T00, T01, T02}, {T01, T11, T12}, {T02, T12, T22}};
+    // P[k] at packed index P + k, M[k] at M + k = P + 9 + k
+    constexpr int K0 = L::P / 2, K1 = (L::PAIRS + 1) / 2, OFF = L::P % 2;
+    f2_t pm[VEC ? 2 * (K1 - K0) : 1];
+    if constexpr (VEC) {
+        const ulonglong2* r2 = reinterpret_cast<const ulonglong2*>(r);
+#pragma unroll
+        for (int k = K0; k < K1; k++) {
+            const ulonglong2 u = r2[k];
+            pm[2 * (k - K0)] = u.x;
+            pm[2 * (k - K0) + 1] = u.y;
+        }
+    }
 #pragma unroll
     for (int d = 0; d < 3; d++)
 #pragma unroll
         for (int jj = 0; jj < 3; jj++) {
-            f2_t w = fma2(S0, r[L::P + 3 * d + jj], W[3 * d + jj]);
-            w = fma2(T[d][0], r[L::M + 0 * 3 + jj], w);
-            w = fma2(T[d][1], r[L::M + 1 * 3 + jj], w);
-            w = fma2(T[d][2], r[L::M + 2 * 3 + jj], w);
+            f2_t p, m0, m1, m2;
+            if constexpr (VEC) {
+                p = pm[OFF + 3 * d + jj];
+                m0 = pm[OFF + 9 + 0 * 3 + jj];
+                m1 = pm[OFF + 9 + 1 * 3 + jj];
+                m2 = pm[OFF + 9 + 2 * 3 + jj];
+            } else {
+                p = r[L::P + 3 * d + jj];
+                m0 = r[L::M + 0 * 3 + jj];
+                m1 = r[L::M + 1 * 3 + jj];
+                m2 = r[L::M + 2 * 3 + jj];
+            }
+            f2_t w = fma2(S0, p, W[3 * d + jj]);
+            w = fma2(T[d][0], m0, w);
+            w = fma2(T[d][1], m1, w);
+            w = fma2(T[d][2], m2, w);
             W[3 * d + jj] = w;
         }
 }

@@ -184,7 +184,10 @@ far_main_rh2(Consts<float> c, Rule2D<float> rule, const float* __restrict__ pts,
         for (int k = 0; k < 9; k++) W[k] = 0ull;
 #pragma unroll 2
         for (int j = 0; j < n_tile; j++) {
-            rh2_pair<NQ, UNIFORM>(reinterpret_cast<const f2_t*>(sm + j * L::LEN), negx, wq, eps, W);
+            // 16-byte record loads for the 3-point rule (measured faster;
+            // the 4- and 7-point forms would need 164-244 registers)
+            rh2_pair<NQ, UNIFORM, NQ == 3>(reinterpret_cast<const f2_t*>(sm + j * L::LEN), negx,
+                                           wq, eps, W);
         }
 #pragma unroll
         for (int k = 0; k < 9; k++) {
