@@ -43,7 +43,7 @@ FLOPS_PER_POINT_PAIR_RH = 36.0
 # DRAM bytes of one far_main_rh2 launch on the 59,858-triangle surface (ncu
 # dram__bytes_read.sum + dram__bytes_write.sum, one full-size capture): the
 # kernel reads its source records through L2 and is compute-bound
-FAR_TRAFFIC_BYTES = 14.586e6
+FAR_TRAFFIC_BYTES = 14.856e6
 # DRAM bytes of one bsr9_kernel launch on the same surface's nearfield matrix
 # (5,477,848 blocks, rows aligned to 32 slots; one full-size capture):
 # 1.06x the algorithmic 1.801e9 bytes
