@@ -106,3 +106,45 @@ def test_panel_workspace_sizes():
     assert L.tct_farfield_rt_panel_workspace_bytes(100, 100, 16, 3) > 0
     assert L.tct_farfield_rh_panel_workspace_bytes(100, 100, 16, 5) == 0
     assert L.tct_farfield_rh_panel_workspace_bytes(100, 100, 16, 7) > 0
+
+
+def test_new_entry_points_reject_bad_arguments():
+    """The batched quasidynamic steps and the RT panel check their
+    arguments before any device work (these calls launch nothing)."""
+    import ctypes
+    from tectosaur_b200 import _lib
+    L = _lib.lib
+    nul = None
+    # RK combinations take 1 to 4 terms and their arrays
+    k = (ctypes.c_void_p * 5)(*([None] * 5))
+    st = (ctypes.c_int64 * 5)(*([0] * 5))
+    cs = (ctypes.c_double * 5)(*([1.0] * 5))
+    # (null device pointers only: a check that stopped working is caught by
+    # the null-pointer check, never by a launch)
+    for n_terms in (5, 0, 2):
+        assert L.tct_qd_combine_batch(10, 2, n_terms, k, st, cs, nul, nul, 0, nul, 10,
+                                      nul) == _lib.TCT_ERR_ARG
+        assert L.tct_qd_error_norm_batch(10, 2, n_terms, k, st, cs, nul, nul, 10, nul, 10, 1e-4,
+                                         nul, nul) == _lib.TCT_ERR_ARG
+    assert L.tct_qd_combine_batch(0, 2, 2, k, st, cs, nul, nul, 0, nul, 10, nul) == _lib.TCT_OK
+    # null arrays, negative sizes; empty problems are no-ops
+    assert L.tct_qd_deficit_batch(9, 2, nul, 1.0, nul, nul, nul, 9, _lib.TCT_F64, nul, 9,
+                                  nul) == _lib.TCT_ERR_ARG
+    assert L.tct_qd_deficit_batch(-9, 2, nul, 1.0, nul, nul, nul, 9, _lib.TCT_F64, nul, 9,
+                                  nul) == _lib.TCT_ERR_ARG
+    assert L.tct_qd_deficit_batch(0, 2, nul, 1.0, nul, nul, nul, 9, _lib.TCT_F64, nul, 9,
+                                  nul) == _lib.TCT_OK
+    assert L.tct_qd_finish_batch(9, 3, 2, nul, 12, nul, 9, nul, 3, 1.2, nul, 12,
+                                 nul) == _lib.TCT_ERR_ARG
+    assert L.tct_qd_finish_batch(9, 3, 0, nul, 12, nul, 9, nul, 3, 1.2, nul, 12,
+                                 nul) == _lib.TCT_OK
+    # the RT panel: R = 16 and the 3-point rule only
+    dp = _lib.dptr(np.zeros(8))
+    assert L.tct_farfield_rt_panel_matvec(nul, nul, nul, nul, 10, nul, 10, 8, 3, dp, dp, dp, 0,
+                                          nul, 0, nul) == _lib.TCT_ERR_ARG
+    assert "R must be 16" in _lib.last_error()
+    assert L.tct_farfield_rt_panel_matvec(nul, nul, nul, nul, 10, nul, 10, 16, 4, dp, dp, dp, 0,
+                                          nul, 0, nul) == _lib.TCT_ERR_ARG
+    assert L.tct_farfield_rt_panel_matvec(nul, nul, nul, nul, 10, nul, 10, 16, 3, dp, dp, dp, 0,
+                                          nul, 0, nul) == _lib.TCT_ERR_ARG  # no workspace
+    assert "workspace" in _lib.last_error()
