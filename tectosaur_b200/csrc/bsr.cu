@@ -24,10 +24,17 @@
 namespace tct {
 namespace {
 
-// At most 64 registers per thread (4 blocks of 256 threads per SM): left
-// unconstrained the compiler hoists all 81 block loads into registers (222
-// registers, 1 block per SM) and the per-row shuffle reduction then leaves
-// the SM with no loads in flight.
+// Long rows (16 or 32 lanes per row): at most 80 registers per thread (3
+// blocks of 256 threads per SM) and streaming loads of the blocks; short
+// rows (8 lanes or fewer): 64 registers (4 blocks) and L2-retaining loads.
+// Left unconstrained the compiler hoists all 81 block loads into registers
+// (222 registers, 1 block per SM) and the per-row shuffle reduction then
+// leaves the SM with no loads in flight; with 64 registers fewer loads are
+// in flight per warp (C2 matrix, ~90 blocks per row: 0.363 ms at 64
+// registers, 0.355 ms at 80, 0.339 ms at 80 with streaming loads; 128
+// registers spill).  On rows of one or two blocks, where the rows a warp
+// serves share lines, the long-row form is slower (0.104 against 0.093 ms
+// for 400k blocks).
 //
 // LPR lanes serve one block row (LPR = 32: a warp per row, the shape for
 // the operator's ~90 blocks per row; 16 down to 1: a warp serves 32 / LPR
@@ -35,7 +42,7 @@ namespace {
 // warp-uniform -- every lane runs the same number of iterations, lanes past
 // the last row carry zeros -- so the shuffles always have the full warp.
 template <typename R, bool TWO, int LPR>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, LPR >= 16 ? 3 : 4)
 bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             const int32_t* __restrict__ indices, const R* __restrict__ data,
             const R* __restrict__ data2, int64_t stride, const R* __restrict__ x,
@@ -70,11 +77,12 @@ bsr9_kernel(int64_t n_rows, const int32_t* __restrict__ indptr,
             for (int i = 0; i < 9; i++)
 #pragma unroll
                 for (int j = 0; j < 9; j++) {
-                    // default (L2-retaining) loads: in an unpadded matrix a
-                    // row's segment of an element plane shares its first and
-                    // last lines with the neighbouring rows
-                    R a = __ldg(data + (int64_t)(i * 9 + j) * stride + s);
-                    if (TWO) a += __ldg(data2 + (int64_t)(i * 9 + j) * stride + s);
+                    // long rows: streaming loads (evict first): every block
+                    // is read once per apply, and with rows starting on
+                    // lines no line is shared with another warp
+                    const int64_t e = (int64_t)(i * 9 + j) * stride + s;
+                    R a = LPR >= 16 ? __ldcs(data + e) : __ldg(data + e);
+                    if (TWO) a += LPR >= 16 ? __ldcs(data2 + e) : __ldg(data2 + e);
                     acc[i] += a * xv[j];
                 }
         }
