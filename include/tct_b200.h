@@ -628,8 +628,9 @@ int tct_cg_csr_batch(int64_t n, int n_sys, const int64_t* indptr, const int64_t*
  *                      and to the partial sums the workspace holds), v1 = 1;
  *   TCT_TUNE_BSR9      kernel = -1, nq = 0, rhs = 1, n0 = block rows,
  *                      n1 = blocks per row (data_stride / n_row_blocks):
- *                      v0 = lanes per block row (32, 16, 8 or 4; below 32 a
- *                      warp serves several short rows), v1 = CTAs per SM;
+ *                      v0 = lanes per block row (32, 16, 8, 4, 2 or 1;
+ *                      below 32 a warp serves several short rows), v1 = CTAs
+ *                      per SM (1 to 64);
  *   TCT_TUNE_FAR_PANEL reserved.
  * A shape changes the floating-point summation order, not the quantity
  * computed.  Host functions; the cache is shared by all threads. */

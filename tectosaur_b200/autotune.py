@@ -138,17 +138,19 @@ def tune_farfield(far, x=None, stream=None):
     return int(chunks.value)
 
 
-def tune_bsr(bsr, x=None, stream=None):
-    """Tune a DeviceBSR9's launch shape; returns (lanes per row, CTAs per SM)."""
+def tune_bsr(bsr, x=None, y=None, stream=None):
+    """Tune a DeviceBSR9's launch shape on its own (padded) layout; returns
+    (lanes per row, CTAs per SM).  `y` (optional) receives A x."""
     t = device.torch()
     if x is None:
         x = t.from_numpy(np.random.default_rng(1).standard_normal(bsr.shape[1])).to(
             device.torch_dtype(bsr.float_type)).cuda()
-    y = t.empty(bsr.shape[0], dtype=x.dtype, device="cuda")
+    if y is None:
+        y = t.empty(bsr.shape[0], dtype=x.dtype, device="cuda")
     lanes, ctas = ctypes.c_int(), ctypes.c_int()
     _lib.check(_lib.lib.tct_bsr9_autotune(
         _lib.prec_of(bsr.float_type), bsr.n_row_blocks, _lib.tptr(bsr.indptr),
-        _lib.tptr(bsr.indices), _lib.tptr(bsr.data), max(bsr.nnzb, 1), _lib.tptr(x),
+        _lib.tptr(bsr.indices), _lib.tptr(bsr.data), bsr.stride, _lib.tptr(x),
         _lib.tptr(y), _lib.stream_ptr(stream), ctypes.byref(lanes), ctypes.byref(ctas)),
         "tct_bsr9_autotune")
     return int(lanes.value), int(ctas.value)

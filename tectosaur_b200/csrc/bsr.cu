@@ -267,8 +267,12 @@ extern "C" int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* in
 }
 
 // Candidate shapes (lanes per row x CTAs per SM), each timed as one untimed
-// launch then the mean of three under CUDA events; the fastest stays in the
-// shape cache.
+// launch then the mean of eight under CUDA events; the fastest stays in the
+// shape cache.  (On the 5.5 M-block C2 matrix, 32 lanes: 4 / 6 / 8 / 12 / 16
+// CTAs per SM took 0.398 / 0.342 / 0.345 / 0.343 / 0.355 ms, and 3 -- one
+// resident wave -- 0.409 ms: warps that finish early leave their SM idle
+// until the whole CTA exits; with three timed launches the 3 % between 8
+// and 16 was within the noise of the pick.)
 extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* indptr,
                                  const int32_t* indices, const void* data, int64_t data_stride,
                                  const void* x, void* y, void* stream, int* lanes,
@@ -278,7 +282,7 @@ extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* 
     TCT_CHECK_ARG(n_row_blocks > 0, "tct_bsr9_autotune: empty matrix");
     const int64_t per_row = std::max<int64_t>(1, data_stride / n_row_blocks);
     static const int kLanes[] = {32, 16, 8, 4, 2, 1};
-    static const int kCtas[] = {4, 8, 16};
+    static const int kCtas[] = {4, 6, 8, 12, 16};
     cudaStream_t st = as_stream(stream);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
@@ -290,7 +294,7 @@ extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* 
     for (int l : kLanes) {
         for (int c : kCtas) {
             tune_store(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, l, c);
-            for (int rep = 0; rep < 4 && rc == TCT_OK; rep++) {
+            for (int rep = 0; rep < 9 && rc == TCT_OK; rep++) {
                 if (rep == 1) cudaEventRecord(e0, st);
                 rc = tct_bsr9_matvec(prec, n_row_blocks, indptr, indices, data, nullptr,
                                      data_stride, x, y, 0, stream);

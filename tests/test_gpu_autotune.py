@@ -45,7 +45,7 @@ def test_bsr_every_shape_matches_scipy(cuda, ft, tol):
     want = A @ x
     xd = device.to_dev(x, ft)
     for lanes in (32, 16, 8, 4, 2, 1):
-        for ctas in (4, 8, 16):
+        for ctas in (4, 6, 8, 12, 16):
             _lib.lib.tct_tune_set(_lib.TCT_TUNE_BSR9, -1, _lib.prec_of(ft), 0, 1,
                                   m.n_row_blocks, max(1, m.nnzb // m.n_row_blocks), lanes, ctas)
             y = device.torch().full((A.shape[0],), 7.0, dtype=xd.dtype, device="cuda")
@@ -56,7 +56,7 @@ def test_bsr_every_shape_matches_scipy(cuda, ft, tol):
             assert rel(y2.cpu().numpy(), want + 1.0) < tol, (lanes, ctas)
     autotune.clear()
     lanes, ctas = autotune.tune_bsr(m)
-    assert lanes in (32, 16, 8, 4, 2, 1) and ctas in (4, 8, 16)
+    assert lanes in (32, 16, 8, 4, 2, 1) and ctas in (4, 6, 8, 12, 16)
     y = device.torch().empty_like(xd)
     m.matvec(xd, y)
     assert rel(y.cpu().numpy(), want) < tol

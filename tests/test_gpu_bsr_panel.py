@@ -32,6 +32,25 @@ def _random_bsr(n_rows, n_cols, nnz, ft, seed, row_align=1):
     return m
 
 
+@pytest.mark.parametrize("align", [1, 32])
+def test_autotune_times_the_padded_layout(cuda, align):
+    """The BSR tuner runs the matrix in its own layout (slot stride, not the
+    block count): its output after tuning is the product."""
+    from tectosaur_b200 import autotune
+    autotune.clear()
+    b = _random_bsr(300, 250, 6000, np.float32, seed=4, row_align=align)
+    x = torch.from_numpy(np.random.default_rng(5).standard_normal(b.shape[1])
+                         .astype(np.float32)).cuda()
+    want = torch.empty(b.shape[0], device="cuda")
+    b.matvec(x, want)
+    y = torch.full((b.shape[0],), 7.0, device="cuda")
+    try:
+        autotune.tune_bsr(b, x, y)
+    finally:
+        autotune.clear()
+    assert float(torch.linalg.norm(y - want) / torch.linalg.norm(want)) < 2e-6
+
+
 @pytest.mark.parametrize("ft", [np.float32, np.float64])
 @pytest.mark.parametrize("align", [8, 32])
 def test_padded_rows_match_unpadded(cuda, ft, align):
