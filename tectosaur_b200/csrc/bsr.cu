@@ -272,7 +272,10 @@ extern "C" int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* in
 // CTAs per SM took 0.398 / 0.342 / 0.345 / 0.343 / 0.355 ms, and 3 -- one
 // resident wave -- 0.409 ms: warps that finish early leave their SM idle
 // until the whole CTA exits; with three timed launches the 3 % between 8
-// and 16 was within the noise of the pick.)
+// and 16 was within the noise of the pick.)  Lane counts below a quarter
+// of min(32, slots per row) are skipped: on rows of ~90 blocks the 1-, 2-
+// and 4-lane shapes take 2 to 8 ms a launch against 0.35 ms, and timing
+// them was most of the tuning time.
 extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* indptr,
                                  const int32_t* indices, const void* data, int64_t data_stride,
                                  const void* x, void* y, void* stream, int* lanes,
@@ -292,6 +295,7 @@ extern "C" int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* 
     int rc = TCT_OK, bl = 0, bc = 0;
     float best_ms = 0.f;
     for (int l : kLanes) {
+        if (4 * (int64_t)l < std::min<int64_t>(32, per_row)) continue;
         for (int c : kCtas) {
             tune_store(kTuneBsr9, -1, prec, 0, 1, n_row_blocks, per_row, l, c);
             for (int rep = 0; rep < 9 && rc == TCT_OK; rep++) {
