@@ -661,7 +661,9 @@ int tct_farfield_autotune(int kernel, int prec, void* out, const void* in, const
                           const double* quad_wts, const double* params, void* workspace,
                           size_t workspace_bytes, void* stream, int* chunks);
 /* Autotune tct_bsr9_matvec's shape (lanes per block row x CTAs per SM) for
- * one matrix, as above (y is overwritten); results in *lanes, *ctas_per_sm. */
+ * one matrix, as above (y is overwritten with A x); data_stride is the
+ * matrix's own plane stride (its slot count when rows are padded), as given
+ * to tct_bsr9_matvec.  Results in *lanes, *ctas_per_sm. */
 int tct_bsr9_autotune(int prec, int64_t n_row_blocks, const int32_t* indptr,
                       const int32_t* indices, const void* data, int64_t data_stride,
                       const void* x, void* y, void* stream, int* lanes, int* ctas_per_sm);
