@@ -170,13 +170,15 @@ int tct_farfield_tris_dense(int kernel, int prec, void* out, int n_quad,
 /* Replaces bsrmv9 / bcoomv9 (tectosaur/util/fast_sparse.cpp:71-163) behind
  * BCOOMatrix.dot / BSRMatrix.dot (tectosaur/util/sparse.py:29-64) as summed
  * by RegularizedNearfieldIntegralOp.dot (nearfield/nearfield_op.py:158-159).
- * Layout: indptr (n_row_blocks + 1) and indices (nnzb) int32; data in
- * structure-of-arrays order, element e (= i*9 + j) of block s at
- * data[e * data_stride + s], data_stride >= nnzb.
+ * Layout: indptr (n_row_blocks + 1) and indices (one per slot,
+ * indptr[n_row_blocks] slots) int32; data in structure-of-arrays order,
+ * element e (= i*9 + j) of the block in slot s at data[e * data_stride + s],
+ * data_stride >= indptr[n_row_blocks].
  * y[9*r + i] (+)= sum_{s in row r} sum_j A_s[i][j] x[9*indices[s] + j].
  * A slot whose index is negative is padding and is skipped (its data is
- * not read): rows may start on 32-byte sector boundaries of the element
- * planes, so that no sector holds the blocks of two rows.
+ * not read): rows may start on 128-byte lines of the element planes (32
+ * FP32 or 16 FP64 slots), so that no line holds the blocks of two rows and
+ * none is fetched from DRAM twice.
  * With data2 != NULL the blocks are data + data2 (no-correction form). */
 int tct_bsr9_matvec(int prec, int64_t n_row_blocks, const int32_t* indptr,
                     const int32_t* indices, const void* data, const void* data2,
