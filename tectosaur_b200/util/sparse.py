@@ -71,8 +71,9 @@ class DeviceBSR9:
 
     With row_align > 1 each block row starts on a multiple of row_align
     slots (the slots between rows are padding, column index -1, zero data,
-    never read by the kernels): no 32-byte sector of an element plane then
-    holds blocks of two rows, and none is fetched from DRAM twice.  `nnzb`
+    never read by the kernels): with 32 FP32 (16 FP64) slots no 128-byte
+    line of an element plane then holds blocks of two rows, and none is
+    fetched from DRAM twice (at 8 or 16 FP32 slots, fewer lines are shared).  `nnzb`
     counts the blocks, `stride` the slots (the element-plane length);
     `pos[k]` is the slot of the k-th block in CSR order, and the host
     views (`indptr_host`, `indices_host`, `blocks_host`) are unpadded.
